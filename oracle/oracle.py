@@ -1,0 +1,191 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Loads oracle/liboracle.so (this directory's C restatement of the IPP core) and,
+when present, oracle/_ref/libm5ref.so (the reference's own mark5access built
+from its sources).  Only tests, the smoke check and the CPU-baseline leg of
+the benchmark import this module; the GPU product never does.
+
+Dispatcher-level behaviour (splitting the sample stream into core runs and
+adding per-run partial spectra) follows src/TaskDispatcher.cpp:92-247 and
+TaskCoreIPP::combineResults (src/IA-32/TaskCoreIPP.cpp:311-349).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+_ref = None
+
+W_NONE, W_COSINE, W_COSINE2, W_HAMMING, W_HANN, W_BLACKMAN, W_BLACKMANHARRIS = range(7)
+WINDOW_NAMES = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
+                "blackmanharris": 6}
+
+
+class OrcCfg(C.Structure):
+    _fields_ = [("fft_points", C.c_int), ("overlap", C.c_int),
+                ("core_overlapped_ffts", C.c_int), ("num_sources", C.c_int),
+                ("num_xpols", C.c_int), ("window", C.c_int), ("extract_pcal", C.c_int),
+                ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
+                ("samplingfreq", C.c_double), ("pcaloffsethz", C.c_double),
+                ("nthreads", C.c_int)]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = C.CDLL(path)
+        _lib.orc_decode.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_int,
+                                    C.c_void_p]
+        _lib.orc_window.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        _lib.orc_fft64.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        _lib.orc_domaths64.argtypes = [C.POINTER(OrcCfg), C.c_void_p, C.c_int64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        _lib.orc_domaths32.argtypes = [C.POINTER(OrcCfg), C.c_void_p, C.c_int64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        _lib.orc_schedule.argtypes = [C.POINTER(OrcCfg), C.c_int64, C.c_void_p, C.c_void_p,
+                                      C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        _lib.orc_pcal_tones.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+    return _lib
+
+
+def ref():
+    """The reference's mark5access (None when it was not built)."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libm5ref.so")
+        if not os.path.exists(path):
+            return None
+        _ref = C.CDLL(path)
+        _ref.m5ref_decode.argtypes = [C.c_char_p, C.c_void_p, C.c_uint, C.c_int, C.c_int,
+                                      C.c_void_p, C.POINTER(C.c_int)]
+        _ref.m5ref_unpack.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        _ref.m5ref_format_info.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 6
+    return _ref
+
+
+# ----------------------------------------------------------------------------
+# decoding
+# ----------------------------------------------------------------------------
+
+FMT_MARK5B, FMT_VDIF = 0, 1
+
+
+def decode(fmt: int, nchan: int, nbit: int, payload: bytes, nsamp: int, chan: int) -> np.ndarray:
+    buf = np.frombuffer(payload, dtype=np.uint8)
+    out = np.empty(nsamp, dtype=np.float32)
+    rc = lib().orc_decode(fmt, nchan, nbit, buf.ctypes.data, nsamp, chan, out.ctypes.data)
+    assert rc == 0
+    return out
+
+
+def m5_format_info(fmt: str) -> dict:
+    r = ref()
+    vals = [C.c_int() for _ in range(6)]
+    rc = r.m5ref_format_info(fmt.encode(), *[C.byref(v) for v in vals])
+    assert rc == 0, fmt
+    keys = ["nchan", "nbit", "framebytes", "payloadoffset", "framesamples", "samplegranularity"]
+    return dict(zip(keys, [v.value for v in vals]))
+
+
+def m5_decode(fmt: str, framed: bytes, nsamp: int) -> tuple[np.ndarray, int]:
+    """mark5access framed decode -> float32[nchan, nsamp], return value."""
+    r = ref()
+    info = m5_format_info(fmt)
+    out = np.zeros((info["nchan"], nsamp), dtype=np.float32)
+    buf = np.frombuffer(framed, dtype=np.uint8).copy()
+    off = C.c_int()
+    rc = r.m5ref_decode(fmt.encode(), buf.ctypes.data, len(buf), nsamp, info["nchan"],
+                        out.ctypes.data, C.byref(off))
+    return out, rc
+
+
+def m5_unpack(fmt: str, payload: bytes, nsamp: int) -> tuple[np.ndarray, int]:
+    r = ref()
+    info = m5_format_info(fmt)
+    out = np.zeros((info["nchan"], nsamp), dtype=np.float32)
+    buf = np.frombuffer(payload, dtype=np.uint8).copy()
+    rc = r.m5ref_unpack(fmt.encode(), buf.ctypes.data, nsamp, info["nchan"], out.ctypes.data)
+    return out, rc
+
+
+# ----------------------------------------------------------------------------
+# windows, FFT
+# ----------------------------------------------------------------------------
+
+def window(wtype: int, n: int) -> np.ndarray:
+    out = np.empty(n, dtype=np.float32)
+    lib().orc_window(wtype, n, out.ctypes.data)
+    return out
+
+
+def fft64(x: np.ndarray) -> np.ndarray:
+    xin = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(xin)
+    lib().orc_fft64(len(xin), xin.ctypes.data, out.ctypes.data)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# doMaths over one buffer
+# ----------------------------------------------------------------------------
+
+def make_cfg(N, overlap=1, core_overlapped_ffts=1, num_sources=1, num_xpols=0, window=W_HANN,
+             extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
+             pcaloffsethz=10e3, nthreads=1) -> OrcCfg:
+    return OrcCfg(N, overlap, core_overlapped_ffts, num_sources, num_xpols, window,
+                  int(bool(extract_pcal)), pcal_tonebins, pcal_rotatorlen, samplingfreq,
+                  pcaloffsethz, nthreads)
+
+
+def schedule(cfg: OrcCfg, nsamp: int):
+    ns, part = C.c_int(), C.c_int()
+    nf = lib().orc_schedule(C.byref(cfg), nsamp, None, None, 0, C.byref(ns), C.byref(part))
+    starts = np.zeros(max(nf, 1), dtype=np.int64)
+    spec = np.zeros(max(nf, 1), dtype=np.int32)
+    lib().orc_schedule(C.byref(cfg), nsamp, starts.ctypes.data, spec.ctypes.data, nf,
+                       C.byref(ns), C.byref(part))
+    return starts[:nf], spec[:nf], ns.value, bool(part.value)
+
+
+def domaths(cfg: OrcCfg, samples: list[np.ndarray], fp64: bool = True):
+    """One core run.  Returns (auto[nspec, nsrc, S], xpol[nspec, nxp, S] complex,
+    pcal[nspec, nsrc, tonebins] complex, nspec)."""
+    N = cfg.fft_points
+    S = N // 2 + 1
+    nsamp = min(len(s) for s in samples)
+    _, _, nspec, _ = schedule(cfg, nsamp)
+    dt = np.float64 if fp64 else np.float32
+    srcs = [np.ascontiguousarray(s, dtype=np.float32) for s in samples]
+    ptrs = (C.c_void_p * len(srcs))(*[s.ctypes.data for s in srcs])
+    na = max(nspec, 1) * cfg.num_sources * S
+    auto = np.zeros(na, dtype=dt)
+    xpol = np.zeros(max(nspec, 1) * max(cfg.num_xpols, 1) * S * 2, dtype=dt)
+    pcal = np.zeros(max(nspec, 1) * cfg.num_sources * max(cfg.pcal_tonebins, 1) * 2, dtype=dt)
+    fn = lib().orc_domaths64 if fp64 else lib().orc_domaths32
+    n = fn(C.byref(cfg), ptrs, nsamp, auto.ctypes.data, xpol.ctypes.data, pcal.ctypes.data)
+    auto = auto[: n * cfg.num_sources * S].reshape(n, cfg.num_sources, S)
+    xp = xpol[: n * cfg.num_xpols * S * 2].reshape(n, cfg.num_xpols, S, 2)
+    xp = xp[..., 0] + 1j * xp[..., 1]
+    tb = cfg.pcal_tonebins
+    pc = pcal[: n * cfg.num_sources * tb * 2].reshape(n, cfg.num_sources, tb, 2)
+    pc = pc[..., 0] + 1j * pc[..., 1]
+    return auto, xp, pc, n
+
+
+def pcal_tones(bins: np.ndarray, nfolded: float, ntones: int) -> np.ndarray:
+    b = np.ascontiguousarray(np.stack([bins.real, bins.imag], -1).reshape(-1), dtype=np.float64)
+    out = np.zeros(2 * ntones)
+    lib().orc_pcal_tones(len(bins), b.ctypes.data, float(nfolded), ntones, out.ctypes.data)
+    return out[0::2] + 1j * out[1::2]
