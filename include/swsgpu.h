@@ -1,0 +1,188 @@
+/*
+ * swsgpu.h -- C ABI of the B200 spectrometer core (libswsgpu.so, sm_100a).
+ *
+ * This is the boundary a TaskCore implementation calls.  It replaces the
+ * compute half of the reference's abstract core, src/TaskCore.h:36-89, whose
+ * only complete implementation is TaskCoreIPP (src/IA-32/TaskCoreIPP.h:49-177):
+ *
+ *   TaskCore::prepare(settings)     (TaskCore.h:47)  -> swsgpu_create
+ *   TaskCore::run(in,out,xpol,pcal) (TaskCore.h:58)  -> swsgpu_submit
+ *   TaskCore::join()                (TaskCore.h:65)  -> swsgpu_wait + swsgpu_fetch
+ *   TaskCore::finalize()            (TaskCore.h:71)  -> swsgpu_destroy
+ *   TaskCore::resetBuffer(buf)      (TaskCore.h:87)  -> host memset (no device work)
+ *   TaskCore::combineResults(...)   (TaskCore.h:81)  -> host add of fetched spectra, or
+ *                                                       swsgpu_process_device with
+ *                                                       runs_per_output > 1
+ *
+ * One call of swsgpu_submit is one core run over one raw buffer per input
+ * stream: the per-buffer loop of TaskCoreIPP::doMaths
+ * (src/IA-32/TaskCoreIPP.cpp:355-560) -- FFTs every N/overlap samples,
+ * spectra of core_overlapped_ffts FFTs scaled by 1/core_overlapped_ffts, the
+ * hop over the overlap remainder between spectra, a trailing partial spectrum
+ * left unscaled, and PCal folding (TaskCoreIPP.cpp:633-693) on every
+ * overlap-th source FFT.  Sample decoding follows mark5access
+ * (mark5_format_mark5b.c, format_vdif.c), bit-exact, including fill-pattern
+ * blanking.
+ *
+ * All entry points return 0 on success and a negative SWSGPU_E* code on
+ * failure; swsgpu_last_error() describes the last failure of a handle (or,
+ * with a NULL handle, the last failure of swsgpu_create on this thread).
+ * Memory passed in is owned by the caller.  A handle is used by one host
+ * thread at a time.
+ */
+#ifndef SWSGPU_H
+#define SWSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWSGPU_OK 0
+#define SWSGPU_EINVAL (-1)       /* bad argument or unsupported configuration */
+#define SWSGPU_ECUDA (-2)        /* CUDA runtime error (message has details) */
+#define SWSGPU_ETIMEOUT (-3)     /* swsgpu_wait timed out; the run is still queued */
+#define SWSGPU_ENODEV (-4)       /* no usable sm_100 device */
+#define SWSGPU_ESTATE (-5)       /* call out of order (e.g. fetch before wait) */
+
+/* Sample tables (level values) of the stream. */
+#define SWSGPU_FMT_MARK5B 0      /* Mark5B: 2-bit {-H,+1,-1,+H}[s+2m], 1-bit {+1,-1} */
+#define SWSGPU_FMT_VDIF 1        /* VDIF: 2-bit {-H,-1,+1,+H}, 1-bit {-1,+1}, 8-bit (2b-255)/256 */
+
+/* Window functions: the reference's WindowFunctionType (src/Settings.h:45)
+ * plus BlackmanHarris (4-term Harris 1978), which the reference lacks. */
+#define SWSGPU_WIN_NONE 0
+#define SWSGPU_WIN_COSINE 1
+#define SWSGPU_WIN_COSINE2 2
+#define SWSGPU_WIN_HAMMING 3
+#define SWSGPU_WIN_HANN 4
+#define SWSGPU_WIN_BLACKMAN 5
+#define SWSGPU_WIN_BLACKMANHARRIS 6
+
+/* Arithmetic of the FFT stages. */
+#define SWSGPU_PREC_FP32 0       /* plain FP32 throughout */
+#define SWSGPU_PREC_TCSPLIT 1    /* inner DFT stages on tensor cores, FP16 hi+lo split, FP32 accumulate */
+
+#define SWSGPU_MAX_SOURCES 64
+#define SWSGPU_MAX_STREAMS 2
+
+/* Byte layout of one input stream.  A stream is a sequence of frames of
+ * frame_bytes bytes, each starting with header_bytes of header followed by
+ * the payload.  header_bytes = 0 describes a header-free payload stream (the
+ * reference's FileSource strips Mk5B/VDIF headers, src/FileSource.cpp:184-215);
+ * frame_bytes then still gives the payload size of one recorded frame, which
+ * delimits mark5access's blanking zones. */
+typedef struct swsgpu_layout {
+   int format;          /* SWSGPU_FMT_* */
+   int nchan;           /* channels per sample-time */
+   int nbit;            /* bits per sample: 1, 2 or 8 */
+   int frame_bytes;     /* header + payload bytes of one frame */
+   int header_bytes;    /* header bytes at the start of each frame (0: payload only) */
+} swsgpu_layout;
+
+/* Processing configuration; the fields mirror swspect_settings_t
+ * (src/Settings.h:59-159) as derived in src/swspectrometer.cpp:166-231. */
+typedef struct swsgpu_config {
+   swsgpu_layout layout[SWSGPU_MAX_STREAMS];
+   int num_streams;                 /* input buffers per run (reference: input files) */
+   int fft_points;                  /* N (even, factors 2,3,5) */
+   int overlap;                     /* fft_overlap_factor */
+   int window;                      /* SWSGPU_WIN_* */
+   int precision;                   /* SWSGPU_PREC_* */
+   int core_overlapped_ffts;        /* FFTs per spectrum within one run */
+   int num_sources;                 /* processed channels */
+   int source_stream[SWSGPU_MAX_SOURCES];   /* stream of each source */
+   int source_channel[SWSGPU_MAX_SOURCES];  /* 0-based channel of each source */
+   int num_xpols;                   /* cross spectra */
+   int xpol_pair[SWSGPU_MAX_SOURCES][2];    /* X_i conj(X_j) source indices */
+   int extract_pcal;                /* fold phase-cal tones */
+   int pcal_tonebins;               /* fs / comb spacing */
+   int pcal_rotatorlen;             /* fs / gcd(fs, offset) */
+   double samplingfreq;             /* Hz */
+   double pcal_offset_hz;           /* Hz */
+   size_t max_run_bytes;            /* largest raw buffer per stream and run */
+} swsgpu_config;
+
+typedef struct swsgpu_handle swsgpu_handle;
+
+/* Spectra of one run: layouts of TaskCoreIPP's output buffers.
+ *   auto_out : float [nspectra][num_sources][N/2+1]
+ *   xpol_out : float [nspectra][num_xpols][N/2+1][2]   (re, im)
+ *   pcal_out : float [nspectra][num_sources][pcal_tonebins][2]
+ * Pointers for outputs that are not configured may be NULL. */
+typedef struct swsgpu_outputs {
+   float *auto_out;
+   float *xpol_out;
+   float *pcal_out;
+} swsgpu_outputs;
+
+/* Library / device checks. */
+int swsgpu_version(void);
+int swsgpu_device_ok(int device);
+
+/* TaskCore::prepare.  Validates the configuration, selects `device`,
+ * allocates device buffers for runs of up to max_run_bytes per stream,
+ * uploads window and twiddle tables. */
+int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out);
+
+/* TaskCore::finalize. */
+void swsgpu_destroy(swsgpu_handle *h);
+
+/* Describes the last failure. */
+const char *swsgpu_last_error(const swsgpu_handle *h);
+
+/* Number of spectra (including a trailing partial one) and FFTs a run of
+ * `nbytes` payload bytes per stream yields; *partial is set when the last
+ * spectrum is an unscaled partial one (TaskCoreIPP.cpp:519-524). */
+int swsgpu_run_shape(const swsgpu_handle *h, size_t nbytes, int *nspectra, int *nffts,
+                     int *partial);
+
+/* TaskCore::run: queue one run on the handle's CUDA stream and return.
+ * raw[s] points to host memory holding nbytes[s] bytes of stream s, whole
+ * frames when the layout has headers.  The host memory must stay valid and
+ * unchanged until swsgpu_wait returns (the reference's double-buffer rule).
+ * stream_payload_offset[s] is the payload byte offset of raw[s] within its
+ * recording (fixes mark5access's per-frame blanking zones; 0 for a run that
+ * starts on a frame). */
+int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                  const int64_t *stream_payload_offset);
+
+/* TaskCore::join: wait up to timeout_ms (<0: forever) for the queued run;
+ * *nspectra gets the spectrum count (TaskCore::join's return value). */
+int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra);
+
+/* Copy the spectra of the completed run into caller memory. */
+int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out);
+
+/* Throughput path with data already in device memory: processes `nruns`
+ * consecutive runs of run_bytes payload bytes per stream (d_raw[s] holds
+ * nruns*run_bytes payload bytes, or the framed bytes that carry them) and
+ * writes the sum of every `runs_per_output` consecutive runs' spectra --
+ * the dispatcher's combineResults path (src/TaskDispatcher.cpp:143-171) --
+ * into the device outputs, using runs * nspectra_per_run / runs_per_output
+ * spectrum slots.  `cuda_stream` is a cudaStream_t (NULL: the handle's). */
+int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
+                          int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream);
+
+/* Sizes (bytes) of device scratch and of per-call work for a process_device
+ * call with these arguments. */
+int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes);
+
+/* Unpack test entry: decode channel `chan` of `nsamp` samples from the
+ * device stream d_raw (layout `lay`, payload offset `payload_offset`) to
+ * float32 d_out on the device, with mark5access blanking.  Returns the
+ * number of non-blanked samples through *nvalid (may be NULL). */
+int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,
+                         int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
+                         int64_t *nvalid, void *cuda_stream);
+
+/* Number of kernel launches the last submit / process_device call issued. */
+int swsgpu_last_launch_count(const swsgpu_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWSGPU_H */

@@ -1,0 +1,945 @@
+// engine.cu -- C ABI of the spectrometer core (include/swsgpu.h).
+//
+// Host side of one GPU TaskCore: validates the configuration, plans the
+// per-run FFT schedule exactly as TaskCoreIPP::doMaths walks a raw buffer
+// (src/IA-32/TaskCoreIPP.cpp:394-524), groups FFT jobs into work items, and
+// launches K1 (frame validity + corner turn), K2 (cluster FFT + accumulate)
+// and K3 (compensated reduction + scaling) on the handle's CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/swsgpu.h"
+#include "kernels.cuh"
+#include "plans.cuh"
+#include "pcal.cuh"
+
+namespace sws {
+__global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any);
+void launch_unpack_codes(int nbit, dim3 grid, int block, cudaStream_t st, StreamIn s,
+                         long long nsamp, const int *chans, int nch, uint32_t *codes,
+                         long long code_words, const int2 *valid, uint32_t *blank);
+__global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
+                               const int2 *valid, unsigned long long *nvalid);
+__global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
+}  // namespace sws
+
+using namespace sws;
+
+static thread_local std::string g_create_error;
+
+struct DevBuf {
+   void *p = nullptr;
+   size_t n = 0;
+   cudaError_t ensure(size_t bytes)
+   {
+      if (bytes <= n) return cudaSuccess;
+      if (p) cudaFree(p);
+      p = nullptr;
+      n = 0;
+      cudaError_t e = cudaMalloc(&p, bytes);
+      if (e == cudaSuccess) n = bytes;
+      return e;
+   }
+   void release()
+   {
+      if (p) cudaFree(p);
+      p = nullptr;
+      n = 0;
+   }
+};
+
+struct HostBuf {
+   void *p = nullptr;
+   size_t n = 0;
+   cudaError_t ensure(size_t bytes)
+   {
+      if (bytes <= n) return cudaSuccess;
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      n = 0;
+      cudaError_t e = cudaMallocHost(&p, bytes);
+      if (e == cudaSuccess) n = bytes;
+      return e;
+   }
+   void release()
+   {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      n = 0;
+   }
+};
+
+// Work schedule of one call (host side).
+struct Schedule {
+   std::vector<Item> items;
+   std::vector<RedEntry> entries;
+   std::vector<OutVec> outs;
+   std::vector<PcalJob> pcal_jobs;
+   std::vector<RedEntry> pcal_entries;
+   std::vector<OutVec> pcal_outs;
+   int nspec_total = 0;
+   long long nsamp = 0;    // chunk sample-times
+   int nffts = 0;
+};
+
+struct swsgpu_handle {
+   swsgpu_config cfg;
+   int device = 0;
+   Plan plan;
+   int S = 0;
+   int max_clusters = 1;
+   std::string err;
+   cudaStream_t stream = nullptr;
+   cudaEvent_t done = nullptr;
+   bool pending = false;
+   int pending_nspec = 0;
+   int last_launches = 0;
+   // code arrays: one per distinct (stream, channel)
+   std::vector<int> code_stream, code_chan;
+   std::vector<int> src_code;     // source -> code index
+   std::vector<int> auto_owner;   // source -> xpol index that owns its auto (-1: none)
+   // constant tables
+   DevBuf d_window, d_twQ, d_twN, d_code_stream;
+   // per-call buffers
+   DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
+   DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
+   DevBuf d_pcal_jobs, d_pcal_part, d_pcal_entries, d_pcal_outs;
+   DevBuf d_out_auto, d_out_xpol, d_out_pcal;
+   HostBuf h_out;   // pinned staging of one run's outputs
+   size_t h_auto_bytes = 0, h_xpol_bytes = 0, h_pcal_bytes = 0;
+};
+
+#define CK(h, call)                                                                                \
+   do {                                                                                           \
+      cudaError_t e_ = (call);                                                                    \
+      if (e_ != cudaSuccess) {                                                                    \
+         (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                           \
+         return SWSGPU_ECUDA;                                                                     \
+      }                                                                                           \
+   } while (0)
+
+static int fail(swsgpu_handle *h, int code, const std::string &msg)
+{
+   if (h) h->err = msg;
+   else g_create_error = msg;
+   return code;
+}
+
+// ---------------------------------------------------------------------------
+// windows (the reference's formulas, TaskCoreIPP.cpp:569-605)
+// ---------------------------------------------------------------------------
+static void make_window(int type, int n, std::vector<float> &w)
+{
+   w.resize(n);
+   for (int i = 0; i < n; i++) {
+      double fi = (double)(float)i, fn = (double)(float)n, v = 1.0;
+      double a = 2.0 * M_PI * (double)i / (double)(n - 1);
+      switch (type) {
+      case SWSGPU_WIN_NONE: v = 1.0; break;
+      case SWSGPU_WIN_COSINE: v = std::cos(M_PI * (fi - 0.5 * fn + 0.5) / fn); break;
+      case SWSGPU_WIN_COSINE2: {
+         double c = std::cos(M_PI * (fi - 0.5 * fn + 0.5) / fn);
+         v = c * c;
+      } break;
+      case SWSGPU_WIN_HAMMING: v = 0.54 - 0.46 * std::cos(a); break;
+      case SWSGPU_WIN_HANN: {
+         double s = std::sin(M_PI * (double)i / (double)(n - 1));
+         v = s * s;
+      } break;
+      case SWSGPU_WIN_BLACKMAN: v = 0.75 - 0.5 * std::cos(a) - 0.25 * std::cos(2.0 * a); break;
+      case SWSGPU_WIN_BLACKMANHARRIS:
+         v = 0.35875 - 0.48829 * std::cos(a) + 0.14128 * std::cos(2.0 * a) - 0.01168 * std::cos(3.0 * a);
+         break;
+      default: v = 1.0;
+      }
+      w[i] = (float)v;
+   }
+}
+
+static void make_twiddles(int n, int count, std::vector<float2> &t)
+{
+   t.resize(count);
+   for (int m = 0; m < count; m++) {
+      double a = -2.0 * M_PI * (double)m / (double)n;
+      t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+   }
+}
+
+static float4 level_table(int format, int nbit)
+{
+   const float H = 3.3359f;  // OPTIMAL_2BIT_HIGH
+   if (format == SWSGPU_FMT_MARK5B) {
+      if (nbit == 2) return make_float4(-H, 1.0f, -1.0f, H);
+      return make_float4(1.0f, -1.0f, 0.0f, 0.0f);
+   }
+   if (nbit == 2) return make_float4(-H, -1.0f, 1.0f, H);
+   return make_float4(-1.0f, 1.0f, 0.0f, 0.0f);
+}
+
+static int payload_bytes(const swsgpu_layout &l) { return l.frame_bytes - l.header_bytes; }
+
+// ---------------------------------------------------------------------------
+// doMaths frame schedule of one run (TaskCoreIPP.cpp:394-524)
+// ---------------------------------------------------------------------------
+struct RunShape {
+   std::vector<long long> starts;  // run-relative first sample of each FFT
+   std::vector<int> spec;          // run-local spectrum of each FFT
+   int nspec = 0;
+   bool partial = false;
+};
+
+static RunShape run_shape(const swsgpu_config &c, long long nsamp)
+{
+   RunShape r;
+   long long pos = 0, hop = c.fft_points / c.overlap;
+   int acc = 0, ns = 0;
+   while (nsamp - pos >= c.fft_points) {
+      r.starts.push_back(pos);
+      r.spec.push_back(ns);
+      pos += hop;
+      if (++acc >= c.core_overlapped_ffts) {
+         ns++;
+         acc = 0;
+         pos += c.fft_points - hop;
+      }
+   }
+   r.partial = acc > 0;
+   r.nspec = ns + (acc > 0);
+   return r;
+}
+
+static long long samples_of(const swsgpu_layout &l, size_t payload_bytes_n)
+{
+   return (long long)((payload_bytes_n * 8ull) / (unsigned long long)(l.nchan * l.nbit));
+}
+
+// Build items, reduction entries and output vectors for `nruns` runs.
+static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int runs_per_output,
+                           float *d_auto, float *d_xpol, float *d_pcal, Schedule &sc)
+{
+   const swsgpu_config &c = h->cfg;
+   const int S = h->S;
+   const long long run_samp = samples_of(c.layout[0], run_bytes);
+   RunShape rs = run_shape(c, run_samp);
+   sc.nsamp = run_samp * nruns;
+   const int groups = (nruns + runs_per_output - 1) / runs_per_output;
+   sc.nspec_total = groups * rs.nspec;
+   sc.nffts = (int)rs.starts.size() * nruns;
+   const long long hop = c.fft_points / c.overlap;
+
+   // jobs per spectrum and item size: aim for ~4 items per resident cluster
+   long long total_jobs = 0;
+   {
+      int nxp = c.num_xpols, nauto = 0;
+      for (int s = 0; s < c.num_sources; s++)
+         if (h->auto_owner[s] < 0) nauto++;
+      total_jobs = (long long)sc.nffts * nxp + (long long)(sc.nffts + 1) / 2 * nauto;
+   }
+   long long target_items = std::max<long long>(1, 4ll * h->max_clusters);
+   int fper = (int)std::max<long long>(1, (total_jobs + target_items - 1) / target_items);
+
+   // key -> output vector index
+   std::map<long long, std::vector<RedEntry>> vec_entries;
+   std::map<long long, OutVec> vec_desc;
+   auto add_entry = [&](long long key, float *dst, int stride, int item, int prod, float scale) {
+      if (!vec_desc.count(key)) {
+         OutVec o;
+         o.first = 0;
+         o.count = 0;
+         o.dst = dst;
+         o.stride = stride;
+         vec_desc[key] = o;
+      }
+      RedEntry e;
+      e.item = item;
+      e.prod = prod;
+      e.scale = scale;
+      vec_entries[key].push_back(e);
+   };
+
+   const int nfr_run = (int)rs.starts.size();
+   for (int r = 0; r < nruns; r++) {
+      const long long base = (long long)r * run_samp;
+      const int g0 = (r / runs_per_output) * rs.nspec;
+      for (int sp = 0; sp < rs.nspec; sp++) {
+         // frames of this spectrum (consecutive, uniform hop)
+         int f0 = -1, nf = 0;
+         for (int f = 0; f < nfr_run; f++)
+            if (rs.spec[f] == sp) {
+               if (f0 < 0) f0 = f;
+               nf++;
+            }
+         if (nf == 0) continue;
+         const bool full = !(rs.partial && sp == rs.nspec - 1);
+         const float scale = 0.25f * (full ? (float)(1.0 / c.core_overlapped_ffts) : 1.0f);
+         const int g = g0 + sp;
+         const long long first = base + rs.starts[f0];
+         // cross pairs
+         for (int xp = 0; xp < c.num_xpols; xp++) {
+            const int si = c.xpol_pair[xp][0], sj = c.xpol_pair[xp][1];
+            for (int j0 = 0; j0 < nf; j0 += fper) {
+               Item it;
+               it.start = first + (long long)j0 * hop;
+               it.src_a = h->src_code[si];
+               it.src_b = h->src_code[sj];
+               it.step = (int)hop;
+               it.offset_b = 0;
+               it.nfr = std::min(fper, nf - j0);
+               it.mode = MODE_XPOL;
+               const int id = (int)sc.items.size();
+               sc.items.push_back(it);
+               if (h->auto_owner[si] == xp && d_auto)
+                  add_entry(((long long)g * 4 + 0) << 32 | (unsigned)si,
+                            d_auto + ((size_t)g * c.num_sources + si) * S, 1, id, 0, scale);
+               if (h->auto_owner[sj] == xp && d_auto)
+                  add_entry(((long long)g * 4 + 0) << 32 | (unsigned)sj,
+                            d_auto + ((size_t)g * c.num_sources + sj) * S, 1, id, 1, scale);
+               if (d_xpol) {
+                  float *xb = d_xpol + ((size_t)g * c.num_xpols + xp) * S * 2;
+                  add_entry(((long long)g * 4 + 1) << 32 | (unsigned)xp, xb, 2, id, 2, scale);
+                  add_entry(((long long)g * 4 + 2) << 32 | (unsigned)xp, xb + 1, 2, id, 3, scale);
+               }
+            }
+         }
+         // auto-only sources: consecutive frame pairs
+         for (int s = 0; s < c.num_sources; s++) {
+            if (h->auto_owner[s] >= 0 || !d_auto) continue;
+            float *dst = d_auto + ((size_t)g * c.num_sources + s) * S;
+            const long long key = ((long long)g * 4 + 0) << 32 | (unsigned)s;
+            const int npairs = nf / 2;
+            const int pper = std::max(1, fper);
+            for (int j0 = 0; j0 < npairs; j0 += pper) {
+               Item it;
+               it.start = first + (long long)(2 * j0) * hop;
+               it.src_a = h->src_code[s];
+               it.src_b = h->src_code[s];
+               it.step = (int)(2 * hop);
+               it.offset_b = (int)hop;
+               it.nfr = std::min(pper, npairs - j0);
+               it.mode = MODE_AUTOSUM;
+               const int id = (int)sc.items.size();
+               sc.items.push_back(it);
+               add_entry(key, dst, 1, id, 0, scale);
+            }
+            if (nf % 2) {
+               Item it;
+               it.start = first + (long long)(nf - 1) * hop;
+               it.src_a = h->src_code[s];
+               it.src_b = -1;
+               it.step = 0;
+               it.offset_b = 0;
+               it.nfr = 1;
+               it.mode = MODE_SINGLE;
+               const int id = (int)sc.items.size();
+               sc.items.push_back(it);
+               add_entry(key, dst, 1, id, 0, scale);
+            }
+         }
+         // phase-cal folding: every overlap-th source FFT, counted per source
+         // FFT within the run (TaskCoreIPP.cpp:414-418, curr_ffts)
+         if (c.extract_pcal && d_pcal) {
+            for (int f = f0; f < f0 + nf; f++)
+               for (int s = 0; s < c.num_sources; s++) {
+                  const int curr = f * c.num_sources + s;
+                  if (curr % c.overlap != 0) continue;
+                  PcalJob pj;
+                  pj.start = base + rs.starts[f];
+                  pj.src = h->src_code[s];
+                  pj.out = (g * c.num_sources + s);
+                  sc.pcal_jobs.push_back(pj);
+               }
+         }
+      }
+   }
+   for (auto &kv : vec_desc) {
+      OutVec o = kv.second;
+      auto &ents = vec_entries[kv.first];
+      o.first = (int)sc.entries.size();
+      o.count = (int)ents.size();
+      sc.entries.insert(sc.entries.end(), ents.begin(), ents.end());
+      sc.outs.push_back(o);
+   }
+}
+
+// ---------------------------------------------------------------------------
+// pipeline launch for a chunk already in device memory
+// ---------------------------------------------------------------------------
+static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t *raw_bytes,
+                        const long long *grid_off, size_t run_bytes, int nruns,
+                        int runs_per_output, float *d_auto, float *d_xpol, float *d_pcal,
+                        cudaStream_t st, int *nspec_out)
+{
+   const swsgpu_config &c = h->cfg;
+   Schedule sc;
+   build_schedule(h, run_bytes, nruns, runs_per_output, d_auto, d_xpol, d_pcal, sc);
+   if (nspec_out) *nspec_out = sc.nspec_total;
+   int launches = 0;
+   const int S = h->S;
+   const int ncode = (int)h->code_stream.size();
+   const int nbit = c.layout[0].nbit;
+   const int spw = 32 / nbit;
+   const long long nsamp = sc.nsamp;
+   const long long code_words = (nsamp + spw - 1) / spw;
+   const long long blank_words = (nsamp + 31) / 32;
+
+   CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 16));
+   CK(h, h->d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
+   CK(h, h->d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
+   CK(h, cudaMemsetAsync(h->d_blank.p, 0, sizeof(uint32_t) * (size_t)blank_words * c.num_streams, st));
+   CK(h, cudaMemsetAsync(h->d_blank_any.p, 0, sizeof(int) * SWSGPU_MAX_STREAMS, st));
+
+   // K1 per stream
+   for (int s = 0; s < c.num_streams; s++) {
+      const swsgpu_layout &L = c.layout[s];
+      StreamIn si;
+      si.data = (const uint8_t *)d_raw[s];
+      si.nbytes = (long long)raw_bytes[s];
+      si.grid_offset = grid_off[s];
+      si.frame_bytes = L.frame_bytes;
+      si.header_bytes = L.header_bytes;
+      si.payload_bytes = payload_bytes(L);
+      si.nchan = L.nchan;
+      si.nbit = L.nbit;
+      si.format = L.format;
+      const long long last_v = si.grid_offset + ((nsamp * (long long)L.nchan * L.nbit - 1) >> 3);
+      si.nframes = last_v / si.payload_bytes + 1;
+      CK(h, h->d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes));
+      k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(
+          si, (int2 *)h->d_valid[s].p, (int *)h->d_blank_any.p + s);
+      launches++;
+      std::vector<int> chans;
+      int first_code = -1;
+      for (int k = 0; k < ncode; k++)
+         if (h->code_stream[k] == s) {
+            if (first_code < 0) first_code = k;
+            chans.push_back(h->code_chan[k]);
+         }
+      if (chans.empty()) continue;
+      CK(h, h->d_chans[s].ensure(sizeof(int) * chans.size()));
+      CK(h, cudaMemcpyAsync(h->d_chans[s].p, chans.data(), sizeof(int) * chans.size(),
+                            cudaMemcpyHostToDevice, st));
+      uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)first_code * code_words;
+      dim3 grid((unsigned)((code_words + 255) / 256), (unsigned)((chans.size() + 15) / 16));
+      uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
+      launch_unpack_codes(nbit, grid, 256, st, si, nsamp, (const int *)h->d_chans[s].p,
+                          (int)chans.size(), codes, code_words, (const int2 *)h->d_valid[s].p, blank);
+      launches++;
+   }
+   CK(h, cudaGetLastError());
+
+   // K2
+   const int nitems = (int)sc.items.size();
+   if (nitems > 0) {
+      CK(h, h->d_items.ensure(sizeof(Item) * nitems));
+      CK(h, cudaMemcpyAsync(h->d_items.p, sc.items.data(), sizeof(Item) * nitems,
+                            cudaMemcpyHostToDevice, st));
+      CK(h, h->d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
+      SpecArgs a;
+      a.codes = (const uint32_t *)h->d_codes.p;
+      a.code_words = code_words;
+      a.blank = (const uint32_t *)h->d_blank.p;
+      a.blank_words = blank_words;
+      a.blank_any = (const int *)h->d_blank_any.p;
+      a.code_stream = (const int *)h->d_code_stream.p;
+      a.items = (const Item *)h->d_items.p;
+      a.nitems = nitems;
+      a.window = (const float *)h->d_window.p;
+      a.twQ = (const float2 *)h->d_twQ.p;
+      a.twN = (const float2 *)h->d_twN.p;
+      a.partial = (float *)h->d_partial.p;
+      a.N = c.fft_points;
+      a.S = S;
+      a.levels = level_table(c.layout[0].format, nbit);
+      const Plan &pl = h->plan;
+      SpecKernel kern = pl.kern[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+      const int ncl = std::max(1, std::min(nitems, h->max_clusters));
+      cudaLaunchConfig_t cfgl = {};
+      cfgl.gridDim = dim3(ncl * pl.P);
+      cfgl.blockDim = dim3(pl.T);
+      cfgl.dynamicSmemBytes = pl.smem;
+      cfgl.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = pl.P;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfgl.attrs = attr;
+      cfgl.numAttrs = 1;
+      CK(h, cudaLaunchKernelEx(&cfgl, kern, a));
+      launches++;
+
+      // K3
+      const int nouts = (int)sc.outs.size();
+      if (nouts > 0) {
+         CK(h, h->d_entries.ensure(sizeof(RedEntry) * sc.entries.size()));
+         CK(h, h->d_outs.ensure(sizeof(OutVec) * nouts));
+         CK(h, cudaMemcpyAsync(h->d_entries.p, sc.entries.data(), sizeof(RedEntry) * sc.entries.size(),
+                               cudaMemcpyHostToDevice, st));
+         CK(h, cudaMemcpyAsync(h->d_outs.p, sc.outs.data(), sizeof(OutVec) * nouts,
+                               cudaMemcpyHostToDevice, st));
+         dim3 grid((S + 255) / 256, nouts);
+         k_reduce<<<grid, 256, 0, st>>>((const float *)h->d_partial.p, S,
+                                         (const RedEntry *)h->d_entries.p, (const OutVec *)h->d_outs.p);
+         launches++;
+      }
+   }
+   // phase cal
+   if (c.extract_pcal && d_pcal) {
+      const int nout = sc.nspec_total * c.num_sources;
+      CK(h, cudaMemsetAsync(d_pcal, 0, sizeof(float) * 2 * c.pcal_tonebins * (size_t)nout, st));
+      launches++;
+      if (!sc.pcal_jobs.empty()) {
+         CK(h, h->d_pcal_part.ensure(sizeof(double) * 2 * c.pcal_tonebins * (size_t)nout));
+         int njobs = (int)sc.pcal_jobs.size();
+         CK(h, h->d_pcal_jobs.ensure(sizeof(PcalJob) * njobs));
+         CK(h, cudaMemcpyAsync(h->d_pcal_jobs.p, sc.pcal_jobs.data(), sizeof(PcalJob) * njobs,
+                               cudaMemcpyHostToDevice, st));
+         PcalArgs pa;
+         pa.codes = (const uint32_t *)h->d_codes.p;
+         pa.code_words = code_words;
+         pa.blank = (const uint32_t *)h->d_blank.p;
+         pa.blank_words = blank_words;
+         pa.blank_any = (const int *)h->d_blank_any.p;
+         pa.code_stream = (const int *)h->d_code_stream.p;
+         pa.jobs = (const PcalJob *)h->d_pcal_jobs.p;
+         pa.njobs = njobs;
+         pa.N = c.fft_points;
+         pa.tonebins = c.pcal_tonebins;
+         pa.rotatorlen = c.pcal_rotatorlen;
+         pa.used = (c.pcal_rotatorlen / c.pcal_tonebins) * c.pcal_tonebins;
+         pa.dphi = 2.0 * M_PI * (-c.pcal_offset_hz / c.samplingfreq);
+         pa.levels = level_table(c.layout[0].format, nbit);
+         pa.out = d_pcal;
+         pa.acc = (double *)h->d_pcal_part.p;
+         pa.nout = nout;
+         int rc = launch_pcal(pa, nbit, st);
+         if (rc) return fail(h, SWSGPU_ECUDA, std::string("pcal launch: ") + cudaGetErrorString(cudaGetLastError()));
+         launches += 2;
+      }
+   }
+   CK(h, cudaGetLastError());
+   h->last_launches = launches;
+   return SWSGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int swsgpu_version(void) { return 10000; }
+
+int swsgpu_device_ok(int device)
+{
+   cudaDeviceProp p;
+   if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return 0;
+   return p.major >= 10 ? 1 : 0;
+}
+
+const char *swsgpu_last_error(const swsgpu_handle *h)
+{
+   return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+static int validate_config(const swsgpu_config *c, std::string &why)
+{
+   if (c->num_streams < 1 || c->num_streams > SWSGPU_MAX_STREAMS) { why = "num_streams must be 1 or 2"; return 0; }
+   for (int s = 0; s < c->num_streams; s++) {
+      const swsgpu_layout &l = c->layout[s];
+      if (l.nbit != 1 && l.nbit != 2 && l.nbit != 8) { why = "nbit must be 1, 2 or 8"; return 0; }
+      if (l.nchan < 1 || l.nchan * l.nbit > 64) { why = "nchan*nbit must be 1..64"; return 0; }
+      if (l.format != SWSGPU_FMT_MARK5B && l.format != SWSGPU_FMT_VDIF) { why = "unknown format"; return 0; }
+      if (l.header_bytes < 0 || l.frame_bytes <= l.header_bytes) { why = "bad frame layout"; return 0; }
+      if ((l.frame_bytes % 8) || (l.header_bytes % 4) || ((l.frame_bytes - l.header_bytes) % 8)) {
+         why = "frame, header and payload sizes must be multiples of 8, 4 and 8 bytes";
+         return 0;
+      }
+      if (l.nbit != c->layout[0].nbit || l.nchan != c->layout[0].nchan || l.format != c->layout[0].format) {
+         why = "all streams must share format, channels and bits (as in the reference's settings)";
+         return 0;
+      }
+   }
+   if (c->overlap < 1 || c->fft_points % c->overlap) { why = "overlap must divide fft_points"; return 0; }
+   if (c->core_overlapped_ffts < 1) { why = "core_overlapped_ffts must be >= 1"; return 0; }
+   if (c->num_sources < 1 || c->num_sources > SWSGPU_MAX_SOURCES) { why = "num_sources out of range"; return 0; }
+   for (int s = 0; s < c->num_sources; s++) {
+      if (c->source_stream[s] < 0 || c->source_stream[s] >= c->num_streams) { why = "source_stream out of range"; return 0; }
+      if (c->source_channel[s] < 0 || c->source_channel[s] >= c->layout[c->source_stream[s]].nchan) {
+         why = "source_channel out of range";
+         return 0;
+      }
+   }
+   if (c->num_xpols < 0 || c->num_xpols > SWSGPU_MAX_SOURCES) { why = "num_xpols out of range"; return 0; }
+   for (int x = 0; x < c->num_xpols; x++)
+      for (int k = 0; k < 2; k++)
+         if (c->xpol_pair[x][k] < 0 || c->xpol_pair[x][k] >= c->num_sources) { why = "xpol_pair out of range"; return 0; }
+   if (c->window < 0 || c->window > SWSGPU_WIN_BLACKMANHARRIS) { why = "unknown window"; return 0; }
+   if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT) { why = "unknown precision"; return 0; }
+   if (c->extract_pcal) {
+      if (c->pcal_tonebins < 1 || c->pcal_rotatorlen < c->pcal_tonebins || c->fft_points % c->pcal_rotatorlen) {
+         why = "pcal: need tonebins >= 1, rotatorlen >= tonebins and N % rotatorlen == 0";
+         return 0;
+      }
+      if (c->pcal_tonebins > 4096) { why = "pcal_tonebins > 4096"; return 0; }
+   }
+   return 1;
+}
+
+int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
+{
+   if (!cfg || !out) return fail(nullptr, SWSGPU_EINVAL, "null argument");
+   *out = nullptr;
+   std::string why;
+   if (!validate_config(cfg, why)) return fail(nullptr, SWSGPU_EINVAL, why);
+   Plan plan;
+   if (!find_plan(cfg->fft_points, &plan))
+      return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
+   int ndev = 0;
+   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+      return fail(nullptr, SWSGPU_ENODEV, "no CUDA device " + std::to_string(device));
+   if (!swsgpu_device_ok(device)) return fail(nullptr, SWSGPU_ENODEV, "device is not sm_100 class");
+   if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, SWSGPU_ENODEV, "cudaSetDevice failed");
+
+   swsgpu_handle *h = new swsgpu_handle();
+   h->cfg = *cfg;
+   h->device = device;
+   h->plan = plan;
+   h->S = cfg->fft_points / 2 + 1;
+   auto bail = [&](int rc) {
+      std::string e = h->err;
+      swsgpu_destroy(h);
+      g_create_error = e;
+      return rc;
+   };
+   // code arrays
+   std::map<std::pair<int, int>, int> code_of;
+   for (int s = 0; s < cfg->num_sources; s++) {
+      auto key = std::make_pair(cfg->source_stream[s], cfg->source_channel[s]);
+      if (!code_of.count(key)) {
+         code_of[key] = (int)h->code_stream.size();
+         h->code_stream.push_back(key.first);
+         h->code_chan.push_back(key.second);
+      }
+      h->src_code.push_back(code_of[key]);
+   }
+   // reorder code arrays so each stream's are contiguous (K1 writes per stream)
+   {
+      std::vector<int> order;
+      for (int st = 0; st < cfg->num_streams; st++)
+         for (int k = 0; k < (int)h->code_stream.size(); k++)
+            if (h->code_stream[k] == st) order.push_back(k);
+      std::vector<int> inv(order.size()), cs, cc;
+      for (int i = 0; i < (int)order.size(); i++) {
+         inv[order[i]] = i;
+         cs.push_back(h->code_stream[order[i]]);
+         cc.push_back(h->code_chan[order[i]]);
+      }
+      h->code_stream = cs;
+      h->code_chan = cc;
+      for (auto &x : h->src_code) x = inv[x];
+   }
+   h->auto_owner.assign(cfg->num_sources, -1);
+   for (int x = 0; x < cfg->num_xpols; x++)
+      for (int k = 0; k < 2; k++)
+         if (h->auto_owner[cfg->xpol_pair[x][k]] < 0) h->auto_owner[cfg->xpol_pair[x][k]] = x;
+   // a pair (i, i) cannot own both autos twice; treat it as owning source i once
+   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming) != cudaSuccess) {
+      h->err = "stream/event creation failed";
+      return bail(SWSGPU_ECUDA);
+   }
+   std::vector<float> win;
+   make_window(cfg->window, cfg->fft_points, win);
+   std::vector<float2> twQ, twN;
+   make_twiddles(plan.Q, plan.Q, twQ);
+   make_twiddles(cfg->fft_points, cfg->fft_points / 2 + 1, twN);
+#define CKB(call)                                                                                  \
+   do {                                                                                           \
+      cudaError_t e_ = (call);                                                                    \
+      if (e_ != cudaSuccess) {                                                                    \
+         h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+         return bail(SWSGPU_ECUDA);                                                               \
+      }                                                                                           \
+   } while (0)
+   CKB(h->d_window.ensure(sizeof(float) * win.size()));
+   CKB(cudaMemcpy(h->d_window.p, win.data(), sizeof(float) * win.size(), cudaMemcpyHostToDevice));
+   CKB(h->d_twQ.ensure(sizeof(float2) * twQ.size()));
+   CKB(cudaMemcpy(h->d_twQ.p, twQ.data(), sizeof(float2) * twQ.size(), cudaMemcpyHostToDevice));
+   CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
+   CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
+   CKB(h->d_code_stream.ensure(sizeof(int) * h->code_stream.size()));
+   CKB(cudaMemcpy(h->d_code_stream.p, h->code_stream.data(), sizeof(int) * h->code_stream.size(),
+                  cudaMemcpyHostToDevice));
+   // kernel attributes and cluster occupancy
+   const int nbit = cfg->layout[0].nbit;
+   SpecKernel kern = plan.kern[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+   CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
+   if (plan.P > 8)
+      CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+   {
+      cudaLaunchConfig_t cfgl = {};
+      cfgl.gridDim = dim3(plan.P);
+      cfgl.blockDim = dim3(plan.T);
+      cfgl.dynamicSmemBytes = plan.smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = plan.P;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfgl.attrs = attr;
+      cfgl.numAttrs = 1;
+      int ncl = 0;
+      CKB(cudaOccupancyMaxActiveClusters(&ncl, (const void *)kern, &cfgl));
+      if (ncl < 1) {
+         h->err = "cluster configuration does not fit on this device";
+         return bail(SWSGPU_ECUDA);
+      }
+      h->max_clusters = ncl;
+   }
+   // device buffers for submit()
+   for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_raw[s].ensure(cfg->max_run_bytes + 64));
+#undef CKB
+   *out = h;
+   return SWSGPU_OK;
+}
+
+void swsgpu_destroy(swsgpu_handle *h)
+{
+   if (!h) return;
+   cudaSetDevice(h->device);
+   if (h->stream) cudaStreamSynchronize(h->stream);
+   DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes,
+                     &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
+                     &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
+                     &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal};
+   for (DevBuf *b : bufs) b->release();
+   for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) {
+      h->d_raw[s].release();
+      h->d_valid[s].release();
+      h->d_chans[s].release();
+   }
+   h->h_out.release();
+   if (h->done) cudaEventDestroy(h->done);
+   if (h->stream) cudaStreamDestroy(h->stream);
+   delete h;
+}
+
+int swsgpu_run_shape(const swsgpu_handle *h, size_t nbytes, int *nspectra, int *nffts, int *partial)
+{
+   if (!h) return SWSGPU_EINVAL;
+   RunShape rs = run_shape(h->cfg, samples_of(h->cfg.layout[0], nbytes));
+   if (nspectra) *nspectra = rs.nspec;
+   if (nffts) *nffts = (int)rs.starts.size();
+   if (partial) *partial = rs.partial ? 1 : 0;
+   return SWSGPU_OK;
+}
+
+int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                  const int64_t *stream_payload_offset)
+{
+   if (!h || !raw || !nbytes) return SWSGPU_EINVAL;
+   if (h->pending) return fail(h, SWSGPU_ESTATE, "submit while a run is pending");
+   const swsgpu_config &c = h->cfg;
+   CK(h, cudaSetDevice(h->device));
+   // payload bytes per stream: the reference walks min over sources
+   size_t payload_min = (size_t)-1;
+   long long grid_off[SWSGPU_MAX_STREAMS];
+   size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   const void *d_raw[SWSGPU_MAX_STREAMS];
+   for (int s = 0; s < c.num_streams; s++) {
+      const swsgpu_layout &L = c.layout[s];
+      const int pb = payload_bytes(L);
+      long long off = stream_payload_offset ? (long long)(stream_payload_offset[s] % pb) : 0;
+      if (off % 4) return fail(h, SWSGPU_EINVAL, "payload offset must be a multiple of 4 bytes");
+      size_t pay;
+      if (L.header_bytes == 0) {
+         pay = nbytes[s];
+         grid_off[s] = off;
+      } else {
+         if (off != 0) return fail(h, SWSGPU_EINVAL, "framed input must start on a frame");
+         size_t nfr = nbytes[s] / L.frame_bytes;
+         size_t rem = nbytes[s] - nfr * L.frame_bytes;
+         pay = nfr * pb + (rem > (size_t)L.header_bytes ? rem - L.header_bytes : 0);
+         grid_off[s] = 0;
+      }
+      if (nbytes[s] > c.max_run_bytes + (size_t)c.max_run_bytes / 8 + 1024 + 64)
+         return fail(h, SWSGPU_EINVAL, "buffer larger than max_run_bytes");
+      payload_min = std::min(payload_min, pay);
+      CK(h, h->d_raw[s].ensure(nbytes[s] + 64));
+      CK(h, cudaMemcpyAsync(h->d_raw[s].p, raw[s], nbytes[s], cudaMemcpyHostToDevice, h->stream));
+      raw_bytes[s] = nbytes[s];
+      d_raw[s] = h->d_raw[s].p;
+   }
+   RunShape rs = run_shape(c, samples_of(c.layout[0], payload_min));
+   const int S = h->S;
+   const int nsp = std::max(rs.nspec, 0);
+   h->h_auto_bytes = sizeof(float) * (size_t)nsp * c.num_sources * S;
+   h->h_xpol_bytes = sizeof(float) * 2 * (size_t)nsp * c.num_xpols * S;
+   h->h_pcal_bytes = c.extract_pcal ? sizeof(float) * 2 * (size_t)nsp * c.num_sources * c.pcal_tonebins : 0;
+   CK(h, h->d_out_auto.ensure(h->h_auto_bytes + 16));
+   CK(h, h->d_out_xpol.ensure(h->h_xpol_bytes + 16));
+   CK(h, h->d_out_pcal.ensure(h->h_pcal_bytes + 16));
+   CK(h, h->h_out.ensure(h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes + 64));
+   int nspec = 0;
+   if (nsp > 0) {
+      int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, payload_min, 1, 1, (float *)h->d_out_auto.p,
+                            c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
+                            c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec);
+      if (rc) return rc;
+      char *hp = (char *)h->h_out.p;
+      CK(h, cudaMemcpyAsync(hp, h->d_out_auto.p, h->h_auto_bytes, cudaMemcpyDeviceToHost, h->stream));
+      if (h->h_xpol_bytes)
+         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes, h->d_out_xpol.p, h->h_xpol_bytes,
+                               cudaMemcpyDeviceToHost, h->stream));
+      if (h->h_pcal_bytes)
+         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes, h->d_out_pcal.p,
+                               h->h_pcal_bytes, cudaMemcpyDeviceToHost, h->stream));
+   } else {
+      h->last_launches = 0;
+   }
+   CK(h, cudaEventRecord(h->done, h->stream));
+   h->pending = true;
+   h->pending_nspec = nspec;
+   return SWSGPU_OK;
+}
+
+int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
+{
+   if (!h) return SWSGPU_EINVAL;
+   if (!h->pending) return fail(h, SWSGPU_ESTATE, "wait without a submitted run");
+   CK(h, cudaSetDevice(h->device));
+   auto t0 = std::chrono::steady_clock::now();
+   while (true) {
+      cudaError_t e = cudaEventQuery(h->done);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) {
+         h->pending = false;
+         return fail(h, SWSGPU_ECUDA, std::string("run failed: ") + cudaGetErrorString(e));
+      }
+      if (timeout_ms >= 0) {
+         auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+         if (ms >= timeout_ms) return fail(h, SWSGPU_ETIMEOUT, "run not complete within timeout");
+      }
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+   }
+   h->pending = false;
+   if (nspectra) *nspectra = h->pending_nspec;
+   return SWSGPU_OK;
+}
+
+int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out)
+{
+   if (!h || !out) return SWSGPU_EINVAL;
+   if (h->pending) return fail(h, SWSGPU_ESTATE, "fetch before wait");
+   const char *hp = (const char *)h->h_out.p;
+   if (!hp) return SWSGPU_OK;
+   if (out->auto_out) memcpy(out->auto_out, hp, h->h_auto_bytes);
+   if (out->xpol_out && h->h_xpol_bytes) memcpy(out->xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);
+   if (out->pcal_out && h->h_pcal_bytes)
+      memcpy(out->pcal_out, hp + h->h_auto_bytes + h->h_xpol_bytes, h->h_pcal_bytes);
+   return SWSGPU_OK;
+}
+
+int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
+                          int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream)
+{
+   if (!h || !d_raw || !d_out || nruns < 1 || runs_per_output < 1) return SWSGPU_EINVAL;
+   const swsgpu_config &c = h->cfg;
+   CK(h, cudaSetDevice(h->device));
+   cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : h->stream;
+   long long grid_off[SWSGPU_MAX_STREAMS];
+   size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   for (int s = 0; s < c.num_streams; s++) {
+      const swsgpu_layout &L = c.layout[s];
+      const int pb = payload_bytes(L);
+      size_t pay = run_bytes * (size_t)nruns;
+      grid_off[s] = 0;
+      if (L.header_bytes == 0) raw_bytes[s] = pay;
+      else raw_bytes[s] = ((pay + pb - 1) / pb) * (size_t)L.frame_bytes;
+   }
+   int nspec = 0;
+   return launch_chunk(h, d_raw, raw_bytes, grid_off, run_bytes, nruns, runs_per_output,
+                       d_out->auto_out, c.num_xpols ? d_out->xpol_out : nullptr,
+                       c.extract_pcal ? d_out->pcal_out : nullptr, st, &nspec);
+}
+
+int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes)
+{
+   if (!h || !bytes) return SWSGPU_EINVAL;
+   const swsgpu_config &c = h->cfg;
+   long long nsamp = samples_of(c.layout[0], run_bytes) * nruns;
+   int spw = 32 / c.layout[0].nbit;
+   size_t code = sizeof(uint32_t) * ((nsamp + spw - 1) / spw) * h->code_stream.size();
+   size_t blank = sizeof(uint32_t) * ((nsamp + 31) / 32) * c.num_streams;
+   *bytes = code + blank;
+   return SWSGPU_OK;
+}
+
+int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,
+                         int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
+                         int64_t *nvalid, void *cuda_stream)
+{
+   if (!lay || !d_raw || !d_out || chan < 0 || chan >= lay->nchan || nsamp < 0) return SWSGPU_EINVAL;
+   if (lay->nbit != 1 && lay->nbit != 2 && lay->nbit != 8) return SWSGPU_EINVAL;
+   const int pb = lay->frame_bytes - lay->header_bytes;
+   if (pb <= 0 || (pb % 8) || (lay->header_bytes % 4) || (payload_offset % 4)) return SWSGPU_EINVAL;
+   if (lay->header_bytes > 0 && payload_offset != 0) return SWSGPU_EINVAL;
+   cudaStream_t st = (cudaStream_t)cuda_stream;
+   StreamIn si;
+   si.data = (const uint8_t *)d_raw;
+   si.nbytes = (long long)nbytes;
+   si.grid_offset = payload_offset % pb;
+   si.frame_bytes = lay->frame_bytes;
+   si.header_bytes = lay->header_bytes;
+   si.payload_bytes = pb;
+   si.nchan = lay->nchan;
+   si.nbit = lay->nbit;
+   si.format = lay->format;
+   if (nsamp == 0) {
+      if (nvalid) *nvalid = 0;
+      return SWSGPU_OK;
+   }
+   const long long last_v = si.grid_offset + ((nsamp * (long long)lay->nchan * lay->nbit - 1) >> 3);
+   si.nframes = last_v / pb + 1;
+   // bytes needed
+   long long need = lay->header_bytes ? si.nframes * lay->frame_bytes - (lay->frame_bytes - lay->header_bytes - (last_v % pb) - 1)
+                                      : (last_v - si.grid_offset + 1);
+   if (need > (long long)nbytes) return SWSGPU_EINVAL;
+   int2 *d_valid = nullptr;
+   int *d_any = nullptr;
+   unsigned long long *d_cnt = nullptr;
+   if (cudaMalloc(&d_valid, sizeof(int2) * si.nframes) != cudaSuccess) return SWSGPU_ECUDA;
+   cudaMalloc(&d_any, sizeof(int));
+   cudaMalloc(&d_cnt, sizeof(unsigned long long));
+   cudaMemsetAsync(d_any, 0, sizeof(int), st);
+   cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
+   k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(si, d_valid, d_any);
+   k_unpack_float<<<(unsigned)((nsamp + 255) / 256), 256, 0, st>>>(si, nsamp, chan,
+                                                                    level_table(lay->format, lay->nbit),
+                                                                    d_out, d_valid, d_cnt);
+   unsigned long long cnt = 0;
+   cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+   cudaError_t e = cudaStreamSynchronize(st);
+   cudaFree(d_valid);
+   cudaFree(d_any);
+   cudaFree(d_cnt);
+   if (e != cudaSuccess) {
+      g_create_error = cudaGetErrorString(e);
+      return SWSGPU_ECUDA;
+   }
+   if (nvalid) *nvalid = (int64_t)cnt;
+   return SWSGPU_OK;
+}
+
+int swsgpu_last_launch_count(const swsgpu_handle *h) { return h ? h->last_launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// kernels.cuh -- device data structures shared by the spectrometer kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sws {
+
+constexpr uint32_t FILL32 = 0x11223344u;              // mark5 fill pattern (blanker_mark5.c:42-48)
+constexpr unsigned long long FILL64 = 0x1122334411223344ull;
+
+// One input stream of a chunk.  data[0] is the first byte of frame 0 (framed
+// layouts) or the first payload byte of the chunk (header-free layouts).
+// grid_offset: payload bytes of frame 0 that precede the chunk's first
+// payload byte.  Virtual payload byte v = grid_offset + x for chunk payload
+// byte x; frame f = v / payload_bytes.
+struct StreamIn {
+   const uint8_t *data;
+   long long nbytes;
+   long long grid_offset;
+   int frame_bytes;
+   int header_bytes;
+   int payload_bytes;
+   int nchan;
+   int nbit;
+   int format;   // 0 Mark5B, 1 VDIF
+   long long nframes;  // frames touched by the chunk
+};
+
+// A run of consecutive FFT jobs that share their accumulators.
+// mode 0 (XPOL):    job j packs A = source a, B = source b, both starting at
+//                   start + j*step; products |A|^2, |B|^2, A conj(B).
+// mode 1 (AUTOSUM): A = source a at start + j*step, B = source a at
+//                   start + j*step + offset_b; product |A|^2 + |B|^2.
+// mode 2 (SINGLE):  A = source a at start (one job), B = 0; product |A|^2.
+struct Item {
+   long long start;
+   int src_a, src_b;
+   int step, offset_b;
+   int nfr, mode;
+};
+
+constexpr int MODE_XPOL = 0, MODE_AUTOSUM = 1, MODE_SINGLE = 2;
+
+struct SpecArgs {
+   const uint32_t *codes;        // [ncode][code_words]
+   long long code_words;         // words per code array
+   const uint32_t *blank;        // [nstream][blank_words] bitmaps (1 = blanked sample-time)
+   long long blank_words;
+   const int *blank_any;         // [nstream]
+   const int *code_stream;       // stream of each code array
+   const Item *items;
+   int nitems;
+   const float *window;          // [N]
+   const float2 *twQ;            // W_Q^m, m < Q
+   const float2 *twN;            // W_N^m, m < N/2 (+1)
+   float *partial;               // [nitems][4][S]
+   int N, S;
+   float4 levels;                // level table for 1/2-bit codes
+};
+
+// Reduction of item partial sums into output spectra.
+struct RedEntry {
+   int item, prod;
+   float scale;
+};
+struct OutVec {
+   int first, count;             // entries [first, first+count)
+   float *dst;                   // base of the output vector
+   int stride;                   // element stride (1 real, 2 complex)
+};
+
+}  // namespace sws

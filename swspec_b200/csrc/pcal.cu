@@ -1,0 +1,92 @@
+// pcal.cu -- K4: phase-cal folding with an FP64 rotator.
+//
+// Restates TaskCoreIPP::extract_PCal (src/IA-32/TaskCoreIPP.cpp:633-693):
+// every block of rotatorlen samples of an FFT's (unwindowed) input is
+// multiplied by exp(i dphi n), n = 0..rotatorlen-1 counted from the FFT start,
+// dphi = 2 pi (-f_offset / fs) (prepare, :129-136), and folded modulo
+// tonebins; only the first (rotatorlen / tonebins) * tonebins samples of each
+// block are folded (the reference's integer division).  The rotator phase is
+// evaluated in FP64 from the integer position in the period, and products and
+// sums are FP64, so folding 1e5 samples per bin per FFT loses nothing; the
+// folded bins are rounded to FP32 once, at the output.
+#include "pcal.cuh"
+
+namespace sws {
+
+template <int NBIT>
+__device__ __forceinline__ float pc_sample(const PcalArgs &a, int src, long long s, bool chk)
+{
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   uint32_t word = __ldg(a.codes + (long long)src * a.code_words + s / SPW);
+   uint32_t code = (word >> (NBIT * (int)(s % SPW))) & MASK;
+   float v;
+   if (NBIT == 8) v = (float)((int)code * 2 - 255) * (1.0f / 256.0f);
+   else if (NBIT == 2) v = (code == 0) ? a.levels.x : (code == 1) ? a.levels.y : (code == 2) ? a.levels.z : a.levels.w;
+   else v = code ? a.levels.y : a.levels.x;
+   if (chk) {
+      int st = a.code_stream[src];
+      uint32_t bw = __ldg(a.blank + (long long)st * a.blank_words + (s >> 5));
+      if ((bw >> (s & 31)) & 1u) v = 0.0f;
+   }
+   return v;
+}
+
+// grid.x: blocks per job, grid.y: job.  Each block folds a contiguous range
+// of rotator periods; thread t visits in-period positions t, t+T, ...
+template <int NBIT>
+__global__ void k_pcal_fold(PcalArgs a)
+{
+   extern __shared__ double pc_smem[];  // [tonebins][2]
+   const PcalJob job = a.jobs[blockIdx.y];
+   const int T = blockDim.x;
+   for (int i = threadIdx.x; i < 2 * a.tonebins; i += T) pc_smem[i] = 0.0;
+   __syncthreads();
+   const int nper = a.N / a.rotatorlen;
+   const int p0 = (int)((long long)nper * blockIdx.x / gridDim.x);
+   const int p1 = (int)((long long)nper * (blockIdx.x + 1) / gridDim.x);
+   const bool chk = a.blank_any[a.code_stream[job.src]] != 0;
+   for (int i = threadIdx.x; i < a.used; i += T) {
+      double sr = 0.0, si = 0.0;
+      for (int p = p0; p < p1; p++) {
+         long long s = job.start + (long long)p * a.rotatorlen + i;
+         double x = (double)pc_sample<NBIT>(a, job.src, s, chk);
+         sr += x;
+         (void)si;
+      }
+      // all samples of this thread share the in-period position i, so the
+      // rotator factor is common: sum(x) * exp(i dphi i)
+      double sn, cs;
+      sincos(a.dphi * (double)i, &sn, &cs);
+      const int b = i % a.tonebins;
+      atomicAdd(&pc_smem[2 * b], sr * cs);
+      atomicAdd(&pc_smem[2 * b + 1], sr * sn);
+   }
+   __syncthreads();
+   double *dst = a.acc + (long long)job.out * 2 * a.tonebins;
+   for (int i = threadIdx.x; i < 2 * a.tonebins; i += T) atomicAdd(&dst[i], pc_smem[i]);
+}
+
+__global__ void k_pcal_out(PcalArgs a)
+{
+   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i < (long long)a.nout * 2 * a.tonebins) a.out[i] = (float)a.acc[i];
+}
+
+int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
+{
+   const size_t n = (size_t)a.nout * 2 * a.tonebins;
+   cudaMemsetAsync(a.acc, 0, sizeof(double) * n, st);
+   const int T = 256;
+   const int nper = a.N / a.rotatorlen;
+   int bpj = nper < 8 ? nper : 8;
+   dim3 grid(bpj, a.njobs);
+   size_t sm = sizeof(double) * 2 * a.tonebins;
+   if (nbit == 1) k_pcal_fold<1><<<grid, T, sm, st>>>(a);
+   else if (nbit == 2) k_pcal_fold<2><<<grid, T, sm, st>>>(a);
+   else k_pcal_fold<8><<<grid, T, sm, st>>>(a);
+   k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+   return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+}  // namespace sws

@@ -1,0 +1,38 @@
+// pcal.cuh -- K4: phase-cal tone folding (TaskCoreIPP::extract_PCal).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sws {
+
+// One folded FFT's worth of samples: N samples of code array `src` from
+// chunk sample `start`, accumulated into output slot `out`.
+struct PcalJob {
+   long long start;
+   int src;
+   int out;
+};
+
+struct PcalArgs {
+   const uint32_t *codes;
+   long long code_words;
+   const uint32_t *blank;
+   long long blank_words;
+   const int *blank_any;
+   const int *code_stream;
+   const PcalJob *jobs;
+   int njobs;
+   int N;
+   int tonebins, rotatorlen, used;
+   double dphi;        // 2 pi (-offset / fs)
+   float4 levels;
+   float *out;         // [nout][tonebins][2]
+   double *acc;        // [nout][tonebins][2] scratch (set by launch_pcal)
+   int nout;
+};
+
+// Queues zeroing, folding and conversion on `st`; returns 0 or a CUDA error.
+int launch_pcal(PcalArgs a, int nbit, cudaStream_t st);
+
+}  // namespace sws

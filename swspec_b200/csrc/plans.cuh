@@ -1,0 +1,20 @@
+// plans.cuh -- FFT size plans of the cluster kernel.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace sws {
+
+typedef void (*SpecKernel)(SpecArgs);
+
+struct Plan {
+   int N, P, Q, T;
+   int R1, R2, R3;
+   SpecKernel kern[3];   // nbit 1, 2, 8
+   size_t smem;
+};
+
+// Returns false when N has no single-launch plan.
+bool find_plan(int N, Plan *out);
+
+}  // namespace sws

@@ -1,0 +1,195 @@
+"""ctypes binding of libswsgpu.so (include/swsgpu.h).
+
+The native library is the product; this module only marshals arguments.  It
+refuses to run without the library: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libswsgpu.so")
+
+FMT_MARK5B, FMT_VDIF = 0, 1
+WIN = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
+       "blackmanharris": 6}
+PREC_FP32, PREC_TCSPLIT = 0, 1
+MAX_SOURCES = 64
+MAX_STREAMS = 2
+
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ETIMEOUT", -4: "ENODEV", -5: "ESTATE"}
+
+
+class Layout(C.Structure):
+    _fields_ = [("format", C.c_int), ("nchan", C.c_int), ("nbit", C.c_int),
+                ("frame_bytes", C.c_int), ("header_bytes", C.c_int)]
+
+
+class Config(C.Structure):
+    _fields_ = [("layout", Layout * MAX_STREAMS), ("num_streams", C.c_int),
+                ("fft_points", C.c_int), ("overlap", C.c_int), ("window", C.c_int),
+                ("precision", C.c_int), ("core_overlapped_ffts", C.c_int),
+                ("num_sources", C.c_int), ("source_stream", C.c_int * MAX_SOURCES),
+                ("source_channel", C.c_int * MAX_SOURCES), ("num_xpols", C.c_int),
+                ("xpol_pair", (C.c_int * 2) * MAX_SOURCES), ("extract_pcal", C.c_int),
+                ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
+                ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
+                ("max_run_bytes", C.c_size_t)]
+
+
+class Outputs(C.Structure):
+    _fields_ = [("auto_out", C.c_void_p), ("xpol_out", C.c_void_p), ("pcal_out", C.c_void_p)]
+
+
+class SwsError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load libswsgpu.so; raises if it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SwsError(f"{LIB_PATH} is not built; run swspec_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        L.swsgpu_create.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(C.c_void_p)]
+        L.swsgpu_destroy.argtypes = [C.c_void_p]
+        L.swsgpu_last_error.argtypes = [C.c_void_p]
+        L.swsgpu_last_error.restype = C.c_char_p
+        L.swsgpu_run_shape.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.swsgpu_submit.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_int64)]
+        L.swsgpu_wait.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.swsgpu_fetch.argtypes = [C.c_void_p, C.POINTER(Outputs)]
+        L.swsgpu_process_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
+                                            C.c_int, C.POINTER(Outputs), C.c_void_p]
+        L.swsgpu_workspace_size.argtypes = [C.c_void_p, C.c_size_t, C.c_int,
+                                            C.POINTER(C.c_size_t)]
+        L.swsgpu_unpack_device.argtypes = [C.POINTER(Layout), C.c_void_p, C.c_size_t, C.c_int64,
+                                           C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_int64),
+                                           C.c_void_p]
+        L.swsgpu_last_launch_count.argtypes = [C.c_void_p]
+        L.swsgpu_device_ok.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, h=None) -> None:
+    if rc != 0:
+        msg = lib().swsgpu_last_error(h).decode()
+        raise SwsError(f"{ERRORS.get(rc, rc)}: {msg}")
+
+
+def layout(fmt: str, nchan: int, nbit: int, framed: bool = True) -> Layout:
+    """Layout of a Mark5B or VDIF stream ("mark5b" / "vdif:<payload>")."""
+    if fmt.lower().startswith("mark5b"):
+        return Layout(FMT_MARK5B, nchan, nbit, 10016 if framed else 10000, 16 if framed else 0)
+    payload = int(fmt.split(":")[1]) if ":" in fmt else 8000
+    return Layout(FMT_VDIF, nchan, nbit, payload + (32 if framed else 0), 32 if framed else 0)
+
+
+def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_ffts=1,
+                sources=((0, 0),), xpols=(), precision=PREC_FP32, max_run_bytes=1 << 24,
+                extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
+                pcal_offset_hz=10e3, layout2: Layout | None = None) -> Config:
+    c = Config()
+    c.layout[0] = lay
+    c.layout[1] = layout2 if layout2 is not None else lay
+    c.num_streams = 1 + max(s for s, _ in sources)
+    c.fft_points = N
+    c.overlap = overlap
+    c.window = WIN[window] if isinstance(window, str) else int(window)
+    c.precision = precision
+    c.core_overlapped_ffts = core_overlapped_ffts
+    c.num_sources = len(sources)
+    for i, (st, ch) in enumerate(sources):
+        c.source_stream[i] = st
+        c.source_channel[i] = ch
+    c.num_xpols = len(xpols)
+    for i, (a, b) in enumerate(xpols):
+        c.xpol_pair[i][0] = a
+        c.xpol_pair[i][1] = b
+    c.extract_pcal = int(bool(extract_pcal))
+    c.pcal_tonebins = pcal_tonebins
+    c.pcal_rotatorlen = pcal_rotatorlen
+    c.samplingfreq = samplingfreq
+    c.pcal_offset_hz = pcal_offset_hz
+    c.max_run_bytes = max_run_bytes
+    return c
+
+
+class Core:
+    """One GPU spectrometer core (a TaskCore's compute half)."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        _check(lib().swsgpu_create(C.byref(cfg), device, C.byref(self.h)))
+        self.S = cfg.fft_points // 2 + 1
+
+    def close(self):
+        if self.h:
+            lib().swsgpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_shape(self, nbytes: int):
+        ns, nf, part = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().swsgpu_run_shape(self.h, nbytes, C.byref(ns), C.byref(nf), C.byref(part)),
+               self.h)
+        return ns.value, nf.value, bool(part.value)
+
+    def last_launches(self) -> int:
+        return lib().swsgpu_last_launch_count(self.h)
+
+    def run(self, raws: list, payload_offsets=None, timeout_ms: int = 60000):
+        """One core run from host bytes (submit + wait + fetch)."""
+        n = len(raws)
+        arrs = [np.frombuffer(r, dtype=np.uint8) if not isinstance(r, np.ndarray) else r
+                for r in raws]
+        ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+        sizes = (C.c_size_t * n)(*[a.nbytes for a in arrs])
+        offs = (C.c_int64 * n)(*(payload_offsets or [0] * n))
+        _check(lib().swsgpu_submit(self.h, ptrs, sizes, offs), self.h)
+        ns = C.c_int()
+        _check(lib().swsgpu_wait(self.h, timeout_ms, C.byref(ns)), self.h)
+        nspec = ns.value
+        c = self.cfg
+        auto = np.zeros((nspec, c.num_sources, self.S), dtype=np.float32)
+        xpol = np.zeros((nspec, max(c.num_xpols, 1), self.S, 2), dtype=np.float32)
+        pcal = np.zeros((nspec, c.num_sources, max(c.pcal_tonebins, 1), 2), dtype=np.float32)
+        out = Outputs(auto.ctypes.data, xpol.ctypes.data, pcal.ctypes.data)
+        _check(lib().swsgpu_fetch(self.h, C.byref(out)), self.h)
+        xp = xpol[:, : c.num_xpols, :, 0] + 1j * xpol[:, : c.num_xpols, :, 1]
+        pc = pcal[:, :, : c.pcal_tonebins, 0] + 1j * pcal[:, :, : c.pcal_tonebins, 1]
+        return auto, xp, pc, nspec
+
+    def process_device(self, d_raw_ptrs: list[int], run_bytes: int, nruns: int,
+                       runs_per_output: int, d_auto: int, d_xpol: int = 0, d_pcal: int = 0,
+                       stream: int = 0) -> None:
+        n = len(d_raw_ptrs)
+        ptrs = (C.c_void_p * n)(*d_raw_ptrs)
+        out = Outputs(d_auto, d_xpol or None, d_pcal or None)
+        _check(lib().swsgpu_process_device(self.h, ptrs, run_bytes, nruns, runs_per_output,
+                                           C.byref(out), C.c_void_p(stream or None)), self.h)
+
+
+def unpack_device(lay: Layout, d_raw: int, nbytes: int, payload_offset: int, chan: int,
+                  nsamp: int, d_out: int, stream: int = 0) -> int:
+    nv = C.c_int64()
+    rc = lib().swsgpu_unpack_device(C.byref(lay), d_raw, nbytes, payload_offset, chan, nsamp,
+                                    d_out, C.byref(nv), C.c_void_p(stream or None))
+    _check(rc)
+    return nv.value

@@ -1,0 +1,149 @@
+"""GPU parity: spectra of the CUDA core vs the FP64 oracle (restated doMaths).
+
+Each case runs one core run (one raw buffer per stream) through the C ABI
+(swsgpu_submit / wait / fetch) and compares every auto spectrum, cross
+spectrum and phase-cal vector with the FP64 restatement of
+TaskCoreIPP::doMaths on the same decoded samples.
+"""
+import numpy as np
+import pytest
+
+from helpers import REL_TOL, decode_channels, oracle_run, rel_err_auto, rel_err_xpol
+from swspec_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _mark5b_noise(nchan, nbit, nframes_m5b, seed, mbps=1024):
+    spf = synth.mark5b_samples_per_frame(nchan, nbit)
+    T = spf * nframes_m5b
+    rng = np.random.default_rng(seed)
+    sig = rng.standard_normal((nchan, T))
+    return synth.mark5b_stream(sig, nbit, mbps), T
+
+
+def test_c1_like_auto_single_channel(gpu):
+    """16 ch x 2 bit Mark5B, channel 1 only, N=32768 Hann, 16 FFTs per spectrum
+    (the default buffer plan's core run), tone at +3.1 MHz."""
+    N, cof = 32768, 16
+    data, info = synth.c1_stream(0, frames=int(np.ceil(N * cof / 2500)) + 1, N=N)
+    lay = gpu.layout("mark5b", 16, 2)
+    run_bytes_payload = N * cof * 4
+    nfr = run_bytes_payload // 10000 + 1
+    raw = data[: nfr * 10016]
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 0),), max_run_bytes=len(raw))
+    core = gpu.Core(cfg)
+    auto, _, _, ns = core.run([raw])
+    samples = decode_channels(raw, info["fmt"], 16, 2, [0], nfr * 2500)
+    ref, _, _, nref = oracle_run(samples, N, "hann", 1, cof)
+    assert ns == nref == 1
+    err = rel_err_auto(auto, ref)
+    assert err < REL_TOL, err
+
+
+def test_c3_like_dual_pol_cross(gpu):
+    """Mark5B-2048-16-2, 8 subband pairs (c, c+8), N=65536, XX/YY/XY*."""
+    N, cof, nfft = 65536, 16, 16
+    data, info = synth.c3_stream(nfft, N=N)
+    lay = gpu.layout("mark5b", 16, 2)
+    pairs = [(c, c + 8) for c in range(8)]
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=tuple((0, c) for c in range(16)),
+                          xpols=pairs, max_run_bytes=len(data), samplingfreq=64e6)
+    core = gpu.Core(cfg)
+    nsamp = info["nsamp"]
+    auto, xp, _, ns = core.run([data])
+    assert ns == 1
+    samples = decode_channels(data, info["fmt"], 16, 2, range(16), nsamp)
+    worst = 0.0
+    for k, (i, j) in enumerate(pairs):
+        ra, rx, _, n = oracle_run([samples[i], samples[j]], N, "hann", 1, cof, nxpols=1)
+        assert n == 1
+        worst = max(worst, rel_err_auto(auto[:, i], ra[:, 0]), rel_err_auto(auto[:, j], ra[:, 1]),
+                    rel_err_xpol(xp[:, k], rx[:, 0], ra[:, 0], ra[:, 1]))
+    assert worst < REL_TOL, worst
+    # the synthesised cross-correlation is rho = 0.3 at 0.7 rad
+    rho = np.mean(xp[0, 0, 100:-100] / np.sqrt(auto[0, 0, 100:-100] * auto[0, 8, 100:-100]))
+    assert abs(abs(rho) - 0.3) < 0.03 and abs(abs(np.angle(rho)) - 0.7) < 0.1
+
+
+@pytest.mark.parametrize("overlap,cof", [(2, 7), (1, 5), (4, 9)])
+def test_two_files_overlap_partial(gpu, overlap, cof):
+    """Two input files (streams), channel 3 of each, cross-pol, overlapped FFTs,
+    spectrum hop and a trailing unscaled partial spectrum."""
+    N = 4096
+    d1, T = _mark5b_noise(8, 2, 12, 11)
+    d2, _ = _mark5b_noise(8, 2, 12, 12)
+    lay = gpu.layout("mark5b", 8, 2)
+    cfg = gpu.make_config(lay, N, "cosine2", overlap, cof, sources=((0, 2), (1, 2)),
+                          xpols=((0, 1),), max_run_bytes=len(d1))
+    core = gpu.Core(cfg)
+    auto, xp, _, ns = core.run([d1, d2])
+    s1 = decode_channels(d1, "Mark5B-1024-8-2", 8, 2, [2], T)[0]
+    s2 = decode_channels(d2, "Mark5B-1024-8-2", 8, 2, [2], T)[0]
+    ra, rx, _, nref = oracle_run([s1, s2], N, "cosine2", overlap, cof, nxpols=1)
+    assert ns == nref and ns >= 2
+    assert rel_err_auto(auto, ra) < REL_TOL
+    assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
+
+
+@pytest.mark.parametrize("nbit,nchan,window", [(1, 16, "none"), (1, 32, "cosine"),
+                                               (2, 4, "hamming"), (2, 1, "blackman")])
+def test_bit_depths_and_windows(gpu, nbit, nchan, window):
+    N, cof = 8192, 4
+    d, T = _mark5b_noise(nchan, nbit, 16 if nchan * nbit >= 8 else 4, 21 + nbit + nchan,
+                         mbps=1024 if nchan * nbit >= 8 else 256)
+    lay = gpu.layout("mark5b", nchan, nbit)
+    ch = nchan - 1
+    cfg = gpu.make_config(lay, N, window, 1, cof, sources=((0, ch),), max_run_bytes=len(d))
+    core = gpu.Core(cfg)
+    auto, _, _, ns = core.run([d])
+    fmt = f"Mark5B-{1024 if nchan * nbit >= 8 else 256}-{nchan}-{nbit}"
+    s = decode_channels(d, fmt, nchan, nbit, [ch], T)
+    ra, _, _, nref = oracle_run(s, N, window, 1, cof)
+    assert ns == nref
+    assert rel_err_auto(auto, ra) < REL_TOL
+
+
+def test_vdif_8bit_blackmanharris(gpu):
+    """VDIF 8-bit single channel (dynamic-range configuration's format)."""
+    N, cof = 20000, 3
+    spf = 8000
+    rng = np.random.default_rng(1005)
+    x = rng.standard_normal(spf * 9)
+    codes = synth.quantize_vdif_8bit(x, 24.0)
+    payload = synth.pack_codes(codes[None, :], 8)
+    data = synth.vdif_frames(payload, 8000, 1, 8, 8000)
+    lay = gpu.layout("vdif:8000", 1, 8)
+    cfg = gpu.make_config(lay, N, "blackmanharris", 1, cof, max_run_bytes=len(data))
+    core = gpu.Core(cfg)
+    auto, _, _, ns = core.run([data])
+    s = decode_channels(data, "VDIF_8000-512-1-8", 1, 8, [0], spf * 9)
+    ra, _, _, nref = oracle_run(s, N, "blackmanharris", 1, cof)
+    assert ns == nref
+    assert rel_err_auto(auto, ra) < REL_TOL
+
+
+def test_pcal_fold(gpu):
+    """Phase-cal folding (offset 15625 Hz at 32 Msps: rotator period 2048,
+    32 tone bins) on every FFT, comb amplitude 5% of sigma."""
+    N, cof, fs, off = 32768, 4, 32e6, 15625.0
+    spf = 2500
+    nfr = N * cof // spf + 2
+    T = nfr * spf
+    rng = np.random.default_rng(7)
+    comb = synth.pcal_comb(T, fs, 1e6, off, 0.05, rng.uniform(0, 2 * np.pi, 16))
+    sig = rng.standard_normal((16, T)) + comb[None, :]
+    data = synth.mark5b_stream(sig, 2, 1024)
+    lay = gpu.layout("mark5b", 16, 2)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 4),), max_run_bytes=len(data),
+                          extract_pcal=True, pcal_tonebins=32, pcal_rotatorlen=2048,
+                          samplingfreq=fs, pcal_offset_hz=off)
+    core = gpu.Core(cfg)
+    auto, _, pc, ns = core.run([data])
+    s = decode_channels(data, "Mark5B-1024-16-2", 16, 2, [4], T)
+    ra, _, rp, nref = oracle_run(s, N, "hann", 1, cof,
+                                 pcal=dict(tonebins=32, rotatorlen=2048, fs=fs, offset=off))
+    assert ns == nref
+    assert rel_err_auto(auto, ra) < REL_TOL
+    scale = np.max(np.abs(rp))
+    assert np.max(np.abs(pc - rp)) / scale < 1e-6

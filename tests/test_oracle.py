@@ -1,0 +1,164 @@
+"""CPU: the oracle pinned against the reference's own code and known answers.
+
+* decode restatement == mark5access (golden fixtures made from the reference's
+  mark5access, and the live oracle/_ref build when present);
+* windows == the formulas written in the reference (Cosine, Cosine2:
+  TaskCoreIPP.cpp:576-586; Hann: TaskCoreMKL.cpp:53 / TaskCoreFFTW.cpp:65);
+* FFT == numpy float64 and a naive long-double DFT;
+* doMaths loop == a numpy restatement; frame schedule and scaling rules;
+* PCal known answer of src/IA-32/PhaseCal/PCal.cpp:904-948 (tone phases
+  -90 + 5*t degrees within 0.1 degree).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from swspec_b200 import synth
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_decode_matches_golden_mark5b():
+    z = np.load(os.path.join(GOLDEN, "mark5b_decode.npz"))
+    raw = z["raw"].tobytes()
+    pay = synth.strip_headers(raw, 10016, 16)
+    nsamp = int(z["nsamp"])
+    for c in range(16):
+        mine = O.decode(O.FMT_MARK5B, 16, 2, pay, nsamp, c)
+        ref = z["decoded"][c]
+        # the restatement has no blanking; compare outside the fill zone of frame 1
+        ok = ref != 0
+        assert np.array_equal(mine[ok].view(np.uint32), ref[ok].view(np.uint32))
+        # blanked: payload bytes 6000..10000 of frame 1 -> sample-times 1500..2500
+        assert np.all(ref[2500 + 1500: 2500 + 2500] == 0)
+        assert np.count_nonzero(ref[2500: 2500 + 1500] == 0) == 0
+
+
+def test_decode_matches_golden_vdif():
+    z = np.load(os.path.join(GOLDEN, "vdif_decode.npz"))
+    pay = synth.strip_headers(z["raw"].tobytes(), 8032, 32)
+    mine = O.decode(O.FMT_VDIF, 1, 8, pay, int(z["nsamp"]), 0)
+    ref = z["decoded"][0]
+    assert np.all(ref[8000:16000] == 0)  # invalid frame blanked by mark5access
+    keep = np.r_[0:8000, 16000:24000]
+    assert np.array_equal(mine[keep].view(np.uint32), ref[keep].view(np.uint32))
+
+
+def test_decode_matches_test_unpacker_pattern():
+    z = np.load(os.path.join(GOLDEN, "unpacker_pattern.npz"))
+    pat = z["pattern"].tobytes()
+    for c in range(16):
+        assert np.array_equal(O.decode(O.FMT_MARK5B, 16, 2, pat, 2500, c), z["m5b_16ch"][c])
+    for c in range(8):
+        assert np.array_equal(O.decode(O.FMT_MARK5B, 8, 2, pat, 5000, c), z["m5b_8ch"][c])
+
+
+@pytest.mark.skipif(O.ref() is None, reason="oracle/_ref not built")
+@pytest.mark.parametrize("nchan,nbit,mbps", [(16, 2, 1024), (32, 1, 1024), (2, 2, 256),
+                                             (8, 1, 1024)])
+def test_decode_matches_live_mark5access(nchan, nbit, mbps):
+    spf = synth.mark5b_samples_per_frame(nchan, nbit)
+    rng = np.random.default_rng(nchan * 10 + nbit)
+    raw = synth.mark5b_stream(rng.standard_normal((nchan, spf * 3)), nbit, mbps)
+    ref, _ = O.m5_decode(f"Mark5B-{mbps}-{nchan}-{nbit}", raw, spf * 2)
+    pay = synth.strip_headers(raw, 10016, 16)
+    for c in range(nchan):
+        assert np.array_equal(O.decode(O.FMT_MARK5B, nchan, nbit, pay, spf * 2, c), ref[c])
+
+
+def test_windows_pinned_formulas():
+    n = 1000
+    i = np.arange(n, dtype=np.float64)
+    c = np.cos(np.pi * (i - 0.5 * n + 0.5) / n)
+    assert np.array_equal(O.window(O.W_COSINE2, n), (c * c).astype(np.float32))
+    assert np.array_equal(O.window(O.W_COSINE, n), c.astype(np.float32))
+    s = np.sin(np.pi * i / (n - 1))
+    assert np.allclose(O.window(O.W_HANN, n), (s * s).astype(np.float32), atol=6e-8)
+    assert np.all(O.window(O.W_NONE, n) == 1)
+
+
+@pytest.mark.parametrize("n", [8, 30, 125, 4096, 20000])
+def test_fft64_vs_numpy(n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    r = O.fft64(x)
+    assert np.max(np.abs(r - np.fft.fft(x))) / np.max(np.abs(r)) < 1e-13
+
+
+def test_fft64_vs_longdouble_dft():
+    n = 60
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    k = np.arange(n, dtype=np.longdouble)
+    ang = -2 * np.pi * np.outer(k, k) / n
+    ref = (np.cos(ang) * x.real - np.sin(ang) * x.imag) + 1j * (np.sin(ang) * x.real + np.cos(ang) * x.imag)
+    ref = ref.sum(axis=1)
+    assert np.max(np.abs(O.fft64(x) - ref.astype(np.complex128))) < 1e-12
+
+
+@pytest.mark.parametrize("overlap,cof,nfr", [(1, 4, 9), (2, 7, 9), (3, 4, 5)])
+def test_domaths_vs_numpy(overlap, cof, nfr):
+    N = 1024
+    rng = np.random.default_rng(overlap * 100 + cof)
+    s = [rng.standard_normal(N * nfr).astype(np.float32) for _ in range(2)]
+    cfg = O.make_cfg(N, overlap=overlap, core_overlapped_ffts=cof, num_sources=2, num_xpols=1,
+                     window=O.W_HANN)
+    a, xp, _, ns = O.domaths(cfg, s)
+    starts, spec, ns2, part = O.schedule(cfg, N * nfr)
+    assert ns == ns2
+    w = O.window(O.W_HANN, N).astype(np.float64)
+    ra = np.zeros((ns, 2, N // 2 + 1))
+    rx = np.zeros((ns, N // 2 + 1), complex)
+    for st, sp in zip(starts, spec):
+        X = [np.fft.rfft(s[i][st:st + N].astype(np.float64) * w) for i in range(2)]
+        for i in range(2):
+            ra[sp, i] += np.abs(X[i]) ** 2
+        rx[sp] += X[0] * np.conj(X[1])
+    full = ns - part
+    ra[:full] /= cof
+    rx[:full] /= cof
+    assert np.allclose(a, ra, rtol=1e-12)
+    assert np.allclose(xp[:, 0], rx, rtol=1e-12, atol=1e-9)
+
+
+def test_schedule_spectrum_hop():
+    """After core_overlapped_ffts FFTs the source pointer hops by
+    raw_fullfft - raw_overlap (TaskCoreIPP.cpp:506-511)."""
+    cfg = O.make_cfg(1000, overlap=2, core_overlapped_ffts=3)
+    starts, spec, ns, part = O.schedule(cfg, 4000)
+    assert list(starts) == [0, 500, 1000, 2000, 2500, 3000]
+    assert list(spec) == [0, 0, 0, 1, 1, 1] and ns == 2 and not part
+
+
+def test_fp32_baseline_close_to_fp64():
+    N = 4096
+    rng = np.random.default_rng(9)
+    s = [rng.standard_normal(N * 6).astype(np.float32)]
+    cfg = O.make_cfg(N, core_overlapped_ffts=6, nthreads=3)
+    a64, _, _, _ = O.domaths(cfg, s)
+    a32, _, _, _ = O.domaths(cfg, s, fp64=False)
+    assert np.max(np.abs(a32 - a64) / a64) < 1e-4
+
+
+def test_pcal_known_answer():
+    """PCal.cpp:861-951: tones sin(pi (n + off)(f_off + t*spacing)/BW + t*5deg)
+    extracted with phase -90 + 5*t degrees, within 0.1 degree."""
+    bw, fs = 16e6, 32e6
+    spacing, off = 1e6, 10e3
+    tonebins, rotatorlen = int(fs / spacing), int(fs / np.gcd(int(fs), int(off)))
+    ntones = int(bw / spacing)
+    N = rotatorlen * 20
+    n = np.arange(N, dtype=np.float64)
+    x = np.zeros(N)
+    for t in range(ntones):
+        x += np.sin(np.pi * n * (off + t * spacing) / bw + np.deg2rad(5.0 * t))
+    cfg = O.make_cfg(N, core_overlapped_ffts=1, extract_pcal=True, pcal_tonebins=tonebins,
+                     pcal_rotatorlen=rotatorlen, samplingfreq=fs, pcaloffsethz=off)
+    _, _, pc, _ = O.domaths(cfg, [x.astype(np.float32)])
+    tones = O.pcal_tones(pc[0, 0], N, ntones)
+    ph = np.rad2deg(np.angle(tones))
+    want = -90.0 + 5.0 * np.arange(ntones)
+    d = (ph - want + 180) % 360 - 180
+    assert np.max(np.abs(d)) < 0.1, d
