@@ -1,0 +1,453 @@
+"""Benchmark: input Gsamples/s of unpack -> window -> FFT -> integrate.
+
+Workload (dual-polarisation cross-spectra): one Mark5B-2048-16-2 stream,
+2 polarisations x 8 subbands of 32 MHz (64 Msps, 2-bit), X/Y correlated
+Gaussian noise (rho = 0.3, 0.7 rad), real FFT N = 65536, Hann window, no
+overlap, XX / YY / XY* for the 8 pairs integrated over 1 s (976 FFTs) with
+the reference's default 32 MiB buffer plan: 4 MiB core runs of 16 FFTs,
+61 runs combined per spectrum.  One step = one integration = 1.02e9 input
+samples (16 channels x 976 x 65536); inputs are synthetic (seeded) and 256 MB
+per step, larger than L2, so consecutive steps re-read HBM.
+
+Lines printed (rank 0, one JSON line):
+  value : device-resident input, the C ABI's process_device path, CUDA
+          events on the launching stream, max over ranks.
+  e2e   : the TaskCore path with host buffers: per 4 MiB run swsgpu_submit
+          (H2D inside) + swsgpu_wait, device-side combining of the 61 runs,
+          one fetch (D2H) per spectrum.
+  roofline of the dominant kernel (FFT + accumulate) from its event-timed
+  launches; cpu_baseline from the FP32 CPU restatement on host cores.
+
+--impl reference times the reference's CPU core restatement (FP32, all host
+threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 65536
+NCHAN = 16
+NPAIRS = 8
+FS = 64e6
+RUN_BYTES = 4 * 1024 * 1024           # default plan's raw buffer (payload bytes)
+RUNS_PER_SPECTRUM = 61
+CORE_FFTS = 16
+FFTS_PER_STEP = RUNS_PER_SPECTRUM * CORE_FFTS          # 976
+SAMPLES_PER_STEP = FFTS_PER_STEP * N * NCHAN
+CONFIG = {"workload": "dual-pol cross-spectra: Mark5B-2048-16-2, 8 subband pairs, "
+                      "N=65536 Hann, XX/YY/XY* over 1 s (976 FFTs), 32 MiB buffer plan",
+          "fft_points": N, "channels": NCHAN, "pairs": NPAIRS, "bits": 2, "sample_rate": FS,
+          "integration_s": 1.0, "ffts_per_spectrum": FFTS_PER_STEP,
+          "run_bytes": RUN_BYTES, "runs_per_spectrum": RUNS_PER_SPECTRUM,
+          "l2": "inputs larger than L2 (256 MB per step)"}
+METRIC = "input Gsamples/s unpack->FFT->integrate"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        time.sleep(0.15)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# helpers
+# ----------------------------------------------------------------------------
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback"}
+
+
+def fp32_peak(device: int) -> float | None:
+    try:
+        L = C.CDLL(os.path.join(ROOT, "swspec_b200", "libswsprobe.so"))
+        v = C.c_double()
+        if L.sws_probe_fp32_tflops(device, C.byref(v)) == 0:
+            return v.value
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(seconds_budget: float = 12.0) -> dict:
+    """FP32 CPU restatement of the IPP core (oracle port) on host cores:
+    whole core runs (16 FFTs x 16 channels, 8 cross pairs) until the budget."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(5)
+    lv = np.array([-3.3359, -1.0, 1.0, 3.3359], dtype=np.float32)
+    nsamp = CORE_FFTS * N
+    chans = [lv[rng.integers(0, 4, nsamp)] for _ in range(NCHAN)]
+    cfg = O.make_cfg(N, core_overlapped_ffts=CORE_FFTS, num_sources=2, num_xpols=1,
+                     window=O.W_HANN, nthreads=cores)
+    runs = 0
+    t0 = time.perf_counter()
+    while True:
+        for p in range(NPAIRS):
+            O.domaths(cfg, [chans[p], chans[p + NPAIRS]], fp64=False)
+        runs += 1
+        if time.perf_counter() - t0 > seconds_budget:
+            break
+    dt = time.perf_counter() - t0
+    samples = runs * CORE_FFTS * N * NCHAN
+    return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "port",
+            "sample": f"{runs} core runs of the workload (16 FFTs x 16 channels each, "
+                      f"{samples / 1e6:.0f} Msamples), FP32 restatement of TaskCoreIPP::doMaths",
+            "seconds": dt}
+
+
+def reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    # each step: one bounded sample of the workload (about 3 s of CPU work)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(seconds_budget=3.0)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = sum(vals) / len(vals)
+    line = {"metric": METRIC, "value": v, "unit": "Gsamples/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": SAMPLES_PER_STEP / (v * 1e9) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": CONFIG,
+            "cpu_baseline": {"value": v, "unit": "Gsamples/s", "cores": cores, "kind": "port",
+                             "sample": "per step ~3 s of core runs (16 FFTs x 16 channels), "
+                                       "FP32 C restatement of TaskCoreIPP::doMaths, all host threads"},
+            "e2e": {"value": v, "unit": "Gsamples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def parity_check(gpu, synth, O, raw_host: bytes, precision: int) -> dict:
+    """Max relative errors of one full integration (976 FFTs) of pair 0 vs
+    the FP64 oracle, through the TaskCore path (61 submits)."""
+    import numpy as np
+    lay = gpu.layout("mark5b", NCHAN, 2, framed=False)
+    cfg = gpu.make_config(lay, N, "hann", 1, CORE_FFTS, sources=((0, 0), (0, NPAIRS)),
+                          xpols=((0, 1),), precision=precision, max_run_bytes=RUN_BYTES,
+                          samplingfreq=FS, runs_per_output=RUNS_PER_SPECTRUM)
+    core = gpu.Core(cfg)
+    core.set_sizes([RUN_BYTES])
+    pay = np.frombuffer(raw_host, dtype=np.uint8)
+    for r in range(RUNS_PER_SPECTRUM):
+        core.submit([pay[r * RUN_BYTES:(r + 1) * RUN_BYTES]], payload_offsets=[r * RUN_BYTES])
+        ns = core.wait()
+    S = N // 2 + 1
+    auto = np.zeros((1, 2, S), np.float32)
+    xp = np.zeros((1, 1, S, 2), np.float32)
+    core.fetch_into(auto, xp)
+    core.close()
+    nsamp = RUNS_PER_SPECTRUM * RUN_BYTES // 4
+    s = [O.decode(O.FMT_MARK5B, NCHAN, 2, raw_host, nsamp, c) for c in (0, NPAIRS)]
+    ra = np.zeros((2, S))
+    rx = np.zeros(S, complex)
+    for r in range(RUNS_PER_SPECTRUM):
+        cfgo = O.make_cfg(N, core_overlapped_ffts=CORE_FFTS, num_sources=2, num_xpols=1,
+                          window=O.W_HANN)
+        a, x, _, n = O.domaths(cfgo, [v[r * CORE_FFTS * N:(r + 1) * CORE_FFTS * N] for v in s])
+        ra += a[0]
+        rx += x[0, 0]
+    xc = xp[0, 0, :, 0] + 1j * xp[0, 0, :, 1]
+    e_auto = float(np.max(np.abs(auto[0] - ra) / ra))
+    e_xpol = float(np.max(np.abs(xc - rx) / np.sqrt(ra[0] * ra[1])))
+    e_rms = float(np.sqrt(np.mean(((auto[0] - ra) / ra) ** 2)))
+    return {"max_rel_err_auto": e_auto, "max_rel_err_xpol": e_xpol, "rms_rel_err_auto": e_rms,
+            "bar": 2e-6, "pair": "subband 0 (channels 1 and 9), one full 1 s integration",
+            "spectra_checked": int(ns)}
+
+
+def gpu_arm(args) -> None:
+    import numpy as np
+    import torch
+
+    from swspec_b200 import gpu, synth, synth_gpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    precisions = [gpu.PREC_FP32]
+    if args.precision in ("tcsplit", "auto") and tc_available(gpu):
+        precisions = [gpu.PREC_TCSPLIT, gpu.PREC_FP32]
+    headline = precisions[0]
+
+    # ---- input: one integration of framed Mark5B on the device ----
+    payload_needed = RUNS_PER_SPECTRUM * RUN_BYTES
+    d_raw, nfr = synth_gpu.c3_framed(payload_needed // 4 + 2500, N=N, npairs=NPAIRS,
+                                     seed=1003 + rank)
+    torch.cuda.synchronize()
+    S = N // 2 + 1
+    d_auto = torch.zeros(NCHAN, S, dtype=torch.float32, device="cuda")
+    d_xpol = torch.zeros(NPAIRS, S, 2, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    lay = gpu.layout("mark5b", NCHAN, 2)
+    sources = tuple((0, c) for c in range(NCHAN))
+    pairs = tuple((c, c + NPAIRS) for c in range(NPAIRS))
+
+    def make_core(prec, framed=True, rpo=1):
+        cfg = gpu.make_config(lay if framed else gpu.layout("mark5b", NCHAN, 2, framed=False), N,
+                              "hann", 1, CORE_FFTS, sources=sources, xpols=pairs, precision=prec,
+                              max_run_bytes=RUN_BYTES, samplingfreq=FS, runs_per_output=rpo)
+        return gpu.Core(cfg, device=local)
+
+    def step(core):
+        core.process_device([d_raw.data_ptr()], RUN_BYTES, RUNS_PER_SPECTRUM, RUNS_PER_SPECTRUM,
+                            d_auto.data_ptr(), d_xpol.data_ptr(), 0, stream.cuda_stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    forms = {}
+    launches_per_step = 0
+    clocks = None
+    for prec in precisions:
+        name = "tcsplit" if prec == gpu.PREC_TCSPLIT else "fp32"
+        core = make_core(prec)
+        for _ in range(args.warmup):
+            step(core)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as cs:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step(core)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        ms = max_over_ranks(ms)
+        launches_per_step = core.last_launches()
+        # dominant kernel timing (separate pass, events around each launch)
+        core.profile(True)
+        for _ in range(max(2, min(args.steps, 5))):
+            step(core)
+        nk, kms = core.profile_read()
+        core.profile(False)
+        core.close()
+        value = SAMPLES_PER_STEP * args.steps * world / (ms * 1e-3) / 1e9
+        forms[name] = {"value": value, "ms_per_step": ms / args.steps,
+                       "kernel_ms_per_launch": kms / max(nk, 1), "kernel_launches": nk,
+                       "launches_per_step": launches_per_step, "clocks": cs.summary()}
+        if prec == headline:
+            clocks = cs.summary()
+        log(f"[{name}] {value:.3f} Gsamples/s, {ms / args.steps:.3f} ms/step, "
+            f"FFT kernel {kms / max(nk, 1):.3f} ms/launch")
+
+    # ---- e2e: TaskCore path, host buffers, per-run submit/wait ----
+    pay_dev = d_raw.view(nfr, 10016)[:, 16:].reshape(-1)[:payload_needed]
+    host = torch.empty(payload_needed, dtype=torch.uint8, pin_memory=True)
+    host.copy_(pay_dev)
+    torch.cuda.synchronize()
+    core = make_core(headline, framed=False, rpo=RUNS_PER_SPECTRUM)
+    core.set_sizes([RUN_BYTES])
+    auto_h = np.zeros((1, NCHAN, S), np.float32)
+    xpol_h = np.zeros((1, NPAIRS, S, 2), np.float32)
+    base = host.data_ptr()
+
+    def e2e_step():
+        for r in range(RUNS_PER_SPECTRUM):
+            core.submit([base + r * RUN_BYTES], payload_offsets=[r * RUN_BYTES])
+            core.wait()
+        core.fetch_into(auto_h, xpol_h)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    core.close()
+    e2e_val = SAMPLES_PER_STEP * args.steps * world / e2e_s / 1e9
+    d2h = auto_h.nbytes + xpol_h.nbytes
+    log(f"[e2e] {e2e_val:.3f} Gsamples/s")
+
+    # ---- parity of the headline form on this workload ----
+    parity = None
+    if rank == 0 and not args.no_parity:
+        import oracle as O
+        parity = parity_check(gpu, synth, O, host.numpy().tobytes(), headline)
+        log(f"[parity] {parity}")
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    hl = forms["tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32"]
+    peaks = measured_peaks()
+    # roofline of the dominant kernel: 5 N log2 N flops per channel-FFT
+    flops_per_launch = 5.0 * N * math.log2(N) * NCHAN * FFTS_PER_STEP
+    bytes_per_launch = (SAMPLES_PER_STEP * 2 / 8            # packed 2-bit input
+                        + (NCHAN + 2 * NPAIRS) * 4 * (N // 2 + 1))  # spectra written
+    kern_s = hl["kernel_ms_per_launch"] * 1e-3
+    p32 = fp32_peak(local)
+    if headline == gpu.PREC_TCSPLIT:
+        achieved = flops_per_launch / kern_s / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                "peak_source": f"bf16 dense burst, {peaks['source']}"}
+    else:
+        achieved = bytes_per_launch / kern_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_source": f"HBM copy, {peaks['source']}"}
+    roof["traffic"] = None
+    roof["kernel"] = "k_spectra (cluster FFT + accumulate)"
+    roof["compute"] = {"achieved_tflops": flops_per_launch / kern_s / 1e12,
+                       "fp32_peak_tflops": p32,
+                       "frac_fp32": (flops_per_launch / kern_s / 1e12 / p32) if p32 else None,
+                       "flops_per_launch": flops_per_launch,
+                       "convention": "5 N log2 N per channel FFT"}
+    roof["algorithmic_bytes_per_launch"] = bytes_per_launch
+    cpu = cpu_baseline() if (world == 1 and not args.no_cpu) else None
+    line = {"metric": METRIC, "value": hl["value"], "unit": "Gsamples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": hl["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if headline == gpu.PREC_FP32 else "f16x2-split/f32",
+            "data": "synthetic", "config": CONFIG,
+            "precision": "tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32",
+            "forms": forms, "clocks": clocks,
+            "e2e": {"value": e2e_val, "unit": "Gsamples/s",
+                    "h2d_bytes_per_step": RUNS_PER_SPECTRUM * RUN_BYTES,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "swsgpu_submit/wait per 4 MiB run (TaskCore path), device combine, "
+                            "one fetch per spectrum"},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": roof, "cpu_baseline": cpu, "parity": parity}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def tc_available(gpu) -> bool:
+    try:
+        cfg = gpu.make_config(gpu.layout("mark5b", NCHAN, 2), N, precision=gpu.PREC_TCSPLIT,
+                              max_run_bytes=1 << 20)
+        c = gpu.Core(cfg)
+        c.close()
+        return True
+    except gpu.SwsError:
+        return False
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "tcsplit"])
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -103,6 +103,13 @@ typedef struct swsgpu_config {
    double samplingfreq;             /* Hz */
    double pcal_offset_hz;           /* Hz */
    size_t max_run_bytes;            /* largest raw buffer per stream and run */
+   int runs_per_output;             /* >1: consecutive submits are summed on the device and
+                                       one combined spectrum set is returned every
+                                       runs_per_output runs -- the dispatcher's
+                                       max_buffers_per_spectrum combining
+                                       (src/TaskDispatcher.cpp:143-171,
+                                       TaskCoreIPP::combineResults :311-349); sums are
+                                       kept in FP64 between runs */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;
@@ -150,7 +157,9 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
                   const int64_t *stream_payload_offset);
 
 /* TaskCore::join: wait up to timeout_ms (<0: forever) for the queued run;
- * *nspectra gets the spectrum count (TaskCore::join's return value). */
+ * *nspectra gets the spectrum count (TaskCore::join's return value).  With
+ * runs_per_output > 1 it is 0 until the run that completes a group, whose
+ * fetch returns the combined spectra. */
 int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra);
 
 /* Copy the spectra of the completed run into caller memory. */
@@ -180,6 +189,13 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
 
 /* Number of kernel launches the last submit / process_device call issued. */
 int swsgpu_last_launch_count(const swsgpu_handle *h);
+
+/* Kernel timing on the launching stream: enable=1 starts recording CUDA
+ * events around every FFT/accumulate kernel launch (resetting the totals),
+ * enable=0 stops.  swsgpu_profile_read waits for the recorded launches and
+ * returns their count and summed duration in milliseconds. */
+int swsgpu_profile(swsgpu_handle *h, int enable);
+int swsgpu_profile_read(swsgpu_handle *h, int *launches, double *total_ms);
 
 #ifdef __cplusplus
 }

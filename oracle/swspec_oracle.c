@@ -152,15 +152,22 @@ static int orc_factor(int n, int *rad)
    return nr;
 }
 
-/* W_n^k table in FP64: angle reduced exactly via integer k < n. */
+/* W_n^k table in FP64: angle reduced exactly via integer k < n.  The last
+ * table is cached per thread (callers free only tables they own). */
+static __thread c64 *tw_cache = NULL;
+static __thread int tw_cache_n = 0;
 static c64 *orc_twiddles64(int n)
 {
+   if (tw_cache_n == n) return tw_cache;
    c64 *w = (c64 *)malloc(sizeof(c64) * (size_t)n);
    for (int k = 0; k < n; k++) {
       double a = -2.0 * M_PI * (double)k / (double)n;
       w[k].re = cos(a);
       w[k].im = sin(a);
    }
+   free(tw_cache);
+   tw_cache = w;
+   tw_cache_n = n;
    return w;
 }
 
@@ -231,7 +238,7 @@ int orc_fft64(int n, const double *in_reim, double *out_reim)
       Ns *= R;
    }
    memcpy(out_reim, d0, sizeof(c64) * (size_t)n);
-   free(w); free(d0); free(d1);
+   free(d0); free(d1);
    return 0;
 }
 

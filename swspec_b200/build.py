@@ -70,6 +70,16 @@ def build_cuda(verbose: bool = False) -> str:
     return out
 
 
+def build_probe() -> str:
+    """FP32 FMA probe used by the benchmark (not part of the C ABI)."""
+    os.makedirs(BUILD, exist_ok=True)
+    out = os.path.join(PKG, "libswsprobe.so")
+    src = os.path.join(CSRC, "probe_fp32.cu")
+    if os.path.exists(src) and _newer(out, [src]):
+        _run([NVCC] + NVFLAGS + ["-shared", "-o", out, src])
+    return out
+
+
 def build_host() -> str:
     os.makedirs(BUILD, exist_ok=True)
     out = os.path.join(PKG, "libswshost.so")
@@ -96,6 +106,7 @@ def build_oracle() -> None:
 
 def build_all() -> None:
     build_cuda()
+    build_probe()
     build_host()
     build_oracle()
 

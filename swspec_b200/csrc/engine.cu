@@ -36,6 +36,7 @@ using namespace sws;
 
 static thread_local std::string g_create_error;
 
+
 struct DevBuf {
    void *p = nullptr;
    size_t n = 0;
@@ -116,6 +117,13 @@ struct swsgpu_handle {
    DevBuf d_out_auto, d_out_xpol, d_out_pcal;
    HostBuf h_out;   // pinned staging of one run's outputs
    size_t h_auto_bytes = 0, h_xpol_bytes = 0, h_pcal_bytes = 0;
+   // combining of consecutive runs on the device (runs_per_output > 1)
+   DevBuf d_acc64;
+   int group_pos = 0;
+   bool fetch_ready = false;
+   // kernel timing
+   bool profiling = false;
+   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
 };
 
 #define CK(h, call)                                                                                \
@@ -376,12 +384,25 @@ static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int ru
 static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t *raw_bytes,
                         const long long *grid_off, size_t run_bytes, int nruns,
                         int runs_per_output, float *d_auto, float *d_xpol, float *d_pcal,
-                        cudaStream_t st, int *nspec_out)
+                        cudaStream_t st, int *nspec_out, int acc_mode = 0, int pcal_zero = 1,
+                        int pcal_write = 1)
 {
    const swsgpu_config &c = h->cfg;
    Schedule sc;
    build_schedule(h, run_bytes, nruns, runs_per_output, d_auto, d_xpol, d_pcal, sc);
    if (nspec_out) *nspec_out = sc.nspec_total;
+   if (acc_mode != 0) {
+      CK(h, h->d_acc64.ensure(sizeof(double) * (size_t)h->S * (sc.outs.size() + 1)));
+      for (size_t i = 0; i < sc.outs.size(); i++) {
+         sc.outs[i].acc = (double *)h->d_acc64.p + i * (size_t)h->S;
+         sc.outs[i].acc_mode = acc_mode;
+      }
+   } else {
+      for (auto &o : sc.outs) {
+         o.acc = nullptr;
+         o.acc_mode = 0;
+      }
+   }
    int launches = 0;
    const int S = h->S;
    const int ncode = (int)h->code_stream.size();
@@ -474,7 +495,17 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       attr[0].val.clusterDim.z = 1;
       cfgl.attrs = attr;
       cfgl.numAttrs = 1;
+      cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+      if (h->profiling) {
+         CK(h, cudaEventCreate(&ev0));
+         CK(h, cudaEventCreate(&ev1));
+         CK(h, cudaEventRecord(ev0, st));
+      }
       CK(h, cudaLaunchKernelEx(&cfgl, kern, a));
+      if (h->profiling) {
+         CK(h, cudaEventRecord(ev1, st));
+         h->prof_events.push_back(std::make_pair(ev0, ev1));
+      }
       launches++;
 
       // K3
@@ -495,8 +526,10 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    // phase cal
    if (c.extract_pcal && d_pcal) {
       const int nout = sc.nspec_total * c.num_sources;
-      CK(h, cudaMemsetAsync(d_pcal, 0, sizeof(float) * 2 * c.pcal_tonebins * (size_t)nout, st));
-      launches++;
+      if (pcal_write && sc.pcal_jobs.empty()) {
+         CK(h, cudaMemsetAsync(d_pcal, 0, sizeof(float) * 2 * c.pcal_tonebins * (size_t)nout, st));
+         launches++;
+      }
       if (!sc.pcal_jobs.empty()) {
          CK(h, h->d_pcal_part.ensure(sizeof(double) * 2 * c.pcal_tonebins * (size_t)nout));
          int njobs = (int)sc.pcal_jobs.size();
@@ -521,6 +554,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          pa.out = d_pcal;
          pa.acc = (double *)h->d_pcal_part.p;
          pa.nout = nout;
+         pa.zero_acc = pcal_zero;
+         pa.write_out = pcal_write;
          int rc = launch_pcal(pa, nbit, st);
          if (rc) return fail(h, SWSGPU_ECUDA, std::string("pcal launch: ") + cudaGetErrorString(cudaGetLastError()));
          launches += 2;
@@ -529,6 +564,15 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    CK(h, cudaGetLastError());
    h->last_launches = launches;
    return SWSGPU_OK;
+}
+
+static void drop_prof_events(swsgpu_handle *h)
+{
+   for (auto &pr : h->prof_events) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+   }
+   h->prof_events.clear();
 }
 
 // ---------------------------------------------------------------------------
@@ -584,6 +628,7 @@ static int validate_config(const swsgpu_config *c, std::string &why)
          if (c->xpol_pair[x][k] < 0 || c->xpol_pair[x][k] >= c->num_sources) { why = "xpol_pair out of range"; return 0; }
    if (c->window < 0 || c->window > SWSGPU_WIN_BLACKMANHARRIS) { why = "unknown window"; return 0; }
    if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT) { why = "unknown precision"; return 0; }
+   if (c->runs_per_output < 0) { why = "runs_per_output must be >= 0"; return 0; }
    if (c->extract_pcal) {
       if (c->pcal_tonebins < 1 || c->pcal_rotatorlen < c->pcal_tonebins || c->fft_points % c->pcal_rotatorlen) {
          why = "pcal: need tonebins >= 1, rotatorlen >= tonebins and N % rotatorlen == 0";
@@ -603,6 +648,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    Plan plan;
    if (!find_plan(cfg->fft_points, &plan))
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
+   if (cfg->precision == SWSGPU_PREC_TCSPLIT)
+      return fail(nullptr, SWSGPU_EINVAL, "tensor-core split form not available for this size");
    int ndev = 0;
    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
       return fail(nullptr, SWSGPU_ENODEV, "no CUDA device " + std::to_string(device));
@@ -728,6 +775,8 @@ void swsgpu_destroy(swsgpu_handle *h)
       h->d_chans[s].release();
    }
    h->h_out.release();
+   h->d_acc64.release();
+   drop_prof_events(h);
    if (h->done) cudaEventDestroy(h->done);
    if (h->stream) cudaStreamDestroy(h->stream);
    delete h;
@@ -790,11 +839,29 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
    CK(h, h->d_out_pcal.ensure(h->h_pcal_bytes + 16));
    CK(h, h->h_out.ensure(h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes + 64));
    int nspec = 0;
+   const int rpo = std::max(1, c.runs_per_output);
+   bool group_end = true;
+   int acc_mode = 0, pcal_zero = 1, pcal_write = 1;
+   if (rpo > 1) {
+      if (rs.nspec != 1 || rs.partial)
+         return fail(h, SWSGPU_EINVAL, "runs_per_output > 1 needs runs of exactly one full spectrum");
+      const bool first = h->group_pos == 0;
+      group_end = h->group_pos == rpo - 1;
+      acc_mode = group_end ? 3 : (first ? 1 : 2);
+      if (first && group_end) acc_mode = 0;
+      pcal_zero = first ? 1 : 0;
+      pcal_write = group_end ? 1 : 0;
+   }
    if (nsp > 0) {
       int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, payload_min, 1, 1, (float *)h->d_out_auto.p,
                             c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
-                            c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec);
+                            c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec,
+                            acc_mode, pcal_zero, pcal_write);
       if (rc) return rc;
+      if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
+   }
+   h->fetch_ready = group_end;
+   if (nsp > 0 && group_end) {
       char *hp = (char *)h->h_out.p;
       CK(h, cudaMemcpyAsync(hp, h->d_out_auto.p, h->h_auto_bytes, cudaMemcpyDeviceToHost, h->stream));
       if (h->h_xpol_bytes)
@@ -808,7 +875,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
    }
    CK(h, cudaEventRecord(h->done, h->stream));
    h->pending = true;
-   h->pending_nspec = nspec;
+   h->pending_nspec = group_end ? nspec : 0;
    return SWSGPU_OK;
 }
 
@@ -841,7 +908,7 @@ int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out)
    if (!h || !out) return SWSGPU_EINVAL;
    if (h->pending) return fail(h, SWSGPU_ESTATE, "fetch before wait");
    const char *hp = (const char *)h->h_out.p;
-   if (!hp) return SWSGPU_OK;
+   if (!hp || !h->fetch_ready) return fail(h, SWSGPU_ESTATE, "no completed spectra to fetch");
    if (out->auto_out) memcpy(out->auto_out, hp, h->h_auto_bytes);
    if (out->xpol_out && h->h_xpol_bytes) memcpy(out->xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);
    if (out->pcal_out && h->h_pcal_bytes)
@@ -941,5 +1008,34 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
 }
 
 int swsgpu_last_launch_count(const swsgpu_handle *h) { return h ? h->last_launches : 0; }
+
+int swsgpu_profile(swsgpu_handle *h, int enable)
+{
+   if (!h) return SWSGPU_EINVAL;
+   CK(h, cudaSetDevice(h->device));
+   if (enable) {
+      CK(h, cudaStreamSynchronize(h->stream));
+      drop_prof_events(h);
+   }
+   h->profiling = enable != 0;
+   return SWSGPU_OK;
+}
+
+int swsgpu_profile_read(swsgpu_handle *h, int *launches, double *total_ms)
+{
+   if (!h) return SWSGPU_EINVAL;
+   CK(h, cudaSetDevice(h->device));
+   double tot = 0.0;
+   for (auto &pr : h->prof_events) {
+      CK(h, cudaEventSynchronize(pr.second));
+      float ms = 0.0f;
+      CK(h, cudaEventElapsedTime(&ms, pr.first, pr.second));
+      tot += ms;
+   }
+   if (launches) *launches = (int)h->prof_events.size();
+   if (total_ms) *total_ms = tot;
+   drop_prof_events(h);
+   return SWSGPU_OK;
+}
 
 }  // extern "C"

@@ -64,10 +64,14 @@ struct RedEntry {
    int item, prod;
    float scale;
 };
+// acc_mode: 0 dst = sum; 1 acc = sum; 2 acc += sum; 3 acc += sum, dst = acc
+// (acc is an FP64 running sum across runs, element k at acc[k])
 struct OutVec {
    int first, count;             // entries [first, first+count)
    float *dst;                   // base of the output vector
    int stride;                   // element stride (1 real, 2 complex)
+   double *acc;
+   int acc_mode;
 };
 
 }  // namespace sws

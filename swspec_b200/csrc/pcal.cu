@@ -76,7 +76,7 @@ __global__ void k_pcal_out(PcalArgs a)
 int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
 {
    const size_t n = (size_t)a.nout * 2 * a.tonebins;
-   cudaMemsetAsync(a.acc, 0, sizeof(double) * n, st);
+   if (a.zero_acc) cudaMemsetAsync(a.acc, 0, sizeof(double) * n, st);
    const int T = 256;
    const int nper = a.N / a.rotatorlen;
    int bpj = nper < 8 ? nper : 8;
@@ -85,7 +85,7 @@ int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
    if (nbit == 1) k_pcal_fold<1><<<grid, T, sm, st>>>(a);
    else if (nbit == 2) k_pcal_fold<2><<<grid, T, sm, st>>>(a);
    else k_pcal_fold<8><<<grid, T, sm, st>>>(a);
-   k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+   if (a.write_out) k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
    return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -28,8 +28,10 @@ struct PcalArgs {
    double dphi;        // 2 pi (-offset / fs)
    float4 levels;
    float *out;         // [nout][tonebins][2]
-   double *acc;        // [nout][tonebins][2] scratch (set by launch_pcal)
+   double *acc;        // [nout][tonebins][2] FP64 running sums
    int nout;
+   int zero_acc;       // clear acc first (start of an output group)
+   int write_out;      // round acc into out (end of an output group)
 };
 
 // Queues zeroing, folding and conversion on `st`; returns 0 or a CUDA error.

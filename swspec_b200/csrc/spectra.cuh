@@ -335,7 +335,15 @@ __global__ void k_reduce(const float *__restrict__ partial, int S, const RedEntr
       comp = (t - sum) - x;
       sum = t;
    }
-   o.dst[(long long)k * o.stride] = sum;
+   if (o.acc_mode == 0) {
+      o.dst[(long long)k * o.stride] = sum;
+   } else if (o.acc_mode == 1) {
+      o.acc[k] = (double)sum;
+   } else {
+      double t = o.acc[k] + (double)sum;
+      o.acc[k] = t;
+      if (o.acc_mode == 3) o.dst[(long long)k * o.stride] = (float)t;
+   }
 }
 
 }  // namespace sws

@@ -37,7 +37,7 @@ class Config(C.Structure):
                 ("xpol_pair", (C.c_int * 2) * MAX_SOURCES), ("extract_pcal", C.c_int),
                 ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
                 ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
-                ("max_run_bytes", C.c_size_t)]
+                ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -77,6 +77,8 @@ def lib():
                                            C.c_void_p]
         L.swsgpu_last_launch_count.argtypes = [C.c_void_p]
         L.swsgpu_device_ok.argtypes = [C.c_int]
+        L.swsgpu_profile.argtypes = [C.c_void_p, C.c_int]
+        L.swsgpu_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -98,7 +100,8 @@ def layout(fmt: str, nchan: int, nbit: int, framed: bool = True) -> Layout:
 def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_ffts=1,
                 sources=((0, 0),), xpols=(), precision=PREC_FP32, max_run_bytes=1 << 24,
                 extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
-                pcal_offset_hz=10e3, layout2: Layout | None = None) -> Config:
+                pcal_offset_hz=10e3, layout2: Layout | None = None,
+                runs_per_output: int = 1) -> Config:
     c = Config()
     c.layout[0] = lay
     c.layout[1] = layout2 if layout2 is not None else lay
@@ -122,6 +125,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
     c.samplingfreq = samplingfreq
     c.pcal_offset_hz = pcal_offset_hz
     c.max_run_bytes = max_run_bytes
+    c.runs_per_output = runs_per_output
     return c
 
 
@@ -153,6 +157,35 @@ class Core:
 
     def last_launches(self) -> int:
         return lib().swsgpu_last_launch_count(self.h)
+
+    def profile(self, enable: bool) -> None:
+        _check(lib().swsgpu_profile(self.h, int(enable)), self.h)
+
+    def profile_read(self) -> tuple[int, float]:
+        n, ms = C.c_int(), C.c_double()
+        _check(lib().swsgpu_profile_read(self.h, C.byref(n), C.byref(ms)), self.h)
+        return n.value, ms.value
+
+    def submit(self, raws: list, payload_offsets=None) -> None:
+        n = len(raws)
+        ptrs = (C.c_void_p * n)(*[int(r) if isinstance(r, int) else r.ctypes.data for r in raws])
+        sizes = (C.c_size_t * n)(*self._sizes)
+        offs = (C.c_int64 * n)(*(payload_offsets or [0] * n))
+        _check(lib().swsgpu_submit(self.h, ptrs, sizes, offs), self.h)
+
+    def set_sizes(self, sizes: list[int]) -> None:
+        self._sizes = list(sizes)
+
+    def wait(self, timeout_ms: int = 60000) -> int:
+        ns = C.c_int()
+        _check(lib().swsgpu_wait(self.h, timeout_ms, C.byref(ns)), self.h)
+        return ns.value
+
+    def fetch_into(self, auto: np.ndarray, xpol: np.ndarray | None = None,
+                   pcal: np.ndarray | None = None) -> None:
+        out = Outputs(auto.ctypes.data, None if xpol is None else xpol.ctypes.data,
+                      None if pcal is None else pcal.ctypes.data)
+        _check(lib().swsgpu_fetch(self.h, C.byref(out)), self.h)
 
     def run(self, raws: list, payload_offsets=None, timeout_ms: int = 60000):
         """One core run from host bytes (submit + wait + fetch)."""

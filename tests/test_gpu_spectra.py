@@ -61,9 +61,10 @@ def test_c3_like_dual_pol_cross(gpu):
         worst = max(worst, rel_err_auto(auto[:, i], ra[:, 0]), rel_err_auto(auto[:, j], ra[:, 1]),
                     rel_err_xpol(xp[:, k], rx[:, 0], ra[:, 0], ra[:, 1]))
     assert worst < REL_TOL, worst
-    # the synthesised cross-correlation is rho = 0.3 at 0.7 rad
+    # the synthesised cross-correlation is rho = 0.3 at 0.7 rad; 2-bit
+    # quantisation at +-0.98 sigma scales |rho| by ~0.88 (Van Vleck)
     rho = np.mean(xp[0, 0, 100:-100] / np.sqrt(auto[0, 0, 100:-100] * auto[0, 8, 100:-100]))
-    assert abs(abs(rho) - 0.3) < 0.03 and abs(abs(np.angle(rho)) - 0.7) < 0.1
+    assert abs(abs(rho) - 0.3 * 0.88) < 0.02 and abs(abs(np.angle(rho)) - 0.7) < 0.1
 
 
 @pytest.mark.parametrize("overlap,cof", [(2, 7), (1, 5), (4, 9)])
@@ -89,8 +90,13 @@ def test_two_files_overlap_partial(gpu, overlap, cof):
 @pytest.mark.parametrize("nbit,nchan,window", [(1, 16, "none"), (1, 32, "cosine"),
                                                (2, 4, "hamming"), (2, 1, "blackman")])
 def test_bit_depths_and_windows(gpu, nbit, nchan, window):
-    N, cof = 8192, 4
-    d, T = _mark5b_noise(nchan, nbit, 16 if nchan * nbit >= 8 else 4, 21 + nbit + nchan,
+    """Integrated spectra (32 FFTs) at the 2e-6 max-relative bar.  FP32 FFT
+    error is absolute, so the bar is meant for integrated spectra; the
+    short-integration case below checks the error against the spectrum level."""
+    N, cof = 8192, 32
+    spf = synth.mark5b_samples_per_frame(nchan, nbit)
+    nfr = N * cof // spf + 1
+    d, T = _mark5b_noise(nchan, nbit, nfr, 21 + nbit + nchan,
                          mbps=1024 if nchan * nbit >= 8 else 256)
     lay = gpu.layout("mark5b", nchan, nbit)
     ch = nchan - 1
@@ -147,3 +153,20 @@ def test_pcal_fold(gpu):
     assert rel_err_auto(auto, ra) < REL_TOL
     scale = np.max(np.abs(rp))
     assert np.max(np.abs(pc - rp)) / scale < 1e-6
+
+
+def test_short_integration_level_relative(gpu):
+    """One FFT per spectrum, rectangular window: error relative to the mean
+    spectral level stays at FP32 FFT accuracy (max relative error per bin is
+    dominated by near-empty bins at this integration)."""
+    N = 8192
+    d, T = _mark5b_noise(16, 1, 9, 5)
+    lay = gpu.layout("mark5b", 16, 1)
+    cfg = gpu.make_config(lay, N, "none", 1, 1, sources=((0, 7),), max_run_bytes=len(d))
+    core = gpu.Core(cfg)
+    auto, _, _, ns = core.run([d])
+    s = decode_channels(d, "Mark5B-1024-16-1", 16, 1, [7], T)
+    ra, _, _, nref = oracle_run(s, N, "none", 1, 1)
+    assert ns == nref == T // N
+    err = np.max(np.abs(auto - ra) / ra.mean(axis=-1, keepdims=True))
+    assert err < 2e-7, err
