@@ -268,7 +268,9 @@ def gpu_arm(args) -> None:
     S = N // 2 + 1
     d_auto = torch.zeros(NCHAN, S, dtype=torch.float32, device="cuda")
     d_xpol = torch.zeros(NPAIRS, S, 2, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: its handle is what the library launches on and
+    # what the timing events are recorded on
+    stream = torch.cuda.Stream()
     lay = gpu.layout("mark5b", NCHAN, 2)
     sources = tuple((0, c) for c in range(NCHAN))
     pairs = tuple((c, c + NPAIRS) for c in range(NPAIRS))
@@ -312,6 +314,7 @@ def gpu_arm(args) -> None:
             for _ in range(args.steps):
                 step(core)
             ev1.record(stream)
+            stream.synchronize()
             torch.cuda.synchronize()
         barrier()
         ms = ev0.elapsed_time(ev1)
