@@ -46,6 +46,7 @@ extern "C" {
 #define SWSGPU_ETIMEOUT (-3)     /* swsgpu_wait timed out; the run is still queued */
 #define SWSGPU_ENODEV (-4)       /* no usable sm_100 device */
 #define SWSGPU_ESTATE (-5)       /* call out of order (e.g. fetch before wait) */
+#define SWSGPU_ETOOBIG (-6)      /* request exceeds a fixed capacity (see the _noalloc entry) */
 
 /* Sample tables (level values) of the stream. */
 #define SWSGPU_FMT_MARK5B 0      /* Mark5B: 2-bit {-H,+1,-1,+H}[s+2m], 1-bit {+1,-1} */
@@ -186,6 +187,28 @@ int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, s
 int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,
                          int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
                          int64_t *nvalid, void *cuda_stream);
+
+/* No counterpart in the reference.  The same decode as swsgpu_unpack_device
+ * without any device allocation, for callers that cannot allocate device
+ * memory at the point where they decode: an acquisition thread that must not
+ * stall on the device-wide synchronisation cudaMalloc/cudaFree can cause, an
+ * application whose memory manager owns every device allocation, or a
+ * process that reserves its device memory once at start-up.  Its scratch is
+ * one fixed array of SWSGPU_NOALLOC_SCRATCH_BYTES compiled into the library;
+ * every device that loads the library holds it until the process exits.
+ * Limit: at most SWSGPU_NOALLOC_MAX_FRAMES frames per call (about 160 MB of
+ * Mark5B data); larger requests return SWSGPU_ETOOBIG.  The caller still
+ * provides d_raw and d_out.  The first call on each device looks up the
+ * scratch address for that device (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  All calls share the one scratch array:
+ * calls that overlap on the GPU (for example on two streams at once) race
+ * and must be serialised by the caller.  Returns like swsgpu_unpack_device,
+ * waiting for its own stream. */
+#define SWSGPU_NOALLOC_MAX_FRAMES 16384
+#define SWSGPU_NOALLOC_SCRATCH_BYTES (SWSGPU_NOALLOC_MAX_FRAMES * 8 + 256)
+int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,
+                                 int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
+                                 int64_t *nvalid, void *cuda_stream);
 
 /* Number of kernel launches the last submit / process_device call issued. */
 int swsgpu_last_launch_count(const swsgpu_handle *h);

@@ -20,7 +20,8 @@ PREC_FP32, PREC_TCSPLIT = 0, 1
 MAX_SOURCES = 64
 MAX_STREAMS = 2
 
-ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ETIMEOUT", -4: "ENODEV", -5: "ESTATE"}
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ETIMEOUT", -4: "ENODEV", -5: "ESTATE",
+          -6: "ETOOBIG"}
 
 
 class Layout(C.Structure):
@@ -76,6 +77,9 @@ def lib():
                                            C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_int64),
                                            C.c_void_p]
         L.swsgpu_last_launch_count.argtypes = [C.c_void_p]
+        L.swsgpu_unpack_device_noalloc.argtypes = [C.POINTER(Layout), C.c_void_p, C.c_size_t,
+                                                   C.c_int64, C.c_int, C.c_int64, C.c_void_p,
+                                                   C.POINTER(C.c_int64), C.c_void_p]
         L.swsgpu_device_ok.argtypes = [C.c_int]
         L.swsgpu_profile.argtypes = [C.c_void_p, C.c_int]
         L.swsgpu_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
@@ -225,4 +229,16 @@ def unpack_device(lay: Layout, d_raw: int, nbytes: int, payload_offset: int, cha
     rc = lib().swsgpu_unpack_device(C.byref(lay), d_raw, nbytes, payload_offset, chan, nsamp,
                                     d_out, C.byref(nv), C.c_void_p(stream or None))
     _check(rc)
+    return nv.value
+
+
+def unpack_device_noalloc(lay: Layout, d_raw: int, nbytes: int, payload_offset: int, chan: int,
+                          nsamp: int, d_out: int, stream: int = 0) -> int:
+    """swsgpu_unpack_device_noalloc: the same decode with the library's fixed
+    scratch array instead of per-call device allocations."""
+    nv = C.c_int64()
+    rc = lib().swsgpu_unpack_device_noalloc(C.byref(lay), d_raw, nbytes, payload_offset, chan,
+                                            nsamp, d_out, C.byref(nv), C.c_void_p(stream or None))
+    if rc != 0:
+        raise SwsError(f"{ERRORS.get(rc, rc)}: swsgpu_unpack_device_noalloc failed")
     return nv.value
