@@ -11,19 +11,24 @@
 //    and B_k = (Z_k - conj Z_{N-k})/(2i) recover both real spectra, and
 //    |A|^2, |B|^2, A conj(B) follow.  A dual-pol pair (X, Y) is one job; an
 //    auto-only channel pairs two consecutive frames of itself.
-//  * The N-point FFT is split N = P*Q over a thread-block cluster of P CTAs
-//    (decimation in time): CTA p decodes, windows and transforms the
-//    subsequence z[p + P q] (q < Q) in its shared memory (Stockham passes,
-//    radices R1 R2 R3), then, after a cluster barrier, each thread gathers
-//    F_p[k1] and F_p[Q-k1] from all P CTAs through distributed shared memory,
-//    applies W_N^{p k1}, finishes a P-point DFT and holds both Z_k and Z_{N-k}
-//    for its bins in registers.
+//  * N = P*Q over a thread-block cluster of P CTAs (decimation in time):
+//    CTA p decodes, windows and transforms z[p + P q] (q < Q) in shared
+//    memory with Stockham passes of radix R1, R2, R3 -- one butterfly per
+//    thread per pass when Q/R = T -- then, after a cluster barrier, threads
+//    gather F_p[k1] (lo side) or F_p[Q-k1] (hi side) from all P CTAs through
+//    distributed shared memory, apply W_N^{p k1}, finish the P-point DFT and
+//    swap half of their outputs with the partner lane, so each lane holds
+//    Z_k and Z_{N-k} for its bins.
+//  * Per-pass twiddles live in thread-major shared tables [r][k] (k = the
+//    butterfly's index mod Ns), filled once per CTA, so every twiddle read is
+//    bank-conflict free; the cluster-stage twiddles W_N^{p k1} likewise.
 //  * Spectra of consecutive jobs of a work item accumulate in registers (the
 //    thread-to-bin map is fixed) and are written once per item; a reduction
-//    kernel adds items with compensated FP32 sums and applies the
-//    1/core_overlapped_ffts scale.
-//  * The first Stockham pass is fused with decode and window: samples come
-//    straight from the packed per-channel codes written by K1.
+//    kernel adds items with compensated sums and applies the scaling.
+//  * The cluster barrier that protects a CTA's buffer from the previous
+//    job's remote readers is split (arrive after the gathers, wait just
+//    before the next job's first stores), so decode and the first radix-R1
+//    butterflies of the next job overlap it.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -36,6 +41,30 @@ namespace sws {
 namespace cg = cooperative_groups;
 
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }  // 1 pad per 16 float2
+
+// Distributed shared memory: 32-bit shared::cluster address of the same
+// offset in CTA `rank` of the cluster, and a 64-bit load from it.
+__device__ __forceinline__ uint32_t dsmem_addr(uint32_t local_addr, uint32_t rank)
+{
+   uint32_t r;
+   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(local_addr), "r"(rank));
+   return r;
+}
+__device__ __forceinline__ float2 dsmem_ld2(uint32_t addr)
+{
+   float2 v;
+   asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+   return v;
+}
+
+__device__ __forceinline__ void cluster_arrive()
+{
+   asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait()
+{
+   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
 
 template <int NBIT>
 __device__ __forceinline__ float decode_level(uint32_t code, float4 lv)
@@ -51,25 +80,56 @@ __device__ __forceinline__ float decode_level(uint32_t code, float4 lv)
    }
 }
 
-template <int NBIT>
-__device__ __forceinline__ float sample_at(const SpecArgs &a, int src, long long s, bool chk_blank,
-                                           int stream)
+// Code stream cursor of one source for one job and CTA: sample
+// s0 + rank + P*q sits at bit  off0 + q*P*NBIT  counted from word w0.
+struct Cursor {
+   const uint32_t *w0;
+   int off0;
+   const uint32_t *blank;  // bitmap of the source's stream, or null
+   long long s0;           // s0 + rank (sample of q = 0)
+};
+
+template <int P, int NBIT>
+__device__ __forceinline__ Cursor make_cursor(const SpecArgs &a, int src, long long s0, int rank,
+                                              bool chk_blank, int stream)
 {
-   constexpr int SPW = 32 / NBIT;
+   Cursor c;
+   const long long s = s0 + rank;
+   const long long bit = s * NBIT;
+   c.w0 = a.codes + (long long)src * a.code_words + (bit >> 5);
+   c.off0 = (int)(bit & 31);
+   c.blank = chk_blank ? a.blank + (long long)stream * a.blank_words : nullptr;
+   c.s0 = s;
+   return c;
+}
+
+template <int P, int NBIT>
+__device__ __forceinline__ float cursor_sample(const Cursor &c, int q, float4 lv)
+{
    constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   uint32_t word = __ldg(a.codes + (long long)src * a.code_words + s / SPW);
-   uint32_t code = (word >> (NBIT * (int)(s % SPW))) & MASK;
-   float v = decode_level<NBIT>(code, a.levels);
-   if (chk_blank) {
-      uint32_t bw = __ldg(a.blank + (long long)stream * a.blank_words + (s >> 5));
-      if ((bw >> (s & 31)) & 1u) v = 0.0f;
+   const int rel = c.off0 + q * (P * NBIT);
+   const uint32_t word = __ldg(c.w0 + (rel >> 5));
+   float v = decode_level<NBIT>((word >> (rel & 31)) & MASK, lv);
+   if (c.blank) {
+      const long long s = c.s0 + (long long)P * q;
+      if ((__ldg(c.blank + (s >> 5)) >> (s & 31)) & 1u) v = 0.0f;
    }
    return v;
 }
 
-// One in-place Stockham pass over the padded shared buffer.
+// Twiddle table of a pass: tw[(r-1)*Ns + k] = W_{Ns R}^{k r}, k < Ns, 0 < r < R.
+template <int Q, int R, int Ns>
+__device__ __forceinline__ void fill_pass_twiddles(float2 *tw, const float2 *__restrict__ twQ, int T)
+{
+   for (int i = threadIdx.x; i < (R - 1) * Ns; i += T) {
+      const int r = i / Ns + 1, k = i % Ns;
+      tw[i] = __ldg(twQ + k * r * (Q / (Ns * R)));
+   }
+}
+
+// One in-place Stockham pass over the padded shared buffer (FP32).
 template <int Q, int T, int R, int Ns>
-__device__ __forceinline__ void smem_pass(float2 *buf, const float2 *__restrict__ twQ)
+__device__ __forceinline__ void smem_pass(float2 *buf, const float2 *tw)
 {
    constexpr int nb = Q / R;
    constexpr int BPT = (nb + T - 1) / T;
@@ -83,7 +143,7 @@ __device__ __forceinline__ void smem_pass(float2 *buf, const float2 *__restrict_
 #pragma unroll
          for (int r = 0; r < R; r++) {
             float2 x = buf[pidx(j + r * nb)];
-            if (r > 0 && Ns > 1) x = cmul(x, __ldg(twQ + k * r * (Q / (Ns * R))));
+            if (r > 0) x = cmul(x, tw[(r - 1) * Ns + k]);
             v[b][r] = x;
          }
          DFT<R>::run(v[b]);
@@ -103,57 +163,10 @@ __device__ __forceinline__ void smem_pass(float2 *buf, const float2 *__restrict_
    __syncthreads();
 }
 
-// First pass (Ns = 1) fused with decode + window + pair packing.
-template <int P, int Q, int T, int R, int NBIT>
-__device__ __forceinline__ void first_pass(float2 *buf, const float *wsl, const SpecArgs &a,
-                                           int rank, int src_a, long long sa, int src_b,
-                                           long long sb, bool has_b, bool blank_a, bool blank_b,
-                                           int stream_a, int stream_b)
-{
-   constexpr int nb = Q / R;
-   constexpr int BPT = (nb + T - 1) / T;
-   const int tid = threadIdx.x;
-   float2 v[BPT][R];
-#pragma unroll
-   for (int b = 0; b < BPT; b++) {
-      const int j = tid + b * T;
-      if (nb % T == 0 || j < nb) {
-#pragma unroll
-         for (int r = 0; r < R; r++) {
-            const int q = j + r * nb;
-            const long long n = rank + (long long)P * q;
-            const float w = wsl[q];
-            float xa = sample_at<NBIT>(a, src_a, sa + n, blank_a, stream_a);
-            float xb = has_b ? sample_at<NBIT>(a, src_b, sb + n, blank_b, stream_b) : 0.0f;
-            v[b][r] = make_float2(xa * w, xb * w);
-         }
-         DFT<R>::run(v[b]);
-      }
-   }
-   // writes go to locations no other thread reads in this pass (out of place
-   // w.r.t. the code stream), so no barrier before the stores
-#pragma unroll
-   for (int b = 0; b < BPT; b++) {
-      const int j = tid + b * T;
-      if (nb % T == 0 || j < nb) {
-#pragma unroll
-         for (int r = 0; r < R; r++) buf[pidx(j * R + r)] = v[b][r];
-      }
-   }
-   __syncthreads();
-}
-
-// Bins handled per k1-pair slot.
-template <int P>
-__host__ __device__ constexpr int slots_per_pair() { return P == 1 ? 2 : P + 1; }
-
-template <int NBIT_>
-struct NbitTag { static constexpr int value = NBIT_; };
-
 // Accumulate the products of one bin from Z_k (zk) and Z_{N-k} (zm).
+// A' = 2A, B' = 2B; the reduction applies the 1/4.
 __device__ __forceinline__ void acc_bin(float *acc4, int mode, float2 zk, float2 zm)
 {
-   // A' = 2A, B' = 2B (the reduction applies the 1/4)
    float2 A = make_float2(zk.x + zm.x, zk.y - zm.y);
    if (mode == MODE_XPOL) {
       float2 B = make_float2(zk.y + zm.y, zm.x - zk.x);
@@ -169,31 +182,56 @@ __device__ __forceinline__ void acc_bin(float *acc4, int mode, float2 zk, float2
    }
 }
 
-template <int P, int Q, int T, int R1, int R2, int R3, int NBIT>
-__global__ void __launch_bounds__(T, 1) k_spectra(SpecArgs a)
+// Shared memory footprint of a plan (bytes).
+template <int P, int Q, int R1, int R2, int R3>
+__host__ __device__ constexpr size_t spectra_smem()
+{
+   return (size_t)(Q + Q / 16) * 8                          // buffer
+          + (size_t)Q * 4                                   // window slice
+          + (size_t)(R2 - 1) * R1 * 8                       // pass-2 twiddles
+          + (size_t)(R3 > 1 ? (R3 - 1) * R1 * R2 : 0) * 8   // pass-3 twiddles
+          + (size_t)(P - 1) * (Q / (2 * P)) * 8;            // cluster twiddles per k1-pair
+}
+
+template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB>
+__global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 {
    static_assert(R1 * R2 * R3 == Q, "radix plan must multiply to Q");
-   constexpr int UC = Q / (2 * P);            // k1-pairs per CTA
-   constexpr int UPT = (UC + T - 1) / T;      // k1-pairs per thread
-   constexpr int NS = slots_per_pair<P>();
+   constexpr int UC = Q / (2 * P);          // k1-pairs per CTA
+   constexpr int SIDES = 2 * UC;            // lo/hi sides per CTA
+   constexpr int SPT = (SIDES + T - 1) / T; // sides per thread
+   constexpr int HB = (P == 1) ? 1 : P / 2; // bins per side (regular)
+   constexpr int NB = HB + 1;               // + the lo special's extra bin
+   constexpr int NX = (P == 1) ? 1 : P / 2; // values exchanged with the partner lane
    extern __shared__ float4 smem_raw[];
    float2 *buf = reinterpret_cast<float2 *>(smem_raw);
    float *wsl = reinterpret_cast<float *>(buf + (Q + Q / 16));
+   float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
+   float2 *tw3 = tw2 + (R2 - 1) * R1;
+   float2 *twc = tw3 + (R3 > 1 ? (R3 - 1) * R1 * R2 : 0);
 
    cg::cluster_group cluster = cg::this_cluster();
    const int rank = (int)cluster.block_rank();
    const int cid = blockIdx.x / P;
    const int ncl = gridDim.x / P;
    const int tid = threadIdx.x;
-   const int N = a.N, S = a.S;
+   const int S = a.S;
 
-   // window slice w[rank + P q]
+   // ---- per-CTA constant tables ----
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
+   if constexpr (R2 > 1) fill_pass_twiddles<Q, R2, R1>(tw2, a.twQ, T);
+   if constexpr (R3 > 1) fill_pass_twiddles<Q, R3, R1 * R2>(tw3, a.twQ, T);
+   // side s of this CTA: pair index u = rank*UC + s/2, lo side if s even;
+   // twc[(p-1)*UC + s/2] = W_N^{p u}, read by both sides of a pair
+   for (int i = tid; i < (P - 1) * UC; i += T) {
+      const int p = i / UC + 1, uu = i % UC;
+      twc[i] = __ldg(a.twN + (long long)p * (rank * UC + uu));
+   }
    __syncthreads();
 
-   float2 *remote[P];
-#pragma unroll
-   for (int p = 0; p < P; p++) remote[p] = cluster.map_shared_rank(buf, p);
+   const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+
+   cluster_arrive();  // pairs with the wait before the first job's stores
 
    for (int it = cid; it < a.nitems; it += ncl) {
       const Item item = a.items[it];
@@ -204,120 +242,161 @@ __global__ void __launch_bounds__(T, 1) k_spectra(SpecArgs a)
       const int stream_b = has_b ? a.code_stream[src_b] : 0;
       const bool blank_a = a.blank_any[stream_a] != 0;
       const bool blank_b = has_b && a.blank_any[stream_b] != 0;
-      float acc[UPT][NS][4];
+      float acc[SPT][NB][4];
 #pragma unroll
-      for (int u = 0; u < UPT; u++)
+      for (int u = 0; u < SPT; u++)
 #pragma unroll
-         for (int s = 0; s < NS; s++)
+         for (int s = 0; s < NB; s++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[u][s][c] = 0.0f;
 
       for (int j = 0; j < item.nfr; j++) {
          const long long sa = item.start + (long long)j * item.step;
          const long long sb = (mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
-         first_pass<P, Q, T, R1, NBIT>(buf, wsl, a, rank, item.src_a, sa, src_b, sb, has_b,
-                                       blank_a, blank_b, stream_a, stream_b);
-         if constexpr (R2 > 1) smem_pass<Q, T, R2, R1>(buf, a.twQ);
-         if constexpr (R3 > 1) smem_pass<Q, T, R3, R1 * R2>(buf, a.twQ);
-         cluster.sync();
-         // ---- final radix-P stage across the cluster + pair separation ----
+         const Cursor ca = make_cursor<P, NBIT>(a, item.src_a, sa, rank, blank_a, stream_a);
+         const Cursor cb = make_cursor<P, NBIT>(a, has_b ? src_b : item.src_a, sb, rank, blank_b,
+                                                stream_b);
+         // ---- pass 1 (Ns = 1): decode + window + radix-R1, in registers ----
+         constexpr int nb1 = Q / R1;
+         constexpr int BPT1 = (nb1 + T - 1) / T;
+         float2 v[BPT1][R1];
 #pragma unroll
-         for (int ui = 0; ui < UPT; ui++) {
-            const int u = rank * UC + tid + ui * T;
-            if (UC % T != 0 && tid + ui * T >= UC) continue;
-            float2 lo[P], hi[P];
-            if (u == 0) {
+         for (int b = 0; b < BPT1; b++) {
+            const int jj = tid + b * T;
+            if (nb1 % T == 0 || jj < nb1) {
 #pragma unroll
-               for (int p = 0; p < P; p++) {
-                  lo[p] = remote[p][pidx(0)];
-                  hi[p] = remote[p][pidx(Q / 2)];
+               for (int r = 0; r < R1; r++) {
+                  const int q = jj + r * nb1;
+                  const float w = wsl[q];
+                  const float xa = cursor_sample<P, NBIT>(ca, q, a.levels);
+                  const float xb = has_b ? cursor_sample<P, NBIT>(cb, q, a.levels) : 0.0f;
+                  v[b][r] = make_float2(xa * w, xb * w);
                }
-               // W_N^{p Q/2} = W_{2P}^p
-               static_for<0, P>([&](auto I) {
-                  constexpr int p = decltype(I)::value;
-                  hi[p] = twmul<p, 2 * P>(hi[p]);
-               });
-               DFT<P>::run(lo);
-               DFT<P>::run(hi);
-               if constexpr (P == 1) {
-                  acc_bin(acc[ui][0], mode, lo[0], lo[0]);
-                  acc_bin(acc[ui][1], mode, hi[0], hi[0]);
+               DFT<R1>::run(v[b]);
+            }
+         }
+         cluster_wait();  // every remote reader of buf from the previous job is done
+#pragma unroll
+         for (int b = 0; b < BPT1; b++) {
+            const int jj = tid + b * T;
+            if (nb1 % T == 0 || jj < nb1) {
+#pragma unroll
+               for (int r = 0; r < R1; r++) buf[pidx(jj * R1 + r)] = v[b][r];
+            }
+         }
+         __syncthreads();
+         if constexpr (R2 > 1) smem_pass<Q, T, R2, R1>(buf, tw2);
+         if constexpr (R3 > 1) smem_pass<Q, T, R3, R1 * R2>(buf, tw3);
+         cluster.sync();  // all CTAs' F_p complete
+         // ---- cluster radix-P stage + pair separation ----
+#pragma unroll
+         for (int si = 0; si < SPT; si++) {
+            const int s = tid + si * T;  // side index within the CTA
+            const bool active = (SIDES % T == 0) || s < SIDES;
+            const bool hi = (s & 1) != 0;
+            const int u = rank * UC + (s >> 1);
+            float2 z[P];
+            if (active) {
+               if (u == 0) {
+                  // lo: k1 = 0 (no twiddle); hi: k1 = Q/2, W_N^{p Q/2} = W_{2P}^p
+                  const int k1 = hi ? Q / 2 : 0;
+                  const uint32_t off = buf_addr + 8u * (uint32_t)pidx(k1);
+#pragma unroll
+                  for (int p = 0; p < P; p++) z[p] = dsmem_ld2(dsmem_addr(off, p));
+                  if (hi) {
+                     static_for<1, P>([&](auto I) {
+                        constexpr int p = decltype(I)::value;
+                        z[p] = twmul<p, 2 * P>(z[p]);
+                     });
+                  }
                } else {
+                  const int k1 = hi ? Q - u : u;
+                  const uint32_t off = buf_addr + 8u * (uint32_t)pidx(k1);
 #pragma unroll
-                  for (int k2 = 0; k2 <= P / 2; k2++) acc_bin(acc[ui][k2], mode, lo[k2], lo[(P - k2) % P]);
+                  for (int p = 0; p < P; p++) z[p] = dsmem_ld2(dsmem_addr(off, p));
 #pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++)
-                     acc_bin(acc[ui][P / 2 + 1 + k2], mode, hi[k2], hi[P - 1 - k2]);
-               }
-            } else {
-#pragma unroll
-               for (int p = 0; p < P; p++) {
-                  float2 fl = remote[p][pidx(u)];
-                  float2 fh = remote[p][pidx(Q - u)];
-                  if (p == 0) {
-                     lo[p] = fl;
-                     hi[p] = fh;
-                  } else {
-                     float2 w = __ldg(a.twN + (long long)p * u);
-                     lo[p] = cmul(fl, w);
-                     hi[p] = cmulconj(fh, w);  // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
+                  for (int p = 1; p < P; p++) {
+                     const float2 w = twc[(p - 1) * UC + (s >> 1)];
+                     z[p] = hi ? cmulconj(z[p], w) : cmul(z[p], w);
+                  }
+                  if (hi) {
+                     // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
+                     static_for<1, P>([&](auto I) {
+                        constexpr int p = decltype(I)::value;
+                        z[p] = twmul<p, P>(z[p]);
+                     });
                   }
                }
-               static_for<1, P>([&](auto I) {
-                  constexpr int p = decltype(I)::value;
-                  hi[p] = twmul<p, P>(hi[p]);
-               });
-               DFT<P>::run(lo);
-               DFT<P>::run(hi);
-               if constexpr (P == 1) {
-                  acc_bin(acc[ui][0], mode, lo[0], hi[0]);
-               } else {
+               DFT<P>::run(z);
+            } else {
 #pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++) {
-                     acc_bin(acc[ui][k2], mode, lo[k2], hi[P - 1 - k2]);
-                     acc_bin(acc[ui][P / 2 + k2], mode, hi[k2], lo[P - 1 - k2]);
+               for (int p = 0; p < P; p++) z[p] = make_float2(0.0f, 0.0f);
+            }
+            // swap the upper half with the partner side (lane ^ 1)
+            float2 rv[NX];
+#pragma unroll
+            for (int i = 0; i < NX; i++) {
+               const int src = (P == 1) ? 0 : P / 2 + i;
+               rv[i].x = __shfl_xor_sync(0xffffffffu, z[src].x, 1);
+               rv[i].y = __shfl_xor_sync(0xffffffffu, z[src].y, 1);
+            }
+            if (active) {
+               if (u == 0) {
+                  if constexpr (P == 1) {
+                     acc_bin(acc[si][0], mode, z[0], z[0]);
+                  } else if (!hi) {
+#pragma unroll
+                     for (int k2 = 0; k2 <= P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[(P - k2) % P]);
+                  } else {
+#pragma unroll
+                     for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[P - 1 - k2]);
+                  }
+               } else {
+                  if constexpr (P == 1) {
+                     if (!hi) acc_bin(acc[si][0], mode, z[0], rv[0]);
+                  } else {
+#pragma unroll
+                     for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], rv[P / 2 - 1 - k2]);
                   }
                }
             }
          }
-         cluster.sync();
+         cluster_arrive();  // this CTA has finished reading remote buffers
       }
       // ---- write this item's partial sums: partial[it][prod][bin] ----
       float *part = a.partial + (long long)it * 4 * S;
       const int nprod = (mode == MODE_XPOL) ? 4 : 1;
 #pragma unroll
-      for (int ui = 0; ui < UPT; ui++) {
-         const int u = rank * UC + tid + ui * T;
-         if (UC % T != 0 && tid + ui * T >= UC) continue;
+      for (int si = 0; si < SPT; si++) {
+         const int s = tid + si * T;
+         if (!((SIDES % T == 0) || s < SIDES)) continue;
+         const bool hi = (s & 1) != 0;
+         const int u = rank * UC + (s >> 1);
          for (int c = 0; c < nprod; c++) {
             float *pc = part + (long long)c * S;
             if (u == 0) {
                if constexpr (P == 1) {
-                  pc[0] = acc[ui][0][c];
-                  pc[Q / 2] = acc[ui][1][c];
+                  pc[hi ? Q / 2 : 0] = acc[si][0][c];
+               } else if (!hi) {
+#pragma unroll
+                  for (int k2 = 0; k2 <= P / 2; k2++) pc[Q * k2] = acc[si][k2][c];
                } else {
 #pragma unroll
-                  for (int k2 = 0; k2 <= P / 2; k2++) pc[Q * k2] = acc[ui][k2][c];
-#pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++) pc[Q / 2 + Q * k2] = acc[ui][P / 2 + 1 + k2][c];
+                  for (int k2 = 0; k2 < P / 2; k2++) pc[Q / 2 + Q * k2] = acc[si][k2][c];
                }
             } else {
                if constexpr (P == 1) {
-                  pc[u] = acc[ui][0][c];
+                  if (!hi) pc[u] = acc[si][0][c];
                } else {
+                  const int k1 = hi ? Q - u : u;
 #pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++) {
-                     pc[u + Q * k2] = acc[ui][k2][c];
-                     pc[(Q - u) + Q * k2] = acc[ui][P / 2 + k2][c];
-                  }
+                  for (int k2 = 0; k2 < P / 2; k2++) pc[k1 + Q * k2] = acc[si][k2][c];
                }
             }
          }
       }
-      (void)N;
    }
-   // keep every CTA's shared memory alive until the whole cluster is done
-   cluster.sync();
+   cluster_wait();  // pairs with the last arrive: no remote reader is left
 }
 
 // K3: out[o][k] = sum over entries of scale * partial[item][prod][k], Kahan.
