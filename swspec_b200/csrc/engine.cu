@@ -25,8 +25,8 @@
 namespace sws {
 __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any);
 void launch_unpack_codes(int nbit, dim3 grid, int block, cudaStream_t st, StreamIn s,
-                         long long nsamp, const int *chans, int nch, uint32_t *codes,
-                         long long code_words, const int2 *valid, uint32_t *blank);
+                         long long nsamp, const int *chans, int nch, uint32_t *codes, int D,
+                         long long wpp, const int2 *valid, uint32_t *blank);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
 __global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
@@ -409,10 +409,13 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    const int nbit = c.layout[0].nbit;
    const int spw = 32 / nbit;
    const long long nsamp = sc.nsamp;
-   const long long code_words = (nsamp + spw - 1) / spw;
+   const int D = h->plan.P;                      // phase decimation of the code arrays
+   const long long per_phase = (nsamp + D - 1) / D;
+   const long long wpp = (per_phase + spw - 1) / spw + 2;  // +2: prefetch may touch one word past
+   const long long code_words = (long long)D * wpp;
    const long long blank_words = (nsamp + 31) / 32;
 
-   CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 16));
+   CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 64));
    CK(h, h->d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
    CK(h, h->d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
    CK(h, cudaMemsetAsync(h->d_blank.p, 0, sizeof(uint32_t) * (size_t)blank_words * c.num_streams, st));
@@ -452,7 +455,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       dim3 grid((unsigned)((code_words + 255) / 256), (unsigned)((chans.size() + 15) / 16));
       uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
       launch_unpack_codes(nbit, grid, 256, st, si, nsamp, (const int *)h->d_chans[s].p,
-                          (int)chans.size(), codes, code_words, (const int2 *)h->d_valid[s].p, blank);
+                          (int)chans.size(), codes, D, wpp, (const int2 *)h->d_valid[s].p, blank);
       launches++;
    }
    CK(h, cudaGetLastError());
@@ -467,6 +470,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       SpecArgs a;
       a.codes = (const uint32_t *)h->d_codes.p;
       a.code_words = code_words;
+      a.wpp = wpp;
+      a.D = D;
       a.blank = (const uint32_t *)h->d_blank.p;
       a.blank_words = blank_words;
       a.blank_any = (const int *)h->d_blank_any.p;
@@ -486,7 +491,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       cudaLaunchConfig_t cfgl = {};
       cfgl.gridDim = dim3(ncl * pl.P);
       cfgl.blockDim = dim3(pl.T);
-      cfgl.dynamicSmemBytes = pl.smem;
+      cfgl.dynamicSmemBytes = pl.smem[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
       cfgl.stream = st;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -539,6 +544,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          PcalArgs pa;
          pa.codes = (const uint32_t *)h->d_codes.p;
          pa.code_words = code_words;
+         pa.wpp = wpp;
+         pa.D = D;
          pa.blank = (const uint32_t *)h->d_blank.p;
          pa.blank_words = blank_words;
          pa.blank_any = (const int *)h->d_blank_any.p;
@@ -729,14 +736,15 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    // kernel attributes and cluster occupancy
    const int nbit = cfg->layout[0].nbit;
    SpecKernel kern = plan.kern[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
-   CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
+   const size_t smem = plan.smem[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+   CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
    if (plan.P > 8)
       CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
    {
       cudaLaunchConfig_t cfgl = {};
       cfgl.gridDim = dim3(plan.P);
       cfgl.blockDim = dim3(plan.T);
-      cfgl.dynamicSmemBytes = plan.smem;
+      cfgl.dynamicSmemBytes = smem;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
       attr[0].val.clusterDim.x = plan.P;

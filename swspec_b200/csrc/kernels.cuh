@@ -42,9 +42,13 @@ struct Item {
 
 constexpr int MODE_XPOL = 0, MODE_AUTOSUM = 1, MODE_SINGLE = 2;
 
+// Code arrays are phase-decimated (see k_unpack_codes): array c holds
+// D phase arrays of wpp words; sample s at phase s % D, index s / D.
 struct SpecArgs {
-   const uint32_t *codes;        // [ncode][code_words]
-   long long code_words;         // words per code array
+   const uint32_t *codes;        // [ncode][D][wpp]
+   long long code_words;         // words per code array (D * wpp)
+   long long wpp;                // words per phase array
+   int D;                        // decimation (the plan's cluster size)
    const uint32_t *blank;        // [nstream][blank_words] bitmaps (1 = blanked sample-time)
    long long blank_words;
    const int *blank_any;         // [nstream]

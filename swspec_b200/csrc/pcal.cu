@@ -18,8 +18,9 @@ __device__ __forceinline__ float pc_sample(const PcalArgs &a, int src, long long
 {
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   uint32_t word = __ldg(a.codes + (long long)src * a.code_words + s / SPW);
-   uint32_t code = (word >> (NBIT * (int)(s % SPW))) & MASK;
+   const long long i = s / a.D;
+   uint32_t word = __ldg(a.codes + (long long)src * a.code_words + (s % a.D) * a.wpp + i / SPW);
+   uint32_t code = (word >> (NBIT * (int)(i % SPW))) & MASK;
    float v;
    if (NBIT == 8) v = (float)((int)code * 2 - 255) * (1.0f / 256.0f);
    else if (NBIT == 2) v = (code == 0) ? a.levels.x : (code == 1) ? a.levels.y : (code == 2) ? a.levels.z : a.levels.w;

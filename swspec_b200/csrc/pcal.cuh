@@ -15,8 +15,10 @@ struct PcalJob {
 };
 
 struct PcalArgs {
-   const uint32_t *codes;
+   const uint32_t *codes;        // phase-decimated code arrays (see SpecArgs)
    long long code_words;
+   long long wpp;
+   int D;
    const uint32_t *blank;
    long long blank_words;
    const int *blank_any;

@@ -12,7 +12,8 @@ namespace sws {
    {N_, P_, Q_, T_, R1_, R2_, R3_,                                                                \
     {k_spectra<P_, Q_, T_, R1_, R2_, R3_, 1, MINB_>, k_spectra<P_, Q_, T_, R1_, R2_, R3_, 2, MINB_>,\
      k_spectra<P_, Q_, T_, R1_, R2_, R3_, 8, MINB_>},                                             \
-    spectra_smem<P_, Q_, R1_, R2_, R3_>()}
+    {spectra_smem<P_, Q_, R1_, R2_, R3_, 1>(), spectra_smem<P_, Q_, R1_, R2_, R3_, 2>(),           \
+     spectra_smem<P_, Q_, R1_, R2_, R3_, 8>()}}
 
 static const Plan kPlans[] = {
     SWS_PLAN(65536, 16, 4096, 256, 16, 16, 16, 2),

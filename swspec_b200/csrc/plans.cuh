@@ -11,7 +11,7 @@ struct Plan {
    int N, P, Q, T;
    int R1, R2, R3;
    SpecKernel kern[3];   // nbit 1, 2, 8
-   size_t smem;
+   size_t smem[3];       // dynamic shared memory of each variant
 };
 
 // Returns false when N has no single-launch plan.

@@ -80,41 +80,19 @@ __device__ __forceinline__ float decode_level(uint32_t code, float4 lv)
    }
 }
 
-// Code stream cursor of one source for one job and CTA: sample
-// s0 + rank + P*q sits at bit  off0 + q*P*NBIT  counted from word w0.
-struct Cursor {
-   const uint32_t *w0;
-   int off0;
-   const uint32_t *blank;  // bitmap of the source's stream, or null
-   long long s0;           // s0 + rank (sample of q = 0)
-};
-
-template <int P, int NBIT>
-__device__ __forceinline__ Cursor make_cursor(const SpecArgs &a, int src, long long s0, int rank,
-                                              bool chk_blank, int stream)
+// Asynchronous 4-byte global -> shared copies (cp.async), for prefetching
+// the next job's codes while the current job computes.
+__device__ __forceinline__ void cp_async4(uint32_t smem_addr, const void *gptr)
 {
-   Cursor c;
-   const long long s = s0 + rank;
-   const long long bit = s * NBIT;
-   c.w0 = a.codes + (long long)src * a.code_words + (bit >> 5);
-   c.off0 = (int)(bit & 31);
-   c.blank = chk_blank ? a.blank + (long long)stream * a.blank_words : nullptr;
-   c.s0 = s;
-   return c;
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr), "l"(gptr) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int P, int NBIT>
-__device__ __forceinline__ float cursor_sample(const Cursor &c, int q, float4 lv)
+__device__ __forceinline__ void dsmem_st2(uint32_t addr, float2 v)
 {
-   constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   const int rel = c.off0 + q * (P * NBIT);
-   const uint32_t word = __ldg(c.w0 + (rel >> 5));
-   float v = decode_level<NBIT>((word >> (rel & 31)) & MASK, lv);
-   if (c.blank) {
-      const long long s = c.s0 + (long long)P * q;
-      if ((__ldg(c.blank + (s >> 5)) >> (s & 31)) & 1u) v = 0.0f;
-   }
-   return v;
+   asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};\n" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
 
 // Twiddle table of a pass: tw[(r-1)*Ns + k] = W_{Ns R}^{k r}, k < Ns, 0 < r < R.
@@ -127,14 +105,50 @@ __device__ __forceinline__ void fill_pass_twiddles(float2 *tw, const float2 *__r
    }
 }
 
-// One in-place Stockham pass over the padded shared buffer (FP32).
-template <int Q, int T, int R, int Ns>
-__device__ __forceinline__ void smem_pass(float2 *buf, const float2 *tw)
+// Two-level twiddles for a wide pass: W^{k r} = TA[r][k/16] * TB[r][k%16]
+// with TA = W^{16 (k/16) r}, TB = W^{(k%16) r} (one extra rounding).
+template <int Ns>
+__host__ __device__ constexpr bool two_level_tw() { return Ns >= 64 && Ns % 16 == 0; }
+
+template <int Q, int R, int Ns>
+__host__ __device__ constexpr int pass_tw_entries()
+{
+   return two_level_tw<Ns>() ? (R - 1) * (Ns / 16 + 16) : (R - 1) * Ns;
+}
+
+template <int Q, int R, int Ns>
+__device__ __forceinline__ void fill_pass_twiddles2(float2 *tw, const float2 *__restrict__ twQ, int T)
+{
+   if constexpr (two_level_tw<Ns>()) {
+      constexpr int NA = Ns / 16;
+      for (int i = threadIdx.x; i < (R - 1) * (NA + 16); i += T) {
+         const int r = i / (NA + 16) + 1, x = i % (NA + 16);
+         const int k = x < NA ? 16 * x : x - NA;
+         tw[i] = __ldg(twQ + k * r * (Q / (Ns * R)));
+      }
+   } else {
+      fill_pass_twiddles<Q, R, Ns>(tw, twQ, T);
+   }
+}
+
+template <int R, int Ns>
+__device__ __forceinline__ float2 pass_tw(const float2 *tw, int r, int k)
+{
+   if constexpr (two_level_tw<Ns>()) {
+      constexpr int NA = Ns / 16;
+      const float2 *row = tw + (r - 1) * (NA + 16);
+      return cmul(row[k >> 4], row[NA + (k & 15)]);
+   } else {
+      return tw[(r - 1) * Ns + k];
+   }
+}
+
+// Load + twiddle + radix-R DFT of one Stockham pass into registers.
+template <int Q, int T, int R, int Ns, int BPT>
+__device__ __forceinline__ void pass_compute(const float2 *buf, const float2 *tw, float2 (&v)[BPT][R])
 {
    constexpr int nb = Q / R;
-   constexpr int BPT = (nb + T - 1) / T;
    const int tid = threadIdx.x;
-   float2 v[BPT][R];
 #pragma unroll
    for (int b = 0; b < BPT; b++) {
       const int j = tid + b * T;
@@ -143,12 +157,23 @@ __device__ __forceinline__ void smem_pass(float2 *buf, const float2 *tw)
 #pragma unroll
          for (int r = 0; r < R; r++) {
             float2 x = buf[pidx(j + r * nb)];
-            if (r > 0) x = cmul(x, tw[(r - 1) * Ns + k]);
+            if (r > 0) x = cmul(x, pass_tw<R, Ns>(tw, r, k));
             v[b][r] = x;
          }
          DFT<R>::run(v[b]);
       }
    }
+}
+
+// One in-place Stockham pass over the padded shared buffer (FP32).
+template <int Q, int T, int R, int Ns>
+__device__ __forceinline__ void smem_pass(float2 *buf, const float2 *tw)
+{
+   constexpr int nb = Q / R;
+   constexpr int BPT = (nb + T - 1) / T;
+   const int tid = threadIdx.x;
+   float2 v[BPT][R];
+   pass_compute<Q, T, R, Ns, BPT>(buf, tw, v);
    __syncthreads();
 #pragma unroll
    for (int b = 0; b < BPT; b++) {
@@ -183,32 +208,43 @@ __device__ __forceinline__ void acc_bin(float *acc4, int mode, float2 zk, float2
 }
 
 // Shared memory footprint of a plan (bytes).
-template <int P, int Q, int R1, int R2, int R3>
+template <int P, int Q, int R1, int R2, int R3, int NBIT>
 __host__ __device__ constexpr size_t spectra_smem()
 {
-   return (size_t)(Q + Q / 16) * 8                          // buffer
-          + (size_t)Q * 4                                   // window slice
-          + (size_t)(R2 - 1) * R1 * 8                       // pass-2 twiddles
-          + (size_t)(R3 > 1 ? (R3 - 1) * R1 * R2 : 0) * 8   // pass-3 twiddles
-          + (size_t)(P - 1) * (Q / (2 * P)) * 8;            // cluster twiddles per k1-pair
+   return (size_t)(Q + Q / 16) * 8                               // FFT buffer
+          + (size_t)P * (Q / P) * 8                              // receive buffer [P][sides]
+          + (size_t)Q * 4                                        // window slice
+          + (size_t)pass_tw_entries<Q, R2, R1>() * 8             // pass-2 twiddles
+          + (size_t)pass_tw_entries<Q, R3, R1 * R2>() * 8        // pass-3 twiddles
+          + (size_t)(P > 1 ? (P - 1) * (Q / (2 * P)) : 1) * 8    // cluster twiddles per k1-pair
+          + (size_t)2 * 2 * (Q / (32 / NBIT) + 2) * 4;           // code staging [2 jobs][2 sources]
 }
 
 template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB>
 __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 {
    static_assert(R1 * R2 * R3 == Q, "radix plan must multiply to Q");
+   static_assert(R3 > 1, "three passes");
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
    constexpr int UC = Q / (2 * P);          // k1-pairs per CTA
    constexpr int SIDES = 2 * UC;            // lo/hi sides per CTA
    constexpr int SPT = (SIDES + T - 1) / T; // sides per thread
    constexpr int HB = (P == 1) ? 1 : P / 2; // bins per side (regular)
    constexpr int NB = HB + 1;               // + the lo special's extra bin
    constexpr int NX = (P == 1) ? 1 : P / 2; // values exchanged with the partner lane
+   constexpr int NW = Q / SPW + 2;          // staged code words per source and job
+   constexpr int NS3 = R1 * R2;             // span of the last pass
+   constexpr int nb3 = Q / R3;
+   constexpr int BPT3 = (nb3 + T - 1) / T;
    extern __shared__ float4 smem_raw[];
    float2 *buf = reinterpret_cast<float2 *>(smem_raw);
-   float *wsl = reinterpret_cast<float *>(buf + (Q + Q / 16));
+   float2 *rbuf = buf + (Q + Q / 16);
+   float *wsl = reinterpret_cast<float *>(rbuf + P * SIDES);
    float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
-   float2 *tw3 = tw2 + (R2 - 1) * R1;
-   float2 *twc = tw3 + (R3 > 1 ? (R3 - 1) * R1 * R2 : 0);
+   float2 *tw3 = tw2 + pass_tw_entries<Q, R2, R1>();
+   float2 *twc = tw3 + pass_tw_entries<Q, R3, NS3>();
+   uint32_t *stage = reinterpret_cast<uint32_t *>(twc + (P > 1 ? (P - 1) * UC : 1));
 
    cg::cluster_group cluster = cg::this_cluster();
    const int rank = (int)cluster.block_rank();
@@ -219,44 +255,84 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 
    // ---- per-CTA constant tables ----
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
-   if constexpr (R2 > 1) fill_pass_twiddles<Q, R2, R1>(tw2, a.twQ, T);
-   if constexpr (R3 > 1) fill_pass_twiddles<Q, R3, R1 * R2>(tw3, a.twQ, T);
-   // side s of this CTA: pair index u = rank*UC + s/2, lo side if s even;
-   // twc[(p-1)*UC + s/2] = W_N^{p u}, read by both sides of a pair
+   fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
+   fill_pass_twiddles2<Q, R3, NS3>(tw3, a.twQ, T);
+   // twc[(p-1)*UC + u_local] = W_N^{p u}, read by both sides of pair u
    for (int i = tid; i < (P - 1) * UC; i += T) {
       const int p = i / UC + 1, uu = i % UC;
       twc[i] = __ldg(a.twN + (long long)p * (rank * UC + uu));
    }
-   __syncthreads();
 
-   const uint32_t buf_addr = (uint32_t)__cvta_generic_to_shared(buf);
+   const uint32_t rbuf_addr = (uint32_t)__cvta_generic_to_shared(rbuf);
+   const uint32_t stage_addr = (uint32_t)__cvta_generic_to_shared(stage);
 
-   cluster_arrive();  // pairs with the wait before the first job's stores
+   // ---- job sequence of this cluster: items cid, cid+ncl, ...; jobs 0..nfr-1 ----
+   struct JobPos {
+      int it, j;
+   };
+   auto job_valid = [&](const JobPos &jp) { return jp.it < a.nitems; };
+   auto next_job = [&](JobPos jp) {
+      if (jp.j + 1 < a.items[jp.it].nfr) return JobPos{jp.it, jp.j + 1};
+      return JobPos{jp.it + ncl, 0};
+   };
+   // prefetch the codes of job jp into staging slot `slot`
+   auto prefetch = [&](const JobPos &jp, int slot) {
+      const Item item = a.items[jp.it];
+      const bool has_b = item.mode != MODE_SINGLE;
+      const long long sa = item.start + (long long)jp.j * item.step;
+      const long long sb = (item.mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
+#pragma unroll
+      for (int src = 0; src < 2; src++) {
+         if (src == 1 && !has_b) break;
+         const int code = src == 0 ? item.src_a : (item.mode == MODE_AUTOSUM ? item.src_a : item.src_b);
+         const long long s0 = (src == 0 ? sa : sb) + rank;
+         const long long i0 = s0 / P;
+         const int ph = (int)(s0 - i0 * P);
+         const uint32_t *g = a.codes + (long long)code * a.code_words + (long long)ph * a.wpp + i0 / SPW;
+         const int nw = (int)(((i0 % SPW) + Q - 1) / SPW) + 1;
+         const uint32_t dst = stage_addr + 4u * (uint32_t)((slot * 2 + src) * NW);
+         for (int w = tid; w < nw; w += T) cp_async4(dst + 4u * w, g + w);
+      }
+   };
 
-   for (int it = cid; it < a.nitems; it += ncl) {
-      const Item item = a.items[it];
+   JobPos cur{cid, 0};
+   if (job_valid(cur)) prefetch(cur, 0);
+   cp_async_commit();
+   __syncthreads();      // tables visible
+   cluster_arrive();     // pairs with the wait before the first job's pushes
+
+   float acc[SPT][NB][4];
+#pragma unroll
+   for (int u = 0; u < SPT; u++)
+#pragma unroll
+      for (int x = 0; x < NB; x++)
+#pragma unroll
+         for (int c = 0; c < 4; c++) acc[u][x][c] = 0.0f;
+
+   int n = 0;  // job counter (staging slot parity)
+   while (job_valid(cur)) {
+      const Item item = a.items[cur.it];
       const int mode = item.mode;
       const bool has_b = mode != MODE_SINGLE;
-      const int src_b = (mode == MODE_AUTOSUM) ? item.src_a : item.src_b;
-      const int stream_a = a.code_stream[item.src_a];
-      const int stream_b = has_b ? a.code_stream[src_b] : 0;
-      const bool blank_a = a.blank_any[stream_a] != 0;
-      const bool blank_b = has_b && a.blank_any[stream_b] != 0;
-      float acc[SPT][NB][4];
-#pragma unroll
-      for (int u = 0; u < SPT; u++)
-#pragma unroll
-         for (int s = 0; s < NB; s++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) acc[u][s][c] = 0.0f;
+      const JobPos nxt = next_job(cur);
+      if (job_valid(nxt)) prefetch(nxt, (n + 1) & 1);
+      cp_async_commit();
+      cp_async_wait1();     // this job's codes have landed
+      __syncthreads();
 
-      for (int j = 0; j < item.nfr; j++) {
-         const long long sa = item.start + (long long)j * item.step;
+      // ---- pass 1 (Ns = 1): decode + window + radix-R1 ----
+      {
+         const long long sa = item.start + (long long)cur.j * item.step;
          const long long sb = (mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
-         const Cursor ca = make_cursor<P, NBIT>(a, item.src_a, sa, rank, blank_a, stream_a);
-         const Cursor cb = make_cursor<P, NBIT>(a, has_b ? src_b : item.src_a, sb, rank, blank_b,
-                                                stream_b);
-         // ---- pass 1 (Ns = 1): decode + window + radix-R1, in registers ----
+         const int offa = (int)(((sa + rank) / P) % SPW);
+         const int offb = (int)(((sb + rank) / P) % SPW);
+         const uint32_t *sta = stage + (n & 1) * 2 * NW;
+         const uint32_t *stb = sta + NW;
+         const int stream_a = a.code_stream[item.src_a];
+         const int src_b = (mode == MODE_AUTOSUM) ? item.src_a : item.src_b;
+         const int stream_b = has_b ? a.code_stream[src_b] : 0;
+         const uint32_t *blank_a = a.blank_any[stream_a] ? a.blank + (long long)stream_a * a.blank_words : nullptr;
+         const uint32_t *blank_b = (has_b && a.blank_any[stream_b]) ? a.blank + (long long)stream_b * a.blank_words : nullptr;
          constexpr int nb1 = Q / R1;
          constexpr int BPT1 = (nb1 + T - 1) / T;
          float2 v[BPT1][R1];
@@ -268,14 +344,26 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                for (int r = 0; r < R1; r++) {
                   const int q = jj + r * nb1;
                   const float w = wsl[q];
-                  const float xa = cursor_sample<P, NBIT>(ca, q, a.levels);
-                  const float xb = has_b ? cursor_sample<P, NBIT>(cb, q, a.levels) : 0.0f;
+                  const int ia = offa + q;
+                  float xa = decode_level<NBIT>((sta[ia / SPW] >> (NBIT * (ia % SPW))) & MASK, a.levels);
+                  if (blank_a) {
+                     const long long smp = sa + rank + (long long)P * q;
+                     if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) xa = 0.0f;
+                  }
+                  float xb = 0.0f;
+                  if (has_b) {
+                     const int ib = offb + q;
+                     xb = decode_level<NBIT>((stb[ib / SPW] >> (NBIT * (ib % SPW))) & MASK, a.levels);
+                     if (blank_b) {
+                        const long long smp = sb + rank + (long long)P * q;
+                        if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) xb = 0.0f;
+                     }
+                  }
                   v[b][r] = make_float2(xa * w, xb * w);
                }
                DFT<R1>::run(v[b]);
             }
          }
-         cluster_wait();  // every remote reader of buf from the previous job is done
 #pragma unroll
          for (int b = 0; b < BPT1; b++) {
             const int jj = tid + b * T;
@@ -284,119 +372,148 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                for (int r = 0; r < R1; r++) buf[pidx(jj * R1 + r)] = v[b][r];
             }
          }
-         __syncthreads();
-         if constexpr (R2 > 1) smem_pass<Q, T, R2, R1>(buf, tw2);
-         if constexpr (R3 > 1) smem_pass<Q, T, R3, R1 * R2>(buf, tw3);
-         cluster.sync();  // all CTAs' F_p complete
-         // ---- cluster radix-P stage + pair separation ----
+      }
+      __syncthreads();
+      // ---- pass 2 in shared memory, pass 3 into registers ----
+      smem_pass<Q, T, R2, R1>(buf, tw2);
+      float2 v3[BPT3][R3];
+      pass_compute<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
+
+      // ---- push F_rank[k1] to the CTA that owns pair min(k1, Q-k1) ----
+      cluster_wait();  // owners have finished reading their receive buffers
 #pragma unroll
-         for (int si = 0; si < SPT; si++) {
-            const int s = tid + si * T;  // side index within the CTA
-            const bool active = (SIDES % T == 0) || s < SIDES;
-            const bool hi = (s & 1) != 0;
-            const int u = rank * UC + (s >> 1);
-            float2 z[P];
-            if (active) {
-               if (u == 0) {
-                  // lo: k1 = 0 (no twiddle); hi: k1 = Q/2, W_N^{p Q/2} = W_{2P}^p
-                  const int k1 = hi ? Q / 2 : 0;
-                  const uint32_t off = buf_addr + 8u * (uint32_t)pidx(k1);
+      for (int b = 0; b < BPT3; b++) {
+         const int j = tid + b * T;
+         if (nb3 % T == 0 || j < nb3) {
 #pragma unroll
-                  for (int p = 0; p < P; p++) z[p] = dsmem_ld2(dsmem_addr(off, p));
-                  if (hi) {
-                     static_for<1, P>([&](auto I) {
-                        constexpr int p = decltype(I)::value;
-                        z[p] = twmul<p, 2 * P>(z[p]);
-                     });
-                  }
-               } else {
-                  const int k1 = hi ? Q - u : u;
-                  const uint32_t off = buf_addr + 8u * (uint32_t)pidx(k1);
-#pragma unroll
-                  for (int p = 0; p < P; p++) z[p] = dsmem_ld2(dsmem_addr(off, p));
-#pragma unroll
-                  for (int p = 1; p < P; p++) {
-                     const float2 w = twc[(p - 1) * UC + (s >> 1)];
-                     z[p] = hi ? cmulconj(z[p], w) : cmul(z[p], w);
-                  }
-                  if (hi) {
-                     // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
-                     static_for<1, P>([&](auto I) {
-                        constexpr int p = decltype(I)::value;
-                        z[p] = twmul<p, P>(z[p]);
-                     });
-                  }
-               }
-               DFT<P>::run(z);
-            } else {
-#pragma unroll
-               for (int p = 0; p < P; p++) z[p] = make_float2(0.0f, 0.0f);
-            }
-            // swap the upper half with the partner side (lane ^ 1)
-            float2 rv[NX];
-#pragma unroll
-            for (int i = 0; i < NX; i++) {
-               const int src = (P == 1) ? 0 : P / 2 + i;
-               rv[i].x = __shfl_xor_sync(0xffffffffu, z[src].x, 1);
-               rv[i].y = __shfl_xor_sync(0xffffffffu, z[src].y, 1);
-            }
-            if (active) {
-               if (u == 0) {
-                  if constexpr (P == 1) {
-                     acc_bin(acc[si][0], mode, z[0], z[0]);
-                  } else if (!hi) {
-#pragma unroll
-                     for (int k2 = 0; k2 <= P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[(P - k2) % P]);
-                  } else {
-#pragma unroll
-                     for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[P - 1 - k2]);
-                  }
-               } else {
-                  if constexpr (P == 1) {
-                     if (!hi) acc_bin(acc[si][0], mode, z[0], rv[0]);
-                  } else {
-#pragma unroll
-                     for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], rv[P / 2 - 1 - k2]);
-                  }
-               }
+            for (int r = 0; r < R3; r++) {
+               const int k1 = j + r * NS3;
+               int u, hi;
+               if (k1 == 0) { u = 0; hi = 0; }
+               else if (2 * k1 == Q) { u = 0; hi = 1; }
+               else if (2 * k1 < Q) { u = k1; hi = 0; }
+               else { u = Q - k1; hi = 1; }
+               const int owner = u / UC;
+               const int side = 2 * (u - owner * UC) + hi;
+               dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + side), owner), v3[b][r]);
             }
          }
-         cluster_arrive();  // this CTA has finished reading remote buffers
       }
-      // ---- write this item's partial sums: partial[it][prod][bin] ----
-      float *part = a.partial + (long long)it * 4 * S;
-      const int nprod = (mode == MODE_XPOL) ? 4 : 1;
+      cluster.sync();  // every CTA's pushes have landed
+
+      // ---- radix-P stage across the cluster + pair separation ----
 #pragma unroll
       for (int si = 0; si < SPT; si++) {
-         const int s = tid + si * T;
-         if (!((SIDES % T == 0) || s < SIDES)) continue;
+         const int s = tid + si * T;  // side index within the CTA
+         const bool active = (SIDES % T == 0) || s < SIDES;
          const bool hi = (s & 1) != 0;
          const int u = rank * UC + (s >> 1);
-         for (int c = 0; c < nprod; c++) {
-            float *pc = part + (long long)c * S;
+         float2 z[P];
+         if (active) {
+#pragma unroll
+            for (int p = 0; p < P; p++) z[p] = rbuf[p * SIDES + s];
+            if (u == 0) {
+               // lo: k1 = 0 (no twiddle); hi: k1 = Q/2, W_N^{p Q/2} = W_{2P}^p
+               if (hi) {
+                  static_for<1, P>([&](auto I) {
+                     constexpr int p = decltype(I)::value;
+                     z[p] = twmul<p, 2 * P>(z[p]);
+                  });
+               }
+            } else {
+#pragma unroll
+               for (int p = 1; p < P; p++) {
+                  const float2 w = twc[(p - 1) * UC + (s >> 1)];
+                  z[p] = hi ? cmulconj(z[p], w) : cmul(z[p], w);
+               }
+               if (hi) {
+                  // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
+                  static_for<1, P>([&](auto I) {
+                     constexpr int p = decltype(I)::value;
+                     z[p] = twmul<p, P>(z[p]);
+                  });
+               }
+            }
+            DFT<P>::run(z);
+         } else {
+#pragma unroll
+            for (int p = 0; p < P; p++) z[p] = make_float2(0.0f, 0.0f);
+         }
+         // swap the upper half with the partner side (lane ^ 1)
+         float2 rv[NX];
+#pragma unroll
+         for (int i = 0; i < NX; i++) {
+            const int src = (P == 1) ? 0 : P / 2 + i;
+            rv[i].x = __shfl_xor_sync(0xffffffffu, z[src].x, 1);
+            rv[i].y = __shfl_xor_sync(0xffffffffu, z[src].y, 1);
+         }
+         if (active) {
             if (u == 0) {
                if constexpr (P == 1) {
-                  pc[hi ? Q / 2 : 0] = acc[si][0][c];
+                  acc_bin(acc[si][0], mode, z[0], z[0]);
                } else if (!hi) {
 #pragma unroll
-                  for (int k2 = 0; k2 <= P / 2; k2++) pc[Q * k2] = acc[si][k2][c];
+                  for (int k2 = 0; k2 <= P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[(P - k2) % P]);
                } else {
 #pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++) pc[Q / 2 + Q * k2] = acc[si][k2][c];
+                  for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], z[P - 1 - k2]);
                }
             } else {
                if constexpr (P == 1) {
-                  if (!hi) pc[u] = acc[si][0][c];
+                  if (!hi) acc_bin(acc[si][0], mode, z[0], rv[0]);
                } else {
-                  const int k1 = hi ? Q - u : u;
 #pragma unroll
-                  for (int k2 = 0; k2 < P / 2; k2++) pc[k1 + Q * k2] = acc[si][k2][c];
+                  for (int k2 = 0; k2 < P / 2; k2++) acc_bin(acc[si][k2], mode, z[k2], rv[P / 2 - 1 - k2]);
                }
             }
          }
       }
+      cluster_arrive();  // this CTA has finished reading its receive buffer
+
+      // ---- end of a work item: write partial sums, reset accumulators ----
+      if (cur.j + 1 == item.nfr) {
+         float *part = a.partial + (long long)cur.it * 4 * S;
+         const int nprod = (mode == MODE_XPOL) ? 4 : 1;
+#pragma unroll
+         for (int si = 0; si < SPT; si++) {
+            const int s = tid + si * T;
+            if ((SIDES % T == 0) || s < SIDES) {
+               const bool hi = (s & 1) != 0;
+               const int u = rank * UC + (s >> 1);
+               for (int c = 0; c < nprod; c++) {
+                  float *pc = part + (long long)c * S;
+                  if (u == 0) {
+                     if constexpr (P == 1) {
+                        pc[hi ? Q / 2 : 0] = acc[si][0][c];
+                     } else if (!hi) {
+#pragma unroll
+                        for (int k2 = 0; k2 <= P / 2; k2++) pc[Q * k2] = acc[si][k2][c];
+                     } else {
+#pragma unroll
+                        for (int k2 = 0; k2 < P / 2; k2++) pc[Q / 2 + Q * k2] = acc[si][k2][c];
+                     }
+                  } else {
+                     if constexpr (P == 1) {
+                        if (!hi) pc[u] = acc[si][0][c];
+                     } else {
+                        const int k1 = hi ? Q - u : u;
+#pragma unroll
+                        for (int k2 = 0; k2 < P / 2; k2++) pc[k1 + Q * k2] = acc[si][k2][c];
+                     }
+                  }
+               }
+            }
+#pragma unroll
+            for (int x = 0; x < NB; x++)
+#pragma unroll
+               for (int c = 0; c < 4; c++) acc[si][x][c] = 0.0f;
+         }
+      }
+      cur = nxt;
+      n++;
    }
-   cluster_wait();  // pairs with the last arrive: no remote reader is left
+   cp_async_wait0();
+   cluster_wait();  // pairs with the last arrive: no one still reads a receive buffer
 }
 
 // K3: out[o][k] = sum over entries of scale * partial[item][prod][k], Kahan.

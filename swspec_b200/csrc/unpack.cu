@@ -103,17 +103,25 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
    if (!(vs <= 0 && ve >= s.payload_bytes)) atomicOr(blank_any, 1);
 }
 
-// Corner turn.  Thread w writes code word w (samples [w*SPW, (w+1)*SPW)) of
-// each requested channel; blank bits go to `blank` (pre-zeroed).
+// Corner turn into a phase-decimated code layout.  For decimation D (the
+// FFT plan's cluster size), sample s of a channel is stored in phase array
+// s % D at index s / D, SPW = 32/NBIT codes per 32-bit word:
+//   codes[c * D * wpp + (s % D) * wpp + (s / D) / SPW], bits NBIT * ((s / D) % SPW).
+// A CTA of the FFT cluster that owns residue p then reads its samples as one
+// contiguous run.  Thread t writes word t / D of phase t % D for every
+// requested channel; each payload word is read by exactly one thread.
+// Blank bits (1 per sample-time, standard order) go to `blank` (pre-zeroed).
 template <int NBIT>
 __global__ void k_unpack_codes(StreamIn s, long long nsamp, const int *chans, int nch,
-                               uint32_t *codes, long long code_words, const int2 *valid,
+                               uint32_t *codes, int D, long long wpp, const int2 *valid,
                                uint32_t *blank)
 {
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (w >= code_words) return;
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= (long long)D * wpp) return;
+   const int ph = (int)(t % D);
+   const long long iw = t / D;
    const long long stride = (long long)s.nchan * NBIT;
    const int nb = s.payload_bytes;
    uint32_t acc[16];
@@ -121,19 +129,20 @@ __global__ void k_unpack_codes(StreamIn s, long long nsamp, const int *chans, in
    int cn = min(16, nch - c0);
 #pragma unroll
    for (int c = 0; c < 16; c++) acc[c] = 0u;
-   uint32_t blankbits = 0u;
    long long cached_idx = -1;
    uint32_t cached = 0u;
-   for (int i = 0; i < SPW; i++) {
-      long long t = w * SPW + i;
-      if (t >= nsamp) break;
-      long long bit0 = t * stride;
+   for (int k = 0; k < SPW; k++) {
+      const long long smp = (iw * SPW + k) * D + ph;
+      if (smp >= nsamp) break;
+      long long bit0 = smp * stride;
       long long v0 = s.grid_offset + (bit0 >> 3);
       long long f = v0 / nb;
       int o = (int)(v0 - f * nb);
       int2 vr = valid[f];
-      bool ok = (o >= vr.x) && (o < vr.y);
-      if (!ok) { blankbits |= 1u << i; continue; }
+      if (!((o >= vr.x) && (o < vr.y))) {
+         if (blockIdx.y == 0) atomicOr(&blank[smp >> 5], 1u << (smp & 31));
+         continue;
+      }
 #pragma unroll
       for (int c = 0; c < 16; c++) {
          if (c < cn) {
@@ -145,23 +154,14 @@ __global__ void k_unpack_codes(StreamIn s, long long nsamp, const int *chans, in
                cached = *reinterpret_cast<const uint32_t *>(s.data + payload_addr(s, s.grid_offset + 4 * widx));
                cached_idx = widx;
             }
-            uint32_t code = (cached >> (bit & 31)) & MASK;
-            acc[c] |= code << (NBIT * i);
+            acc[c] |= ((cached >> (bit & 31)) & MASK) << (NBIT * k);
          }
       }
    }
+   const long long code_words = (long long)D * wpp;
 #pragma unroll
    for (int c = 0; c < 16; c++)
-      if (c < cn) codes[(long long)(c0 + c) * code_words + w] = acc[c];
-   if (blankbits && blockIdx.y == 0) {
-      // bit index t = w*SPW + i
-      long long t0 = w * SPW;
-      for (int i = 0; i < SPW; i++)
-         if (blankbits & (1u << i)) {
-            long long t = t0 + i;
-            atomicOr(&blank[t >> 5], 1u << (t & 31));
-         }
-   }
+      if (c < cn) codes[(long long)(c0 + c) * code_words + (long long)ph * wpp + iw] = acc[c];
 }
 
 // Decoded float samples of one channel (test path; same rules as above).
@@ -190,15 +190,15 @@ __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 lev
 }
 
 void launch_unpack_codes(int nbit, dim3 grid, int block, cudaStream_t st, StreamIn s,
-                         long long nsamp, const int *chans, int nch, uint32_t *codes,
-                         long long code_words, const int2 *valid, uint32_t *blank)
+                         long long nsamp, const int *chans, int nch, uint32_t *codes, int D,
+                         long long wpp, const int2 *valid, uint32_t *blank)
 {
    if (nbit == 1)
-      k_unpack_codes<1><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, code_words, valid, blank);
+      k_unpack_codes<1><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
    else if (nbit == 2)
-      k_unpack_codes<2><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, code_words, valid, blank);
+      k_unpack_codes<2><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
    else
-      k_unpack_codes<8><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, code_words, valid, blank);
+      k_unpack_codes<8><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
 }
 
 }  // namespace sws
