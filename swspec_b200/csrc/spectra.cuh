@@ -143,6 +143,60 @@ __device__ __forceinline__ float2 pass_tw(const float2 *tw, int r, int k)
    }
 }
 
+// Twiddles by powers: with base[i] = W^{2^i k} (i < log2 R), x[r] *= W^{r k}
+// where W^{r k} is built from the bases of r's set bits (at most
+// popcount(r) - 1 products, one rounding each).
+__host__ __device__ constexpr int hibit(int r) { return r >= 16 ? 16 : r >= 8 ? 8 : r >= 4 ? 4 : r >= 2 ? 2 : 1; }
+__host__ __device__ constexpr int ilog2c(int r) { return r >= 16 ? 4 : r >= 8 ? 3 : r >= 4 ? 2 : r >= 2 ? 1 : 0; }
+__host__ __device__ constexpr int nbases(int R) { return ilog2c(R - 1) + 1; }
+
+template <int R>
+__device__ __forceinline__ void twiddle_by_powers(float2 *x, const float2 *base)
+{
+   float2 w[R];
+   static_for<1, R>([&](auto I) {
+      constexpr int r = decltype(I)::value;
+      constexpr int hb = hibit(r);
+      if constexpr (r == hb) w[r] = base[ilog2c(hb)];
+      else w[r] = cmul(w[r - hb], base[ilog2c(hb)]);
+      x[r] = cmul(x[r], w[r]);
+   });
+}
+
+// Base table of a pass: tb[i*Ns + k] = W_{Ns R}^{2^i k}.
+template <int Q, int R, int Ns>
+__device__ __forceinline__ void fill_pass_bases(float2 *tb, const float2 *__restrict__ twQ, int T)
+{
+   constexpr int NBASE = nbases(R);
+   for (int idx = threadIdx.x; idx < NBASE * Ns; idx += T) {
+      const int i = idx / Ns, k = idx % Ns;
+      tb[idx] = __ldg(twQ + ((long long)k << i) % (Ns * R) * (Q / (Ns * R)));
+   }
+}
+
+// Load + twiddle (by powers) + radix-R DFT of one Stockham pass into registers.
+template <int Q, int T, int R, int Ns, int BPT>
+__device__ __forceinline__ void pass_compute_pw(const float2 *buf, const float2 *tb, float2 (&v)[BPT][R])
+{
+   constexpr int nb = Q / R;
+   constexpr int NBASE = nbases(R);
+   const int tid = threadIdx.x;
+#pragma unroll
+   for (int b = 0; b < BPT; b++) {
+      const int j = tid + b * T;
+      if (nb % T == 0 || j < nb) {
+         const int k = j % Ns;
+#pragma unroll
+         for (int r = 0; r < R; r++) v[b][r] = buf[pidx(j + r * nb)];
+         float2 base[NBASE];
+#pragma unroll
+         for (int i = 0; i < NBASE; i++) base[i] = tb[i * Ns + k];
+         twiddle_by_powers<R>(v[b], base);
+         DFT<R>::run(v[b]);
+      }
+   }
+}
+
 // Load + twiddle + radix-R DFT of one Stockham pass into registers.
 template <int Q, int T, int R, int Ns, int BPT>
 __device__ __forceinline__ void pass_compute(const float2 *buf, const float2 *tw, float2 (&v)[BPT][R])
@@ -207,6 +261,16 @@ __device__ __forceinline__ void acc_bin(float *acc4, int mode, float2 zk, float2
    }
 }
 
+// Staged code words per source and job (see PERM in k_spectra); 256-thread
+// plans use the permuted layout whenever Q/R1 <= 256.
+template <int Q, int R1, int NBIT>
+__host__ __device__ constexpr int stage_slots()
+{
+   constexpr int SPW = 32 / NBIT, NW = Q / SPW + 2, nb1 = Q / R1;
+   constexpr int ST = (nb1 % SPW == 0) ? nb1 / SPW : 1;
+   return (nb1 % SPW == 0) ? ST * ((((NW + ST - 1) / ST) + 3) / 4) * 4 : NW;
+}
+
 // Shared memory footprint of a plan (bytes).
 template <int P, int Q, int R1, int R2, int R3, int NBIT>
 __host__ __device__ constexpr size_t spectra_smem()
@@ -215,9 +279,9 @@ __host__ __device__ constexpr size_t spectra_smem()
           + (size_t)P * (Q / P) * 8                              // receive buffer [P][sides]
           + (size_t)Q * 4                                        // window slice
           + (size_t)pass_tw_entries<Q, R2, R1>() * 8             // pass-2 twiddles
-          + (size_t)pass_tw_entries<Q, R3, R1 * R2>() * 8        // pass-3 twiddles
+          + (size_t)nbases(R3) * R1 * R2 * 8                     // pass-3 twiddle bases
           + (size_t)(P > 1 ? (P - 1) * (Q / (2 * P)) : 1) * 8    // cluster twiddles per k1-pair
-          + (size_t)2 * 2 * (Q / (32 / NBIT) + 2) * 4;           // code staging [2 jobs][2 sources]
+          + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4 + 16; // code staging [2 jobs][2 sources]
 }
 
 template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB>
@@ -234,6 +298,14 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    constexpr int NB = HB + 1;               // + the lo special's extra bin
    constexpr int NX = (P == 1) ? 1 : P / 2; // values exchanged with the partner lane
    constexpr int NW = Q / SPW + 2;          // staged code words per source and job
+   // Pass 1 thread jj needs code words g + r*ST (g = (off + jj)/SPW, r < R1,
+   // ST = (Q/R1)/SPW).  With PERM the prefetch stores word w at slot
+   // (w % ST)*GS + w/ST, so those R1 words are contiguous (128-bit loads).
+   constexpr int nb1c = Q / R1;
+   constexpr bool PERM = (nb1c % SPW == 0) && (R1 % 4 == 0) && (nb1c <= T);
+   constexpr int ST = PERM ? nb1c / SPW : 1;
+   constexpr int GS = PERM ? (((NW + ST - 1) / ST + 3) / 4) * 4 : NW;
+   constexpr int NSLOT = PERM ? ST * GS : NW;  // staged words per source and job
    constexpr int NS3 = R1 * R2;             // span of the last pass
    constexpr int nb3 = Q / R3;
    constexpr int BPT3 = (nb3 + T - 1) / T;
@@ -243,8 +315,10 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    float *wsl = reinterpret_cast<float *>(rbuf + P * SIDES);
    float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
    float2 *tw3 = tw2 + pass_tw_entries<Q, R2, R1>();
-   float2 *twc = tw3 + pass_tw_entries<Q, R3, NS3>();
-   uint32_t *stage = reinterpret_cast<uint32_t *>(twc + (P > 1 ? (P - 1) * UC : 1));
+   float2 *twc = tw3 + nbases(R3) * NS3;
+   // staging must be 16-byte aligned for the 128-bit reads
+   uint32_t *stage = reinterpret_cast<uint32_t *>(
+       (reinterpret_cast<uintptr_t>(twc + (P > 1 ? (P - 1) * UC : 1)) + 15) & ~(uintptr_t)15);
 
    cg::cluster_group cluster = cg::this_cluster();
    const int rank = (int)cluster.block_rank();
@@ -256,7 +330,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    // ---- per-CTA constant tables ----
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
    fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
-   fill_pass_twiddles2<Q, R3, NS3>(tw3, a.twQ, T);
+   fill_pass_bases<Q, R3, NS3>(tw3, a.twQ, T);
    // twc[(p-1)*UC + u_local] = W_N^{p u}, read by both sides of pair u
    for (int i = tid; i < (P - 1) * UC; i += T) {
       const int p = i / UC + 1, uu = i % UC;
@@ -290,8 +364,11 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          const int ph = (int)(s0 - i0 * P);
          const uint32_t *g = a.codes + (long long)code * a.code_words + (long long)ph * a.wpp + i0 / SPW;
          const int nw = (int)(((i0 % SPW) + Q - 1) / SPW) + 1;
-         const uint32_t dst = stage_addr + 4u * (uint32_t)((slot * 2 + src) * NW);
-         for (int w = tid; w < nw; w += T) cp_async4(dst + 4u * w, g + w);
+         const uint32_t dst = stage_addr + 4u * (uint32_t)((slot * 2 + src) * NSLOT);
+         for (int w = tid; w < nw; w += T) {
+            const int sl = PERM ? (w % ST) * GS + w / ST : w;
+            cp_async4(dst + 4u * sl, g + w);
+         }
       }
    };
 
@@ -326,8 +403,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          const long long sb = (mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
          const int offa = (int)(((sa + rank) / P) % SPW);
          const int offb = (int)(((sb + rank) / P) % SPW);
-         const uint32_t *sta = stage + (n & 1) * 2 * NW;
-         const uint32_t *stb = sta + NW;
+         const uint32_t *sta = stage + (n & 1) * 2 * NSLOT;
+         const uint32_t *stb = sta + NSLOT;
          const int stream_a = a.code_stream[item.src_a];
          const int src_b = (mode == MODE_AUTOSUM) ? item.src_a : item.src_b;
          const int stream_b = has_b ? a.code_stream[src_b] : 0;
@@ -340,12 +417,41 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          for (int b = 0; b < BPT1; b++) {
             const int jj = tid + b * T;
             if (nb1 % T == 0 || jj < nb1) {
+               uint32_t wa[R1], wb[R1];
+               if constexpr (PERM) {
+                  // this thread's R1 words of each source, contiguous after the permutation
+                  const int ga = (offa + jj) / SPW, gb = (offb + jj) / SPW;
+                  const int sa0 = (ga % ST) * GS + ga / ST, sb0 = (gb % ST) * GS + gb / ST;
+                  if ((sa0 & 3) == 0) {
+#pragma unroll
+                     for (int r = 0; r < R1; r += 4) {
+                        const uint4 t4 = *reinterpret_cast<const uint4 *>(sta + sa0 + r);
+                        wa[r] = t4.x; wa[r + 1] = t4.y; wa[r + 2] = t4.z; wa[r + 3] = t4.w;
+                     }
+                  } else {
+#pragma unroll
+                     for (int r = 0; r < R1; r++) wa[r] = sta[sa0 + r];
+                  }
+                  if (has_b) {
+                     if ((sb0 & 3) == 0) {
+#pragma unroll
+                        for (int r = 0; r < R1; r += 4) {
+                           const uint4 t4 = *reinterpret_cast<const uint4 *>(stb + sb0 + r);
+                           wb[r] = t4.x; wb[r + 1] = t4.y; wb[r + 2] = t4.z; wb[r + 3] = t4.w;
+                        }
+                     } else {
+#pragma unroll
+                        for (int r = 0; r < R1; r++) wb[r] = stb[sb0 + r];
+                     }
+                  }
+               }
 #pragma unroll
                for (int r = 0; r < R1; r++) {
                   const int q = jj + r * nb1;
                   const float w = wsl[q];
                   const int ia = offa + q;
-                  float xa = decode_level<NBIT>((sta[ia / SPW] >> (NBIT * (ia % SPW))) & MASK, a.levels);
+                  const uint32_t worda = PERM ? wa[r] : sta[ia / SPW];
+                  float xa = decode_level<NBIT>((worda >> (NBIT * (ia % SPW))) & MASK, a.levels);
                   if (blank_a) {
                      const long long smp = sa + rank + (long long)P * q;
                      if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) xa = 0.0f;
@@ -353,7 +459,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                   float xb = 0.0f;
                   if (has_b) {
                      const int ib = offb + q;
-                     xb = decode_level<NBIT>((stb[ib / SPW] >> (NBIT * (ib % SPW))) & MASK, a.levels);
+                     const uint32_t wordb = PERM ? wb[r] : stb[ib / SPW];
+                     xb = decode_level<NBIT>((wordb >> (NBIT * (ib % SPW))) & MASK, a.levels);
                      if (blank_b) {
                         const long long smp = sb + rank + (long long)P * q;
                         if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) xb = 0.0f;
@@ -377,7 +484,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       // ---- pass 2 in shared memory, pass 3 into registers ----
       smem_pass<Q, T, R2, R1>(buf, tw2);
       float2 v3[BPT3][R3];
-      pass_compute<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
+      pass_compute_pw<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
 
       // ---- push F_rank[k1] to the CTA that owns pair min(k1, Q-k1) ----
       cluster_wait();  // owners have finished reading their receive buffers
@@ -394,8 +501,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                else if (2 * k1 < Q) { u = k1; hi = 0; }
                else { u = Q - k1; hi = 1; }
                const int owner = u / UC;
-               const int side = 2 * (u - owner * UC) + hi;
-               dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + side), owner), v3[b][r]);
+               const int slot = hi * UC + (u - owner * UC);  // receive layout [p][hi][u]
+               dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + slot), owner), v3[b][r]);
             }
          }
       }
@@ -411,7 +518,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          float2 z[P];
          if (active) {
 #pragma unroll
-            for (int p = 0; p < P; p++) z[p] = rbuf[p * SIDES + s];
+            for (int p = 0; p < P; p++) z[p] = rbuf[p * SIDES + (hi ? UC : 0) + (s >> 1)];
             if (u == 0) {
                // lo: k1 = 0 (no twiddle); hi: k1 = Q/2, W_N^{p Q/2} = W_{2P}^p
                if (hi) {
