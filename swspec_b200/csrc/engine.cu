@@ -486,7 +486,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       a.S = S;
       a.levels = level_table(c.layout[0].format, nbit);
       const Plan &pl = h->plan;
-      SpecKernel kern = pl.kern[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+      const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+      SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
       const int ncl = std::max(1, std::min(nitems, h->max_clusters));
       cudaLaunchConfig_t cfgl = {};
       cfgl.gridDim = dim3(ncl * pl.P);
@@ -655,8 +656,9 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    Plan plan;
    if (!find_plan(cfg->fft_points, &plan))
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
-   if (cfg->precision == SWSGPU_PREC_TCSPLIT)
-      return fail(nullptr, SWSGPU_EINVAL, "tensor-core split form not available for this size");
+   if (cfg->precision == SWSGPU_PREC_TCSPLIT && !plan.kern_tc[1])
+      return fail(nullptr, SWSGPU_EINVAL,
+                  "tensor-core split form not available for fft_points " + std::to_string(cfg->fft_points));
    int ndev = 0;
    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
       return fail(nullptr, SWSGPU_ENODEV, "no CUDA device " + std::to_string(device));
@@ -735,7 +737,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
                   cudaMemcpyHostToDevice));
    // kernel attributes and cluster occupancy
    const int nbit = cfg->layout[0].nbit;
-   SpecKernel kern = plan.kern[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   SpecKernel kern = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.kern_tc[nbi] : plan.kern[nbi];
    const size_t smem = plan.smem[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
    CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
    if (plan.P > 8)

@@ -8,18 +8,26 @@
 
 namespace sws {
 
+#define SWS_KERN(P_, Q_, T_, R1_, R2_, R3_, MINB_, PREC_)                                        \
+   {k_spectra<P_, Q_, T_, R1_, R2_, R3_, 1, MINB_, PREC_>,                                        \
+    k_spectra<P_, Q_, T_, R1_, R2_, R3_, 2, MINB_, PREC_>,                                        \
+    k_spectra<P_, Q_, T_, R1_, R2_, R3_, 8, MINB_, PREC_>}
+#define SWS_SMEM(P_, Q_, R1_, R2_, R3_)                                                           \
+   {spectra_smem<P_, Q_, R1_, R2_, R3_, 1>(), spectra_smem<P_, Q_, R1_, R2_, R3_, 2>(),            \
+    spectra_smem<P_, Q_, R1_, R2_, R3_, 8>()}
+// plans with a tensor-core split form (Q = 4096 = 16 x 256, T = 256)
+#define SWS_PLAN_TC(N_, P_, MINB_)                                                                \
+   {N_, P_, 4096, 256, 16, 16, 16, SWS_KERN(P_, 4096, 256, 16, 16, 16, MINB_, 0),                 \
+    SWS_SMEM(P_, 4096, 16, 16, 16), SWS_KERN(P_, 4096, 256, 16, 16, 16, MINB_, 1)}
 #define SWS_PLAN(N_, P_, Q_, T_, R1_, R2_, R3_, MINB_)                                            \
-   {N_, P_, Q_, T_, R1_, R2_, R3_,                                                                \
-    {k_spectra<P_, Q_, T_, R1_, R2_, R3_, 1, MINB_>, k_spectra<P_, Q_, T_, R1_, R2_, R3_, 2, MINB_>,\
-     k_spectra<P_, Q_, T_, R1_, R2_, R3_, 8, MINB_>},                                             \
-    {spectra_smem<P_, Q_, R1_, R2_, R3_, 1>(), spectra_smem<P_, Q_, R1_, R2_, R3_, 2>(),           \
-     spectra_smem<P_, Q_, R1_, R2_, R3_, 8>()}}
+   {N_, P_, Q_, T_, R1_, R2_, R3_, SWS_KERN(P_, Q_, T_, R1_, R2_, R3_, MINB_, 0),                 \
+    SWS_SMEM(P_, Q_, R1_, R2_, R3_), {nullptr, nullptr, nullptr}}
 
 static const Plan kPlans[] = {
-    SWS_PLAN(65536, 16, 4096, 256, 16, 16, 16, 2),
-    SWS_PLAN(32768, 8, 4096, 256, 16, 16, 16, 2),
-    SWS_PLAN(16384, 4, 4096, 256, 16, 16, 16, 2),
-    SWS_PLAN(8192, 2, 4096, 256, 16, 16, 16, 2),
+    SWS_PLAN_TC(65536, 16, 2),
+    SWS_PLAN_TC(32768, 8, 2),
+    SWS_PLAN_TC(16384, 4, 2),
+    SWS_PLAN_TC(8192, 2, 2),
     SWS_PLAN(4096, 2, 2048, 128, 16, 16, 8, 4),
     SWS_PLAN(20000, 4, 5000, 320, 8, 25, 25, 1),
     SWS_PLAN(131072, 16, 8192, 256, 16, 16, 32, 1),

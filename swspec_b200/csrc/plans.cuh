@@ -10,8 +10,9 @@ typedef void (*SpecKernel)(SpecArgs);
 struct Plan {
    int N, P, Q, T;
    int R1, R2, R3;
-   SpecKernel kern[3];   // nbit 1, 2, 8
+   SpecKernel kern[3];   // nbit 1, 2, 8 (FP32 form)
    size_t smem[3];       // dynamic shared memory of each variant
+   SpecKernel kern_tc[3];  // tensor-core split form, or null where the plan has none
 };
 
 // Returns false when N has no single-launch plan.

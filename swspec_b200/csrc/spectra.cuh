@@ -32,6 +32,7 @@
 #pragma once
 
 #include <cooperative_groups.h>
+#include <cuda_fp16.h>
 
 #include "dft.cuh"
 #include "kernels.cuh"
@@ -271,11 +272,100 @@ __host__ __device__ constexpr int stage_slots()
    return (nb1 % SPW == 0) ? ST * ((((NW + ST - 1) / ST) + 3) / 4) * 4 : NW;
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core split-precision stages (mma.sync m16n8k16, f16 x f16 -> f32)
+// ---------------------------------------------------------------------------
+// A 256-point DFT is done as 16 x 16: stage 1 DFT16 over n2 of x[n1 + 16 n2]
+// for the 16 columns n1, twiddle W_256^{n1 m2}, stage 2 DFT16 over n1, giving
+// X[16 m1 + m2].  Each complex DFT16 is the real block product
+//   [Re; Im] = [[Fr, -Fi], [Fi, Fr]] [Re; Im],
+// and every real product A.B is evaluated as Ah.Bh + Ah.Bl + Al.Bh with
+// FP16 hi/lo splits (hi = rn(x), lo = rn(x - hi)) and FP32 accumulation --
+// about 22 significant bits, FP32-level accuracy.  The D fragment of stage 1
+// (rows m2, columns n1) is exactly the B fragment stage 2 needs (rows n1,
+// columns m2), so the data never leaves registers between the two stages.
+
+// hi/lo split of two floats into f16x2 words (lower half = first value)
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+   const __half2 h = __floats2half2_rn(a, b);
+   const float2 hf = __half22float2(h);
+   const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+   hi = *reinterpret_cast<const uint32_t *>(&h);
+   lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+   asm volatile(
+       "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+       "{%0,%1,%2,%3};\n"
+       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// A fragments of the DFT16 matrix F[m][n] = W_16^{m n}: real part, imaginary
+// part and its negation, each split hi/lo.
+struct Dft16Frags {
+   uint32_t rh[4], rl[4], ih[4], il[4], nih[4], nil[4];
+};
+
+__device__ __forceinline__ void make_dft16_frags(Dft16Frags &f)
+{
+   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+   // fragment element (row, col) pairs: a0 (g, 2t..2t+1), a1 (g+8, ...), a2 (g, 2t+8..), a3 (g+8, 2t+8..)
+#pragma unroll
+   for (int i = 0; i < 4; i++) {
+      const int row = g + ((i & 1) ? 8 : 0);
+      const int col = 2 * t + ((i & 2) ? 8 : 0);
+      float re[2], im[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+         double sn, cs;
+         sincospi(-2.0 * (double)((row * (col + e)) & 15) / 16.0, &sn, &cs);
+         re[e] = (float)cs;
+         im[e] = (float)sn;
+      }
+      split2(re[0], re[1], f.rh[i], f.rl[i]);
+      split2(im[0], im[1], f.ih[i], f.il[i]);
+      split2(-im[0], -im[1], f.nih[i], f.nil[i]);
+   }
+}
+
+// One complex DFT16 stage on an 8-column tile: inputs as B fragments
+// (re/im x hi/lo, b0 rows 2t..2t+1, b1 rows 2t+8..2t+9), outputs D (re, im).
+__device__ __forceinline__ void dft16_mma(const Dft16Frags &f, const uint32_t (&brh)[2],
+                                          const uint32_t (&brl)[2], const uint32_t (&bih)[2],
+                                          const uint32_t (&bil)[2], float (&dre)[4], float (&dim)[4])
+{
+#pragma unroll
+   for (int i = 0; i < 4; i++) dre[i] = dim[i] = 0.0f;
+   // small products first, then the hi.hi terms
+   mma16816(dre, f.rh, brl[0], brl[1]);
+   mma16816(dre, f.rl, brh[0], brh[1]);
+   mma16816(dre, f.nih, bil[0], bil[1]);
+   mma16816(dre, f.nil, bih[0], bih[1]);
+   mma16816(dre, f.rh, brh[0], brh[1]);
+   mma16816(dre, f.nih, bih[0], bih[1]);
+   mma16816(dim, f.ih, brl[0], brl[1]);
+   mma16816(dim, f.il, brh[0], brh[1]);
+   mma16816(dim, f.rh, bil[0], bil[1]);
+   mma16816(dim, f.rl, bih[0], bih[1]);
+   mma16816(dim, f.ih, brh[0], brh[1]);
+   mma16816(dim, f.rh, bih[0], bih[1]);
+}
+
+// Padded row layout of the 16 x 256 intermediate: 4 float2 of padding per 32
+// keeps the B-fragment loads (lanes at n1 = g, n2 = 2t..) bank-conflict free.
+__device__ __forceinline__ int ridx(int q2) { return q2 + 4 * (q2 >> 5); }
+constexpr int TC_ROW = 256 + 32;
+
 // Shared memory footprint of a plan (bytes).
 template <int P, int Q, int R1, int R2, int R3, int NBIT>
 __host__ __device__ constexpr size_t spectra_smem()
 {
-   return (size_t)(Q + Q / 16) * 8                               // FFT buffer
+   return (size_t)((Q + Q / 16) > 16 * TC_ROW ? (Q + Q / 16) : 16 * TC_ROW) * 8  // FFT buffer
+          + 256 * 8                                              // W_256 table (tensor-core form)
           + (size_t)P * (Q / P) * 8                              // receive buffer [P][sides]
           + (size_t)Q * 4                                        // window slice
           + (size_t)pass_tw_entries<Q, R2, R1>() * 8             // pass-2 twiddles
@@ -284,9 +374,13 @@ __host__ __device__ constexpr size_t spectra_smem()
           + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4 + 16; // code staging [2 jobs][2 sources]
 }
 
-template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB>
+template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB, int PREC>
 __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 {
+   // PREC 1: passes 2 and 3 (two radix-16 levels) as in-register 256-point
+   // DFTs on tensor cores; needs Q = 16 * 256 and one 256-row pair per warp.
+   static_assert(PREC == 0 || (Q == 4096 && R1 == 16 && R2 == 16 && R3 == 16 && T == 256),
+                 "tensor-core form plan");
    static_assert(R1 * R2 * R3 == Q, "radix plan must multiply to Q");
    static_assert(R3 > 1, "three passes");
    constexpr int SPW = 32 / NBIT;
@@ -311,7 +405,9 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    constexpr int BPT3 = (nb3 + T - 1) / T;
    extern __shared__ float4 smem_raw[];
    float2 *buf = reinterpret_cast<float2 *>(smem_raw);
-   float2 *rbuf = buf + (Q + Q / 16);
+   constexpr int BUFN = (Q + Q / 16) > 16 * TC_ROW ? (Q + Q / 16) : 16 * TC_ROW;
+   float2 *w256 = buf + BUFN;
+   float2 *rbuf = w256 + 256;
    float *wsl = reinterpret_cast<float *>(rbuf + P * SIDES);
    float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
    float2 *tw3 = tw2 + pass_tw_entries<Q, R2, R1>();
@@ -331,6 +427,10 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
    fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
    fill_pass_bases<Q, R3, NS3>(tw3, a.twQ, T);
+   if constexpr (PREC == 1)
+      for (int i = tid; i < 256; i += T) w256[i] = __ldg(a.twQ + 16 * i);  // W_256^i = W_4096^{16 i}
+   Dft16Frags F16;
+   if constexpr (PREC == 1) make_dft16_frags(F16);
    // twc[(p-1)*UC + u_local] = W_N^{p u}, read by both sides of pair u
    for (int i = tid; i < (P - 1) * UC; i += T) {
       const int p = i / UC + 1, uu = i % UC;
@@ -471,40 +571,112 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                DFT<R1>::run(v[b]);
             }
          }
+         if constexpr (PREC == 0) {
 #pragma unroll
-         for (int b = 0; b < BPT1; b++) {
-            const int jj = tid + b * T;
-            if (nb1 % T == 0 || jj < nb1) {
+            for (int b = 0; b < BPT1; b++) {
+               const int jj = tid + b * T;
+               if (nb1 % T == 0 || jj < nb1) {
 #pragma unroll
-               for (int r = 0; r < R1; r++) buf[pidx(jj * R1 + r)] = v[b][r];
+                  for (int r = 0; r < R1; r++) buf[pidx(jj * R1 + r)] = v[b][r];
+               }
             }
+         } else {
+            // four-step twiddle W_Q^{q2 k1} (q2 = tid, k1 = r), then rows y[k1][q2];
+            // tw3 holds W_Q^{2^i q2}, the same bases the FP32 form's last pass uses
+            float2 base[nbases(R3)];
+#pragma unroll
+            for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
+            twiddle_by_powers<R1>(v[0], base);
+#pragma unroll
+            for (int r = 0; r < R1; r++) buf[r * TC_ROW + ridx(tid)] = v[0][r];
          }
       }
       __syncthreads();
-      // ---- pass 2 in shared memory, pass 3 into registers ----
-      smem_pass<Q, T, R2, R1>(buf, tw2);
-      float2 v3[BPT3][R3];
-      pass_compute_pw<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
-
-      // ---- push F_rank[k1] to the CTA that owns pair min(k1, Q-k1) ----
-      cluster_wait();  // owners have finished reading their receive buffers
+      // push F_rank[k1] to the CTA that owns pair min(k1, Q-k1); receive layout [p][hi][u]
+      auto push = [&](int k1, float2 val) {
+         int u, hi;
+         if (k1 == 0) { u = 0; hi = 0; }
+         else if (2 * k1 == Q) { u = 0; hi = 1; }
+         else if (2 * k1 < Q) { u = k1; hi = 0; }
+         else { u = Q - k1; hi = 1; }
+         const int owner = u / UC;
+         const int slot = hi * UC + (u - owner * UC);
+         dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + slot), owner), val);
+      };
+      if constexpr (PREC == 0) {
+         // ---- pass 2 in shared memory, pass 3 into registers ----
+         smem_pass<Q, T, R2, R1>(buf, tw2);
+         float2 v3[BPT3][R3];
+         pass_compute_pw<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
+         cluster_wait();  // owners have finished reading their receive buffers
 #pragma unroll
-      for (int b = 0; b < BPT3; b++) {
-         const int j = tid + b * T;
-         if (nb3 % T == 0 || j < nb3) {
+         for (int b = 0; b < BPT3; b++) {
+            const int j = tid + b * T;
+            if (nb3 % T == 0 || j < nb3) {
 #pragma unroll
-            for (int r = 0; r < R3; r++) {
-               const int k1 = j + r * NS3;
-               int u, hi;
-               if (k1 == 0) { u = 0; hi = 0; }
-               else if (2 * k1 == Q) { u = 0; hi = 1; }
-               else if (2 * k1 < Q) { u = k1; hi = 0; }
-               else { u = Q - k1; hi = 1; }
-               const int owner = u / UC;
-               const int slot = hi * UC + (u - owner * UC);  // receive layout [p][hi][u]
-               dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + slot), owner), v3[b][r]);
+               for (int r = 0; r < R3; r++) push(j + r * NS3, v3[b][r]);
             }
          }
+      } else {
+         // ---- two radix-16 levels per warp on tensor cores: rows k1 = 2w, 2w+1 ----
+         const int lane = tid & 31, g = lane >> 2, t = lane & 3, warp = tid >> 5;
+         float ore[2][2][4], oim[2][2][4];  // [row][tile][frag]
+#pragma unroll
+         for (int rr = 0; rr < 2; rr++) {
+            const float2 *row = buf + (2 * warp + rr) * TC_ROW;
+            // stage 1: B[n2][n1] = x[n1 + 16 n2], n1 = g (+8 for tile 1), n2 = 2t, 2t+1, 2t+8, 2t+9
+            float d1re[2][4], d1im[2][4];
+#pragma unroll
+            for (int tile = 0; tile < 2; tile++) {
+               const int n1 = g + 8 * tile;
+               const float2 x0 = row[ridx(n1 + 16 * (2 * t))];
+               const float2 x1 = row[ridx(n1 + 16 * (2 * t + 1))];
+               const float2 x2 = row[ridx(n1 + 16 * (2 * t + 8))];
+               const float2 x3 = row[ridx(n1 + 16 * (2 * t + 9))];
+               uint32_t brh[2], brl[2], bih[2], bil[2];
+               split2(x0.x, x1.x, brh[0], brl[0]);
+               split2(x2.x, x3.x, brh[1], brl[1]);
+               split2(x0.y, x1.y, bih[0], bil[0]);
+               split2(x2.y, x3.y, bih[1], bil[1]);
+               dft16_mma(F16, brh, brl, bih, bil, d1re[tile], d1im[tile]);
+            }
+            // twiddle W_256^{n1 m2}: D1 element (m2 = g (+8 for frags 2,3), n1 = 2t (+1 for odd frags) + 8*tile)
+#pragma unroll
+            for (int tile = 0; tile < 2; tile++)
+#pragma unroll
+               for (int e = 0; e < 4; e++) {
+                  const int m2 = g + ((e & 2) ? 8 : 0);
+                  const int n1 = 2 * t + (e & 1) + 8 * tile;
+                  const float2 w = w256[(n1 * m2) & 255];
+                  const float2 y = cmul(make_float2(d1re[tile][e], d1im[tile][e]), w);
+                  d1re[tile][e] = y.x;
+                  d1im[tile][e] = y.y;
+               }
+            // stage 2: B2[n1][m2] from D1: tile' 0 (m2 = g): b0 = tile0 (c0, c1), b1 = tile1 (c0, c1);
+            //                               tile' 1 (m2 = g+8): b0 = tile0 (c2, c3), b1 = tile1 (c2, c3)
+#pragma unroll
+            for (int tp = 0; tp < 2; tp++) {
+               const int e0 = 2 * tp;
+               uint32_t brh[2], brl[2], bih[2], bil[2];
+               split2(d1re[0][e0], d1re[0][e0 + 1], brh[0], brl[0]);
+               split2(d1re[1][e0], d1re[1][e0 + 1], brh[1], brl[1]);
+               split2(d1im[0][e0], d1im[0][e0 + 1], bih[0], bil[0]);
+               split2(d1im[1][e0], d1im[1][e0 + 1], bih[1], bil[1]);
+               dft16_mma(F16, brh, brl, bih, bil, ore[rr][tp], oim[rr][tp]);
+            }
+         }
+         cluster_wait();  // owners have finished reading their receive buffers
+         // D2 element (m1 = g (+8 for frags 2,3), m2 = 2t (+1) + 8*tile') -> X[16 m1 + m2] = F[k1 + 16 X-index]
+#pragma unroll
+         for (int rr = 0; rr < 2; rr++)
+#pragma unroll
+            for (int tp = 0; tp < 2; tp++)
+#pragma unroll
+               for (int e = 0; e < 4; e++) {
+                  const int m1 = g + ((e & 2) ? 8 : 0);
+                  const int m2 = 2 * t + (e & 1) + 8 * tp;
+                  push((2 * warp + rr) + 16 * (16 * m1 + m2), make_float2(ore[rr][tp][e], oim[rr][tp][e]));
+               }
       }
       cluster.sync();  // every CTA's pushes have landed
 

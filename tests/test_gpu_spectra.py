@@ -22,16 +22,19 @@ def _mark5b_noise(nchan, nbit, nframes_m5b, seed, mbps=1024):
     return synth.mark5b_stream(sig, nbit, mbps), T
 
 
-def test_c1_like_auto_single_channel(gpu):
+@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+def test_c1_like_auto_single_channel(gpu, prec):
     """16 ch x 2 bit Mark5B, channel 1 only, N=32768 Hann, 16 FFTs per spectrum
-    (the default buffer plan's core run), tone at +3.1 MHz."""
+    (the default buffer plan's core run), tone at +3.1 MHz; both FFT forms."""
     N, cof = 32768, 16
+    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
     data, info = synth.c1_stream(0, frames=int(np.ceil(N * cof / 2500)) + 1, N=N)
     lay = gpu.layout("mark5b", 16, 2)
     run_bytes_payload = N * cof * 4
     nfr = run_bytes_payload // 10000 + 1
     raw = data[: nfr * 10016]
-    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 0),), max_run_bytes=len(raw))
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 0),), max_run_bytes=len(raw),
+                          precision=precision)
     core = gpu.Core(cfg)
     auto, _, _, ns = core.run([raw])
     samples = decode_channels(raw, info["fmt"], 16, 2, [0], nfr * 2500)
@@ -41,14 +44,18 @@ def test_c1_like_auto_single_channel(gpu):
     assert err < REL_TOL, err
 
 
-def test_c3_like_dual_pol_cross(gpu):
-    """Mark5B-2048-16-2, 8 subband pairs (c, c+8), N=65536, XX/YY/XY*."""
+@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+def test_c3_like_dual_pol_cross(gpu, prec):
+    """Mark5B-2048-16-2, 8 subband pairs (c, c+8), N=65536, XX/YY/XY*; both
+    the plain FP32 form and the tensor-core split form meet the bar."""
     N, cof, nfft = 65536, 16, 16
+    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
     data, info = synth.c3_stream(nfft, N=N)
     lay = gpu.layout("mark5b", 16, 2)
     pairs = [(c, c + 8) for c in range(8)]
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=tuple((0, c) for c in range(16)),
-                          xpols=pairs, max_run_bytes=len(data), samplingfreq=64e6)
+                          xpols=pairs, max_run_bytes=len(data), samplingfreq=64e6,
+                          precision=precision)
     core = gpu.Core(cfg)
     nsamp = info["nsamp"]
     auto, xp, _, ns = core.run([data])
@@ -177,3 +184,28 @@ def test_short_integration_level_relative(gpu):
     # the GPU packs two real frames into one complex FFT, whose FP32 rounding
     # scales with the pair's combined norm: allow sqrt(2) times the CPU error
     assert err <= max(np.sqrt(2.0) * 1.1 * err_cpu32, 1e-6), (err, err_cpu32)
+
+
+@pytest.mark.parametrize("N", [8192, 16384])
+def test_tcsplit_two_files_overlap(gpu, N):
+    """Tensor-core form on the remaining Q=4096 plans, overlapped FFTs, two files."""
+    d1, T = _mark5b_noise(8, 2, 40, 51)
+    d2, _ = _mark5b_noise(8, 2, 40, 52)
+    lay = gpu.layout("mark5b", 8, 2)
+    cof = 2 * (T // N) - 1
+    cfg = gpu.make_config(lay, N, "hann", 2, cof, sources=((0, 1), (1, 6)), xpols=((0, 1),),
+                          max_run_bytes=len(d1), precision=gpu.PREC_TCSPLIT)
+    core = gpu.Core(cfg)
+    auto, xp, _, ns = core.run([d1, d2])
+    s1 = decode_channels(d1, "Mark5B-1024-8-2", 8, 2, [1], T)[0]
+    s2 = decode_channels(d2, "Mark5B-1024-8-2", 8, 2, [6], T)[0]
+    ra, rx, _, nref = oracle_run([s1, s2], N, "hann", 2, cof, nxpols=1)
+    assert ns == nref
+    assert rel_err_auto(auto, ra) < REL_TOL
+    assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
+
+
+def test_tcsplit_rejected_without_plan(gpu):
+    cfg = gpu.make_config(gpu.layout("vdif:8000", 1, 8), 20000, precision=gpu.PREC_TCSPLIT)
+    with pytest.raises(gpu.SwsError, match="tensor-core"):
+        gpu.Core(cfg)
