@@ -492,7 +492,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       cudaLaunchConfig_t cfgl = {};
       cfgl.gridDim = dim3(ncl * pl.P);
       cfgl.blockDim = dim3(pl.T);
-      cfgl.dynamicSmemBytes = pl.smem[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+      cfgl.dynamicSmemBytes = c.precision == SWSGPU_PREC_TCSPLIT ? pl.smem_tc[nbi] : pl.smem[nbi];
       cfgl.stream = st;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -739,7 +739,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    const int nbit = cfg->layout[0].nbit;
    const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
    SpecKernel kern = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.kern_tc[nbi] : plan.kern[nbi];
-   const size_t smem = plan.smem[nbit == 1 ? 0 : nbit == 2 ? 1 : 2];
+   const size_t smem = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.smem_tc[nbi] : plan.smem[nbi];
    CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
    if (plan.P > 8)
       CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));

@@ -13,6 +13,7 @@ struct Plan {
    SpecKernel kern[3];   // nbit 1, 2, 8 (FP32 form)
    size_t smem[3];       // dynamic shared memory of each variant
    SpecKernel kern_tc[3];  // tensor-core split form, or null where the plan has none
+   size_t smem_tc[3];
 };
 
 // Returns false when N has no single-launch plan.

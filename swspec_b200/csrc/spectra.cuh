@@ -338,21 +338,25 @@ __device__ __forceinline__ void dft16_mma(const Dft16Frags &f, const uint32_t (&
                                           const uint32_t (&brl)[2], const uint32_t (&bih)[2],
                                           const uint32_t (&bil)[2], float (&dre)[4], float (&dim)[4])
 {
+   // four independent accumulation chains of three products each
+   float are[4] = {0, 0, 0, 0}, bre[4] = {0, 0, 0, 0}, aim[4] = {0, 0, 0, 0}, bim[4] = {0, 0, 0, 0};
+   mma16816(are, f.rh, brl[0], brl[1]);
+   mma16816(bre, f.nih, bil[0], bil[1]);
+   mma16816(aim, f.ih, brl[0], brl[1]);
+   mma16816(bim, f.rh, bil[0], bil[1]);
+   mma16816(are, f.rl, brh[0], brh[1]);
+   mma16816(bre, f.nil, bih[0], bih[1]);
+   mma16816(aim, f.il, brh[0], brh[1]);
+   mma16816(bim, f.rl, bih[0], bih[1]);
+   mma16816(are, f.rh, brh[0], brh[1]);
+   mma16816(bre, f.nih, bih[0], bih[1]);
+   mma16816(aim, f.ih, brh[0], brh[1]);
+   mma16816(bim, f.rh, bih[0], bih[1]);
 #pragma unroll
-   for (int i = 0; i < 4; i++) dre[i] = dim[i] = 0.0f;
-   // small products first, then the hi.hi terms
-   mma16816(dre, f.rh, brl[0], brl[1]);
-   mma16816(dre, f.rl, brh[0], brh[1]);
-   mma16816(dre, f.nih, bil[0], bil[1]);
-   mma16816(dre, f.nil, bih[0], bih[1]);
-   mma16816(dre, f.rh, brh[0], brh[1]);
-   mma16816(dre, f.nih, bih[0], bih[1]);
-   mma16816(dim, f.ih, brl[0], brl[1]);
-   mma16816(dim, f.il, brh[0], brh[1]);
-   mma16816(dim, f.rh, bil[0], bil[1]);
-   mma16816(dim, f.rl, bih[0], bih[1]);
-   mma16816(dim, f.ih, brh[0], brh[1]);
-   mma16816(dim, f.rh, bih[0], bih[1]);
+   for (int i = 0; i < 4; i++) {
+      dre[i] = are[i] + bre[i];
+      dim[i] = aim[i] + bim[i];
+   }
 }
 
 // Padded row layout of the 16 x 256 intermediate: 4 float2 of padding per 32
@@ -361,17 +365,17 @@ __device__ __forceinline__ int ridx(int q2) { return q2 + 4 * (q2 >> 5); }
 constexpr int TC_ROW = 256 + 32;
 
 // Shared memory footprint of a plan (bytes).
-template <int P, int Q, int R1, int R2, int R3, int NBIT>
+template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
 __host__ __device__ constexpr size_t spectra_smem()
 {
-   return (size_t)((Q + Q / 16) > 16 * TC_ROW ? (Q + Q / 16) : 16 * TC_ROW) * 8  // FFT buffer
-          + 256 * 8                                              // W_256 table (tensor-core form)
-          + (size_t)P * (Q / P) * 8                              // receive buffer [P][sides]
-          + (size_t)Q * 4                                        // window slice
-          + (size_t)pass_tw_entries<Q, R2, R1>() * 8             // pass-2 twiddles
-          + (size_t)nbases(R3) * R1 * R2 * 8                     // pass-3 twiddle bases
-          + (size_t)(P > 1 ? (P - 1) * (Q / (2 * P)) : 1) * 8    // cluster twiddles per k1-pair
-          + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4 + 16; // code staging [2 jobs][2 sources]
+   return (size_t)(PREC ? 16 * TC_ROW : (Q + Q / 16)) * 8                 // FFT buffer
+          + (size_t)(PREC ? 256 : 0) * 8                                 // W_256 table
+          + (size_t)P * (Q / P) * 8                                      // receive buffer [P][sides]
+          + (size_t)Q * 4                                                // window slice
+          + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8         // pass-2 twiddles
+          + (size_t)nbases(R3) * R1 * R2 * 8                             // pass-3 twiddle bases
+          + (size_t)nbases(P) * (Q / (2 * P)) * 8                        // cluster twiddle bases
+          + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4 + 16;         // code staging
 }
 
 template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB, int PREC>
@@ -405,13 +409,13 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    constexpr int BPT3 = (nb3 + T - 1) / T;
    extern __shared__ float4 smem_raw[];
    float2 *buf = reinterpret_cast<float2 *>(smem_raw);
-   constexpr int BUFN = (Q + Q / 16) > 16 * TC_ROW ? (Q + Q / 16) : 16 * TC_ROW;
+   constexpr int BUFN = PREC ? 16 * TC_ROW : (Q + Q / 16);
    float2 *w256 = buf + BUFN;
-   float2 *rbuf = w256 + 256;
+   float2 *rbuf = w256 + (PREC ? 256 : 0);
    float *wsl = reinterpret_cast<float *>(rbuf + P * SIDES);
    float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
-   float2 *tw3 = tw2 + pass_tw_entries<Q, R2, R1>();
-   float2 *twc = tw3 + nbases(R3) * NS3;
+   float2 *tw3 = tw2 + (PREC ? 0 : pass_tw_entries<Q, R2, R1>());
+   float2 *twc = tw3 + nbases(R3) * NS3;  // cluster bases [i][u_local] = W_N^{2^i u}
    // staging must be 16-byte aligned for the 128-bit reads
    uint32_t *stage = reinterpret_cast<uint32_t *>(
        (reinterpret_cast<uintptr_t>(twc + (P > 1 ? (P - 1) * UC : 1)) + 15) & ~(uintptr_t)15);
@@ -425,16 +429,16 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 
    // ---- per-CTA constant tables ----
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
-   fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
+   if constexpr (PREC == 0) fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
    fill_pass_bases<Q, R3, NS3>(tw3, a.twQ, T);
    if constexpr (PREC == 1)
       for (int i = tid; i < 256; i += T) w256[i] = __ldg(a.twQ + 16 * i);  // W_256^i = W_4096^{16 i}
    Dft16Frags F16;
    if constexpr (PREC == 1) make_dft16_frags(F16);
-   // twc[(p-1)*UC + u_local] = W_N^{p u}, read by both sides of pair u
-   for (int i = tid; i < (P - 1) * UC; i += T) {
-      const int p = i / UC + 1, uu = i % UC;
-      twc[i] = __ldg(a.twN + (long long)p * (rank * UC + uu));
+   // twc[i*UC + u_local] = W_N^{2^i u}, read by both sides of pair u
+   for (int idx = tid; idx < nbases(P) * UC; idx += T) {
+      const int i = idx / UC, uu = idx % UC;
+      twc[idx] = __ldg(a.twN + ((long long)(rank * UC + uu) << i));
    }
 
    const uint32_t rbuf_addr = (uint32_t)__cvta_generic_to_shared(rbuf);
@@ -700,11 +704,14 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                   });
                }
             } else {
+               // z[p] *= W_N^{p u} (lo) or conj of it (hi), from the power bases
+               float2 base[nbases(P)];
 #pragma unroll
-               for (int p = 1; p < P; p++) {
-                  const float2 w = twc[(p - 1) * UC + (s >> 1)];
-                  z[p] = hi ? cmulconj(z[p], w) : cmul(z[p], w);
+               for (int i = 0; i < nbases(P); i++) {
+                  const float2 w = twc[i * UC + (s >> 1)];
+                  base[i] = hi ? make_float2(w.x, -w.y) : w;
                }
+               twiddle_by_powers<P>(z, base);
                if (hi) {
                   // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
                   static_for<1, P>([&](auto I) {
