@@ -364,18 +364,26 @@ __device__ __forceinline__ void dft16_mma(const Dft16Frags &f, const uint32_t (&
 __device__ __forceinline__ int ridx(int q2) { return q2 + 4 * (q2 >> 5); }
 constexpr int TC_ROW = 256 + 32;
 
-// Shared memory footprint of a plan (bytes).
+// Shared memory layout of a plan: byte offsets of every region, used both
+// for the kernel's pointers and for the host-side launch size.
+template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
+struct SmemLayout {
+   static constexpr size_t BUFN = PREC ? 16 * TC_ROW : (Q + Q / 16);
+   static constexpr size_t buf = 0;                                             // FFT buffer (float2)
+   static constexpr size_t w256 = buf + BUFN * 8;                               // W_256 table
+   static constexpr size_t rbuf = w256 + (PREC ? 256 : 0) * 8;                  // receive [P][sides]
+   static constexpr size_t wsl = rbuf + (size_t)P * (Q / P) * 8;                // window slice (float)
+   static constexpr size_t tw2 = wsl + (size_t)Q * 4;                           // pass-2 twiddles
+   static constexpr size_t tw3 = tw2 + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8;
+   static constexpr size_t twc = tw3 + (size_t)nbases(R3) * R1 * R2 * 8;        // pass-3 bases
+   static constexpr size_t stage = ((twc + (size_t)nbases(P) * (Q / (2 * P)) * 8) + 15) / 16 * 16;
+   static constexpr size_t total = stage + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4;
+};
+
 template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
 __host__ __device__ constexpr size_t spectra_smem()
 {
-   return (size_t)(PREC ? 16 * TC_ROW : (Q + Q / 16)) * 8                 // FFT buffer
-          + (size_t)(PREC ? 256 : 0) * 8                                 // W_256 table
-          + (size_t)P * (Q / P) * 8                                      // receive buffer [P][sides]
-          + (size_t)Q * 4                                                // window slice
-          + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8         // pass-2 twiddles
-          + (size_t)nbases(R3) * R1 * R2 * 8                             // pass-3 twiddle bases
-          + (size_t)nbases(P) * (Q / (2 * P)) * 8                        // cluster twiddle bases
-          + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4 + 16;         // code staging
+   return SmemLayout<P, Q, R1, R2, R3, NBIT, PREC>::total;
 }
 
 template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB, int PREC>
@@ -404,21 +412,21 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    constexpr int ST = PERM ? nb1c / SPW : 1;
    constexpr int GS = PERM ? (((NW + ST - 1) / ST + 3) / 4) * 4 : NW;
    constexpr int NSLOT = PERM ? ST * GS : NW;  // staged words per source and job
+   static_assert(NSLOT <= stage_slots<Q, R1, NBIT>(), "code staging exceeds its shared-memory region");
    constexpr int NS3 = R1 * R2;             // span of the last pass
    constexpr int nb3 = Q / R3;
    constexpr int BPT3 = (nb3 + T - 1) / T;
    extern __shared__ float4 smem_raw[];
-   float2 *buf = reinterpret_cast<float2 *>(smem_raw);
-   constexpr int BUFN = PREC ? 16 * TC_ROW : (Q + Q / 16);
-   float2 *w256 = buf + BUFN;
-   float2 *rbuf = w256 + (PREC ? 256 : 0);
-   float *wsl = reinterpret_cast<float *>(rbuf + P * SIDES);
-   float2 *tw2 = reinterpret_cast<float2 *>(wsl + Q);
-   float2 *tw3 = tw2 + (PREC ? 0 : pass_tw_entries<Q, R2, R1>());
-   float2 *twc = tw3 + nbases(R3) * NS3;  // cluster bases [i][u_local] = W_N^{2^i u}
-   // staging must be 16-byte aligned for the 128-bit reads
-   uint32_t *stage = reinterpret_cast<uint32_t *>(
-       (reinterpret_cast<uintptr_t>(twc + (P > 1 ? (P - 1) * UC : 1)) + 15) & ~(uintptr_t)15);
+   using L = SmemLayout<P, Q, R1, R2, R3, NBIT, PREC>;
+   char *smem = reinterpret_cast<char *>(smem_raw);
+   float2 *buf = reinterpret_cast<float2 *>(smem + L::buf);
+   float2 *w256 = reinterpret_cast<float2 *>(smem + L::w256);
+   float2 *rbuf = reinterpret_cast<float2 *>(smem + L::rbuf);
+   float *wsl = reinterpret_cast<float *>(smem + L::wsl);
+   float2 *tw2 = reinterpret_cast<float2 *>(smem + L::tw2);
+   float2 *tw3 = reinterpret_cast<float2 *>(smem + L::tw3);
+   float2 *twc = reinterpret_cast<float2 *>(smem + L::twc);  // cluster bases [i][u_local] = W_N^{2^i u}
+   uint32_t *stage = reinterpret_cast<uint32_t *>(smem + L::stage);
 
    cg::cluster_group cluster = cg::this_cluster();
    const int rank = (int)cluster.block_rank();
