@@ -1,0 +1,131 @@
+// filesource.cpp -- framed recordings to payload-only buffers.
+//
+// Follows the reference's framed reading (src/FileSource.cpp:36-250):
+// locate the first frame header, optionally skip whole seconds, then fill
+// each buffer with payload bytes, consuming every frame header on the way.
+// Mark5B frames are found by two consecutive sync words 10016 bytes apart
+// (as mark5access's findfirstframe, mark5_format_mark5b.c:98-131); the first
+// frame's BCD time is written to the start-timing log.
+#include <cmath>
+#include <cstring>
+
+#include "sws_host.h"
+
+namespace swshost {
+
+static const uint32_t kMark5BSync = 0xABADDEEDu;
+
+int FileSource::open(const std::string &uri)
+{
+   const Settings &s = *cfg_;
+   const bool mark5b = (s.sourceformat == Mark5B || s.sourceformat == Mk5B);
+   header_bytes_ = mark5b ? 16 : (s.sourceformat_str.size() > 4 && s.sourceformat_str[4] == '_' ? 32 : 16);
+   frame_bytes_ = header_bytes_ + s.layout.frame_bytes;
+   ifile_.open(uri.c_str(), std::ios::binary | std::ios::in);
+   if (!ifile_.is_open()) {
+      *cfg_->tlog << "Could not open input file " << uri << std::endl;
+      got_eof_ = true;
+      return -1;
+   }
+   // locate the first frame
+   first_frame_ = 0;
+   if (mark5b) {
+      std::vector<unsigned char> win(1 << 20);
+      ifile_.read(reinterpret_cast<char *>(win.data()), win.size());
+      const int64_t got = ifile_.gcount();
+      int64_t found = -1;
+      for (int64_t i = 0; i + 10020 <= got; i++) {
+         uint32_t a, b;
+         memcpy(&a, &win[i], 4);
+         memcpy(&b, &win[i + 10016], 4);
+         if (a == kMark5BSync && b == kMark5BSync) {
+            found = i;
+            break;
+         }
+      }
+      if (found < 0) {
+         *cfg_->tlog << "FileSource: no Mark5B frame found in " << uri << std::endl;
+         return -1;
+      }
+      first_frame_ = found;
+      if (cfg_->startlog) {
+         const unsigned char *h = &win[found + 8];
+         int nib[8];
+         for (int i = 0; i < 4; i++) {
+            nib[2 * i] = h[3 - i] >> 4;
+            nib[2 * i + 1] = h[3 - i] & 15;
+         }
+         const int mjd3 = nib[0] * 100 + nib[1] * 10 + nib[2];
+         const int sec = nib[3] * 10000 + nib[4] * 1000 + nib[5] * 100 + nib[6] * 10 + nib[7];
+         *cfg_->startlog << "First frame at byte " << found << ": MJD(mod 1000) " << mjd3 << " second " << sec
+                         << std::endl;
+      }
+   }
+   // skip whole seconds (FileSource.cpp:132-153)
+   int64_t seek = first_frame_;
+   if (s.seconds_to_skip > 0) {
+      const double smp_bytes = (double)s.bits_per_sample * s.source_channels * s.samplingfreq / 8.0 * s.seconds_to_skip;
+      const int64_t frames = (int64_t)std::ceil(smp_bytes / (double)s.layout.frame_bytes);
+      seek += frames * frame_bytes_;
+      *cfg_->tlog << "Skipping " << s.seconds_to_skip << " sample-seconds: " << frames << " frames" << std::endl;
+   }
+   ifile_.clear();
+   ifile_.seekg(seek, std::ios::beg);
+   *cfg_->tlog << "FileSource   : processing framed data with " << header_bytes_ << "-byte headers and "
+               << s.layout.frame_bytes << "-byte payloads" << std::endl;
+   got_eof_ = false;
+   pending_header_ = true;
+   in_frame_ = 0;
+   return 0;
+}
+
+int FileSource::read(Buffer *buf)
+{
+   last_offset_ = payload_total_;
+   if (!ifile_.is_open() || !buf) {
+      if (buf) buf->setLength(0);
+      return 0;
+   }
+   const int64_t payload = cfg_->layout.frame_bytes;
+   char *dst = buf->getData();
+   int64_t want = (int64_t)buf->getAllocated(), got = 0;
+   std::vector<char> hdr(header_bytes_);
+   while (want > 0 && !got_eof_) {
+      if (pending_header_) {
+         ifile_.read(hdr.data(), header_bytes_);
+         if (ifile_.gcount() != header_bytes_) {
+            got_eof_ = true;
+            break;
+         }
+         if (cfg_->sourceformat == Mark5B || cfg_->sourceformat == Mk5B) {
+            uint32_t sync;
+            memcpy(&sync, hdr.data(), 4);
+            if (sync != kMark5BSync) *cfg_->tlog << "FileSource: Mark5B sync word mismatch" << std::endl;
+         }
+         pending_header_ = false;
+         in_frame_ = 0;
+      }
+      const int64_t n = std::min(want, payload - in_frame_);
+      ifile_.read(dst + got, n);
+      const int64_t r = ifile_.gcount();
+      got += r;
+      want -= r;
+      in_frame_ += r;
+      if (r < n) {
+         got_eof_ = true;
+         break;
+      }
+      if (in_frame_ == payload) pending_header_ = true;
+   }
+   payload_total_ += got;
+   buf->setLength((size_t)got);
+   return (int)got;
+}
+
+int FileSource::close()
+{
+   ifile_.close();
+   return 0;
+}
+
+}  // namespace swshost
