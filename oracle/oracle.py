@@ -48,6 +48,9 @@ def lib():
         _lib = C.CDLL(path)
         _lib.orc_decode.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_int,
                                     C.c_void_p]
+        _lib.orc_decode_blanked.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_int,
+                                            C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        _lib.orc_decode_blanked.restype = C.c_int64
         _lib.orc_window.argtypes = [C.c_int, C.c_int, C.c_void_p]
         _lib.orc_fft64.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         _lib.orc_domaths64.argtypes = [C.POINTER(OrcCfg), C.c_void_p, C.c_int64, C.c_void_p,
@@ -82,12 +85,32 @@ def ref():
 FMT_MARK5B, FMT_VDIF = 0, 1
 
 
-def decode(fmt: int, nchan: int, nbit: int, payload: bytes, nsamp: int, chan: int) -> np.ndarray:
+def decode(fmt: int, nchan: int, nbit: int, payload: bytes, nsamp: int, chan: int,
+           payload_bytes: int | None = None, frame_invalid=None) -> np.ndarray:
+    """Samples of one channel of a header-free payload stream.  With
+    payload_bytes (frame payload size; the stream starts at a frame) the
+    mark5access blanking rules apply; frame_invalid holds VDIF header
+    invalid bits per frame."""
     buf = np.frombuffer(payload, dtype=np.uint8)
     out = np.empty(nsamp, dtype=np.float32)
-    rc = lib().orc_decode(fmt, nchan, nbit, buf.ctypes.data, nsamp, chan, out.ctypes.data)
-    assert rc == 0
+    if payload_bytes is None:
+        rc = lib().orc_decode(fmt, nchan, nbit, buf.ctypes.data, nsamp, chan, out.ctypes.data)
+        assert rc == 0
+        return out
+    inv = None
+    if frame_invalid is not None:
+        inv = np.ascontiguousarray(frame_invalid, dtype=np.uint8)
+    rc = lib().orc_decode_blanked(fmt, nchan, nbit, buf.ctypes.data, len(buf), payload_bytes,
+                                  None if inv is None else inv.ctypes.data, nsamp, chan, out.ctypes.data)
+    assert rc >= 0
     return out
+
+
+def vdif_invalid_bits(framed: bytes, frame_bytes: int) -> np.ndarray:
+    """Invalid bit (word 0, bit 31) of every VDIF frame header."""
+    a = np.frombuffer(framed, dtype=np.uint8).reshape(-1, frame_bytes)
+    w0 = a[:, :4].copy().view(np.uint32)[:, 0]
+    return ((w0 >> 31) & 1).astype(np.uint8)
 
 
 def m5_format_info(fmt: str) -> dict:

@@ -98,6 +98,134 @@ int orc_decode(int fmt, int nchan, int nbit, const uint8_t *payload, int64_t nsa
 }
 
 /* ------------------------------------------------------------------------ */
+/* Blanking (mark5access blankers)                                          */
+/* ------------------------------------------------------------------------ */
+
+#define ORC_FILL32 0x11223344u
+#define ORC_FILL64 0x1122334411223344ull
+#define ORC_ZONE_LOG2 15 /* blanker_mark5.c:138, 32768-byte zones */
+#define ORC_BIG (1 << 30)
+
+static uint64_t orc_w64(const uint8_t *p, int64_t w)
+{
+   uint64_t v;
+   memcpy(&v, p + 8 * w, 8);
+   return v;
+}
+static uint32_t orc_w32(const uint8_t *p, int64_t w)
+{
+   uint32_t v;
+   memcpy(&v, p + 4 * w, 4);
+   return v;
+}
+
+/* Binary search for the edge of a fill zone between 64-bit words [b, e) of
+ * a payload, then the 32-bit straggler check (blanker_mark5.c:53-123).
+ * want_fill = 1 finds the first fill word (start of a trailing zone),
+ * 0 the first data word (end of a leading zone); byte offsets. */
+static int orc_zone_edge(const uint8_t *pay, int b, int e, int want_fill)
+{
+   int n = e - b, i = n / 2, r = n - 1;
+   for (int s = n / 4; s > 0; s >>= 1) {
+      const int hit = (orc_w64(pay, b + i) == ORC_FILL64) == want_fill;
+      if (hit) {
+         r = i;
+         i -= s;
+      } else {
+         i += s;
+      }
+   }
+   r = 8 * (b + r);
+   if (want_fill) {
+      if (orc_w32(pay, r / 4 - 1) == ORC_FILL32) r -= 4;
+   } else {
+      if (orc_w32(pay, r / 4 - 2) == ORC_FILL32) r += 4;
+   }
+   return r;
+}
+
+/* Valid byte range [zs[z], ze[z]) of each zone of one frame payload:
+ * Mark5B checks the first and last 64-bit word of every 32 KiB zone
+ * (blanker_mark5.c:126-200), VDIF blanks a whole frame whose first or last
+ * word is fill (:282-310) or whose header has the invalid bit set
+ * (format_vdif.c:2873-2914).  Returns the number of zones. */
+static int orc_frame_zones(int fmt, const uint8_t *pay, int payload_bytes, int invalid, int *zs, int *ze)
+{
+   const int nword = payload_bytes / 8;
+   if (fmt == ORC_FMT_VDIF) {
+      zs[0] = 0;
+      ze[0] = (invalid || orc_w64(pay, 0) == ORC_FILL64 || orc_w64(pay, nword - 1) == ORC_FILL64) ? 0 : ORC_BIG;
+      if (invalid) zs[0] = ORC_BIG;
+      return 1;
+   }
+   const int zw = 1 << (ORC_ZONE_LOG2 - 3);
+   int z = 0;
+   for (int b = 0; b < nword; b += zw, z++) {
+      const int e = (b + zw > nword) ? nword : b + zw;
+      const int startOK = orc_w64(pay, b) != ORC_FILL64;
+      const int endOK = orc_w64(pay, e - 1) != ORC_FILL64;
+      if (startOK && endOK) {
+         zs[z] = 0;
+         ze[z] = ORC_BIG;
+      } else if (!startOK && !endOK) {
+         zs[z] = ORC_BIG;
+         ze[z] = 0;
+      } else if (startOK) {
+         zs[z] = 0;
+         ze[z] = orc_zone_edge(pay, b, e, 1);
+      } else {
+         zs[z] = orc_zone_edge(pay, b, e, 0);
+         ze[z] = ORC_BIG;
+      }
+   }
+   return z;
+}
+
+/* orc_decode with mark5access's blanking: the payload stream starts at a
+ * frame boundary, frames are payload_bytes long, frame_invalid[f] (or NULL)
+ * carries VDIF header invalid bits.  A sample-time whose first byte lies
+ * outside its zone's valid range decodes to 0 (the per-byte test of every
+ * mark5access decoder, e.g. mark5_format_mark5b.c:1216-1223).  Returns the
+ * number of blanked sample-times, or -1. */
+int64_t orc_decode_blanked(int fmt, int nchan, int nbit, const uint8_t *payload, int64_t payload_len,
+                           int payload_bytes, const uint8_t *frame_invalid, int64_t nsamp, int chan,
+                           float *out)
+{
+   if (chan < 0 || chan >= nchan || payload_bytes <= 0 || (payload_bytes % 8)) return -1;
+   const int64_t stride = (int64_t)nchan * nbit;
+   if (nsamp > 0 && ((nsamp * stride + 7) >> 3) > payload_len) return -1;
+   if (orc_decode(fmt, nchan, nbit, payload, nsamp, chan, out)) return -1;
+   const int maxz = (payload_bytes >> ORC_ZONE_LOG2) + 2;
+   int *zs = (int *)malloc(sizeof(int) * maxz), *ze = (int *)malloc(sizeof(int) * maxz);
+   int64_t nblank = 0, cur = -1;
+   for (int64_t t = 0; t < nsamp; t++) {
+      const int64_t byte = (t * stride) >> 3;
+      const int64_t f = byte / payload_bytes;
+      const int o = (int)(byte - f * payload_bytes);
+      if (f != cur) {
+         /* a frame cut short by the end of the stream is checked as far as it goes */
+         if ((f + 1) * payload_bytes <= payload_len) {
+            orc_frame_zones(fmt, payload + f * payload_bytes, payload_bytes, frame_invalid ? frame_invalid[f] : 0,
+                            zs, ze);
+         } else {
+            zs[0] = 0;
+            ze[0] = ORC_BIG;
+            for (int z = 1; z < maxz; z++) zs[z] = 0, ze[z] = ORC_BIG;
+         }
+         cur = f;
+      }
+      const int z = (fmt == ORC_FMT_VDIF) ? 0 : (o >> ORC_ZONE_LOG2);
+      if (o < zs[z] || o >= ze[z]) {
+         out[t] = 0.0f;
+         nblank++;
+      }
+   }
+   free(zs);
+   free(ze);
+   return nblank;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Windows                                                                  */
 /* ------------------------------------------------------------------------ */
 

@@ -24,9 +24,9 @@
 
 namespace sws {
 __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any);
-void launch_unpack_codes(int nbit, dim3 grid, int block, cudaStream_t st, StreamIn s,
-                         long long nsamp, const int *chans, int nch, uint32_t *codes, int D,
-                         long long wpp, const int2 *valid, uint32_t *blank);
+cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, const int *chans, int nch,
+                                uint32_t *codes, int D, long long wpp, const int2 *valid,
+                                const int *blank_any, uint32_t *blank);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
 __global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
@@ -418,7 +418,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 64));
    CK(h, h->d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
    CK(h, h->d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
-   CK(h, cudaMemsetAsync(h->d_blank.p, 0, sizeof(uint32_t) * (size_t)blank_words * c.num_streams, st));
+   // the blank bitmap is written by K1 and read by K2/PCal only for streams
+   // with a blanked frame (blank_any), so it needs no clearing
    CK(h, cudaMemsetAsync(h->d_blank_any.p, 0, sizeof(int) * SWSGPU_MAX_STREAMS, st));
 
    // K1 per stream
@@ -452,10 +453,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       CK(h, cudaMemcpyAsync(h->d_chans[s].p, chans.data(), sizeof(int) * chans.size(),
                             cudaMemcpyHostToDevice, st));
       uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)first_code * code_words;
-      dim3 grid((unsigned)((code_words + 255) / 256), (unsigned)((chans.size() + 15) / 16));
       uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
-      launch_unpack_codes(nbit, grid, 256, st, si, nsamp, (const int *)h->d_chans[s].p,
-                          (int)chans.size(), codes, D, wpp, (const int2 *)h->d_valid[s].p, blank);
+      CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(), codes, D, wpp,
+                                (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank));
       launches++;
    }
    CK(h, cudaGetLastError());

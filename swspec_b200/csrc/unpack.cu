@@ -16,6 +16,8 @@
 // mark5_stream.c:136-145); a sample-time whose first byte lies outside the
 // range decodes to 0.  Blanked sample-times are marked in a bitmap the FFT
 // kernel consults only when a chunk has any.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace sws {
@@ -108,60 +110,247 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
 // s % D at index s / D, SPW = 32/NBIT codes per 32-bit word:
 //   codes[c * D * wpp + (s % D) * wpp + (s / D) / SPW], bits NBIT * ((s / D) % SPW).
 // A CTA of the FFT cluster that owns residue p then reads its samples as one
-// contiguous run.  Thread t writes word t / D of phase t % D for every
-// requested channel; each payload word is read by exactly one thread.
-// Blank bits (1 per sample-time, standard order) go to `blank` (pre-zeroed).
+// contiguous run.
+//
+// One CTA owns G consecutive code words (a multiple of 32) of every phase of
+// every requested channel, i.e. the sample-times of G*SW payload words
+// (SW = D * nchan words hold the SPW*D sample-times behind one code word).
+//   1. The chunk's payload words are read once, coalesced (16-byte loads
+//      when frames allow), into shared memory with one pad word per SW so
+//      that lanes reading the same offset of consecutive blocks hit
+//      distinct banks.  Words outside their frame's valid range read as 0
+//      and are flagged in a shared bitmap.
+//   2. A warp builds 32 consecutive code words of one phase: each lane
+//      gathers its SPW sample-times.  When one payload word is exactly one
+//      sample-time of 32/NBIT channels (16 ch x 2 bit, 32 x 1, 4 x 8) the
+//      lane loads SPW words and transposes the SPW x SPW matrix of NBIT-bit
+//      codes in registers, giving every channel's code word at once; other
+//      layouts extract channel by channel.  Stores are 128-byte rows.
+//   3. With any blanked frame in the run, the CTA writes the blank bitmap
+//      words of its sample-times (1 bit per sample-time, standard order);
+//      otherwise the bitmap is left unwritten and unread.
+__host__ __device__ constexpr uint32_t transpose_mask(int sh)
+{
+   // low sh bits of every 2*sh-bit group
+   uint32_t m = 0u;
+   for (int i = 0; i < 32; i += 2 * sh) m |= ((1u << sh) - 1u) << i;
+   return m;
+}
+
+// In-register transpose of the E x E matrix of NBIT-bit codes held in
+// x[0..E), E = 32/NBIT: code (r, c) at bits NBIT*c of x[r] moves to bits
+// NBIT*r of x[c].  Block swaps of halving size (E/2, ..., 1 codes).
 template <int NBIT>
-__global__ void k_unpack_codes(StreamIn s, long long nsamp, const int *chans, int nch,
-                               uint32_t *codes, int D, long long wpp, const int2 *valid,
-                               uint32_t *blank)
+__device__ __forceinline__ void transpose_codes(uint32_t (&x)[32 / NBIT])
+{
+   constexpr int E = 32 / NBIT;
+#pragma unroll
+   for (int j = E / 2; j >= 1; j >>= 1) {
+      const int sh = NBIT * j;
+      const uint32_t mask = transpose_mask(sh);
+#pragma unroll
+      for (int r = 0; r < E; r++)
+         if (!(r & j)) {
+            const uint32_t t = ((x[r] >> sh) ^ x[r + j]) & mask;
+            x[r + j] ^= t;
+            x[r] ^= t << sh;
+         }
+   }
+}
+
+struct UnpackGeom {
+   int D, G, SW, nw;   // decimation, code words per CTA, payload words per block, per chunk
+   int vec16;          // 16-byte payload loads allowed
+   long long wpp, words_total, blank_words;
+};
+
+template <int NBIT>
+__global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsamp, const int *chans, int nch,
+                                                      uint32_t *codes, UnpackGeom g, const int2 *valid,
+                                                      const int *blank_any, uint32_t *blank)
 {
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= (long long)D * wpp) return;
-   const int ph = (int)(t % D);
-   const long long iw = t / D;
-   const long long stride = (long long)s.nchan * NBIT;
-   const int nb = s.payload_bytes;
-   uint32_t acc[16];
-   int c0 = blockIdx.y * 16;
-   int cn = min(16, nch - c0);
-#pragma unroll
-   for (int c = 0; c < 16; c++) acc[c] = 0u;
-   long long cached_idx = -1;
-   uint32_t cached = 0u;
-   for (int k = 0; k < SPW; k++) {
-      const long long smp = (iw * SPW + k) * D + ph;
-      if (smp >= nsamp) break;
-      long long bit0 = smp * stride;
-      long long v0 = s.grid_offset + (bit0 >> 3);
-      long long f = v0 / nb;
-      int o = (int)(v0 - f * nb);
-      int2 vr = valid[f];
-      if (!((o >= vr.x) && (o < vr.y))) {
-         if (blockIdx.y == 0) atomicOr(&blank[smp >> 5], 1u << (smp & 31));
-         continue;
+   extern __shared__ uint32_t sm[];
+   const int SW = g.SW, SWp = g.SW + 1, nw = g.nw, D = g.D;
+   uint32_t *vbits = sm + (size_t)g.G * SWp;          // invalid-word flags, nw / 32 words
+   int *pos = reinterpret_cast<int *>(vbits + nw / 32);  // channel -> output slot (transpose path)
+   int *sch = pos + SPW;                                 // requested channels
+   const bool any = *blank_any != 0;
+   const long long w0 = (long long)blockIdx.x * nw;
+   const bool tpath = (s.nchan * NBIT == 32);
+   for (int j = threadIdx.x; j < nch; j += blockDim.x) sch[j] = chans[j];
+   if (tpath)
+      for (int c = threadIdx.x; c < SPW; c += blockDim.x) {
+         int p = -1;
+         for (int k = 0; k < nch; k++)
+            if (chans[k] == c) p = k;
+         pos[c] = p;
       }
+   if (any)
+      for (int j = threadIdx.x; j < nw / 32; j += blockDim.x) vbits[j] = 0u;
+   __syncthreads();
+
+   // 1. payload words -> shared memory
+   const int pb = s.payload_bytes;
+   if (g.vec16) {
+      // UNR 16-byte loads in flight per thread before any shared store
+      constexpr int UNR = 4;
+      const int step = 16 * blockDim.x;
+      long long v = s.grid_offset + 4 * (w0 + 4 * threadIdx.x);
+      long long f = v / pb;
+      int o = (int)(v - f * pb);
+      for (int jb = 4 * threadIdx.x; jb < nw; jb += UNR * 4 * blockDim.x) {
+         uint4 q[UNR];
+         long long fu[UNR];
+         int ou[UNR];
 #pragma unroll
-      for (int c = 0; c < 16; c++) {
-         if (c < cn) {
-            long long bit = bit0 + (long long)chans[c0 + c] * NBIT;
-            long long widx = bit >> 5;   // 32-bit payload word (frames are multiples of 4 bytes)
-            if (widx != cached_idx) {
-               // grid_offset and payload sizes are multiples of 4 bytes, so a
-               // payload word never straddles a frame boundary
-               cached = *reinterpret_cast<const uint32_t *>(s.data + payload_addr(s, s.grid_offset + 4 * widx));
-               cached_idx = widx;
+         for (int u = 0; u < UNR; u++) {
+            const int j = jb + u * 4 * blockDim.x;
+            const long long w = w0 + j;
+            fu[u] = f;
+            ou[u] = o;
+            q[u] = make_uint4(0u, 0u, 0u, 0u);
+            if (j < nw && w < g.words_total) {
+               const long long a = s.header_bytes ? f * s.frame_bytes + s.header_bytes + o : v - s.grid_offset;
+               if (a + 16 <= s.nbytes) {
+                  q[u] = __ldg(reinterpret_cast<const uint4 *>(s.data + a));
+               } else {
+                  // ragged end of the buffer: word by word
+                  uint32_t t4[4] = {0u, 0u, 0u, 0u};
+                  for (int i = 0; i < 4; i++)
+                     if (a + 4 * i + 4 <= s.nbytes) t4[i] = __ldg(reinterpret_cast<const uint32_t *>(s.data + a + 4 * i));
+                  q[u] = make_uint4(t4[0], t4[1], t4[2], t4[3]);
+               }
             }
-            acc[c] |= ((cached >> (bit & 31)) & MASK) << (NBIT * k);
+            v += step;
+            o += step;
+            while (o >= pb) {
+               o -= pb;
+               f++;
+            }
+         }
+#pragma unroll
+         for (int u = 0; u < UNR; u++) {
+            const int j = jb + u * 4 * blockDim.x;
+            if (j >= nw) break;
+            const long long w = w0 + j;
+            uint32_t val[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+               if (w + i >= g.words_total) val[i] = 0u;
+               else if (any) {
+                  const int2 vr = valid[fu[u]];
+                  const int oi = ou[u] + 4 * i;
+                  if (!(oi >= vr.x && oi < vr.y)) {
+                     val[i] = 0u;
+                     atomicOr(&vbits[(j + i) >> 5], 1u << ((j + i) & 31));
+                  }
+               }
+               sm[j + i + (j + i) / SW] = val[i];
+            }
+         }
+      }
+   } else {
+      const int step = 4 * blockDim.x;
+      long long v = s.grid_offset + 4 * (w0 + threadIdx.x);
+      long long f = v / pb;
+      int o = (int)(v - f * pb);
+      for (int j = threadIdx.x; j < nw; j += blockDim.x) {
+         uint32_t val = 0u;
+         const long long w = w0 + j;
+         if (w < g.words_total) {
+            const long long a = s.header_bytes ? f * s.frame_bytes + s.header_bytes + o : v - s.grid_offset;
+            if (a + 4 <= s.nbytes) val = __ldg(reinterpret_cast<const uint32_t *>(s.data + a));
+            if (any) {
+               const int2 vr = valid[f];
+               if (!(o >= vr.x && o < vr.y)) {
+                  val = 0u;
+                  atomicOr(&vbits[j >> 5], 1u << (j & 31));
+               }
+            }
+         }
+         sm[j + j / SW] = val;
+         v += step;
+         o += step;
+         while (o >= pb) {
+            o -= pb;
+            f++;
          }
       }
    }
-   const long long code_words = (long long)D * wpp;
+   __syncthreads();
+
+   // 2. code words, one warp task = 32 consecutive words of one phase
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+   const long long code_words = (long long)D * g.wpp;
+   const int ntask = D * (g.G / 32);
+   for (int t = warp; t < ntask; t += nwarp) {
+      const int ph = t % D;
+      const int iw = (t / D) * 32 + lane;
+      const long long iwg = (long long)blockIdx.x * g.G + iw;
+      const uint32_t *blk = sm + (size_t)iw * SWp;
+      if (tpath) {
+         uint32_t x[SPW];
 #pragma unroll
-   for (int c = 0; c < 16; c++)
-      if (c < cn) codes[(long long)(c0 + c) * code_words + (long long)ph * wpp + iw] = acc[c];
+         for (int k = 0; k < SPW; k++) x[k] = blk[k * D + ph];
+         transpose_codes<NBIT>(x);
+         if (iwg < g.wpp) {
+#pragma unroll
+            for (int c = 0; c < SPW; c++) {
+               const int p = pos[c];
+               if (p >= 0) codes[(long long)p * code_words + (long long)ph * g.wpp + iwg] = x[c];
+            }
+         }
+      } else {
+         const int stride = s.nchan * NBIT;
+         for (int c0 = 0; c0 < nch; c0 += 16) {
+            const int cn = min(16, nch - c0);
+            uint32_t acc[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) acc[c] = 0u;
+            int cached_idx = -1;
+            uint32_t cached = 0u;
+            for (int k = 0; k < SPW; k++) {
+               const int bit0 = (k * D + ph) * stride;
+#pragma unroll
+               for (int c = 0; c < 16; c++) {
+                  if (c < cn) {
+                     const int bit = bit0 + sch[c0 + c] * NBIT;
+                     const int widx = bit >> 5;
+                     if (widx != cached_idx) {
+                        cached = blk[widx];
+                        cached_idx = widx;
+                     }
+                     acc[c] |= ((cached >> (bit & 31)) & MASK) << (NBIT * k);
+                  }
+               }
+            }
+            if (iwg < g.wpp) {
+#pragma unroll
+               for (int c = 0; c < 16; c++)
+                  if (c < cn) codes[(long long)(c0 + c) * code_words + (long long)ph * g.wpp + iwg] = acc[c];
+            }
+         }
+      }
+   }
+
+   // 3. blank bitmap words of the chunk's sample-times
+   if (any) {
+      const int stride = s.nchan * NBIT;
+      const int nbw = g.G * SPW * D / 32;
+      const long long b0 = (long long)blockIdx.x * nbw;
+      for (int j = threadIdx.x; j < nbw; j += blockDim.x) {
+         if (b0 + j >= g.blank_words) break;
+         uint32_t m = 0u;
+         for (int i = 0; i < 32; i++) {
+            const long long st = 32ll * j + i;   // sample-time within the chunk
+            const int widx = (int)((st * stride) >> 5);
+            if ((b0 + j) * 32 + i < nsamp && ((vbits[widx >> 5] >> (widx & 31)) & 1u)) m |= 1u << i;
+         }
+         blank[b0 + j] = m;
+      }
+   }
 }
 
 // Decoded float samples of one channel (test path; same rules as above).
@@ -189,16 +378,51 @@ __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 lev
    out[t] = val;
 }
 
-void launch_unpack_codes(int nbit, dim3 grid, int block, cudaStream_t st, StreamIn s,
-                         long long nsamp, const int *chans, int nch, uint32_t *codes, int D,
-                         long long wpp, const int2 *valid, uint32_t *blank)
+UnpackGeom unpack_geometry(const StreamIn &s, long long nsamp, int D, long long wpp)
 {
-   if (nbit == 1)
-      k_unpack_codes<1><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
-   else if (nbit == 2)
-      k_unpack_codes<2><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
-   else
-      k_unpack_codes<8><<<grid, block, 0, st>>>(s, nsamp, chans, nch, codes, D, wpp, valid, blank);
+   UnpackGeom g;
+   g.D = D;
+   g.SW = D * s.nchan;
+   g.G = 32 * std::max(1, (8192 / g.SW) / 32);
+   g.nw = g.G * g.SW;
+   g.wpp = wpp;
+   g.words_total = (nsamp * s.nchan * s.nbit + 31) / 32;
+   g.blank_words = (nsamp + 31) / 32;
+   const bool frames16 = (s.payload_bytes % 16 == 0) &&
+                         (s.header_bytes == 0 || (s.header_bytes % 16 == 0 && s.frame_bytes % 16 == 0));
+   g.vec16 = frames16 && (s.grid_offset % 16 == 0) && ((uintptr_t)s.data % 16 == 0);
+   return g;
+}
+
+size_t unpack_smem_bytes(const UnpackGeom &g, int nch)
+{
+   return sizeof(uint32_t) * ((size_t)g.G * (g.SW + 1) + g.nw / 32 + 32 + nch);
+}
+
+template <int NBIT>
+static cudaError_t launch_codes_t(const UnpackGeom &g, cudaStream_t st, StreamIn s, long long nsamp,
+                                  const int *chans, int nch, uint32_t *codes, const int2 *valid,
+                                  const int *blank_any, uint32_t *blank)
+{
+   const size_t smem = unpack_smem_bytes(g, nch);
+   if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_unpack_codes<NBIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+   }
+   const unsigned nblk = (unsigned)((g.wpp + g.G - 1) / g.G);
+   k_unpack_codes<NBIT><<<nblk, 256, smem, st>>>(s, nsamp, chans, nch, codes, g, valid, blank_any, blank);
+   return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, const int *chans, int nch,
+                                uint32_t *codes, int D, long long wpp, const int2 *valid,
+                                const int *blank_any, uint32_t *blank)
+{
+   const UnpackGeom g = unpack_geometry(s, nsamp, D, wpp);
+   if (unpack_smem_bytes(g, nch) > 227 * 1024) return cudaErrorInvalidValue;
+   if (s.nbit == 1) return launch_codes_t<1>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   if (s.nbit == 2) return launch_codes_t<2>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   return launch_codes_t<8>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
 }
 
 }  // namespace sws

@@ -18,9 +18,15 @@ def payload_of(framed: bytes, fmt: str) -> bytes:
 
 
 def decode_channels(framed: bytes, fmt: str, nchan: int, nbit: int, chans, nsamp: int):
-    ofmt = O.FMT_MARK5B if fmt.startswith("Mark5B") else O.FMT_VDIF
+    """Oracle decode of a framed stream with mark5access's blanking (fill
+    zones; VDIF frames with the invalid bit)."""
+    if fmt.startswith("Mark5B"):
+        ofmt, pb, inv = O.FMT_MARK5B, 10000, None
+    else:
+        ofmt, pb = O.FMT_VDIF, int(fmt.split("_")[1].split("-")[0])
+        inv = O.vdif_invalid_bits(framed, pb + 32)
     pay = payload_of(framed, fmt)
-    return [O.decode(ofmt, nchan, nbit, pay, nsamp, c) for c in chans]
+    return [O.decode(ofmt, nchan, nbit, pay, nsamp, c, payload_bytes=pb, frame_invalid=inv) for c in chans]
 
 
 def oracle_run(samples, N, window, overlap, cof, nxpols=0, pcal=None):

@@ -209,3 +209,63 @@ def test_tcsplit_rejected_without_plan(gpu):
     cfg = gpu.make_config(gpu.layout("vdif:8000", 1, 8), 20000, precision=gpu.PREC_TCSPLIT)
     with pytest.raises(gpu.SwsError, match="tensor-core"):
         gpu.Core(cfg)
+
+
+def _fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hdr: int) -> bytes:
+    a = bytearray(raw)
+    base = frame * frame_bytes + hdr
+    a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
+    return bytes(a)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+def test_blanked_mark5b_frames(gpu, prec):
+    """Fill-pattern zones (trailing, whole frame, leading, interior) through
+    the whole path: blanked sample-times enter the FFTs and the phase-cal
+    fold as zeros, interior fill decodes as data (blanker_mark5.c:126-200)."""
+    N, cof, fs, off = 16384, 5, 32e6, 15625.0
+    nfr = N * cof // 2500 + 3
+    rng = np.random.default_rng(404)
+    comb = synth.pcal_comb(nfr * 2500, fs, 1e6, off, 0.05, rng.uniform(0, 6.28, 16))
+    data = synth.mark5b_stream(rng.standard_normal((16, nfr * 2500)) + comb[None, :], 2, 1024)
+    for f, a, b in [(2, 6000, 10000), (5, 0, 10000), (8, 0, 4000), (11, 2000, 3000), (20, 4, 9996)]:
+        data = _fill_zone(data, f, a, b, 10016, 16)
+    lay = gpu.layout("mark5b", 16, 2)
+    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 2), (0, 9)), xpols=((0, 1),),
+                          max_run_bytes=len(data), extract_pcal=True, pcal_tonebins=32,
+                          pcal_rotatorlen=2048, samplingfreq=fs, pcal_offset_hz=off, precision=precision)
+    core = gpu.Core(cfg)
+    auto, xp, pc, ns = core.run([data])
+    s = decode_channels(data, "Mark5B-1024-16-2", 16, 2, [2, 9], nfr * 2500)
+    assert np.count_nonzero(s[0][5 * 2500:6 * 2500]) == 0 and np.count_nonzero(s[0][11 * 2500:12 * 2500]) > 2000
+    ra, rx, rp, nref = oracle_run(s, N, "hann", 1, cof, nxpols=1,
+                                  pcal=dict(tonebins=32, rotatorlen=2048, fs=fs, offset=off))
+    assert ns == nref
+    assert rel_err_auto(auto[:, 0], ra[:, 0]) < REL_TOL and rel_err_auto(auto[:, 1], ra[:, 1]) < REL_TOL
+    assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
+    assert np.max(np.abs(pc - rp)) / np.max(np.abs(rp)) < 1e-6
+
+
+def test_blanked_vdif_frames(gpu):
+    """VDIF 2-bit, 4 channels: a frame with its invalid bit set and a frame
+    whose first payload word is fill are blanked whole."""
+    N, cof = 8192, 6
+    spf = 8000 * 8 // (4 * 2)
+    nfr = N * cof // spf + 2
+    rng = np.random.default_rng(405)
+    codes = synth.quantize_vdif_2bit(rng.standard_normal((4, nfr * spf)), 0.98)
+    payload = synth.pack_codes(codes, 2)
+    data = synth.vdif_frames(payload, 8000, 4, 2, 4000, invalid={3})
+    data = _fill_zone(data, 5, 0, 8, 8032, 32)
+    lay = gpu.layout("vdif:8000", 4, 2)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 1), (0, 3)), xpols=((0, 1),),
+                          max_run_bytes=len(data))
+    core = gpu.Core(cfg)
+    auto, xp, _, ns = core.run([data])
+    s = decode_channels(data, "VDIF_8000-64-4-2", 4, 2, [1, 3], nfr * spf)
+    assert np.count_nonzero(s[0][3 * spf:4 * spf]) == 0 and np.count_nonzero(s[0][5 * spf:6 * spf]) == 0
+    ra, rx, _, nref = oracle_run(s, N, "hann", 1, cof, nxpols=1)
+    assert ns == nref
+    assert rel_err_auto(auto[:, 0], ra[:, 0]) < REL_TOL and rel_err_auto(auto[:, 1], ra[:, 1]) < REL_TOL
+    assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL

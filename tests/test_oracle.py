@@ -26,24 +26,65 @@ def test_decode_matches_golden_mark5b():
     pay = synth.strip_headers(raw, 10016, 16)
     nsamp = int(z["nsamp"])
     for c in range(16):
-        mine = O.decode(O.FMT_MARK5B, 16, 2, pay, nsamp, c)
         ref = z["decoded"][c]
-        # the restatement has no blanking; compare outside the fill zone of frame 1
-        ok = ref != 0
-        assert np.array_equal(mine[ok].view(np.uint32), ref[ok].view(np.uint32))
         # blanked: payload bytes 6000..10000 of frame 1 -> sample-times 1500..2500
         assert np.all(ref[2500 + 1500: 2500 + 2500] == 0)
         assert np.count_nonzero(ref[2500: 2500 + 1500] == 0) == 0
+        mine = O.decode(O.FMT_MARK5B, 16, 2, pay, nsamp, c, payload_bytes=10000)
+        assert np.array_equal(mine.view(np.uint32), ref.view(np.uint32))
+        # without the blanker only the fill zone differs
+        plain = O.decode(O.FMT_MARK5B, 16, 2, pay, nsamp, c)
+        ok = ref != 0
+        assert np.array_equal(plain[ok].view(np.uint32), ref[ok].view(np.uint32))
 
 
 def test_decode_matches_golden_vdif():
     z = np.load(os.path.join(GOLDEN, "vdif_decode.npz"))
-    pay = synth.strip_headers(z["raw"].tobytes(), 8032, 32)
-    mine = O.decode(O.FMT_VDIF, 1, 8, pay, int(z["nsamp"]), 0)
+    raw = z["raw"].tobytes()
+    pay = synth.strip_headers(raw, 8032, 32)
     ref = z["decoded"][0]
     assert np.all(ref[8000:16000] == 0)  # invalid frame blanked by mark5access
-    keep = np.r_[0:8000, 16000:24000]
-    assert np.array_equal(mine[keep].view(np.uint32), ref[keep].view(np.uint32))
+    inv = O.vdif_invalid_bits(raw, 8032)
+    assert list(inv) == [0, 1, 0]
+    mine = O.decode(O.FMT_VDIF, 1, 8, pay, int(z["nsamp"]), 0, payload_bytes=8000, frame_invalid=inv)
+    assert np.array_equal(mine.view(np.uint32), ref.view(np.uint32))
+
+
+def _fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hdr: int) -> bytes:
+    a = bytearray(raw)
+    base = frame * frame_bytes + hdr
+    a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
+    return bytes(a)
+
+
+@pytest.mark.skipif(O.ref() is None, reason="mark5access not built from the reference sources")
+def test_blanker_matches_live_mark5access():
+    """Fill zones of every shape (whole, leading, trailing, interior, 8-byte
+    edges, 32-bit stragglers) and VDIF invalid/fill frames, decoded by the
+    restated blankers and by mark5access itself."""
+    rng = np.random.default_rng(404)
+    data = synth.mark5b_stream(rng.standard_normal((16, 30 * 2500)), 2, 1024)
+    zones = [(2, 6000, 10000), (5, 0, 10000), (8, 0, 4000), (11, 2000, 3000), (20, 4, 9996),
+             (22, 8, 10000), (24, 0, 9992), (26, 0, 8), (27, 9992, 10000), (28, 0, 4004), (29, 5996, 10000)]
+    for f, a, b in zones:
+        data = _fill_zone(data, f, a, b, 10016, 16)
+    ref, _ = O.m5_decode("Mark5B-1024-16-2", data, 30 * 2500)
+    pay = synth.strip_headers(data, 10016, 16)
+    for c in range(16):
+        mine = O.decode(O.FMT_MARK5B, 16, 2, pay, 30 * 2500, c, payload_bytes=10000)
+        assert np.array_equal(mine.view(np.uint32), ref[c].view(np.uint32)), c
+    spf = 8000
+    codes = synth.quantize_vdif_2bit(rng.standard_normal((4, 8 * spf)), 0.98)
+    vd = synth.vdif_frames(synth.pack_codes(codes, 2), 8000, 4, 2, 4000, invalid={3})
+    vd = _fill_zone(vd, 5, 0, 8, 8032, 32)
+    vd = _fill_zone(vd, 6, 7992, 8000, 8032, 32)
+    vref, _ = O.m5_decode("VDIF_8000-64-4-2", vd, 8 * spf)
+    inv = O.vdif_invalid_bits(vd, 8032)
+    vpay = synth.strip_headers(vd, 8032, 32)
+    for c in range(4):
+        mine = O.decode(O.FMT_VDIF, 4, 2, vpay, 8 * spf, c, payload_bytes=8000, frame_invalid=inv)
+        assert np.array_equal(mine.view(np.uint32), vref[c].view(np.uint32)), c
+        assert np.count_nonzero(mine[3 * spf:7 * spf].reshape(4, spf), axis=1).tolist() == [0, spf, 0, 0]
 
 
 def test_decode_matches_test_unpacker_pattern():
