@@ -248,24 +248,27 @@ def test_blanked_mark5b_frames(gpu, prec):
 
 
 def test_blanked_vdif_frames(gpu):
-    """VDIF 2-bit, 4 channels: a frame with its invalid bit set and a frame
-    whose first payload word is fill are blanked whole."""
-    N, cof = 8192, 6
+    """VDIF 2-bit, 4 channels: frames with the invalid bit set and frames
+    whose first or last payload word is fill are blanked whole.  128 frames
+    = 125 FFTs = 5 whole spectra (no single-FFT partial spectrum, whose
+    near-empty bins make relative errors meaningless)."""
+    N, cof = 8192, 25
     spf = 8000 * 8 // (4 * 2)
-    nfr = N * cof // spf + 2
+    nfr = 128
     rng = np.random.default_rng(405)
     codes = synth.quantize_vdif_2bit(rng.standard_normal((4, nfr * spf)), 0.98)
     payload = synth.pack_codes(codes, 2)
-    data = synth.vdif_frames(payload, 8000, 4, 2, 4000, invalid={3})
+    data = synth.vdif_frames(payload, 8000, 4, 2, 4000, invalid={3, 64})
     data = _fill_zone(data, 5, 0, 8, 8032, 32)
+    data = _fill_zone(data, 90, 7992, 8000, 8032, 32)
     lay = gpu.layout("vdif:8000", 4, 2)
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 1), (0, 3)), xpols=((0, 1),),
                           max_run_bytes=len(data))
     core = gpu.Core(cfg)
     auto, xp, _, ns = core.run([data])
     s = decode_channels(data, "VDIF_8000-64-4-2", 4, 2, [1, 3], nfr * spf)
-    assert np.count_nonzero(s[0][3 * spf:4 * spf]) == 0 and np.count_nonzero(s[0][5 * spf:6 * spf]) == 0
+    assert all(np.count_nonzero(s[0][f * spf:(f + 1) * spf]) == 0 for f in (3, 5, 64, 90))
     ra, rx, _, nref = oracle_run(s, N, "hann", 1, cof, nxpols=1)
-    assert ns == nref
+    assert ns == nref == 5
     assert rel_err_auto(auto[:, 0], ra[:, 0]) < REL_TOL and rel_err_auto(auto[:, 1], ra[:, 1]) < REL_TOL
     assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
