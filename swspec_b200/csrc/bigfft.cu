@@ -1,0 +1,260 @@
+// bigfft.cu -- four-step FFT of the long transforms (N = N1 * N2).
+//
+// The same spectra as the cluster kernel -- window, real FFT of every frame,
+// |X|^2 and X.Y* accumulated per spectrum (TaskCoreIPP.cpp:427-487) -- for
+// lengths whose working set (8N bytes per pair FFT) exceeds a cluster's
+// shared memory.  Two real frames are packed into one complex transform
+// z = w (a + i b) as in the cluster kernel; the transform is split four-step
+// (Bailey) with the intermediate in HBM:
+//
+//   column pass  X1[k1][n2] = W_N^(n2 k1) sum_n1 z[n1 N2 + n2] W_N1^(n1 k1)
+//     one CTA per C adjacent columns n2 of one pair job: decode + window +
+//     first radix fused, the N1-point Stockham FFT in shared memory, the
+//     four-step twiddle from two small tables (W_N^(2048 h) W_N^l, both
+//     rounded once from double), 32-byte row segments written to scratch.
+//   row pass     X[k1 + N1 k2] = sum_n2 X1[k1][n2] W_N2^(n2 k2)
+//     one CTA per row pair (k1, N1 - k1) of one work item: both rows'
+//     N2-point FFTs, the pair separation Z_k / Z_(N-k) -- bin N-k of row k1
+//     sits in row N1 - k1 at column N2 - 1 - k2 -- and the products of every
+//     job of the item accumulated in registers, written once per bin into the
+//     partial rows the reduction kernel scales and combines.
+//
+// Traffic per pair job: the packed codes once, 8N bytes written and read
+// back; the window and twiddle tables stay in L2.
+#include "bigfft.cuh"
+#include "bins.cuh"
+#include "dft.cuh"
+
+namespace sws {
+
+__host__ __device__ constexpr int big_col_stride(int M)
+{
+   // column stride in float2: one pad per 16 entries, rounded to 16, + 4
+   // (a stride of 4 mod 16 spreads four columns over distinct banks)
+   return ((M + M / 16 + 15) / 16) * 16 + 4;
+}
+__device__ __forceinline__ int bpad(int i) { return i + (i >> 4); }
+
+// One Stockham pass (radix R, span NS) over C columns of M points held in
+// shared memory, in place through registers.  Butterfly j of column c reads
+// x[j + i M/R], twiddles by W_(NS R)^(k i) (k = j mod NS) from the W_M table
+// and writes d + i NS, d = (j / NS) NS R + k.
+template <int M, int C, int T, int R, int NS>
+__device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
+{
+   constexpr int CS = big_col_stride(M);
+   constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
+   constexpr int TS = M / (NS * R);
+   const int tid = threadIdx.x;
+   float2 v[BPT][R];
+#pragma unroll
+   for (int b = 0; b < BPT; b++) {
+      const int idx = tid + b * T;
+      if (TOT % T == 0 || idx < TOT) {
+         const int c = idx % C, j = idx / C, k = j % NS;
+#pragma unroll
+         for (int i = 0; i < R; i++) {
+            float2 x = buf[c * CS + bpad(j + i * NB)];
+            if (NS > 1 && i > 0) x = cmul(x, tw[k * i * TS]);
+            v[b][i] = x;
+         }
+         DFT<R>::run(v[b]);
+      }
+   }
+   __syncthreads();
+#pragma unroll
+   for (int b = 0; b < BPT; b++) {
+      const int idx = tid + b * T;
+      if (TOT % T == 0 || idx < TOT) {
+         const int c = idx % C, j = idx / C, k = j % NS;
+         const int d = (j / NS) * NS * R + k;
+#pragma unroll
+         for (int i = 0; i < R; i++) buf[c * CS + bpad(d + i * NS)] = v[b][i];
+      }
+   }
+   __syncthreads();
+}
+
+template <int NBIT>
+__device__ __forceinline__ float big_sample(const BigArgs &a, int code, long long s, const uint32_t *blank)
+{
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   const uint32_t w = __ldg(a.codes + (long long)code * a.code_words + s / SPW);
+   float x = decode_level<NBIT>((w >> (NBIT * (int)(s % SPW))) & MASK, a.levels);
+   if (blank && ((__ldg(blank + (s >> 5)) >> (s & 31)) & 1u)) x = 0.0f;
+   return x;
+}
+
+// Column pass: grid (N2 / C, jobs of the batch).
+template <int N1, int N2, int C, int T, int R1, int R2, int R3, int NBIT>
+__global__ void __launch_bounds__(T) k_big_cols(BigArgs a)
+{
+   static_assert(R1 * R2 * R3 == N1, "radices must multiply to N1");
+   static_assert(N2 % C == 0, "columns per CTA must divide N2");
+   constexpr int CS = big_col_stride(N1);
+   extern __shared__ float2 smf[];
+   float2 *buf = smf;
+   float2 *tw1 = smf + C * CS;
+   const int tid = threadIdx.x;
+   for (int i = tid; i < N1; i += T) tw1[i] = a.tw1[i];
+
+   const int c0 = blockIdx.x * C;
+   const BigJob jb = a.jobs[blockIdx.y];
+   const bool has_b = jb.mode != MODE_SINGLE;
+   const int sta = a.code_stream[jb.code_a];
+   const uint32_t *blank_a = a.blank_any[sta] ? a.blank + (long long)sta * a.blank_words : nullptr;
+   const uint32_t *blank_b = nullptr;
+   if (has_b) {
+      const int stb = a.code_stream[jb.code_b];
+      blank_b = a.blank_any[stb] ? a.blank + (long long)stb * a.blank_words : nullptr;
+   }
+
+   // pass 1 (span 1): decode + window + radix R1
+   {
+      constexpr int NB = N1 / R1, TOT = C * NB, BPT = (TOT + T - 1) / T;
+#pragma unroll
+      for (int b = 0; b < BPT; b++) {
+         const int idx = tid + b * T;
+         if (TOT % T == 0 || idx < TOT) {
+            const int c = idx % C, j = idx / C;
+            float2 v[R1];
+#pragma unroll
+            for (int i = 0; i < R1; i++) {
+               const long long n = (long long)(j + i * NB) * N2 + c0 + c;
+               const float w = __ldg(a.window + n);
+               const float xa = big_sample<NBIT>(a, jb.code_a, jb.sa + n, blank_a);
+               const float xb = has_b ? big_sample<NBIT>(a, jb.code_b, jb.sb + n, blank_b) : 0.0f;
+               v[i] = make_float2(xa * w, xb * w);
+            }
+            DFT<R1>::run(v);
+#pragma unroll
+            for (int i = 0; i < R1; i++) buf[c * CS + bpad(j * R1 + i)] = v[i];
+         }
+      }
+   }
+   __syncthreads();
+   big_pass<N1, C, T, R2, R1>(buf, tw1);
+   if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1);
+
+   // four-step twiddle and the 32-byte row segments of scratch
+   float2 *dst = a.scratch + (long long)blockIdx.y * N1 * N2 + c0;
+   for (int idx = tid; idx < C * N1; idx += T) {
+      const int c = idx % C, k1 = idx / C;
+      const float2 x = buf[c * CS + bpad(k1)];
+      const int m = (c0 + c) * k1;  // < N
+      const float2 w = cmul(__ldg(a.twA + (m >> 11)), __ldg(a.twB + (m & 2047)));
+      dst[(long long)k1 * N2 + c] = cmul(x, w);
+   }
+}
+
+// Row pass: grid (N1 / 2 + 1 row pairs, items of the batch).
+template <int N1, int N2, int T, int R1, int R2, int R3>
+__global__ void __launch_bounds__(T) k_big_rows(BigArgs a)
+{
+   static_assert(R1 * R2 * R3 == N2, "radices must multiply to N2");
+   static_assert(N1 % 2 == 0, "row pairs need an even N1");
+   constexpr int CS = big_col_stride(N2);
+   constexpr int KPT = (N2 + T - 1) / T;
+   extern __shared__ float2 smf[];
+   float2 *buf = smf;
+   float2 *tw2 = smf + 2 * CS;
+   const int tid = threadIdx.x;
+   for (int i = tid; i < N2; i += T) tw2[i] = a.tw2[i];
+
+   const int rp = blockIdx.x;
+   const int k1a = rp, k1b = (N1 - rp) % N1;
+   const bool two = k1a != k1b;
+   const BigItem bi = a.bitems[blockIdx.y];
+   const long long N = (long long)N1 * N2;
+
+   float acc[KPT][4];
+#pragma unroll
+   for (int q = 0; q < KPT; q++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
+
+   for (int j = 0; j < bi.nfr; j++) {
+      const float2 *ra = a.scratch + ((long long)(bi.job0 + j) * N1 + k1a) * N2;
+      const float2 *rb = a.scratch + ((long long)(bi.job0 + j) * N1 + k1b) * N2;
+      for (int i = tid; i < N2; i += T) {
+         buf[bpad(i)] = __ldcs(ra + i);
+         buf[CS + bpad(i)] = two ? __ldcs(rb + i) : make_float2(0.0f, 0.0f);
+      }
+      __syncthreads();
+      big_pass<N2, 2, T, R1, 1>(buf, tw2);
+      big_pass<N2, 2, T, R2, R1>(buf, tw2);
+      if constexpr (R3 > 1) big_pass<N2, 2, T, R3, R1 * R2>(buf, tw2);
+#pragma unroll
+      for (int q = 0; q < KPT; q++) {
+         const int k2 = tid + q * T;
+         if (N2 % T == 0 || k2 < N2) {
+            const float2 zk = buf[bpad(k2)];
+            float2 zm;
+            if (rp == 0) zm = buf[bpad((N2 - k2) % N2)];
+            else if (two) zm = buf[CS + bpad(N2 - 1 - k2)];
+            else zm = buf[bpad(N2 - 1 - k2)];
+            acc_bin(acc[q], bi.mode, zk, zm);
+         }
+      }
+      __syncthreads();
+   }
+
+   // bin k = k1 + N1 k2 of row k1, or its mirror N - k (conjugate cross
+   // product) when k lies above N/2; self-paired rows keep k <= N/2 only
+   float *part = a.partial + (long long)bi.item * 4 * a.S;
+   const int nprod = (bi.mode == MODE_XPOL) ? 4 : 1;
+#pragma unroll
+   for (int q = 0; q < KPT; q++) {
+      const int k2 = tid + q * T;
+      if (!(N2 % T == 0 || k2 < N2)) continue;
+      const long long k = rp + (long long)N1 * k2;
+      long long bin = k;
+      bool conj = false;
+      if (k > N / 2) {
+         if (!two) continue;
+         bin = N - k;
+         conj = true;
+      }
+      for (int c = 0; c < nprod; c++) part[(long long)c * a.S + bin] = (c == 3 && conj) ? -acc[q][c] : acc[q][c];
+   }
+}
+
+template <int N1, int N2, int C, int T, int R1, int R2, int R3>
+constexpr size_t big_cols_smem()
+{
+   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1);
+}
+template <int N2>
+constexpr size_t big_rows_smem()
+{
+   return sizeof(float2) * ((size_t)2 * big_col_stride(N2) + N2);
+}
+
+#define SWS_BIG(N1_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)                                       \
+   {N1_ * N2_, N1_, N2_, 4, TA_, TB_,                                                             \
+    {k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 1>, k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 2>,    \
+     k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 8>},                                                \
+    k_big_rows<N1_, N2_, TB_, B1, B2, B3>, big_cols_smem<N1_, N2_, 4, TA_, A1, A2, A3>(),         \
+    big_rows_smem<N2_>()}
+
+static const BigPlan kBigPlans[] = {
+    SWS_BIG(512, 256, 16, 16, 2, 512, 256, 16, 16, 2),        // 2^18
+    SWS_BIG(512, 256, 16, 16, 2, 1024, 512, 16, 16, 4),       // 2^19
+    SWS_BIG(1024, 256, 16, 16, 4, 1024, 512, 16, 16, 4),      // 2^20
+    SWS_BIG(1024, 256, 16, 16, 4, 2048, 512, 16, 16, 8),      // 2^21
+    SWS_BIG(2048, 512, 16, 16, 8, 2048, 512, 16, 16, 8),      // 2^22
+    SWS_BIG(1600, 512, 16, 4, 25, 2000, 512, 16, 5, 25),      // 3,200,000 = 2^10 5^5
+};
+
+bool find_big_plan(int N, BigPlan *out)
+{
+   for (const BigPlan &p : kBigPlans)
+      if (p.N == N) {
+         *out = p;
+         return true;
+      }
+   return false;
+}
+
+}  // namespace sws

@@ -20,6 +20,7 @@
 #include "../../include/swsgpu.h"
 #include "kernels.cuh"
 #include "plans.cuh"
+#include "bigfft.cuh"
 #include "pcal.cuh"
 
 namespace sws {
@@ -96,6 +97,8 @@ struct swsgpu_handle {
    swsgpu_config cfg;
    int device = 0;
    Plan plan;
+   bool big = false;   // four-step path (bplan) instead of the cluster kernel
+   BigPlan bplan;
    int S = 0;
    int max_clusters = 1;
    std::string err;
@@ -110,6 +113,8 @@ struct swsgpu_handle {
    std::vector<int> auto_owner;   // source -> xpol index that owns its auto (-1: none)
    // constant tables
    DevBuf d_window, d_twQ, d_twN, d_code_stream;
+   DevBuf d_tw1, d_tw2, d_twA, d_twB;               // four-step tables
+   DevBuf d_scratch, d_bjobs, d_bitems;             // four-step intermediate and job lists
    // per-call buffers
    DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
    DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
@@ -254,6 +259,9 @@ static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int ru
    }
    long long target_items = std::max<long long>(1, 4ll * h->max_clusters);
    int fper = (int)std::max<long long>(1, (total_jobs + target_items - 1) / target_items);
+   // the four-step row kernel accumulates a whole item per CTA: one item per
+   // source pair and spectrum
+   if (h->big) fper = 1 << 30;
 
    // key -> output vector index
    std::map<long long, std::vector<RedEntry>> vec_entries;
@@ -379,6 +387,92 @@ static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int ru
 }
 
 // ---------------------------------------------------------------------------
+// four-step path: column and row passes over batches of whole work items
+// ---------------------------------------------------------------------------
+static const size_t kBigScratchBudget = (size_t)1 << 30;  // bytes of column-pass output per batch
+
+static int launch_big(swsgpu_handle *h, const Schedule &sc, long long code_words, long long blank_words,
+                      cudaStream_t st, int &launches)
+{
+   const swsgpu_config &c = h->cfg;
+   const BigPlan &bp = h->bplan;
+   const int nbit = c.layout[0].nbit;
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   const size_t job_bytes = sizeof(float2) * (size_t)c.fft_points;
+   BigArgs a;
+   a.codes = (const uint32_t *)h->d_codes.p;
+   a.code_words = code_words;
+   a.blank = (const uint32_t *)h->d_blank.p;
+   a.blank_words = blank_words;
+   a.blank_any = (const int *)h->d_blank_any.p;
+   a.code_stream = (const int *)h->d_code_stream.p;
+   a.window = (const float *)h->d_window.p;
+   a.tw1 = (const float2 *)h->d_tw1.p;
+   a.tw2 = (const float2 *)h->d_tw2.p;
+   a.twA = (const float2 *)h->d_twA.p;
+   a.twB = (const float2 *)h->d_twB.p;
+   a.partial = (float *)h->d_partial.p;
+   a.N = c.fft_points;
+   a.S = h->S;
+   a.levels = level_table(c.layout[0].format, nbit);
+   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+   if (h->profiling) {
+      CK(h, cudaEventCreate(&ev0));
+      CK(h, cudaEventCreate(&ev1));
+      CK(h, cudaEventRecord(ev0, st));
+   }
+   std::vector<BigJob> jobs;
+   std::vector<BigItem> bitems;
+   size_t i0 = 0;
+   while (i0 < sc.items.size()) {
+      jobs.clear();
+      bitems.clear();
+      size_t i = i0;
+      // whole items per batch; a single item above the budget runs alone
+      while (i < sc.items.size()) {
+         const Item &it = sc.items[i];
+         if (!bitems.empty() && (jobs.size() + it.nfr) * job_bytes > kBigScratchBudget) break;
+         BigItem bi;
+         bi.job0 = (int)jobs.size();
+         bi.nfr = it.nfr;
+         bi.mode = it.mode;
+         bi.item = (int)i;
+         for (int j = 0; j < it.nfr; j++) {
+            BigJob jb;
+            jb.sa = it.start + (long long)j * it.step;
+            jb.sb = (it.mode == MODE_AUTOSUM) ? jb.sa + it.offset_b : jb.sa;
+            jb.code_a = it.src_a;
+            jb.code_b = (it.mode == MODE_XPOL) ? it.src_b : it.src_a;
+            jb.mode = it.mode;
+            jb.pad = 0;
+            jobs.push_back(jb);
+         }
+         bitems.push_back(bi);
+         i++;
+      }
+      CK(h, h->d_scratch.ensure(job_bytes * jobs.size()));
+      CK(h, h->d_bjobs.ensure(sizeof(BigJob) * jobs.size()));
+      CK(h, h->d_bitems.ensure(sizeof(BigItem) * bitems.size()));
+      CK(h, cudaMemcpyAsync(h->d_bjobs.p, jobs.data(), sizeof(BigJob) * jobs.size(), cudaMemcpyHostToDevice, st));
+      CK(h, cudaMemcpyAsync(h->d_bitems.p, bitems.data(), sizeof(BigItem) * bitems.size(),
+                            cudaMemcpyHostToDevice, st));
+      a.jobs = (const BigJob *)h->d_bjobs.p;
+      a.bitems = (const BigItem *)h->d_bitems.p;
+      a.scratch = (float2 *)h->d_scratch.p;
+      bp.cols[nbi]<<<dim3(bp.N2 / bp.C, (unsigned)jobs.size()), bp.TA, bp.smem_cols, st>>>(a);
+      bp.rows<<<dim3(bp.N1 / 2 + 1, (unsigned)bitems.size()), bp.TB, bp.smem_rows, st>>>(a);
+      CK(h, cudaGetLastError());
+      launches += 2;
+      i0 = i;
+   }
+   if (h->profiling) {
+      CK(h, cudaEventRecord(ev1, st));
+      h->prof_events.push_back(std::make_pair(ev0, ev1));
+   }
+   return SWSGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
 // pipeline launch for a chunk already in device memory
 // ---------------------------------------------------------------------------
 static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t *raw_bytes,
@@ -409,7 +503,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    const int nbit = c.layout[0].nbit;
    const int spw = 32 / nbit;
    const long long nsamp = sc.nsamp;
-   const int D = h->plan.P;                      // phase decimation of the code arrays
+   const int D = h->big ? 1 : h->plan.P;         // phase decimation of the code arrays
    const long long per_phase = (nsamp + D - 1) / D;
    const long long wpp = (per_phase + spw - 1) / spw + 2;  // +2: prefetch may touch one word past
    const long long code_words = (long long)D * wpp;
@@ -467,52 +561,57 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       CK(h, cudaMemcpyAsync(h->d_items.p, sc.items.data(), sizeof(Item) * nitems,
                             cudaMemcpyHostToDevice, st));
       CK(h, h->d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
-      SpecArgs a;
-      a.codes = (const uint32_t *)h->d_codes.p;
-      a.code_words = code_words;
-      a.wpp = wpp;
-      a.D = D;
-      a.blank = (const uint32_t *)h->d_blank.p;
-      a.blank_words = blank_words;
-      a.blank_any = (const int *)h->d_blank_any.p;
-      a.code_stream = (const int *)h->d_code_stream.p;
-      a.items = (const Item *)h->d_items.p;
-      a.nitems = nitems;
-      a.window = (const float *)h->d_window.p;
-      a.twQ = (const float2 *)h->d_twQ.p;
-      a.twN = (const float2 *)h->d_twN.p;
-      a.partial = (float *)h->d_partial.p;
-      a.N = c.fft_points;
-      a.S = S;
-      a.levels = level_table(c.layout[0].format, nbit);
-      const Plan &pl = h->plan;
-      const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
-      SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
-      const int ncl = std::max(1, std::min(nitems, h->max_clusters));
-      cudaLaunchConfig_t cfgl = {};
-      cfgl.gridDim = dim3(ncl * pl.P);
-      cfgl.blockDim = dim3(pl.T);
-      cfgl.dynamicSmemBytes = c.precision == SWSGPU_PREC_TCSPLIT ? pl.smem_tc[nbi] : pl.smem[nbi];
-      cfgl.stream = st;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = pl.P;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfgl.attrs = attr;
-      cfgl.numAttrs = 1;
-      cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-      if (h->profiling) {
-         CK(h, cudaEventCreate(&ev0));
-         CK(h, cudaEventCreate(&ev1));
-         CK(h, cudaEventRecord(ev0, st));
+      if (h->big) {
+         int rc = launch_big(h, sc, code_words, blank_words, st, launches);
+         if (rc != SWSGPU_OK) return rc;
+      } else {
+         SpecArgs a;
+         a.codes = (const uint32_t *)h->d_codes.p;
+         a.code_words = code_words;
+         a.wpp = wpp;
+         a.D = D;
+         a.blank = (const uint32_t *)h->d_blank.p;
+         a.blank_words = blank_words;
+         a.blank_any = (const int *)h->d_blank_any.p;
+         a.code_stream = (const int *)h->d_code_stream.p;
+         a.items = (const Item *)h->d_items.p;
+         a.nitems = nitems;
+         a.window = (const float *)h->d_window.p;
+         a.twQ = (const float2 *)h->d_twQ.p;
+         a.twN = (const float2 *)h->d_twN.p;
+         a.partial = (float *)h->d_partial.p;
+         a.N = c.fft_points;
+         a.S = S;
+         a.levels = level_table(c.layout[0].format, nbit);
+         const Plan &pl = h->plan;
+         const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+         SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
+         const int ncl = std::max(1, std::min(nitems, h->max_clusters));
+         cudaLaunchConfig_t cfgl = {};
+         cfgl.gridDim = dim3(ncl * pl.P);
+         cfgl.blockDim = dim3(pl.T);
+         cfgl.dynamicSmemBytes = c.precision == SWSGPU_PREC_TCSPLIT ? pl.smem_tc[nbi] : pl.smem[nbi];
+         cfgl.stream = st;
+         cudaLaunchAttribute attr[1];
+         attr[0].id = cudaLaunchAttributeClusterDimension;
+         attr[0].val.clusterDim.x = pl.P;
+         attr[0].val.clusterDim.y = 1;
+         attr[0].val.clusterDim.z = 1;
+         cfgl.attrs = attr;
+         cfgl.numAttrs = 1;
+         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+         if (h->profiling) {
+            CK(h, cudaEventCreate(&ev0));
+            CK(h, cudaEventCreate(&ev1));
+            CK(h, cudaEventRecord(ev0, st));
+         }
+         CK(h, cudaLaunchKernelEx(&cfgl, kern, a));
+         if (h->profiling) {
+            CK(h, cudaEventRecord(ev1, st));
+            h->prof_events.push_back(std::make_pair(ev0, ev1));
+         }
+         launches++;
       }
-      CK(h, cudaLaunchKernelEx(&cfgl, kern, a));
-      if (h->profiling) {
-         CK(h, cudaEventRecord(ev1, st));
-         h->prof_events.push_back(std::make_pair(ev0, ev1));
-      }
-      launches++;
 
       // K3
       const int nouts = (int)sc.outs.size();
@@ -653,10 +752,12 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    *out = nullptr;
    std::string why;
    if (!validate_config(cfg, why)) return fail(nullptr, SWSGPU_EINVAL, why);
-   Plan plan;
-   if (!find_plan(cfg->fft_points, &plan))
+   Plan plan = {};
+   BigPlan bplan = {};
+   const bool cluster_plan = find_plan(cfg->fft_points, &plan);
+   if (!cluster_plan && !find_big_plan(cfg->fft_points, &bplan))
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
-   if (cfg->precision == SWSGPU_PREC_TCSPLIT && !plan.kern_tc[1])
+   if (cfg->precision == SWSGPU_PREC_TCSPLIT && !(cluster_plan && plan.kern_tc[1]))
       return fail(nullptr, SWSGPU_EINVAL,
                   "tensor-core split form not available for fft_points " + std::to_string(cfg->fft_points));
    int ndev = 0;
@@ -669,6 +770,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    h->cfg = *cfg;
    h->device = device;
    h->plan = plan;
+   h->big = !cluster_plan;
+   h->bplan = bplan;
    h->S = cfg->fft_points / 2 + 1;
    auto bail = [&](int rc) {
       std::string e = h->err;
@@ -716,8 +819,10 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    std::vector<float> win;
    make_window(cfg->window, cfg->fft_points, win);
    std::vector<float2> twQ, twN;
-   make_twiddles(plan.Q, plan.Q, twQ);
-   make_twiddles(cfg->fft_points, cfg->fft_points / 2 + 1, twN);
+   if (!h->big) {
+      make_twiddles(plan.Q, plan.Q, twQ);
+      make_twiddles(cfg->fft_points, cfg->fft_points / 2 + 1, twN);
+   }
 #define CKB(call)                                                                                  \
    do {                                                                                           \
       cudaError_t e_ = (call);                                                                    \
@@ -728,16 +833,45 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    } while (0)
    CKB(h->d_window.ensure(sizeof(float) * win.size()));
    CKB(cudaMemcpy(h->d_window.p, win.data(), sizeof(float) * win.size(), cudaMemcpyHostToDevice));
-   CKB(h->d_twQ.ensure(sizeof(float2) * twQ.size()));
-   CKB(cudaMemcpy(h->d_twQ.p, twQ.data(), sizeof(float2) * twQ.size(), cudaMemcpyHostToDevice));
-   CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
-   CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
+   if (!h->big) {
+      CKB(h->d_twQ.ensure(sizeof(float2) * twQ.size()));
+      CKB(cudaMemcpy(h->d_twQ.p, twQ.data(), sizeof(float2) * twQ.size(), cudaMemcpyHostToDevice));
+      CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
+      CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
+   } else {
+      // four-step tables, each entry rounded once from double
+      std::vector<float2> t1, t2, tA, tB;
+      make_twiddles(bplan.N1, bplan.N1, t1);
+      make_twiddles(bplan.N2, bplan.N2, t2);
+      make_twiddles(cfg->fft_points, 2048, tB);
+      const int nA = (cfg->fft_points + 2047) / 2048;
+      tA.resize(nA);
+      for (int k = 0; k < nA; k++) {
+         const double ang = -2.0 * M_PI * (double)((long long)k * 2048) / (double)cfg->fft_points;
+         tA[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+      }
+      const std::pair<DevBuf *, std::vector<float2> *> tabs[4] = {
+          {&h->d_tw1, &t1}, {&h->d_tw2, &t2}, {&h->d_twA, &tA}, {&h->d_twB, &tB}};
+      for (const auto &t : tabs) {
+         CKB(t.first->ensure(sizeof(float2) * t.second->size()));
+         CKB(cudaMemcpy(t.first->p, t.second->data(), sizeof(float2) * t.second->size(), cudaMemcpyHostToDevice));
+      }
+   }
    CKB(h->d_code_stream.ensure(sizeof(int) * h->code_stream.size()));
    CKB(cudaMemcpy(h->d_code_stream.p, h->code_stream.data(), sizeof(int) * h->code_stream.size(),
                   cudaMemcpyHostToDevice));
    // kernel attributes and cluster occupancy
    const int nbit = cfg->layout[0].nbit;
    const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   if (h->big) {
+      CKB(cudaFuncSetAttribute((const void *)bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bplan.smem_cols));
+      CKB(cudaFuncSetAttribute((const void *)bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bplan.smem_rows));
+      for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_raw[s].ensure(cfg->max_run_bytes + 64));
+      *out = h;
+      return SWSGPU_OK;
+   }
    SpecKernel kern = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.kern_tc[nbi] : plan.kern[nbi];
    const size_t smem = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.smem_tc[nbi] : plan.smem[nbi];
    CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -778,7 +912,9 @@ void swsgpu_destroy(swsgpu_handle *h)
    DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes,
                      &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
                      &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
-                     &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal};
+                     &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal,
+                     &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs,
+                     &h->d_bitems};
    for (DevBuf *b : bufs) b->release();
    for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) {
       h->d_raw[s].release();

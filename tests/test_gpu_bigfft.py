@@ -1,0 +1,145 @@
+"""GPU parity of the four-step path (transform lengths beyond one cluster:
+2^18 .. 2^22 and 3,200,000 = 2^10 5^5) against the FP64 oracle.
+
+With a handful of FFTs per spectrum and millions of bins, chi-square
+statistics put some bins near zero, where a relative error says nothing
+about the arithmetic, and the reference's own FP32 arithmetic already misses
+2e-6 there at these lengths.  Each spectrum is therefore checked on
+(a) the error relative to max(bin, median bin), bounded by the 2e-6 bar or
+twice the FP32 restatement of TaskCoreIPP::doMaths on the same samples,
+whichever is larger, and (b) the max relative error per bin, bounded by
+twice that FP32 restatement's.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import REL_TOL, decode_channels, oracle_run
+from swspec_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _fp32_run(samples, N, window, overlap, cof, nxpols=0):
+    cfg = O.make_cfg(N, overlap=overlap, core_overlapped_ffts=cof, num_sources=len(samples),
+                     num_xpols=nxpols, window=O.WINDOW_NAMES[window], nthreads=8)
+    return O.domaths(cfg, samples, fp64=False)
+
+
+def _robust(got, ref):
+    d = np.abs(got.astype(np.float64) - ref)
+    return float(np.max(d / np.maximum(ref, np.median(ref)))), float(np.max(d / ref))
+
+
+def _check_auto(got, ref, ref32):
+    e_rob, e_rel = _robust(got, ref)
+    c_rob, c_rel = _robust(ref32, ref)
+    assert e_rob < max(REL_TOL, 2.0 * c_rob), (e_rob, c_rob)
+    assert e_rel < 2.0 * c_rel + 1e-7, (e_rel, c_rel)
+    return e_rob, e_rel, c_rob, c_rel
+
+
+def _mark5b(nchan, nbit, nframes, seed, mbps=1024, tones=None):
+    spf = synth.mark5b_samples_per_frame(nchan, nbit)
+    T = spf * nframes
+    rng = np.random.default_rng(seed)
+    sig = rng.standard_normal((nchan, T))
+    if tones is not None:
+        sig += tones(T)[None, :]
+    return synth.mark5b_stream(sig, nbit, mbps), T
+
+
+@pytest.mark.parametrize("N,nbit", [(1 << 18, 2), (1 << 20, 1)])
+def test_four_step_cross_pair(gpu, N, nbit):
+    """Mark5B 16 channels, one cross pair (channels 3 and 10) plus an
+    auto-only channel, 3 FFTs per spectrum and a trailing partial spectrum."""
+    cof = 3
+    spf = synth.mark5b_samples_per_frame(16, nbit)
+    nfr = (N * (cof + 1)) // spf + 1
+    data, T = _mark5b(16, nbit, nfr, 300 + nbit)
+    lay = gpu.layout("mark5b", 16, nbit)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 3), (0, 10), (0, 5)), xpols=((0, 1),),
+                          max_run_bytes=len(data))
+    core = gpu.Core(cfg)
+    auto, xp, _, ns = core.run([data])
+    s = decode_channels(data, f"Mark5B-1024-16-{nbit}", 16, nbit, [3, 10, 5], T)
+    ra, rx, _, nref = oracle_run(s[:2], N, "hann", 1, cof, nxpols=1)
+    r5, _, _, _ = oracle_run(s[2:], N, "hann", 1, cof)
+    a32, x32, _, _ = _fp32_run(s[:2], N, "hann", 1, cof, nxpols=1)
+    b32, _, _, _ = _fp32_run(s[2:], N, "hann", 1, cof)
+    assert ns == nref == 2
+    full = 0  # the full spectrum; the partial one holds a single FFT
+    for k in range(2):
+        _check_auto(auto[full, k], ra[full, k], a32[full, k])
+    _check_auto(auto[full, 2], r5[full, 0], b32[full, 0])
+    norm = np.sqrt(ra[full, 0] * ra[full, 1])
+    floor = np.maximum(norm, np.median(norm))
+    e_x = float(np.max(np.abs(xp[full, 0] - rx[full, 0]) / floor))
+    c_x = float(np.max(np.abs(x32[full, 0] - rx[full, 0]) / floor))
+    assert e_x < max(REL_TOL, 2.0 * c_x), (e_x, c_x)
+    # partial spectrum: one unscaled FFT
+    for k in range(2):
+        _check_auto(auto[1, k], ra[1, k], a32[1, k])
+
+
+def test_dynamic_range_vdif_8bit_2p22(gpu):
+    """Dynamic-range configuration: VDIF 8-bit, N = 2^22, Blackman-Harris,
+    a carrier 50 dB above the per-bin noise floor drifting 1 Hz/s; noise
+    floor level and carrier leakage vs FP64."""
+    N, cof, fs = 1 << 22, 3, 64e6
+    nsamp = N * cof
+    spf = 8000
+    nfr = (nsamp + spf - 1) // spf
+    rng = np.random.default_rng(1005)
+    t = np.arange(nfr * spf, dtype=np.float64) / fs
+    A = np.sqrt(4 * 1e5 * 2.0 / N)
+    f0 = 12.3456e6
+    x = rng.standard_normal(nfr * spf) + A * np.cos(2 * np.pi * (f0 * t + 0.5 * 1.0 * t * t))
+    codes = synth.quantize_vdif_8bit(x, 24.0)
+    data = synth.vdif_frames(synth.pack_codes(codes[None, :], 8), 8000, 1, 8, 8000)
+    lay = gpu.layout("vdif:8000", 1, 8)
+    cfg = gpu.make_config(lay, N, "blackmanharris", 1, cof, max_run_bytes=len(data), samplingfreq=fs)
+    core = gpu.Core(cfg)
+    auto, _, _, ns = core.run([data])
+    s = decode_channels(data, "VDIF_8000-512-1-8", 1, 8, [0], nfr * spf)
+    ra, _, _, nref = oracle_run(s, N, "blackmanharris", 1, cof)
+    r32, _, _, _ = _fp32_run(s, N, "blackmanharris", 1, cof)
+    assert ns == nref == 1
+    got, ref = auto[0, 0].astype(np.float64), ra[0, 0]
+    kc = int(round(f0 / fs * N))
+    far = np.r_[0:kc - 2000, kc + 2000:len(ref)]
+    floor_g, floor_r = np.median(got[far]), np.median(ref[far])
+    assert abs(floor_g / floor_r - 1) < 1e-6
+    # the carrier sits ~50 dB over the floor; its leakage skirt matches FP64
+    assert ref[kc - 2:kc + 3].max() / floor_r > 3e4
+    skirt = np.r_[kc - 200:kc - 4, kc + 5:kc + 200]
+    assert np.max(np.abs(got[skirt] - ref[skirt]) / ref[skirt]) < 1e-4
+    e_rob, e_rel, c_rob, c_rel = _check_auto(got, ref, r32[0, 0])
+    print(f"2^22: robust {e_rob:.2e} (FP32 CPU {c_rob:.2e}), max rel {e_rel:.2e} (FP32 CPU {c_rel:.2e})")
+
+
+def test_spacecraft_tone_3p2M_cosine2_pcal(gpu):
+    """N = 3,200,000 (2^10 5^5), cosine-squared window, two channels of a
+    Mark5B stream with a 1 MHz phase-cal comb at +10 kHz (rotator period
+    3200 at 32 Msps, 32 tone bins)."""
+    N, cof, fs, off = 3_200_000, 2, 32e6, 10e3
+    spf = 2500
+    nfr = N * cof // spf + 2
+    rng = np.random.default_rng(1002)
+    phases = rng.uniform(0, 2 * np.pi, 16)
+    data, T = _mark5b(16, 2, nfr, 1002,
+                      tones=lambda T: synth.pcal_comb(T, fs, 1e6, off, 0.05, phases))
+    lay = gpu.layout("mark5b", 16, 2)
+    cfg = gpu.make_config(lay, N, "cosine2", 1, cof, sources=((0, 0), (0, 7)), max_run_bytes=len(data),
+                          extract_pcal=True, pcal_tonebins=32, pcal_rotatorlen=3200, samplingfreq=fs,
+                          pcal_offset_hz=off)
+    core = gpu.Core(cfg)
+    auto, _, pc, ns = core.run([data])
+    s = decode_channels(data, "Mark5B-1024-16-2", 16, 2, [0, 7], T)
+    ra, _, rp, nref = oracle_run(s, N, "cosine2", 1, cof,
+                                 pcal=dict(tonebins=32, rotatorlen=3200, fs=fs, offset=off))
+    r32, _, _, _ = _fp32_run(s, N, "cosine2", 1, cof)
+    assert ns == nref == 1
+    for k in range(2):
+        _check_auto(auto[0, k], ra[0, k], r32[0, k])
+    assert np.max(np.abs(pc - rp)) / np.max(np.abs(rp)) < 1e-6
