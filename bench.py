@@ -244,16 +244,11 @@ def gpu_arm(args) -> None:
 
     from swspec_b200 import gpu, synth, synth_gpu
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from swspec_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    reps = Replicas("nccl")
+    world, rank = reps.world, reps.rank
 
     precisions = [gpu.PREC_FP32]
     if args.precision in ("tcsplit", "auto") and tc_available(gpu):
@@ -285,16 +280,8 @@ def gpu_arm(args) -> None:
         core.process_device([d_raw.data_ptr()], RUN_BYTES, RUNS_PER_SPECTRUM, RUNS_PER_SPECTRUM,
                             d_auto.data_ptr(), d_xpol.data_ptr(), 0, stream.cuda_stream)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = reps.barrier
+    max_over_ranks = reps.max
 
     forms = {}
     launches_per_step = 0
@@ -381,8 +368,7 @@ def gpu_arm(args) -> None:
         log(f"[parity] {parity}")
 
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        reps.close()
         return
 
     hl = forms["tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32"]
@@ -427,8 +413,7 @@ def gpu_arm(args) -> None:
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "parity": parity}
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
 
 
 def tc_available(gpu) -> bool:
