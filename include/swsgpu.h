@@ -151,20 +151,39 @@ int swsgpu_run_shape(const swsgpu_handle *h, size_t nbytes, int *nspectra, int *
  * raw[s] points to host memory holding nbytes[s] bytes of stream s, whole
  * frames when the layout has headers.  The host memory must stay valid and
  * unchanged until swsgpu_wait returns (the reference's double-buffer rule).
+ * Input copies run on their own stream into one of two device slots, so a
+ * run's copy overlaps the previous run's kernels; pinned host memory (see
+ * swsgpu_host_register) makes them asynchronous.  A run that completes no
+ * spectrum (runs_per_output > 1, not the last of its group) may be followed
+ * by the next submit before its wait; a run that completes spectra must be
+ * waited for (and fetched) first, else SWSGPU_ESTATE.
  * stream_payload_offset[s] is the payload byte offset of raw[s] within its
  * recording (fixes mark5access's per-frame blanking zones; 0 for a run that
  * starts on a frame). */
 int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
                   const int64_t *stream_payload_offset);
 
-/* TaskCore::join: wait up to timeout_ms (<0: forever) for the queued run;
- * *nspectra gets the spectrum count (TaskCore::join's return value).  With
- * runs_per_output > 1 it is 0 until the run that completes a group, whose
- * fetch returns the combined spectra. */
+/* TaskCore::join: wait up to timeout_ms (<0: forever) until the submitted
+ * input buffers may be reused and any spectra the run completes are in
+ * host memory; *nspectra gets the spectrum count (TaskCore::join's return
+ * value).  With runs_per_output > 1 it is 0 until the run that completes a
+ * group, whose fetch returns the combined spectra; for the other runs the
+ * wait ends when their input copy has finished (their kernels keep running
+ * and are ordered before the group's last run).  Device errors of earlier
+ * runs are reported by the wait that follows them. */
 int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra);
 
 /* Copy the spectra of the completed run into caller memory. */
 int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out);
+
+/* Page-lock caller memory that will be passed to swsgpu_submit, so its
+ * input copies are DMA transfers that overlap kernels (the reference's raw
+ * buffers are allocated once by main, src/swspectrometer.cpp:373-413, and
+ * live for the whole run).  Memory already pinned is accepted as is.  No
+ * counterpart in the reference (its cores read host memory directly). */
+int swsgpu_host_register(void *p, size_t bytes);
+/* Undo swsgpu_host_register before the memory is freed. */
+int swsgpu_host_unregister(void *p);
 
 /* Throughput path with data already in device memory: processes `nruns`
  * consecutive runs of run_bytes payload bytes per stream (d_raw[s] holds

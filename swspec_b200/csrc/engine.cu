@@ -93,6 +93,29 @@ struct Schedule {
    int nffts = 0;
 };
 
+// A schedule built once and kept on the device: runs of the same size and
+// outputs reuse it, so a submit uploads nothing but its raw bytes.
+struct SchedEntry {
+   // key
+   size_t run_bytes = 0;
+   int nruns = 0, rpo = 0, acc_mode = 0;
+   float *d_auto = nullptr, *d_xpol = nullptr, *d_pcal = nullptr;
+   void *acc_base = nullptr;
+   // value
+   Schedule sc;
+   DevBuf d_items, d_entries, d_outs, d_pcal_jobs, d_bjobs, d_bitems;
+   std::vector<int4> batches;  // four-step: {job0, njobs, item0, nitems}
+   void release()
+   {
+      d_items.release();
+      d_entries.release();
+      d_outs.release();
+      d_pcal_jobs.release();
+      d_bjobs.release();
+      d_bitems.release();
+   }
+};
+
 struct swsgpu_handle {
    swsgpu_config cfg;
    int device = 0;
@@ -102,8 +125,16 @@ struct swsgpu_handle {
    int S = 0;
    int max_clusters = 1;
    std::string err;
-   cudaStream_t stream = nullptr;
-   cudaEvent_t done = nullptr;
+   cudaStream_t stream = nullptr;     // kernels and result copies
+   cudaStream_t cstream = nullptr;    // input copies of submit()
+   cudaEvent_t done = nullptr;        // results of the last submitted run copied back
+   // two device input slots per stream: run r+1's copy overlaps run r's kernels
+   DevBuf d_slot[2][SWSGPU_MAX_STREAMS];
+   cudaEvent_t slot_h2d[2] = {nullptr, nullptr};   // input copy into the slot finished
+   cudaEvent_t slot_free[2] = {nullptr, nullptr};  // kernels finished reading the slot
+   int next_slot = 0;
+   cudaEvent_t last_h2d = nullptr;    // input copy of the last submitted run
+   bool pending_out = false;          // the pending run completes spectra
    bool pending = false;
    int pending_nspec = 0;
    int last_launches = 0;
@@ -126,6 +157,11 @@ struct swsgpu_handle {
    DevBuf d_acc64;
    int group_pos = 0;
    bool fetch_ready = false;
+   // device-resident schedules (a few distinct run shapes per handle)
+   std::vector<SchedEntry *> sched;
+   // per-stream channel lists of the code arrays (K1), uploaded at create
+   std::vector<int> chans_of[SWSGPU_MAX_STREAMS];
+   int first_code[SWSGPU_MAX_STREAMS] = {-1, -1};
    // kernel timing
    bool profiling = false;
    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
@@ -391,49 +427,21 @@ static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int ru
 // ---------------------------------------------------------------------------
 static const size_t kBigScratchBudget = (size_t)1 << 30;  // bytes of column-pass output per batch
 
-static int launch_big(swsgpu_handle *h, const Schedule &sc, long long code_words, long long blank_words,
-                      cudaStream_t st, int &launches)
+// Whole work items per batch; a single item above the budget runs alone.
+static void big_batches(const swsgpu_handle *h, const Schedule &sc, std::vector<BigJob> &jobs,
+                        std::vector<BigItem> &bitems, std::vector<int4> &batches)
 {
-   const swsgpu_config &c = h->cfg;
-   const BigPlan &bp = h->bplan;
-   const int nbit = c.layout[0].nbit;
-   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
-   const size_t job_bytes = sizeof(float2) * (size_t)c.fft_points;
-   BigArgs a;
-   a.codes = (const uint32_t *)h->d_codes.p;
-   a.code_words = code_words;
-   a.blank = (const uint32_t *)h->d_blank.p;
-   a.blank_words = blank_words;
-   a.blank_any = (const int *)h->d_blank_any.p;
-   a.code_stream = (const int *)h->d_code_stream.p;
-   a.window = (const float *)h->d_window.p;
-   a.tw1 = (const float2 *)h->d_tw1.p;
-   a.tw2 = (const float2 *)h->d_tw2.p;
-   a.twA = (const float2 *)h->d_twA.p;
-   a.twB = (const float2 *)h->d_twB.p;
-   a.partial = (float *)h->d_partial.p;
-   a.N = c.fft_points;
-   a.S = h->S;
-   a.levels = level_table(c.layout[0].format, nbit);
-   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-   if (h->profiling) {
-      CK(h, cudaEventCreate(&ev0));
-      CK(h, cudaEventCreate(&ev1));
-      CK(h, cudaEventRecord(ev0, st));
-   }
-   std::vector<BigJob> jobs;
-   std::vector<BigItem> bitems;
+   const size_t job_bytes = sizeof(float2) * (size_t)h->cfg.fft_points;
    size_t i0 = 0;
    while (i0 < sc.items.size()) {
-      jobs.clear();
-      bitems.clear();
+      const int job_base = (int)jobs.size(), item_base = (int)bitems.size();
       size_t i = i0;
-      // whole items per batch; a single item above the budget runs alone
       while (i < sc.items.size()) {
          const Item &it = sc.items[i];
-         if (!bitems.empty() && (jobs.size() + it.nfr) * job_bytes > kBigScratchBudget) break;
+         const size_t in_batch = jobs.size() - job_base;
+         if (i > i0 && (in_batch + it.nfr) * job_bytes > kBigScratchBudget) break;
          BigItem bi;
-         bi.job0 = (int)jobs.size();
+         bi.job0 = (int)in_batch;
          bi.nfr = it.nfr;
          bi.mode = it.mode;
          bi.item = (int)i;
@@ -450,25 +458,147 @@ static int launch_big(swsgpu_handle *h, const Schedule &sc, long long code_words
          bitems.push_back(bi);
          i++;
       }
-      CK(h, h->d_scratch.ensure(job_bytes * jobs.size()));
-      CK(h, h->d_bjobs.ensure(sizeof(BigJob) * jobs.size()));
-      CK(h, h->d_bitems.ensure(sizeof(BigItem) * bitems.size()));
-      CK(h, cudaMemcpyAsync(h->d_bjobs.p, jobs.data(), sizeof(BigJob) * jobs.size(), cudaMemcpyHostToDevice, st));
-      CK(h, cudaMemcpyAsync(h->d_bitems.p, bitems.data(), sizeof(BigItem) * bitems.size(),
-                            cudaMemcpyHostToDevice, st));
-      a.jobs = (const BigJob *)h->d_bjobs.p;
-      a.bitems = (const BigItem *)h->d_bitems.p;
-      a.scratch = (float2 *)h->d_scratch.p;
-      bp.cols[nbi]<<<dim3(bp.N2 / bp.C, (unsigned)jobs.size()), bp.TA, bp.smem_cols, st>>>(a);
-      bp.rows<<<dim3(bp.N1 / 2 + 1, (unsigned)bitems.size()), bp.TB, bp.smem_rows, st>>>(a);
+      batches.push_back(make_int4(job_base, (int)jobs.size() - job_base, item_base,
+                                  (int)bitems.size() - item_base));
+      i0 = i;
+   }
+}
+
+static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_words, long long blank_words,
+                      cudaStream_t st, int &launches)
+{
+   const swsgpu_config &c = h->cfg;
+   const BigPlan &bp = h->bplan;
+   const int nbit = c.layout[0].nbit;
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   const size_t job_bytes = sizeof(float2) * (size_t)c.fft_points;
+   int max_jobs = 0;
+   for (const int4 &b : se.batches) max_jobs = std::max(max_jobs, b.y);
+   CK(h, h->d_scratch.ensure(job_bytes * (size_t)max_jobs));
+   BigArgs a;
+   a.codes = (const uint32_t *)h->d_codes.p;
+   a.code_words = code_words;
+   a.blank = (const uint32_t *)h->d_blank.p;
+   a.blank_words = blank_words;
+   a.blank_any = (const int *)h->d_blank_any.p;
+   a.code_stream = (const int *)h->d_code_stream.p;
+   a.window = (const float *)h->d_window.p;
+   a.tw1 = (const float2 *)h->d_tw1.p;
+   a.tw2 = (const float2 *)h->d_tw2.p;
+   a.twA = (const float2 *)h->d_twA.p;
+   a.twB = (const float2 *)h->d_twB.p;
+   a.scratch = (float2 *)h->d_scratch.p;
+   a.partial = (float *)h->d_partial.p;
+   a.N = c.fft_points;
+   a.S = h->S;
+   a.levels = level_table(c.layout[0].format, nbit);
+   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+   if (h->profiling) {
+      CK(h, cudaEventCreate(&ev0));
+      CK(h, cudaEventCreate(&ev1));
+      CK(h, cudaEventRecord(ev0, st));
+   }
+   for (const int4 &b : se.batches) {
+      a.jobs = (const BigJob *)se.d_bjobs.p + b.x;
+      a.bitems = (const BigItem *)se.d_bitems.p + b.z;
+      bp.cols[nbi]<<<dim3(bp.N2 / bp.C, (unsigned)b.y), bp.TA, bp.smem_cols, st>>>(a);
+      bp.rows<<<dim3(bp.N1 / 2 + 1, (unsigned)b.w), bp.TB, bp.smem_rows, st>>>(a);
       CK(h, cudaGetLastError());
       launches += 2;
-      i0 = i;
    }
    if (h->profiling) {
       CK(h, cudaEventRecord(ev1, st));
       h->prof_events.push_back(std::make_pair(ev0, ev1));
    }
+   return SWSGPU_OK;
+}
+
+static void drop_schedules(swsgpu_handle *h)
+{
+   for (SchedEntry *e : h->sched) {
+      e->release();
+      delete e;
+   }
+   h->sched.clear();
+}
+
+// The device-resident schedule of a run shape (built and uploaded once).
+static int get_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int rpo, float *d_auto, float *d_xpol,
+                        float *d_pcal, int acc_mode, SchedEntry **out)
+{
+   for (SchedEntry *e : h->sched)
+      if (e->run_bytes == run_bytes && e->nruns == nruns && e->rpo == rpo && e->d_auto == d_auto &&
+          e->d_xpol == d_xpol && e->d_pcal == d_pcal && e->acc_mode == acc_mode &&
+          (acc_mode == 0 || e->acc_base == h->d_acc64.p)) {
+         *out = e;
+         return SWSGPU_OK;
+      }
+   if (h->sched.size() >= 8) drop_schedules(h);  // cudaFree waits for work that may still use them
+   SchedEntry *e = new SchedEntry();
+   e->run_bytes = run_bytes;
+   e->nruns = nruns;
+   e->rpo = rpo;
+   e->d_auto = d_auto;
+   e->d_xpol = d_xpol;
+   e->d_pcal = d_pcal;
+   e->acc_mode = acc_mode;
+   Schedule &sc = e->sc;
+   build_schedule(h, run_bytes, nruns, rpo, d_auto, d_xpol, d_pcal, sc);
+   auto bail = [&](cudaError_t err, const char *what) {
+      e->release();
+      delete e;
+      return fail(h, SWSGPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(err));
+   };
+   if (acc_mode != 0) {
+      const size_t need = sizeof(double) * (size_t)h->S * (sc.outs.size() + 1);
+      if (need > h->d_acc64.n) {
+         // the running sums move: schedules pointing at the old ones go
+         std::vector<SchedEntry *> keep;
+         for (SchedEntry *o : h->sched) {
+            if (o->acc_mode != 0) {
+               o->release();
+               delete o;
+            } else {
+               keep.push_back(o);
+            }
+         }
+         h->sched = keep;
+         cudaError_t err = h->d_acc64.ensure(need);
+         if (err != cudaSuccess) return bail(err, "accumulator allocation");
+      }
+      e->acc_base = h->d_acc64.p;
+      for (size_t i = 0; i < sc.outs.size(); i++) {
+         sc.outs[i].acc = (double *)h->d_acc64.p + i * (size_t)h->S;
+         sc.outs[i].acc_mode = acc_mode;
+      }
+   } else {
+      for (auto &o : sc.outs) {
+         o.acc = nullptr;
+         o.acc_mode = 0;
+      }
+   }
+   auto upload = [&](DevBuf &d, const void *src, size_t bytes) {
+      if (bytes == 0) return cudaSuccess;
+      cudaError_t err = d.ensure(bytes);
+      if (err != cudaSuccess) return err;
+      return cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice);
+   };
+   cudaError_t err;
+   if ((err = upload(e->d_items, sc.items.data(), sizeof(Item) * sc.items.size())) != cudaSuccess ||
+       (err = upload(e->d_entries, sc.entries.data(), sizeof(RedEntry) * sc.entries.size())) != cudaSuccess ||
+       (err = upload(e->d_outs, sc.outs.data(), sizeof(OutVec) * sc.outs.size())) != cudaSuccess ||
+       (err = upload(e->d_pcal_jobs, sc.pcal_jobs.data(), sizeof(PcalJob) * sc.pcal_jobs.size())) != cudaSuccess)
+      return bail(err, "schedule upload");
+   if (h->big) {
+      std::vector<BigJob> jobs;
+      std::vector<BigItem> bitems;
+      big_batches(h, sc, jobs, bitems, e->batches);
+      if ((err = upload(e->d_bjobs, jobs.data(), sizeof(BigJob) * jobs.size())) != cudaSuccess ||
+          (err = upload(e->d_bitems, bitems.data(), sizeof(BigItem) * bitems.size())) != cudaSuccess)
+         return bail(err, "four-step job upload");
+   }
+   h->sched.push_back(e);
+   *out = e;
    return SWSGPU_OK;
 }
 
@@ -482,21 +612,13 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
                         int pcal_write = 1)
 {
    const swsgpu_config &c = h->cfg;
-   Schedule sc;
-   build_schedule(h, run_bytes, nruns, runs_per_output, d_auto, d_xpol, d_pcal, sc);
-   if (nspec_out) *nspec_out = sc.nspec_total;
-   if (acc_mode != 0) {
-      CK(h, h->d_acc64.ensure(sizeof(double) * (size_t)h->S * (sc.outs.size() + 1)));
-      for (size_t i = 0; i < sc.outs.size(); i++) {
-         sc.outs[i].acc = (double *)h->d_acc64.p + i * (size_t)h->S;
-         sc.outs[i].acc_mode = acc_mode;
-      }
-   } else {
-      for (auto &o : sc.outs) {
-         o.acc = nullptr;
-         o.acc_mode = 0;
-      }
+   SchedEntry *se = nullptr;
+   {
+      int rc = get_schedule(h, run_bytes, nruns, runs_per_output, d_auto, d_xpol, d_pcal, acc_mode, &se);
+      if (rc != SWSGPU_OK) return rc;
    }
+   const Schedule &sc = se->sc;
+   if (nspec_out) *nspec_out = sc.nspec_total;
    int launches = 0;
    const int S = h->S;
    const int ncode = (int)h->code_stream.size();
@@ -535,18 +657,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(
           si, (int2 *)h->d_valid[s].p, (int *)h->d_blank_any.p + s);
       launches++;
-      std::vector<int> chans;
-      int first_code = -1;
-      for (int k = 0; k < ncode; k++)
-         if (h->code_stream[k] == s) {
-            if (first_code < 0) first_code = k;
-            chans.push_back(h->code_chan[k]);
-         }
+      const std::vector<int> &chans = h->chans_of[s];
       if (chans.empty()) continue;
-      CK(h, h->d_chans[s].ensure(sizeof(int) * chans.size()));
-      CK(h, cudaMemcpyAsync(h->d_chans[s].p, chans.data(), sizeof(int) * chans.size(),
-                            cudaMemcpyHostToDevice, st));
-      uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)first_code * code_words;
+      uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)h->first_code[s] * code_words;
       uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
       CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(), codes, D, wpp,
                                 (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank));
@@ -557,12 +670,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    // K2
    const int nitems = (int)sc.items.size();
    if (nitems > 0) {
-      CK(h, h->d_items.ensure(sizeof(Item) * nitems));
-      CK(h, cudaMemcpyAsync(h->d_items.p, sc.items.data(), sizeof(Item) * nitems,
-                            cudaMemcpyHostToDevice, st));
       CK(h, h->d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
       if (h->big) {
-         int rc = launch_big(h, sc, code_words, blank_words, st, launches);
+         int rc = launch_big(h, *se, code_words, blank_words, st, launches);
          if (rc != SWSGPU_OK) return rc;
       } else {
          SpecArgs a;
@@ -574,7 +684,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          a.blank_words = blank_words;
          a.blank_any = (const int *)h->d_blank_any.p;
          a.code_stream = (const int *)h->d_code_stream.p;
-         a.items = (const Item *)h->d_items.p;
+         a.items = (const Item *)se->d_items.p;
          a.nitems = nitems;
          a.window = (const float *)h->d_window.p;
          a.twQ = (const float2 *)h->d_twQ.p;
@@ -616,15 +726,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       // K3
       const int nouts = (int)sc.outs.size();
       if (nouts > 0) {
-         CK(h, h->d_entries.ensure(sizeof(RedEntry) * sc.entries.size()));
-         CK(h, h->d_outs.ensure(sizeof(OutVec) * nouts));
-         CK(h, cudaMemcpyAsync(h->d_entries.p, sc.entries.data(), sizeof(RedEntry) * sc.entries.size(),
-                               cudaMemcpyHostToDevice, st));
-         CK(h, cudaMemcpyAsync(h->d_outs.p, sc.outs.data(), sizeof(OutVec) * nouts,
-                               cudaMemcpyHostToDevice, st));
          dim3 grid((S + 255) / 256, nouts);
          k_reduce<<<grid, 256, 0, st>>>((const float *)h->d_partial.p, S,
-                                         (const RedEntry *)h->d_entries.p, (const OutVec *)h->d_outs.p);
+                                         (const RedEntry *)se->d_entries.p, (const OutVec *)se->d_outs.p);
          launches++;
       }
    }
@@ -638,9 +742,6 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       if (!sc.pcal_jobs.empty()) {
          CK(h, h->d_pcal_part.ensure(sizeof(double) * 2 * c.pcal_tonebins * (size_t)nout));
          int njobs = (int)sc.pcal_jobs.size();
-         CK(h, h->d_pcal_jobs.ensure(sizeof(PcalJob) * njobs));
-         CK(h, cudaMemcpyAsync(h->d_pcal_jobs.p, sc.pcal_jobs.data(), sizeof(PcalJob) * njobs,
-                               cudaMemcpyHostToDevice, st));
          PcalArgs pa;
          pa.codes = (const uint32_t *)h->d_codes.p;
          pa.code_words = code_words;
@@ -650,7 +751,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          pa.blank_words = blank_words;
          pa.blank_any = (const int *)h->d_blank_any.p;
          pa.code_stream = (const int *)h->d_code_stream.p;
-         pa.jobs = (const PcalJob *)h->d_pcal_jobs.p;
+         pa.jobs = (const PcalJob *)se->d_pcal_jobs.p;
          pa.njobs = njobs;
          pa.N = c.fft_points;
          pa.tonebins = c.pcal_tonebins;
@@ -806,12 +907,23 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       h->code_chan = cc;
       for (auto &x : h->src_code) x = inv[x];
    }
+   for (int s = 0; s < cfg->num_streams; s++) {
+      for (int k = 0; k < (int)h->code_stream.size(); k++)
+         if (h->code_stream[k] == s) {
+            if (h->first_code[s] < 0) h->first_code[s] = k;
+            h->chans_of[s].push_back(h->code_chan[k]);
+         }
+   }
    h->auto_owner.assign(cfg->num_sources, -1);
    for (int x = 0; x < cfg->num_xpols; x++)
       for (int k = 0; k < 2; k++)
          if (h->auto_owner[cfg->xpol_pair[x][k]] < 0) h->auto_owner[cfg->xpol_pair[x][k]] = x;
    // a pair (i, i) cannot own both autos twice; treat it as owning source i once
-   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+   bool ev_ok = cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) == cudaSuccess;
+   for (int k = 0; k < 2 && ev_ok; k++)
+      ev_ok = cudaEventCreateWithFlags(&h->slot_h2d[k], cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&h->slot_free[k], cudaEventDisableTiming) == cudaSuccess;
+   if (!ev_ok || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
        cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming) != cudaSuccess) {
       h->err = "stream/event creation failed";
       return bail(SWSGPU_ECUDA);
@@ -857,6 +969,12 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
          CKB(cudaMemcpy(t.first->p, t.second->data(), sizeof(float2) * t.second->size(), cudaMemcpyHostToDevice));
       }
    }
+   for (int s = 0; s < cfg->num_streams; s++) {
+      if (h->chans_of[s].empty()) continue;
+      CKB(h->d_chans[s].ensure(sizeof(int) * h->chans_of[s].size()));
+      CKB(cudaMemcpy(h->d_chans[s].p, h->chans_of[s].data(), sizeof(int) * h->chans_of[s].size(),
+                     cudaMemcpyHostToDevice));
+   }
    CKB(h->d_code_stream.ensure(sizeof(int) * h->code_stream.size()));
    CKB(cudaMemcpy(h->d_code_stream.p, h->code_stream.data(), sizeof(int) * h->code_stream.size(),
                   cudaMemcpyHostToDevice));
@@ -868,7 +986,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
                                (int)bplan.smem_cols));
       CKB(cudaFuncSetAttribute((const void *)bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)bplan.smem_rows));
-      for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_raw[s].ensure(cfg->max_run_bytes + 64));
+      for (int k = 0; k < 2; k++)
+      for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
       *out = h;
       return SWSGPU_OK;
    }
@@ -898,7 +1017,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       h->max_clusters = ncl;
    }
    // device buffers for submit()
-   for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_raw[s].ensure(cfg->max_run_bytes + 64));
+   for (int k = 0; k < 2; k++)
+      for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
 #undef CKB
    *out = h;
    return SWSGPU_OK;
@@ -916,6 +1036,13 @@ void swsgpu_destroy(swsgpu_handle *h)
                      &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs,
                      &h->d_bitems};
    for (DevBuf *b : bufs) b->release();
+   drop_schedules(h);
+   if (h->cstream) cudaStreamSynchronize(h->cstream);
+   for (int k = 0; k < 2; k++) {
+      for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) h->d_slot[k][s].release();
+      if (h->slot_h2d[k]) cudaEventDestroy(h->slot_h2d[k]);
+      if (h->slot_free[k]) cudaEventDestroy(h->slot_free[k]);
+   }
    for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) {
       h->d_raw[s].release();
       h->d_valid[s].release();
@@ -926,6 +1053,7 @@ void swsgpu_destroy(swsgpu_handle *h)
    drop_prof_events(h);
    if (h->done) cudaEventDestroy(h->done);
    if (h->stream) cudaStreamDestroy(h->stream);
+   if (h->cstream) cudaStreamDestroy(h->cstream);
    delete h;
 }
 
@@ -943,9 +1071,13 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
                   const int64_t *stream_payload_offset)
 {
    if (!h || !raw || !nbytes) return SWSGPU_EINVAL;
-   if (h->pending) return fail(h, SWSGPU_ESTATE, "submit while a run is pending");
+   if (h->pending && h->pending_out)
+      return fail(h, SWSGPU_ESTATE, "submit while a run's spectra are pending (wait and fetch first)");
    const swsgpu_config &c = h->cfg;
    CK(h, cudaSetDevice(h->device));
+   // input slot: its previous run's kernels must have finished reading it
+   const int slot = h->next_slot;
+   CK(h, cudaStreamWaitEvent(h->cstream, h->slot_free[slot], 0));
    // payload bytes per stream: the reference walks min over sources
    size_t payload_min = (size_t)-1;
    long long grid_off[SWSGPU_MAX_STREAMS];
@@ -970,11 +1102,14 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       if (nbytes[s] > c.max_run_bytes + (size_t)c.max_run_bytes / 8 + 1024 + 64)
          return fail(h, SWSGPU_EINVAL, "buffer larger than max_run_bytes");
       payload_min = std::min(payload_min, pay);
-      CK(h, h->d_raw[s].ensure(nbytes[s] + 64));
-      CK(h, cudaMemcpyAsync(h->d_raw[s].p, raw[s], nbytes[s], cudaMemcpyHostToDevice, h->stream));
+      CK(h, cudaMemcpyAsync(h->d_slot[slot][s].p, raw[s], nbytes[s], cudaMemcpyHostToDevice, h->cstream));
       raw_bytes[s] = nbytes[s];
-      d_raw[s] = h->d_raw[s].p;
+      d_raw[s] = h->d_slot[slot][s].p;
    }
+   CK(h, cudaEventRecord(h->slot_h2d[slot], h->cstream));
+   CK(h, cudaStreamWaitEvent(h->stream, h->slot_h2d[slot], 0));
+   h->last_h2d = h->slot_h2d[slot];
+   h->next_slot ^= 1;
    RunShape rs = run_shape(c, samples_of(c.layout[0], payload_min));
    const int S = h->S;
    const int nsp = std::max(rs.nspec, 0);
@@ -1007,6 +1142,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       if (rc) return rc;
       if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
    }
+   CK(h, cudaEventRecord(h->slot_free[slot], h->stream));
    h->fetch_ready = group_end;
    if (nsp > 0 && group_end) {
       char *hp = (char *)h->h_out.p;
@@ -1022,6 +1158,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
    }
    CK(h, cudaEventRecord(h->done, h->stream));
    h->pending = true;
+   h->pending_out = nsp > 0 && group_end;
    h->pending_nspec = group_end ? nspec : 0;
    return SWSGPU_OK;
 }
@@ -1031,9 +1168,11 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
    if (!h) return SWSGPU_EINVAL;
    if (!h->pending) return fail(h, SWSGPU_ESTATE, "wait without a submitted run");
    CK(h, cudaSetDevice(h->device));
+   // a run that completes no spectrum only has to release its input buffers
+   cudaEvent_t ev = (h->pending_out || !h->last_h2d) ? h->done : h->last_h2d;
    auto t0 = std::chrono::steady_clock::now();
    while (true) {
-      cudaError_t e = cudaEventQuery(h->done);
+      cudaError_t e = cudaEventQuery(ev);
       if (e == cudaSuccess) break;
       if (e != cudaErrorNotReady) {
          h->pending = false;
@@ -1046,7 +1185,38 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
       std::this_thread::sleep_for(std::chrono::microseconds(50));
    }
    h->pending = false;
+   h->pending_out = false;
    if (nspectra) *nspectra = h->pending_nspec;
+   return SWSGPU_OK;
+}
+
+int swsgpu_host_register(void *p, size_t bytes)
+{
+   if (!p || bytes == 0) return SWSGPU_EINVAL;
+   cudaPointerAttributes at;
+   if (cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost) return SWSGPU_OK;
+   cudaGetLastError();
+   cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterDefault);
+   if (e == cudaErrorHostMemoryAlreadyRegistered) {
+      cudaGetLastError();
+      return SWSGPU_OK;
+   }
+   if (e != cudaSuccess) {
+      cudaGetLastError();
+      g_create_error = std::string("cudaHostRegister: ") + cudaGetErrorString(e);
+      return SWSGPU_ECUDA;
+   }
+   return SWSGPU_OK;
+}
+
+int swsgpu_host_unregister(void *p)
+{
+   if (!p) return SWSGPU_EINVAL;
+   cudaError_t e = cudaHostUnregister(p);
+   if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e == cudaErrorHostMemoryNotRegistered ? SWSGPU_EINVAL : SWSGPU_ECUDA;
+   }
    return SWSGPU_OK;
 }
 

@@ -238,6 +238,7 @@ private:
    int64_t t_submit_ = 0;
    double total_runtime_ = 0;
    std::vector<float> staged_, stagedx_, stagedp_;
+   std::vector<void *> pinned_;  // raw buffers page-locked for asynchronous input copies
 };
 
 class TaskDispatcher {

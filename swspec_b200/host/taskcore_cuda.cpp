@@ -7,6 +7,7 @@
 // them into the dispatcher's buffers (:311-349).  With GpuCombineOnDevice the
 // runs of one spectrum are summed on the device (FP64 between runs) and only
 // the completed spectrum is copied back.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 
@@ -17,6 +18,7 @@ namespace swshost {
 TaskCoreCUDA::~TaskCoreCUDA()
 {
    if (h_) swsgpu_destroy(h_);
+   for (void *p : pinned_) swsgpu_host_unregister(p);
 }
 
 static int window_code(WindowFunctionType w)
@@ -83,6 +85,12 @@ int TaskCoreCUDA::run(Buffer **inbuf, Buffer **outbuf, Buffer **xpolbuf, Buffer 
    for (int s = 0; s < cfg_->num_sources; s++) {
       raw[s] = inbuf[s]->getData();
       nbytes[s] = minlen;  // doMaths walks the shortest source buffer
+      // main allocates the raw buffers once (swspectrometer.cpp:373-413):
+      // page-lock each on first sight so its copy is an asynchronous DMA
+      void *p = inbuf[s]->getData();
+      if (std::find(pinned_.begin(), pinned_.end(), p) == pinned_.end() &&
+          swsgpu_host_register(p, inbuf[s]->getAllocated()) == SWSGPU_OK)
+         pinned_.push_back(p);
    }
    int nspec = 0, nffts = 0, partial = 0;
    swsgpu_run_shape(h_, minlen, &nspec, &nffts, &partial);
@@ -199,6 +207,8 @@ int TaskCoreCUDA::finalize()
                << total_ffts_ << " FFTs" << std::endl;
    if (h_) swsgpu_destroy(h_);
    h_ = nullptr;
+   for (void *p : pinned_) swsgpu_host_unregister(p);
+   pinned_.clear();
    return 0;
 }
 
