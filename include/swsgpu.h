@@ -111,6 +111,10 @@ typedef struct swsgpu_config {
                                        (src/TaskDispatcher.cpp:143-171,
                                        TaskCoreIPP::combineResults :311-349); sums are
                                        kept in FP64 between runs */
+   int pcal_ntones;                 /* >0: also return the phasors of the first pcal_ntones
+                                       tones (k * spacing + offset, k < ntones <= tonebins/2),
+                                       the PCal library's tone output (src/IA-32/PhaseCal/
+                                       PCal.cpp:654-678), computed in FP64 */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;
@@ -119,11 +123,14 @@ typedef struct swsgpu_handle swsgpu_handle;
  *   auto_out : float [nspectra][num_sources][N/2+1]
  *   xpol_out : float [nspectra][num_xpols][N/2+1][2]   (re, im)
  *   pcal_out : float [nspectra][num_sources][pcal_tonebins][2]
+ *   tones_out: double [nspectra][num_sources][pcal_ntones][2]  (re, im of each tone
+ *              phasor: mean over the folded samples; amplitude = |.|, phase = arg)
  * Pointers for outputs that are not configured may be NULL. */
 typedef struct swsgpu_outputs {
    float *auto_out;
    float *xpol_out;
    float *pcal_out;
+   double *tones_out;
 } swsgpu_outputs;
 
 /* Library / device checks. */

@@ -150,9 +150,9 @@ struct swsgpu_handle {
    DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
    DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
    DevBuf d_pcal_jobs, d_pcal_part, d_pcal_entries, d_pcal_outs;
-   DevBuf d_out_auto, d_out_xpol, d_out_pcal;
+   DevBuf d_out_auto, d_out_xpol, d_out_pcal, d_out_tones;
    HostBuf h_out;   // pinned staging of one run's outputs
-   size_t h_auto_bytes = 0, h_xpol_bytes = 0, h_pcal_bytes = 0;
+   size_t h_auto_bytes = 0, h_xpol_bytes = 0, h_pcal_bytes = 0, h_tones_bytes = 0;
    // combining of consecutive runs on the device (runs_per_output > 1)
    DevBuf d_acc64;
    int group_pos = 0;
@@ -609,7 +609,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
                         const long long *grid_off, size_t run_bytes, int nruns,
                         int runs_per_output, float *d_auto, float *d_xpol, float *d_pcal,
                         cudaStream_t st, int *nspec_out, int acc_mode = 0, int pcal_zero = 1,
-                        int pcal_write = 1)
+                        int pcal_write = 1, double *d_tones = nullptr)
 {
    const swsgpu_config &c = h->cfg;
    SchedEntry *se = nullptr;
@@ -737,10 +737,13 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       const int nout = sc.nspec_total * c.num_sources;
       if (pcal_write && sc.pcal_jobs.empty()) {
          CK(h, cudaMemsetAsync(d_pcal, 0, sizeof(float) * 2 * c.pcal_tonebins * (size_t)nout, st));
+         if (d_tones && c.pcal_ntones > 0)
+            CK(h, cudaMemsetAsync(d_tones, 0, sizeof(double) * 2 * c.pcal_ntones * (size_t)nout, st));
          launches++;
       }
       if (!sc.pcal_jobs.empty()) {
-         CK(h, h->d_pcal_part.ensure(sizeof(double) * 2 * c.pcal_tonebins * (size_t)nout));
+         // FP64 sums [nout][tonebins][2] followed by the samples folded per output
+         CK(h, h->d_pcal_part.ensure(sizeof(double) * (2 * c.pcal_tonebins + 1) * (size_t)nout));
          int njobs = (int)sc.pcal_jobs.size();
          PcalArgs pa;
          pa.codes = (const uint32_t *)h->d_codes.p;
@@ -761,6 +764,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          pa.levels = level_table(c.layout[0].format, nbit);
          pa.out = d_pcal;
          pa.acc = (double *)h->d_pcal_part.p;
+         pa.tones = d_tones;
+         pa.ntones = d_tones ? c.pcal_ntones : 0;
          pa.nout = nout;
          pa.zero_acc = pcal_zero;
          pa.write_out = pcal_write;
@@ -843,6 +848,13 @@ static int validate_config(const swsgpu_config *c, std::string &why)
          return 0;
       }
       if (c->pcal_tonebins > 4096) { why = "pcal_tonebins > 4096"; return 0; }
+      if (c->pcal_ntones < 0 || c->pcal_ntones > c->pcal_tonebins / 2) {
+         why = "pcal_ntones must be 0..pcal_tonebins/2";
+         return 0;
+      }
+   } else if (c->pcal_ntones != 0) {
+      why = "pcal_ntones needs extract_pcal";
+      return 0;
    }
    return 1;
 }
@@ -1032,7 +1044,7 @@ void swsgpu_destroy(swsgpu_handle *h)
    DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes,
                      &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
                      &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
-                     &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal,
+                     &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal, &h->d_out_tones,
                      &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs,
                      &h->d_bitems};
    for (DevBuf *b : bufs) b->release();
@@ -1116,10 +1128,13 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
    h->h_auto_bytes = sizeof(float) * (size_t)nsp * c.num_sources * S;
    h->h_xpol_bytes = sizeof(float) * 2 * (size_t)nsp * c.num_xpols * S;
    h->h_pcal_bytes = c.extract_pcal ? sizeof(float) * 2 * (size_t)nsp * c.num_sources * c.pcal_tonebins : 0;
+   h->h_tones_bytes = (c.extract_pcal && c.pcal_ntones > 0)
+                          ? sizeof(double) * 2 * (size_t)nsp * c.num_sources * c.pcal_ntones : 0;
    CK(h, h->d_out_auto.ensure(h->h_auto_bytes + 16));
    CK(h, h->d_out_xpol.ensure(h->h_xpol_bytes + 16));
    CK(h, h->d_out_pcal.ensure(h->h_pcal_bytes + 16));
-   CK(h, h->h_out.ensure(h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes + 64));
+   CK(h, h->d_out_tones.ensure(h->h_tones_bytes + 16));
+   CK(h, h->h_out.ensure(h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes + h->h_tones_bytes + 64));
    int nspec = 0;
    const int rpo = std::max(1, c.runs_per_output);
    bool group_end = true;
@@ -1138,7 +1153,8 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, payload_min, 1, 1, (float *)h->d_out_auto.p,
                             c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
                             c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec,
-                            acc_mode, pcal_zero, pcal_write);
+                            acc_mode, pcal_zero, pcal_write,
+                            h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
       if (rc) return rc;
       if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
    }
@@ -1153,6 +1169,9 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       if (h->h_pcal_bytes)
          CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes, h->d_out_pcal.p,
                                h->h_pcal_bytes, cudaMemcpyDeviceToHost, h->stream));
+      if (h->h_tones_bytes)
+         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->d_out_tones.p,
+                               h->h_tones_bytes, cudaMemcpyDeviceToHost, h->stream));
    } else {
       h->last_launches = 0;
    }
@@ -1230,6 +1249,8 @@ int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out)
    if (out->xpol_out && h->h_xpol_bytes) memcpy(out->xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);
    if (out->pcal_out && h->h_pcal_bytes)
       memcpy(out->pcal_out, hp + h->h_auto_bytes + h->h_xpol_bytes, h->h_pcal_bytes);
+   if (out->tones_out && h->h_tones_bytes)
+      memcpy(out->tones_out, hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->h_tones_bytes);
    return SWSGPU_OK;
 }
 
@@ -1253,7 +1274,8 @@ int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run
    int nspec = 0;
    return launch_chunk(h, d_raw, raw_bytes, grid_off, run_bytes, nruns, runs_per_output,
                        d_out->auto_out, c.num_xpols ? d_out->xpol_out : nullptr,
-                       c.extract_pcal ? d_out->pcal_out : nullptr, st, &nspec);
+                       c.extract_pcal ? d_out->pcal_out : nullptr, st, &nspec, 0, 1, 1,
+                       (c.extract_pcal && c.pcal_ntones > 0) ? d_out->tones_out : nullptr);
 }
 
 int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes)

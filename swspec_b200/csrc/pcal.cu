@@ -66,6 +66,35 @@ __global__ void k_pcal_fold(PcalArgs a)
    __syncthreads();
    double *dst = a.acc + (long long)job.out * 2 * a.tonebins;
    for (int i = threadIdx.x; i < 2 * a.tonebins; i += T) atomicAdd(&dst[i], pc_smem[i]);
+   if (threadIdx.x == 0)
+      atomicAdd(a.acc + (long long)a.nout * 2 * a.tonebins + job.out, (double)(p1 - p0) * (double)a.used);
+}
+
+// Tone phasors of the folded bins: tone k (frequency k * spacing + offset,
+// moved to k * spacing by the rotator) is DFT bin k of the tonebins folded
+// sums, divided by the number of samples folded -- the final step of the
+// PCal library's extractors (src/IA-32/PhaseCal/PCal.cpp:654-678: forward DFT
+// normalised by the length, bins picked per tone), in FP64 throughout.
+__global__ void k_pcal_tones(PcalArgs a)
+{
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= (long long)a.nout * a.ntones) return;
+   const int o = (int)(t / a.ntones), k = (int)(t % a.ntones);
+   const double *bins = a.acc + (long long)o * 2 * a.tonebins;
+   const double cnt = a.acc[(long long)a.nout * 2 * a.tonebins + o];
+   double sr = 0.0, si = 0.0;
+   for (int b = 0; b < a.tonebins; b++) {
+      // exp(-2 pi i k b / tonebins), the angle reduced exactly in integers
+      const int m = (int)(((long long)k * b) % a.tonebins);
+      double s, c;
+      sincospi(-2.0 * (double)m / (double)a.tonebins, &s, &c);
+      const double re = bins[2 * b], im = bins[2 * b + 1];
+      sr += re * c - im * s;
+      si += re * s + im * c;
+   }
+   const double inv = cnt > 0.0 ? 1.0 / cnt : 0.0;
+   a.tones[2 * t] = sr * inv;
+   a.tones[2 * t + 1] = si * inv;
 }
 
 __global__ void k_pcal_out(PcalArgs a)
@@ -77,7 +106,7 @@ __global__ void k_pcal_out(PcalArgs a)
 int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
 {
    const size_t n = (size_t)a.nout * 2 * a.tonebins;
-   if (a.zero_acc) cudaMemsetAsync(a.acc, 0, sizeof(double) * n, st);
+   if (a.zero_acc) cudaMemsetAsync(a.acc, 0, sizeof(double) * (n + a.nout), st);
    const int T = 256;
    const int nper = a.N / a.rotatorlen;
    int bpj = nper < 8 ? nper : 8;
@@ -86,7 +115,13 @@ int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
    if (nbit == 1) k_pcal_fold<1><<<grid, T, sm, st>>>(a);
    else if (nbit == 2) k_pcal_fold<2><<<grid, T, sm, st>>>(a);
    else k_pcal_fold<8><<<grid, T, sm, st>>>(a);
-   if (a.write_out) k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+   if (a.write_out) {
+      k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+      if (a.tones && a.ntones > 0) {
+         const long long nt = (long long)a.nout * a.ntones;
+         k_pcal_tones<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(a);
+      }
+   }
    return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -30,7 +30,9 @@ struct PcalArgs {
    double dphi;        // 2 pi (-offset / fs)
    float4 levels;
    float *out;         // [nout][tonebins][2]
-   double *acc;        // [nout][tonebins][2] FP64 running sums
+   double *acc;        // [nout][tonebins][2] FP64 running sums, then [nout] samples folded
+   double *tones;      // [nout][ntones][2] tone phasors (null: none)
+   int ntones;
    int nout;
    int zero_acc;       // clear acc first (start of an output group)
    int write_out;      // round acc into out (end of an output group)

@@ -38,11 +38,13 @@ class Config(C.Structure):
                 ("xpol_pair", (C.c_int * 2) * MAX_SOURCES), ("extract_pcal", C.c_int),
                 ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
                 ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
-                ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int)]
+                ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int),
+                ("pcal_ntones", C.c_int)]
 
 
 class Outputs(C.Structure):
-    _fields_ = [("auto_out", C.c_void_p), ("xpol_out", C.c_void_p), ("pcal_out", C.c_void_p)]
+    _fields_ = [("auto_out", C.c_void_p), ("xpol_out", C.c_void_p), ("pcal_out", C.c_void_p),
+                ("tones_out", C.c_void_p)]
 
 
 class SwsError(RuntimeError):
@@ -105,7 +107,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
                 sources=((0, 0),), xpols=(), precision=PREC_FP32, max_run_bytes=1 << 24,
                 extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
                 pcal_offset_hz=10e3, layout2: Layout | None = None,
-                runs_per_output: int = 1) -> Config:
+                runs_per_output: int = 1, pcal_ntones: int = 0) -> Config:
     c = Config()
     c.layout[0] = lay
     c.layout[1] = layout2 if layout2 is not None else lay
@@ -130,6 +132,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
     c.pcal_offset_hz = pcal_offset_hz
     c.max_run_bytes = max_run_bytes
     c.runs_per_output = runs_per_output
+    c.pcal_ntones = pcal_ntones
     return c
 
 
@@ -186,13 +189,16 @@ class Core:
         return ns.value
 
     def fetch_into(self, auto: np.ndarray, xpol: np.ndarray | None = None,
-                   pcal: np.ndarray | None = None) -> None:
+                   pcal: np.ndarray | None = None, tones: np.ndarray | None = None) -> None:
         out = Outputs(auto.ctypes.data, None if xpol is None else xpol.ctypes.data,
-                      None if pcal is None else pcal.ctypes.data)
+                      None if pcal is None else pcal.ctypes.data,
+                      None if tones is None else tones.ctypes.data)
         _check(lib().swsgpu_fetch(self.h, C.byref(out)), self.h)
 
     def run(self, raws: list, payload_offsets=None, timeout_ms: int = 60000):
-        """One core run from host bytes (submit + wait + fetch)."""
+        """One core run from host bytes (submit + wait + fetch).  Returns
+        (auto, xpol, pcal, nspectra); tone phasors (when configured) are left
+        in self.tones as complex128 [nspectra][num_sources][pcal_ntones]."""
         n = len(raws)
         arrs = [np.frombuffer(r, dtype=np.uint8) if not isinstance(r, np.ndarray) else r
                 for r in raws]
@@ -207,18 +213,20 @@ class Core:
         auto = np.zeros((nspec, c.num_sources, self.S), dtype=np.float32)
         xpol = np.zeros((nspec, max(c.num_xpols, 1), self.S, 2), dtype=np.float32)
         pcal = np.zeros((nspec, c.num_sources, max(c.pcal_tonebins, 1), 2), dtype=np.float32)
-        out = Outputs(auto.ctypes.data, xpol.ctypes.data, pcal.ctypes.data)
+        tones = np.zeros((nspec, c.num_sources, max(c.pcal_ntones, 1), 2), dtype=np.float64)
+        out = Outputs(auto.ctypes.data, xpol.ctypes.data, pcal.ctypes.data, tones.ctypes.data)
         _check(lib().swsgpu_fetch(self.h, C.byref(out)), self.h)
+        self.tones = tones[:, :, : c.pcal_ntones, 0] + 1j * tones[:, :, : c.pcal_ntones, 1]
         xp = xpol[:, : c.num_xpols, :, 0] + 1j * xpol[:, : c.num_xpols, :, 1]
         pc = pcal[:, :, : c.pcal_tonebins, 0] + 1j * pcal[:, :, : c.pcal_tonebins, 1]
         return auto, xp, pc, nspec
 
     def process_device(self, d_raw_ptrs: list[int], run_bytes: int, nruns: int,
                        runs_per_output: int, d_auto: int, d_xpol: int = 0, d_pcal: int = 0,
-                       stream: int = 0) -> None:
+                       stream: int = 0, d_tones: int = 0) -> None:
         n = len(d_raw_ptrs)
         ptrs = (C.c_void_p * n)(*d_raw_ptrs)
-        out = Outputs(d_auto, d_xpol or None, d_pcal or None)
+        out = Outputs(d_auto, d_xpol or None, d_pcal or None, d_tones or None)
         _check(lib().swsgpu_process_device(self.h, ptrs, run_bytes, nruns, runs_per_output,
                                            C.byref(out), C.c_void_p(stream or None)), self.h)
 

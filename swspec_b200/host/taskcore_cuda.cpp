@@ -119,7 +119,7 @@ int TaskCoreCUDA::join()
    }
    total_runtime_ += 1e-9 * (double)(std::chrono::steady_clock::now().time_since_epoch().count() - t_submit_);
    if (nready > 0) {
-      swsgpu_outputs o;
+      swsgpu_outputs o = {};
       // the C ABI writes [spec][source][bins]; the reference keeps one buffer
       // per source, so fetch into a staging copy and scatter
       staged_.resize((size_t)nready * cfg_->num_sources * cfg_->fft_ssb_points);

@@ -132,7 +132,7 @@ def test_spacecraft_tone_3p2M_cosine2_pcal(gpu):
     lay = gpu.layout("mark5b", 16, 2)
     cfg = gpu.make_config(lay, N, "cosine2", 1, cof, sources=((0, 0), (0, 7)), max_run_bytes=len(data),
                           extract_pcal=True, pcal_tonebins=32, pcal_rotatorlen=3200, samplingfreq=fs,
-                          pcal_offset_hz=off)
+                          pcal_offset_hz=off, pcal_ntones=16)
     core = gpu.Core(cfg)
     auto, _, pc, ns = core.run([data])
     s = decode_channels(data, "Mark5B-1024-16-2", 16, 2, [0, 7], T)
@@ -143,3 +143,10 @@ def test_spacecraft_tone_3p2M_cosine2_pcal(gpu):
     for k in range(2):
         _check_auto(auto[0, k], ra[0, k], r32[0, k])
     assert np.max(np.abs(pc - rp)) / np.max(np.abs(rp)) < 1e-6
+    # tone phasors: FP64 on the device vs the oracle's from its folded bins;
+    # the comb's amplitude is 0.05 sigma, scaled by the 2-bit quantiser
+    for k in range(2):
+        ref = O.pcal_tones(rp[0, k], float(N * cof), 16)
+        got = core.tones[0, k]
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-6
+        assert np.max(np.abs(np.angle(got * np.conj(ref)))) < 1e-5

@@ -272,3 +272,45 @@ def test_blanked_vdif_frames(gpu):
     assert ns == nref == 5
     assert rel_err_auto(auto[:, 0], ra[:, 0]) < REL_TOL and rel_err_auto(auto[:, 1], ra[:, 1]) < REL_TOL
     assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
+
+
+def test_pcal_tones_known_answer(gpu):
+    """Tone phasors on the GPU (PCal.cpp:654-678 final step, FP64) equal the
+    FP64 oracle's from the same folded samples, and reproduce the PCal
+    library's known answer (PCal.cpp:861-951: tones
+    sin(pi n (f_off + t spacing)/BW + t 5 deg) -> phase -90 + 5 t degrees).
+    The reference checks 0.1 degree on float samples (pinned in the oracle
+    tests); an 8-bit stream of a comb that repeats every rotator period
+    carries a periodic quantisation error that no averaging removes (0.17
+    degree at 24 codes per unit), so the phase bar here is 0.5 degree."""
+    import oracle as O
+    bw, fs, spacing, off = 16e6, 32e6, 1e6, 15625.0
+    tonebins, rotatorlen = int(fs / spacing), int(fs / np.gcd(int(fs), int(off)))
+    ntones, N, cof = int(bw / spacing), 65536, 8
+    spf = 8000
+    nfr = N * cof // spf + 1
+    n = np.arange(nfr * spf, dtype=np.float64)
+    x = np.zeros(nfr * spf)
+    for t in range(ntones):
+        x += 0.5 * np.sin(np.pi * n * (off + t * spacing) / bw + np.deg2rad(5.0 * t))
+    codes = synth.quantize_vdif_8bit(x, 24.0)
+    data = synth.vdif_frames(synth.pack_codes(codes[None, :], 8), 8000, 1, 8, 4000)
+    lay = gpu.layout("vdif:8000", 1, 8)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, max_run_bytes=len(data), extract_pcal=True,
+                          pcal_tonebins=tonebins, pcal_rotatorlen=rotatorlen, samplingfreq=fs,
+                          pcal_offset_hz=off, pcal_ntones=ntones)
+    core = gpu.Core(cfg)
+    _, _, pc, ns = core.run([data])
+    tones = core.tones[0, 0]
+    ph = np.rad2deg(np.angle(tones))
+    want = -90.0 + 5.0 * np.arange(ntones)
+    d = (ph - want + 180) % 360 - 180
+    assert np.max(np.abs(d)) < 0.5, d
+    s = decode_channels(data, "VDIF_8000-256-1-8", 1, 8, [0], nfr * spf)
+    _, _, rp, nref = oracle_run(s, N, "hann", 1, cof,
+                                pcal=dict(tonebins=tonebins, rotatorlen=rotatorlen, fs=fs, offset=off))
+    assert ns == nref == 1
+    ref = O.pcal_tones(rp[0, 0], float(N * cof), ntones)
+    assert np.max(np.abs(tones - ref)) / np.max(np.abs(ref)) < 1e-6
+    # phasor = amplitude / 2 in decoded units: 0.5 / 2 * 24 / 256
+    assert np.allclose(np.abs(tones), 0.25 * 24.0 / 256.0, rtol=2e-2)
