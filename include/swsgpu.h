@@ -115,6 +115,9 @@ typedef struct swsgpu_config {
                                        tones (k * spacing + offset, k < ntones <= tonebins/2),
                                        the PCal library's tone output (src/IA-32/PhaseCal/
                                        PCal.cpp:654-678), computed in FP64 */
+   int autotune;                    /* 1: swsgpu_create times the candidate splits of a
+                                       four-step length and keeps the fastest (once per
+                                       length and bit depth per process; see swsgpu_autotune) */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;
@@ -191,6 +194,37 @@ int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out);
 int swsgpu_host_register(void *p, size_t bytes);
 /* Undo swsgpu_host_register before the memory is freed. */
 int swsgpu_host_unregister(void *p);
+
+/* Autotuner (no counterpart in the reference, whose IPP core has one FFT
+ * plan per length): for a length on the four-step path, times every
+ * candidate split N = N1 x N2 and columns-per-CTA width on a hash-filled run
+ * of two frames per source with this core's sources, pairs and window, and
+ * keeps the fastest; later cores of the same length and bit depth in this
+ * process start with that choice.  Cluster lengths have one plan and return
+ * at once.  Synchronous; call it with no run pending. */
+int swsgpu_autotune(swsgpu_handle *h, int iterations);
+
+/* Text description of the plan a core uses (split, tile, candidate). */
+int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len);
+
+/* Batches: the runs of many cores -- streams of different FFT lengths, bit
+ * depths and integrations -- recorded once as a CUDA graph and then issued
+ * with a single launch per step; each core's kernels go on its own forked
+ * stream inside the graph, so the cores run concurrently.  No counterpart
+ * in the reference (one dispatcher per recording).  swsgpu_batch_set gives
+ * core i its device inputs and outputs as for swsgpu_process_device.  The
+ * first swsgpu_batch_launch after a set runs every core eagerly (that run
+ * makes all allocations and device schedules and produces this launch's
+ * results) and records the graph; later launches replay it on cuda_stream
+ * (asynchronous, over the same device buffers).  *kernels (optional) gets
+ * the kernel count of one batch.  The cores must not be used otherwise
+ * while their batch is in flight. */
+typedef struct swsgpu_batch swsgpu_batch;
+int swsgpu_batch_create(swsgpu_handle *const *cores, int ncores, swsgpu_batch **out);
+int swsgpu_batch_set(swsgpu_batch *b, int i, const void *const *d_raw, size_t run_bytes, int nruns,
+                     int runs_per_output, const swsgpu_outputs *d_out);
+int swsgpu_batch_launch(swsgpu_batch *b, void *cuda_stream, int *kernels);
+void swsgpu_batch_destroy(swsgpu_batch *b);
 
 /* Throughput path with data already in device memory: processes `nruns`
  * consecutive runs of run_bytes payload bytes per stream (d_raw[s] holds

@@ -231,20 +231,35 @@ constexpr size_t big_rows_smem()
    return sizeof(float2) * ((size_t)2 * big_col_stride(N2) + N2);
 }
 
-#define SWS_BIG(N1_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)                                       \
-   {N1_ * N2_, N1_, N2_, 4, TA_, TB_,                                                             \
-    {k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 1>, k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 2>,    \
-     k_big_cols<N1_, N2_, 4, TA_, A1, A2, A3, 8>},                                                \
-    k_big_rows<N1_, N2_, TB_, B1, B2, B3>, big_cols_smem<N1_, N2_, 4, TA_, A1, A2, A3>(),         \
+#define SWS_BIG_C(N1_, C_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)                                 \
+   {N1_ * N2_, N1_, N2_, C_, TA_, TB_,                                                            \
+    {k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 1>, k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 2>,  \
+     k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 8>},                                               \
+    k_big_rows<N1_, N2_, TB_, B1, B2, B3>, big_cols_smem<N1_, N2_, C_, TA_, A1, A2, A3>(),        \
     big_rows_smem<N2_>()}
+#define SWS_BIG(N1_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3) SWS_BIG_C(N1_, 4, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)
 
+// Candidate splits per length; the first of each length is the default,
+// the others are timed by the autotuner (swsgpu_autotune).
 static const BigPlan kBigPlans[] = {
     SWS_BIG(512, 256, 16, 16, 2, 512, 256, 16, 16, 2),        // 2^18
+    SWS_BIG(256, 256, 16, 16, 1, 1024, 512, 16, 16, 4),
+    SWS_BIG(1024, 256, 16, 16, 4, 256, 256, 16, 16, 1),
     SWS_BIG(512, 256, 16, 16, 2, 1024, 512, 16, 16, 4),       // 2^19
+    SWS_BIG(1024, 256, 16, 16, 4, 512, 256, 16, 16, 2),
     SWS_BIG(1024, 256, 16, 16, 4, 1024, 512, 16, 16, 4),      // 2^20
+    SWS_BIG_C(1024, 8, 512, 16, 16, 4, 1024, 512, 16, 16, 4),
+    SWS_BIG(512, 256, 16, 16, 2, 2048, 512, 16, 16, 8),
+    SWS_BIG(2048, 512, 16, 16, 8, 512, 256, 16, 16, 2),
     SWS_BIG(1024, 256, 16, 16, 4, 2048, 512, 16, 16, 8),      // 2^21
+    SWS_BIG(2048, 512, 16, 16, 8, 1024, 512, 16, 16, 4),
     SWS_BIG(2048, 512, 16, 16, 8, 2048, 512, 16, 16, 8),      // 2^22
+    SWS_BIG(1024, 256, 16, 16, 4, 4096, 512, 16, 16, 16),
+    SWS_BIG(4096, 512, 16, 16, 16, 1024, 512, 16, 16, 4),
     SWS_BIG(1600, 512, 16, 4, 25, 2000, 512, 16, 5, 25),      // 3,200,000 = 2^10 5^5
+    SWS_BIG(2000, 512, 16, 5, 25, 1600, 512, 16, 4, 25),
+    SWS_BIG(3200, 512, 16, 8, 25, 1000, 512, 8, 5, 25),
+    SWS_BIG(1280, 512, 16, 16, 5, 2500, 512, 4, 25, 25),
 };
 
 bool find_big_plan(int N, BigPlan *out)
@@ -255,6 +270,14 @@ bool find_big_plan(int N, BigPlan *out)
          return true;
       }
    return false;
+}
+
+int big_plan_candidates(int N, BigPlan *out, int max)
+{
+   int n = 0;
+   for (const BigPlan &p : kBigPlans)
+      if (p.N == N && n < max) out[n++] = p;
+   return n;
 }
 
 }  // namespace sws

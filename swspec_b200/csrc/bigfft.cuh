@@ -52,5 +52,7 @@ struct BigPlan {
 };
 
 bool find_big_plan(int N, BigPlan *out);
+// Every candidate split of N (default first); returns how many were written.
+int big_plan_candidates(int N, BigPlan *out, int max);
 
 }  // namespace sws

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -122,6 +123,8 @@ struct swsgpu_handle {
    Plan plan;
    bool big = false;   // four-step path (bplan) instead of the cluster kernel
    BigPlan bplan;
+   int big_cands = 0;  // candidate splits of N
+   int tuned = -1;     // candidate chosen by the autotuner (-1: default)
    int S = 0;
    int max_clusters = 1;
    std::string err;
@@ -788,6 +791,10 @@ static void drop_prof_events(swsgpu_handle *h)
    h->prof_events.clear();
 }
 
+static int autotune_big(swsgpu_handle *h, int iters);
+static std::mutex &tune_mutex();
+static int tuned_choice(int N, int nbit);
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -994,12 +1001,27 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    const int nbit = cfg->layout[0].nbit;
    const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
    if (h->big) {
-      CKB(cudaFuncSetAttribute((const void *)bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bplan.smem_cols));
-      CKB(cudaFuncSetAttribute((const void *)bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bplan.smem_rows));
+      {
+         BigPlan cand[16];
+         h->big_cands = big_plan_candidates(cfg->fft_points, cand, 16);
+         // a split tuned earlier in this process for the same length and bits
+         const int t = tuned_choice(cfg->fft_points, nbit);
+         if (t >= 0 && t < h->big_cands) {
+            h->bplan = cand[t];
+            h->tuned = t;
+         }
+      }
+      CKB(cudaFuncSetAttribute((const void *)h->bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)h->bplan.smem_cols));
+      CKB(cudaFuncSetAttribute((const void *)h->bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)h->bplan.smem_rows));
       for (int k = 0; k < 2; k++)
-      for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
+         for (int s = 0; s < cfg->num_streams; s++)
+            CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
+      if (cfg->autotune && h->tuned < 0) {
+         const int rc = autotune_big(h, 3);
+         if (rc != SWSGPU_OK) return bail(rc);
+      }
       *out = h;
       return SWSGPU_OK;
    }
@@ -1254,13 +1276,24 @@ int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out)
    return SWSGPU_OK;
 }
 
+static int process_device_on(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
+                             int runs_per_output, const swsgpu_outputs *d_out, cudaStream_t st);
+
 int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
                           int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream)
 {
    if (!h || !d_raw || !d_out || nruns < 1 || runs_per_output < 1) return SWSGPU_EINVAL;
-   const swsgpu_config &c = h->cfg;
    CK(h, cudaSetDevice(h->device));
-   cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : h->stream;
+   return process_device_on(h, d_raw, run_bytes, nruns, runs_per_output, d_out,
+                            cuda_stream ? (cudaStream_t)cuda_stream : h->stream);
+}
+
+}  // extern "C"
+
+static int process_device_on(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
+                             int runs_per_output, const swsgpu_outputs *d_out, cudaStream_t st)
+{
+   const swsgpu_config &c = h->cfg;
    long long grid_off[SWSGPU_MAX_STREAMS];
    size_t raw_bytes[SWSGPU_MAX_STREAMS];
    for (int s = 0; s < c.num_streams; s++) {
@@ -1277,6 +1310,153 @@ int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run
                        c.extract_pcal ? d_out->pcal_out : nullptr, st, &nspec, 0, 1, 1,
                        (c.extract_pcal && c.pcal_ntones > 0) ? d_out->tones_out : nullptr);
 }
+
+// ---------------------------------------------------------------------------
+// autotuning of the four-step split
+// ---------------------------------------------------------------------------
+__global__ void k_fill_hash(uint32_t *p, size_t n, uint32_t seed)
+{
+   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   uint32_t x = (uint32_t)i * 2654435761u ^ seed;
+   x ^= x >> 16;
+   x *= 0x7feb352du;
+   x ^= x >> 15;
+   x *= 0x846ca68bu;
+   x ^= x >> 16;
+   p[i] = x;
+}
+
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, int>, int> g_tuned;  // (N, nbit) -> chosen candidate
+
+static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
+{
+   const int nbit = h->cfg.layout[0].nbit;
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   cudaError_t e = cudaFuncSetAttribute((const void *)bp.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)bp.smem_cols);
+   if (e != cudaSuccess) return e;
+   return cudaFuncSetAttribute((const void *)bp.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bp.smem_rows);
+}
+
+// Times every candidate split on a hash-filled run of two frames per source
+// (the handle's own sources, pairs and window) and keeps the fastest.
+static int autotune_big(swsgpu_handle *h, int iters)
+{
+   const swsgpu_config &c = h->cfg;
+   BigPlan cand[16];
+   const int nc = big_plan_candidates(c.fft_points, cand, 16);
+   h->big_cands = nc;
+   if (nc <= 1) return SWSGPU_OK;
+   const int nbit = c.layout[0].nbit;
+   const long long nsamp = 2ll * c.fft_points;
+   const int pb = payload_bytes(c.layout[0]);
+   size_t pay = (size_t)((nsamp * c.layout[0].nchan * nbit + 7) / 8);
+   pay = ((pay + pb - 1) / pb) * pb;
+   DevBuf raw[SWSGPU_MAX_STREAMS], oa, ox;
+   const void *d_raw[SWSGPU_MAX_STREAMS];
+   size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   long long grid_off[SWSGPU_MAX_STREAMS];
+   auto cleanup = [&]() {
+      cudaStreamSynchronize(h->stream);
+      for (auto &r : raw) r.release();
+      oa.release();
+      ox.release();
+      drop_schedules(h);
+   };
+   for (int s = 0; s < c.num_streams; s++) {
+      const swsgpu_layout &L = c.layout[s];
+      raw_bytes[s] = L.header_bytes ? (pay / pb) * (size_t)L.frame_bytes : pay;
+      grid_off[s] = 0;
+      if (raw[s].ensure(raw_bytes[s] + 64) != cudaSuccess) {
+         cleanup();
+         return fail(h, SWSGPU_ECUDA, "autotune: allocation failed");
+      }
+      const size_t nw = raw_bytes[s] / 4;
+      k_fill_hash<<<(unsigned)((nw + 255) / 256), 256, 0, h->stream>>>((uint32_t *)raw[s].p, nw, 1234u + s);
+      d_raw[s] = raw[s].p;
+   }
+   if (oa.ensure(sizeof(float) * (size_t)h->S * c.num_sources * 2 + 64) != cudaSuccess ||
+       ox.ensure(sizeof(float) * 2 * (size_t)h->S * std::max(c.num_xpols, 1) * 2 + 64) != cudaSuccess) {
+      cleanup();
+      return fail(h, SWSGPU_ECUDA, "autotune: allocation failed");
+   }
+   int best = -1;
+   float best_ms = 0.0f;
+   cudaEvent_t e0, e1;
+   cudaEventCreate(&e0);
+   cudaEventCreate(&e1);
+   for (int k = 0; k < nc; k++) {
+      if (set_big_attrs(h, cand[k]) != cudaSuccess) {
+         cudaGetLastError();
+         continue;
+      }
+      h->bplan = cand[k];
+      int nspec = 0, rc = SWSGPU_OK;
+      for (int it = 0; it <= iters && rc == SWSGPU_OK; it++) {
+         if (it == 1) cudaEventRecord(e0, h->stream);
+         rc = launch_chunk(h, d_raw, raw_bytes, grid_off, pay, 1, 1, (float *)oa.p,
+                           c.num_xpols ? (float *)ox.p : nullptr, nullptr, h->stream, &nspec);
+      }
+      cudaEventRecord(e1, h->stream);
+      if (rc != SWSGPU_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+         cudaGetLastError();
+         continue;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best < 0 || ms < best_ms) {
+         best = k;
+         best_ms = ms;
+      }
+   }
+   cudaEventDestroy(e0);
+   cudaEventDestroy(e1);
+   cleanup();
+   if (best < 0) return fail(h, SWSGPU_ECUDA, "autotune: no candidate ran");
+   h->bplan = cand[best];
+   h->tuned = best;
+   CK(h, set_big_attrs(h, h->bplan));
+   std::lock_guard<std::mutex> lk(g_tune_mu);
+   g_tuned[std::make_pair(c.fft_points, nbit)] = best;
+   return SWSGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches: many cores' runs captured as one CUDA graph
+// ---------------------------------------------------------------------------
+struct swsgpu_batch {
+   int device = 0;
+   std::vector<swsgpu_handle *> cores;
+   struct Work {
+      bool set = false;
+      const void *d_raw[SWSGPU_MAX_STREAMS] = {nullptr, nullptr};
+      size_t run_bytes = 0;
+      int nruns = 0, rpo = 0;
+      swsgpu_outputs out = {};
+   };
+   std::vector<Work> work;
+   cudaStream_t cap = nullptr;
+   cudaEvent_t fork = nullptr;
+   std::vector<cudaEvent_t> join;
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t exec = nullptr;
+   bool dirty = true;
+   int kernels = 0;
+};
+
+static void batch_drop_graph(swsgpu_batch *b)
+{
+   if (b->exec) cudaGraphExecDestroy(b->exec);
+   if (b->graph) cudaGraphDestroy(b->graph);
+   b->exec = nullptr;
+   b->graph = nullptr;
+   b->dirty = true;
+}
+
+extern "C" {
 
 int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes)
 {
@@ -1377,4 +1557,159 @@ int swsgpu_profile_read(swsgpu_handle *h, int *launches, double *total_ms)
    return SWSGPU_OK;
 }
 
+int swsgpu_autotune(swsgpu_handle *h, int iterations)
+{
+   if (!h || iterations < 1) return SWSGPU_EINVAL;
+   CK(h, cudaSetDevice(h->device));
+   if (h->pending) return fail(h, SWSGPU_ESTATE, "autotune while a run is pending");
+   if (!h->big) return SWSGPU_OK;  // one plan per cluster length
+   return autotune_big(h, iterations);
+}
+
+int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len)
+{
+   if (!h || !buf || len == 0) return SWSGPU_EINVAL;
+   if (h->big) {
+      snprintf(buf, len, "four-step %d x %d, %d columns per CTA, candidate %d of %d%s", h->bplan.N1, h->bplan.N2,
+               h->bplan.C, h->tuned < 0 ? 0 : h->tuned, h->big_cands, h->tuned < 0 ? " (default)" : " (tuned)");
+   } else {
+      snprintf(buf, len, "cluster %d x %d (CTAs x points), radices %d/%d/%d, %s form", h->plan.P, h->plan.Q,
+               h->plan.R1, h->plan.R2, h->plan.R3,
+               h->cfg.precision == SWSGPU_PREC_TCSPLIT ? "tensor-core split" : "FP32");
+   }
+   return SWSGPU_OK;
+}
+
+int swsgpu_batch_create(swsgpu_handle *const *cores, int ncores, swsgpu_batch **out)
+{
+   if (!cores || ncores < 1 || !out) return fail(nullptr, SWSGPU_EINVAL, "batch: no cores");
+   *out = nullptr;
+   for (int i = 0; i < ncores; i++) {
+      if (!cores[i]) return fail(nullptr, SWSGPU_EINVAL, "batch: null core");
+      if (cores[i]->device != cores[0]->device) return fail(nullptr, SWSGPU_EINVAL, "batch: cores on different devices");
+      for (int j = 0; j < i; j++)
+         if (cores[j] == cores[i]) return fail(nullptr, SWSGPU_EINVAL, "batch: a core appears twice");
+   }
+   if (cudaSetDevice(cores[0]->device) != cudaSuccess) return fail(nullptr, SWSGPU_ENODEV, "batch: cudaSetDevice");
+   swsgpu_batch *b = new swsgpu_batch();
+   b->device = cores[0]->device;
+   b->cores.assign(cores, cores + ncores);
+   b->work.resize(ncores);
+   b->join.assign(ncores, nullptr);
+   bool ok = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess;
+   for (int i = 0; i < ncores && ok; i++) ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+   if (!ok) {
+      swsgpu_batch_destroy(b);
+      return fail(nullptr, SWSGPU_ECUDA, "batch: stream/event creation failed");
+   }
+   *out = b;
+   return SWSGPU_OK;
+}
+
+int swsgpu_batch_set(swsgpu_batch *b, int i, const void *const *d_raw, size_t run_bytes, int nruns,
+                     int runs_per_output, const swsgpu_outputs *d_out)
+{
+   if (!b || i < 0 || i >= (int)b->cores.size() || !d_raw || !d_out || nruns < 1 || runs_per_output < 1)
+      return fail(nullptr, SWSGPU_EINVAL, "batch_set: bad argument");
+   swsgpu_batch::Work &w = b->work[i];
+   for (int s = 0; s < b->cores[i]->cfg.num_streams; s++) w.d_raw[s] = d_raw[s];
+   w.run_bytes = run_bytes;
+   w.nruns = nruns;
+   w.rpo = runs_per_output;
+   w.out = *d_out;
+   w.set = true;
+   batch_drop_graph(b);
+   return SWSGPU_OK;
+}
+
+int swsgpu_batch_launch(swsgpu_batch *b, void *cuda_stream, int *kernels)
+{
+   if (!b) return SWSGPU_EINVAL;
+   for (const auto &w : b->work)
+      if (!w.set) return fail(nullptr, SWSGPU_EINVAL, "batch_launch: a core has no work (swsgpu_batch_set)");
+   if (cudaSetDevice(b->device) != cudaSuccess) return fail(nullptr, SWSGPU_ENODEV, "batch: cudaSetDevice");
+   const int n = (int)b->cores.size();
+   auto cuda_fail = [&](cudaError_t e, const char *what) {
+      cudaGetLastError();
+      return fail(nullptr, SWSGPU_ECUDA, std::string("batch ") + what + ": " + cudaGetErrorString(e));
+   };
+   if (b->dirty) {
+      // eager pass: every allocation and device schedule is made here, so the
+      // captured launches allocate and upload nothing
+      int total = 0;
+      for (int i = 0; i < n; i++) {
+         swsgpu_handle *h = b->cores[i];
+         if (h->pending) return fail(nullptr, SWSGPU_ESTATE, "batch: a core has a run pending");
+         const auto &w = b->work[i];
+         const int rc = process_device_on(h, w.d_raw, w.run_bytes, w.nruns, w.rpo, &w.out, h->stream);
+         if (rc != SWSGPU_OK) return fail(nullptr, rc, "batch eager run of core " + std::to_string(i) + ": " + h->err);
+         total += h->last_launches;
+      }
+      for (int i = 0; i < n; i++) {
+         cudaError_t e = cudaStreamSynchronize(b->cores[i]->stream);
+         if (e != cudaSuccess) return cuda_fail(e, "eager run");
+      }
+      // capture: each core's pipeline on its own stream, forked from and
+      // joined back into the capture stream, so the cores run concurrently
+      cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+      int rc = SWSGPU_OK;
+      e = cudaEventRecord(b->fork, b->cap);
+      for (int i = 0; i < n && e == cudaSuccess && rc == SWSGPU_OK; i++) {
+         swsgpu_handle *h = b->cores[i];
+         const auto &w = b->work[i];
+         e = cudaStreamWaitEvent(h->stream, b->fork, 0);
+         if (e != cudaSuccess) break;
+         rc = process_device_on(h, w.d_raw, w.run_bytes, w.nruns, w.rpo, &w.out, h->stream);
+         if (rc != SWSGPU_OK) break;
+         e = cudaEventRecord(b->join[i], h->stream);
+         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cap, b->join[i], 0);
+      }
+      cudaGraph_t g = nullptr;
+      cudaError_t e2 = cudaStreamEndCapture(b->cap, &g);
+      if (e != cudaSuccess || rc != SWSGPU_OK || e2 != cudaSuccess) {
+         if (g) cudaGraphDestroy(g);
+         if (rc != SWSGPU_OK) return fail(nullptr, rc, "batch capture");
+         return cuda_fail(e != cudaSuccess ? e : e2, "capture");
+      }
+      b->graph = g;
+      e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+      if (e != cudaSuccess) {
+         batch_drop_graph(b);
+         return cuda_fail(e, "instantiate");
+      }
+      b->dirty = false;
+      b->kernels = total;
+      if (kernels) *kernels = total;
+      return SWSGPU_OK;  // the eager pass produced this launch's results
+   }
+   cudaError_t e = cudaGraphLaunch(b->exec, (cudaStream_t)cuda_stream);
+   if (e != cudaSuccess) return cuda_fail(e, "graph launch");
+   if (kernels) *kernels = b->kernels;
+   return SWSGPU_OK;
+}
+
+void swsgpu_batch_destroy(swsgpu_batch *b)
+{
+   if (!b) return;
+   cudaSetDevice(b->device);
+   if (b->cap) cudaStreamSynchronize(b->cap);
+   batch_drop_graph(b);
+   for (cudaEvent_t e : b->join)
+      if (e) cudaEventDestroy(e);
+   if (b->fork) cudaEventDestroy(b->fork);
+   if (b->cap) cudaStreamDestroy(b->cap);
+   delete b;
+}
+
 }  // extern "C"
+
+static std::mutex &tune_mutex() { return g_tune_mu; }
+
+static int tuned_choice(int N, int nbit)
+{
+   std::lock_guard<std::mutex> lk(tune_mutex());
+   auto it = g_tuned.find(std::make_pair(N, nbit));
+   return it == g_tuned.end() ? -1 : it->second;
+}

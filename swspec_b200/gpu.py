@@ -39,7 +39,7 @@ class Config(C.Structure):
                 ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
                 ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
                 ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int),
-                ("pcal_ntones", C.c_int)]
+                ("pcal_ntones", C.c_int), ("autotune", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -85,6 +85,16 @@ def lib():
         L.swsgpu_device_ok.argtypes = [C.c_int]
         L.swsgpu_profile.argtypes = [C.c_void_p, C.c_int]
         L.swsgpu_profile_read.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.swsgpu_autotune.argtypes = [C.c_void_p, C.c_int]
+        L.swsgpu_plan_info.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        L.swsgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+        L.swsgpu_batch_set.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
+                                       C.c_int, C.POINTER(Outputs)]
+        L.swsgpu_batch_launch.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+        L.swsgpu_batch_destroy.argtypes = [C.c_void_p]
+        L.swsgpu_batch_destroy.restype = None
+        L.swsgpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
+        L.swsgpu_host_unregister.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -107,7 +117,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
                 sources=((0, 0),), xpols=(), precision=PREC_FP32, max_run_bytes=1 << 24,
                 extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
                 pcal_offset_hz=10e3, layout2: Layout | None = None,
-                runs_per_output: int = 1, pcal_ntones: int = 0) -> Config:
+                runs_per_output: int = 1, pcal_ntones: int = 0, autotune: bool = False) -> Config:
     c = Config()
     c.layout[0] = lay
     c.layout[1] = layout2 if layout2 is not None else lay
@@ -133,6 +143,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
     c.max_run_bytes = max_run_bytes
     c.runs_per_output = runs_per_output
     c.pcal_ntones = pcal_ntones
+    c.autotune = int(bool(autotune))
     return c
 
 
@@ -221,6 +232,15 @@ class Core:
         pc = pcal[:, :, : c.pcal_tonebins, 0] + 1j * pcal[:, :, : c.pcal_tonebins, 1]
         return auto, xp, pc, nspec
 
+    def plan_info(self) -> str:
+        buf = C.create_string_buffer(256)
+        _check(lib().swsgpu_plan_info(self.h, buf, 256), self.h)
+        return buf.value.decode()
+
+    def autotune(self, iterations: int = 3) -> str:
+        _check(lib().swsgpu_autotune(self.h, iterations), self.h)
+        return self.plan_info()
+
     def process_device(self, d_raw_ptrs: list[int], run_bytes: int, nruns: int,
                        runs_per_output: int, d_auto: int, d_xpol: int = 0, d_pcal: int = 0,
                        stream: int = 0, d_tones: int = 0) -> None:
@@ -229,6 +249,39 @@ class Core:
         out = Outputs(d_auto, d_xpol or None, d_pcal or None, d_tones or None)
         _check(lib().swsgpu_process_device(self.h, ptrs, run_bytes, nruns, runs_per_output,
                                            C.byref(out), C.c_void_p(stream or None)), self.h)
+
+
+class Batch:
+    """Many cores' runs recorded as one CUDA graph (swsgpu_batch_*)."""
+
+    def __init__(self, cores: list):
+        self.cores = list(cores)
+        arr = (C.c_void_p * len(cores))(*[c.h.value for c in cores])
+        self.b = C.c_void_p()
+        _check(lib().swsgpu_batch_create(arr, len(cores), C.byref(self.b)))
+
+    def set(self, i: int, d_raw_ptrs: list[int], run_bytes: int, nruns: int, runs_per_output: int,
+            d_auto: int, d_xpol: int = 0, d_pcal: int = 0, d_tones: int = 0) -> None:
+        n = len(d_raw_ptrs)
+        ptrs = (C.c_void_p * n)(*d_raw_ptrs)
+        out = Outputs(d_auto, d_xpol or None, d_pcal or None, d_tones or None)
+        _check(lib().swsgpu_batch_set(self.b, i, ptrs, run_bytes, nruns, runs_per_output, C.byref(out)))
+
+    def launch(self, stream: int = 0) -> int:
+        k = C.c_int()
+        _check(lib().swsgpu_batch_launch(self.b, C.c_void_p(stream or None), C.byref(k)))
+        return k.value
+
+    def close(self) -> None:
+        if self.b:
+            lib().swsgpu_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def unpack_device(lay: Layout, d_raw: int, nbytes: int, payload_offset: int, chan: int,

@@ -1,0 +1,108 @@
+"""Batched uneven streams through one CUDA graph, and the autotuner.
+
+Cores of different FFT lengths (cluster and four-step paths) and bit depths
+are recorded into one graph (swsgpu_batch_*); a replay must give the same
+spectra, bit for bit, as each core's own process_device run (the kernels
+are deterministic without phase-cal), and the autotuned four-step split
+must stay within the parity bars of the four-step tests."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from helpers import REL_TOL, oracle_run
+from swspec_b200.workloads import StreamSpec, stream_payload
+from test_gpu_bigfft import _check_auto, _fp32_run
+
+pytestmark = pytest.mark.gpu
+
+# (N, bits, FFTs per run): every plan family and both bit depths
+MIX = [(4096, 2, 16), (20000, 1, 3), (131072, 2, 2), (1 << 18, 1, 2), (1 << 20, 2, 2), (3_200_000, 1, 2)]
+
+
+def _spec(i, N, nbit, cof):
+    run_bytes = (N * cof * nbit // 8 + 7) // 8 * 8
+    return StreamSpec(i, N, nbit, 16e6, 1.0, 1, (3.1e6,), run_bytes, cof, 1)
+
+
+def _core(gpu, spec, autotune=False):
+    lay = gpu.layout("vdif:8000", 1, spec.nbit, framed=False)
+    cfg = gpu.make_config(lay, spec.fft_points, "hann", 1, spec.core_overlapped_ffts,
+                          max_run_bytes=spec.run_bytes, samplingfreq=spec.samplingfreq,
+                          autotune=autotune)
+    return gpu.Core(cfg)
+
+
+def test_batch_graph_equals_eager(gpu):
+    specs = [_spec(i, *m) for i, m in enumerate(MIX)]
+    cores = [_core(gpu, s) for s in specs]
+    raws, outs_e, outs_b = [], [], []
+    for s, c in zip(specs, cores):
+        pay = np.frombuffer(stream_payload(s), dtype=np.uint8)
+        raws.append(torch.from_numpy(pay.copy()).cuda())
+        ns, _, _ = c.run_shape(s.run_bytes)
+        outs_e.append(torch.zeros(ns, 1, c.S, dtype=torch.float32, device="cuda"))
+        outs_b.append(torch.zeros(ns, 1, c.S, dtype=torch.float32, device="cuda"))
+    for s, c, r, o in zip(specs, cores, raws, outs_e):
+        c.process_device([r.data_ptr()], s.run_bytes, 1, 1, o.data_ptr())
+    torch.cuda.synchronize()
+    b = gpu.Batch(cores)
+    for i, (s, r, o) in enumerate(zip(specs, raws, outs_b)):
+        b.set(i, [r.data_ptr()], s.run_bytes, 1, 1, o.data_ptr())
+    k = b.launch()                     # eager pass + graph recording
+    torch.cuda.synchronize()
+    assert k >= 4 * len(cores)
+    for e, o in zip(outs_e, outs_b):
+        assert torch.equal(e, o)
+    st = torch.cuda.Stream()
+    for rep in range(2):               # graph replays
+        for o in outs_b:
+            o.zero_()
+        torch.cuda.synchronize()
+        b.launch(st.cuda_stream)
+        st.synchronize()
+        for e, o in zip(outs_e, outs_b):
+            assert torch.equal(e, o), rep
+    b.close()
+    # the N = 4096 core (16 FFTs) against the FP64 oracle
+    s0 = specs[0]
+    x = O.decode(O.FMT_VDIF, 1, 2, stream_payload(s0), s0.samples_per_run, 0, payload_bytes=8000)
+    ra, _, _, nref = oracle_run([x], 4096, "hann", 1, 16)
+    got = outs_e[0].cpu().numpy()
+    assert got.shape[0] == nref
+    assert np.max(np.abs(got[0, 0] - ra[0, 0]) / ra[0, 0]) < REL_TOL
+
+
+def test_batch_rejects_unset_and_duplicate(gpu):
+    s = _spec(0, 4096, 2, 4)
+    c = _core(gpu, s)
+    with pytest.raises(gpu.SwsError):
+        gpu.Batch([c, c])
+    b = gpu.Batch([c])
+    with pytest.raises(gpu.SwsError, match="no work"):
+        b.launch()
+    b.close()
+
+
+def test_autotune_four_step(gpu):
+    """2^20, 1-bit: every candidate split is timed, the fastest kept; the
+    result stays within the four-step parity bars; a later core of the same
+    length and bits starts from the tuned split."""
+    N, cof = 1 << 20, 3
+    s = _spec(0, N, 1, cof)
+    s.run_bytes = (N * (cof + 1) // 8 + 7) // 8 * 8
+    c = _core(gpu, s, autotune=True)
+    info = c.plan_info()
+    assert "tuned" in info and "four-step" in info, info
+    pay = stream_payload(s)
+    auto, _, _, ns = c.run([pay])
+    x = O.decode(O.FMT_VDIF, 1, 1, pay, s.samples_per_run, 0, payload_bytes=8000)
+    ra, _, _, nref = oracle_run([x], N, "hann", 1, cof)
+    r32, _, _, _ = _fp32_run([x], N, "hann", 1, cof)
+    assert ns == nref
+    _check_auto(auto[0, 0], ra[0, 0], r32[0, 0])
+    c2 = _core(gpu, s)
+    assert c2.plan_info() == info
+    # a cluster length has one plan
+    c3 = _core(gpu, _spec(1, 65536, 2, 2))
+    assert "cluster" in c3.autotune()
