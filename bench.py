@@ -251,7 +251,7 @@ def gpu_arm(args) -> None:
     world, rank = reps.world, reps.rank
 
     precisions = [gpu.PREC_FP32]
-    if args.precision in ("tcsplit", "auto") and tc_available(gpu):
+    if args.precision in ("tcsplit", "auto") and args.plan != "fourstep" and tc_available(gpu):
         precisions = [gpu.PREC_TCSPLIT, gpu.PREC_FP32]
     headline = precisions[0]
 
@@ -270,10 +270,13 @@ def gpu_arm(args) -> None:
     sources = tuple((0, c) for c in range(NCHAN))
     pairs = tuple((c, c + NPAIRS) for c in range(NPAIRS))
 
+    family = {"auto": gpu.PLAN_DEFAULT, "cluster": gpu.PLAN_CLUSTER, "fourstep": gpu.PLAN_FOURSTEP}[args.plan]
+
     def make_core(prec, framed=True, rpo=1):
         cfg = gpu.make_config(lay if framed else gpu.layout("mark5b", NCHAN, 2, framed=False), N,
                               "hann", 1, CORE_FFTS, sources=sources, xpols=pairs, precision=prec,
-                              max_run_bytes=RUN_BYTES, samplingfreq=FS, runs_per_output=rpo)
+                              max_run_bytes=RUN_BYTES, samplingfreq=FS, runs_per_output=rpo,
+                              plan_family=family, autotune=family == gpu.PLAN_FOURSTEP)
         return gpu.Core(cfg, device=local)
 
     def step(core):
@@ -289,6 +292,7 @@ def gpu_arm(args) -> None:
     for prec in precisions:
         name = "tcsplit" if prec == gpu.PREC_TCSPLIT else "fp32"
         core = make_core(prec)
+        plan_desc = core.plan_info()
         for _ in range(args.warmup):
             step(core)
         torch.cuda.synchronize()
@@ -315,7 +319,7 @@ def gpu_arm(args) -> None:
         core.profile(False)
         core.close()
         value = SAMPLES_PER_STEP * args.steps * world / (ms * 1e-3) / 1e9
-        forms[name] = {"value": value, "ms_per_step": ms / args.steps,
+        forms[name] = {"value": value, "ms_per_step": ms / args.steps, "plan": plan_desc,
                        "kernel_ms_per_launch": kms / max(nk, 1), "kernel_launches": nk,
                        "launches_per_step": launches_per_step, "clocks": cs.summary()}
         if prec == headline:
@@ -511,6 +515,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "tcsplit"])
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plan", default="auto", choices=["auto", "cluster", "fourstep"],
+                    help="FFT path for the cross-spectra workload (auto: cluster kernel)")
     ap.add_argument("--workload", default="c3", choices=["c3", "c4"],
                     help="c3: dual-pol cross-spectra (default line); c4: batched uneven streams")
     args = ap.parse_args()

@@ -63,6 +63,12 @@ extern "C" {
 #define SWSGPU_WIN_BLACKMANHARRIS 6
 
 /* Arithmetic of the FFT stages. */
+/* FFT paths: the cluster kernel (one thread-block cluster per pair FFT,
+ * N <= 131072) or the four-step column/row kernels (intermediate in HBM). */
+#define SWSGPU_PLAN_DEFAULT 0     /* cluster kernel where it exists, else four-step */
+#define SWSGPU_PLAN_CLUSTER 1
+#define SWSGPU_PLAN_FOURSTEP 2
+
 #define SWSGPU_PREC_FP32 0       /* plain FP32 throughout */
 #define SWSGPU_PREC_TCSPLIT 1    /* inner DFT stages on tensor cores, FP16 hi+lo split, FP32 accumulate */
 
@@ -118,6 +124,7 @@ typedef struct swsgpu_config {
    int autotune;                    /* 1: swsgpu_create times the candidate splits of a
                                        four-step length and keeps the fastest (once per
                                        length and bit depth per process; see swsgpu_autotune) */
+   int plan_family;                 /* SWSGPU_PLAN_*: which FFT path a length with both uses */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;

@@ -242,6 +242,9 @@ constexpr size_t big_rows_smem()
 // Candidate splits per length; the first of each length is the default,
 // the others are timed by the autotuner (swsgpu_autotune).
 static const BigPlan kBigPlans[] = {
+    SWS_BIG_C(256, 16, 256, 16, 16, 1, 256, 128, 16, 16, 1),  // 2^16 (the cluster kernel is the default)
+    SWS_BIG_C(256, 32, 512, 16, 16, 1, 256, 128, 16, 16, 1),
+    SWS_BIG_C(128, 32, 256, 16, 8, 1, 512, 256, 16, 16, 2),
     SWS_BIG(512, 256, 16, 16, 2, 512, 256, 16, 16, 2),        // 2^18
     SWS_BIG(256, 256, 16, 16, 1, 1024, 512, 16, 16, 4),
     SWS_BIG(1024, 256, 16, 16, 4, 256, 256, 16, 16, 1),

@@ -849,6 +849,7 @@ static int validate_config(const swsgpu_config *c, std::string &why)
    if (c->window < 0 || c->window > SWSGPU_WIN_BLACKMANHARRIS) { why = "unknown window"; return 0; }
    if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT) { why = "unknown precision"; return 0; }
    if (c->runs_per_output < 0) { why = "runs_per_output must be >= 0"; return 0; }
+   if (c->plan_family < SWSGPU_PLAN_DEFAULT || c->plan_family > SWSGPU_PLAN_FOURSTEP) { why = "unknown plan_family"; return 0; }
    if (c->extract_pcal) {
       if (c->pcal_tonebins < 1 || c->pcal_rotatorlen < c->pcal_tonebins || c->fft_points % c->pcal_rotatorlen) {
          why = "pcal: need tonebins >= 1, rotatorlen >= tonebins and N % rotatorlen == 0";
@@ -874,8 +875,16 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    if (!validate_config(cfg, why)) return fail(nullptr, SWSGPU_EINVAL, why);
    Plan plan = {};
    BigPlan bplan = {};
-   const bool cluster_plan = find_plan(cfg->fft_points, &plan);
-   if (!cluster_plan && !find_big_plan(cfg->fft_points, &bplan))
+   bool cluster_plan = find_plan(cfg->fft_points, &plan);
+   const bool four_step = find_big_plan(cfg->fft_points, &bplan);
+   if (cfg->plan_family == SWSGPU_PLAN_FOURSTEP) {
+      if (!four_step)
+         return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no four-step plan");
+      cluster_plan = false;
+   } else if (cfg->plan_family == SWSGPU_PLAN_CLUSTER && !cluster_plan) {
+      return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no cluster plan");
+   }
+   if (!cluster_plan && !four_step)
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
    if (cfg->precision == SWSGPU_PREC_TCSPLIT && !(cluster_plan && plan.kern_tc[1]))
       return fail(nullptr, SWSGPU_EINVAL,

@@ -17,6 +17,7 @@ FMT_MARK5B, FMT_VDIF = 0, 1
 WIN = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
        "blackmanharris": 6}
 PREC_FP32, PREC_TCSPLIT = 0, 1
+PLAN_DEFAULT, PLAN_CLUSTER, PLAN_FOURSTEP = 0, 1, 2
 MAX_SOURCES = 64
 MAX_STREAMS = 2
 
@@ -39,7 +40,7 @@ class Config(C.Structure):
                 ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
                 ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
                 ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int),
-                ("pcal_ntones", C.c_int), ("autotune", C.c_int)]
+                ("pcal_ntones", C.c_int), ("autotune", C.c_int), ("plan_family", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -117,7 +118,8 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
                 sources=((0, 0),), xpols=(), precision=PREC_FP32, max_run_bytes=1 << 24,
                 extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
                 pcal_offset_hz=10e3, layout2: Layout | None = None,
-                runs_per_output: int = 1, pcal_ntones: int = 0, autotune: bool = False) -> Config:
+                runs_per_output: int = 1, pcal_ntones: int = 0, autotune: bool = False,
+                plan_family: int = 0) -> Config:
     c = Config()
     c.layout[0] = lay
     c.layout[1] = layout2 if layout2 is not None else lay
@@ -144,6 +146,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
     c.runs_per_output = runs_per_output
     c.pcal_ntones = pcal_ntones
     c.autotune = int(bool(autotune))
+    c.plan_family = plan_family
     return c
 
 
