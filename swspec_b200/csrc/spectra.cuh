@@ -174,8 +174,14 @@ __device__ __forceinline__ void pass_compute_pw(const float2 *buf, const float2 
       const int j = tid + b * T;
       if (nb % T == 0 || j < nb) {
          const int k = j % Ns;
+         if constexpr (nb % 16 == 0) {
+            const int pj = pidx(j);
 #pragma unroll
-         for (int r = 0; r < R; r++) v[b][r] = buf[pidx(j + r * nb)];
+            for (int r = 0; r < R; r++) v[b][r] = buf[pj + r * (nb + nb / 16)];
+         } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[b][r] = buf[pidx(j + r * nb)];
+         }
          float2 base[NBASE];
 #pragma unroll
          for (int i = 0; i < NBASE; i++) base[i] = tb[i * Ns + k];
@@ -196,9 +202,10 @@ __device__ __forceinline__ void pass_compute(const float2 *buf, const float2 *tw
       const int j = tid + b * T;
       if (nb % T == 0 || j < nb) {
          const int k = j % Ns;
+         const int pj = pidx(j);
 #pragma unroll
          for (int r = 0; r < R; r++) {
-            float2 x = buf[pidx(j + r * nb)];
+            float2 x = (nb % 16 == 0) ? buf[pj + r * (nb + nb / 16)] : buf[pidx(j + r * nb)];
             if (r > 0) x = cmul(x, pass_tw<R, Ns>(tw, r, k));
             v[b][r] = x;
          }
@@ -223,8 +230,9 @@ __device__ __forceinline__ void smem_pass(float2 *buf, const float2 *tw)
       if (nb % T == 0 || j < nb) {
          const int k = j % Ns;
          const int d = (j / Ns) * Ns * R + k;
+         const int pd = pidx(d);
 #pragma unroll
-         for (int r = 0; r < R; r++) buf[pidx(d + r * Ns)] = v[b][r];
+         for (int r = 0; r < R; r++) buf[(Ns % 16 == 0) ? pd + r * (Ns + Ns / 16) : pidx(d + r * Ns)] = v[b][r];
       }
    }
    __syncthreads();
@@ -419,6 +427,15 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 
    const uint32_t rbuf_addr = (uint32_t)__cvta_generic_to_shared(rbuf);
    const uint32_t stage_addr = (uint32_t)__cvta_generic_to_shared(stage);
+   // levels of a (code_a, code_b) pair, and every CTA's receive buffer as a
+   // shared::cluster address (mapped once instead of per pushed value)
+   __shared__ float2 pair_lut[NBIT <= 2 ? (1 << (2 * NBIT)) : 1];
+   __shared__ uint32_t rbase[P];
+   if constexpr (NBIT <= 2)
+      for (int i = tid; i < (1 << (2 * NBIT)); i += T)
+         pair_lut[i] = make_float2(decode_level<NBIT>((uint32_t)i & MASK, a.levels),
+                                   decode_level<NBIT>((uint32_t)i >> NBIT, a.levels));
+   for (int i = tid; i < P; i += T) rbase[i] = dsmem_addr(rbuf_addr, (uint32_t)i);
 
    // ---- job sequence of this cluster: items cid, cid+ncl, ...; jobs 0..nfr-1 ----
    struct JobPos {
@@ -525,6 +542,32 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                      }
                   }
                }
+               if constexpr (PERM && NBIT <= 2) {
+                  if (has_b) {
+                     // both sources' codes of sample q index one table entry
+                     // holding both levels; nb1 % SPW == 0, so the bit offset
+                     // within the word is the same for all r
+                     const int sha = NBIT * ((offa + jj) % SPW), shb = NBIT * ((offb + jj) % SPW);
+#pragma unroll
+                     for (int r = 0; r < R1; r++) {
+                        const int q = jj + r * nb1;
+                        const float w = wsl[q];
+                        const uint32_t ca = (wa[r] >> sha) & MASK, cb = (wb[r] >> shb) & MASK;
+                        float2 lv = pair_lut[(cb << NBIT) | ca];
+                        if (blank_a) {
+                           const long long smp = sa + rank + (long long)P * q;
+                           if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) lv.x = 0.0f;
+                        }
+                        if (blank_b) {
+                           const long long smp = sb + rank + (long long)P * q;
+                           if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) lv.y = 0.0f;
+                        }
+                        v[b][r] = make_float2(lv.x * w, lv.y * w);
+                     }
+                     DFT<R1>::run(v[b]);
+                     continue;
+                  }
+               }
 #pragma unroll
                for (int r = 0; r < R1; r++) {
                   const int q = jj + r * nb1;
@@ -557,7 +600,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                const int jj = tid + b * T;
                if (nb1 % T == 0 || jj < nb1) {
 #pragma unroll
-                  for (int r = 0; r < R1; r++) buf[pidx(jj * R1 + r)] = v[b][r];
+                  for (int r = 0; r < R1; r++)
+                     buf[(R1 == 16) ? jj * 17 + r : pidx(jj * R1 + r)] = v[b][r];  // pidx(16 jj + r), r < 16
                }
             }
          } else {
@@ -589,12 +633,27 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          float2 v3[BPT3][R3];
          pass_compute_pw<Q, T, R3, NS3, BPT3>(buf, tw3, v3);
          cluster_wait();  // owners have finished reading their receive buffers
+         // k1 = j + r NS3 with j < NS3 and Q = R3 NS3: for even R3 the side
+         // (lo: k1 < Q/2, hi otherwise) is fixed by r, and with power-of-two
+         // Q and UC the owner and slot are shifts and masks
+         constexpr bool FASTPUSH = (R3 % 2 == 0) && ((Q & (Q - 1)) == 0) && ((UC & (UC - 1)) == 0);
 #pragma unroll
          for (int b = 0; b < BPT3; b++) {
             const int j = tid + b * T;
             if (nb3 % T == 0 || j < nb3) {
+               if constexpr (FASTPUSH) {
+                  const uint32_t self = 8u * (uint32_t)(rank * SIDES);
 #pragma unroll
-               for (int r = 0; r < R3; r++) push(j + r * NS3, v3[b][r]);
+                  for (int r = 0; r < R3; r++) {
+                     const int k1 = j + r * NS3;
+                     const int uu = (r < R3 / 2) ? k1 : ((Q - k1) & (Q / 2 - 1));
+                     const int slot = ((r < R3 / 2) ? 0 : UC) + (uu & (UC - 1));
+                     dsmem_st2(rbase[uu / UC] + self + 8u * (uint32_t)slot, v3[b][r]);
+                  }
+               } else {
+#pragma unroll
+                  for (int r = 0; r < R3; r++) push(j + r * NS3, v3[b][r]);
+               }
             }
          }
       } else {
