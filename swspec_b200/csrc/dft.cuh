@@ -63,6 +63,24 @@ __device__ __forceinline__ void static_for(F &&f)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// The same sums as one packed two-lane instruction (add/sub.rn.f32x2, sm_100);
+// for operands that are plain register pairs, where no swizzle is needed.
+__device__ __forceinline__ float2 padd(float2 a, float2 b)
+{
+   float2 d;
+   asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+       " add.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}\n"
+       : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+   return d;
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b)
+{
+   float2 d;
+   asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+       " sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}\n"
+       : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+   return d;
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 w)
 {
    return make_float2(fmaf(a.x, w.x, -a.y * w.y), fmaf(a.x, w.y, a.y * w.x));
@@ -122,8 +140,8 @@ struct DFT<2> {
    __device__ __forceinline__ static void run(float2 *v)
    {
       float2 a = v[0], b = v[1];
-      v[0] = cadd(a, b);
-      v[1] = csub(a, b);
+      v[0] = padd(a, b);
+      v[1] = psub(a, b);
    }
 };
 
@@ -132,9 +150,9 @@ struct DFT<3> {
    __device__ __forceinline__ static void run(float2 *v)
    {
       constexpr float s = 0.86602540378443864676f;  // sin(2 pi / 3)
-      float2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+      float2 t1 = padd(v[1], v[2]), t2 = psub(v[1], v[2]);
       float2 m = make_float2(fmaf(-0.5f, t1.x, v[0].x), fmaf(-0.5f, t1.y, v[0].y));
-      v[0] = cadd(v[0], t1);
+      v[0] = padd(v[0], t1);
       v[1] = make_float2(fmaf(s, t2.y, m.x), fmaf(-s, t2.x, m.y));
       v[2] = make_float2(fmaf(-s, t2.y, m.x), fmaf(s, t2.x, m.y));
    }
@@ -144,10 +162,10 @@ template <>
 struct DFT<4> {
    __device__ __forceinline__ static void run(float2 *v)
    {
-      float2 s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]);
-      float2 s2 = cadd(v[1], v[3]), s3 = csub(v[1], v[3]);
-      v[0] = cadd(s0, s2);
-      v[2] = csub(s0, s2);
+      float2 s0 = padd(v[0], v[2]), s1 = psub(v[0], v[2]);
+      float2 s2 = padd(v[1], v[3]), s3 = psub(v[1], v[3]);
+      v[0] = padd(s0, s2);
+      v[2] = psub(s0, s2);
       v[1] = cadd(s1, mul_negi(s3));
       v[3] = csub(s1, mul_negi(s3));
    }
@@ -161,14 +179,14 @@ struct DFT<5> {
       constexpr float c2 = -0.80901699437494742410f;  // cos(4 pi / 5)
       constexpr float s1 = 0.95105651629515357212f;   // sin(2 pi / 5)
       constexpr float s2 = 0.58778525229247312917f;   // sin(4 pi / 5)
-      float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-      float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+      float2 t1 = padd(v[1], v[4]), t2 = padd(v[2], v[3]);
+      float2 t3 = psub(v[1], v[4]), t4 = psub(v[2], v[3]);
       float2 x0 = v[0];
       float2 a1 = make_float2(fmaf(c2, t2.x, fmaf(c1, t1.x, x0.x)), fmaf(c2, t2.y, fmaf(c1, t1.y, x0.y)));
       float2 a2 = make_float2(fmaf(c1, t2.x, fmaf(c2, t1.x, x0.x)), fmaf(c1, t2.y, fmaf(c2, t1.y, x0.y)));
       float2 b1 = make_float2(fmaf(s1, t3.x, s2 * t4.x), fmaf(s1, t3.y, s2 * t4.y));
       float2 b2 = make_float2(fmaf(s2, t3.x, -s1 * t4.x), fmaf(s2, t3.y, -s1 * t4.y));
-      v[0] = cadd(x0, cadd(t1, t2));
+      v[0] = padd(x0, padd(t1, t2));
       v[1] = cadd(a1, mul_negi(b1));
       v[4] = csub(a1, mul_negi(b1));
       v[2] = cadd(a2, mul_negi(b2));
