@@ -125,6 +125,9 @@ typedef struct swsgpu_config {
                                        four-step length and keeps the fastest (once per
                                        length and bit depth per process; see swsgpu_autotune) */
    int plan_family;                 /* SWSGPU_PLAN_*: which FFT path a length with both uses */
+   int plan_candidate;              /* four-step path: 0 = default split, k > 0 = the k-th
+                                       candidate (as the autotuner numbers them); ignored
+                                       when autotune is set */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;

@@ -125,6 +125,8 @@ struct swsgpu_handle {
    BigPlan bplan;
    int big_cands = 0;  // candidate splits of N
    int tuned = -1;     // candidate chosen by the autotuner (-1: default)
+   int cand = 0;       // candidate in use (index into tw_off)
+   std::vector<int2> tw_off;  // per candidate: offsets of its W_N1 and W_N2 tables in d_tw1
    int S = 0;
    int max_clusters = 1;
    std::string err;
@@ -149,6 +151,7 @@ struct swsgpu_handle {
    DevBuf d_window, d_twQ, d_twN, d_code_stream;
    DevBuf d_tw1, d_tw2, d_twA, d_twB;               // four-step tables
    DevBuf d_scratch, d_bjobs, d_bitems;             // four-step intermediate and job lists
+   DevBuf d_status;                                 // kernel status word (1: a bounded wait gave up)
    // per-call buffers
    DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
    DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
@@ -486,8 +489,8 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.blank_any = (const int *)h->d_blank_any.p;
    a.code_stream = (const int *)h->d_code_stream.p;
    a.window = (const float *)h->d_window.p;
-   a.tw1 = (const float2 *)h->d_tw1.p;
-   a.tw2 = (const float2 *)h->d_tw2.p;
+   a.tw1 = (const float2 *)h->d_tw1.p + h->tw_off[h->cand].x;
+   a.tw2 = (const float2 *)h->d_tw1.p + h->tw_off[h->cand].y;
    a.twA = (const float2 *)h->d_twA.p;
    a.twB = (const float2 *)h->d_twB.p;
    a.scratch = (float2 *)h->d_scratch.p;
@@ -696,6 +699,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          a.N = c.fft_points;
          a.S = S;
          a.levels = level_table(c.layout[0].format, nbit);
+         a.status = (int *)h->d_status.p;
          const Plan &pl = h->plan;
          const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
          SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
@@ -850,6 +854,7 @@ static int validate_config(const swsgpu_config *c, std::string &why)
    if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT) { why = "unknown precision"; return 0; }
    if (c->runs_per_output < 0) { why = "runs_per_output must be >= 0"; return 0; }
    if (c->plan_family < SWSGPU_PLAN_DEFAULT || c->plan_family > SWSGPU_PLAN_FOURSTEP) { why = "unknown plan_family"; return 0; }
+   if (c->plan_candidate < 0) { why = "plan_candidate must be >= 0"; return 0; }
    if (c->extract_pcal) {
       if (c->pcal_tonebins < 1 || c->pcal_rotatorlen < c->pcal_tonebins || c->fft_points % c->pcal_rotatorlen) {
          why = "pcal: need tonebins >= 1, rotatorlen >= tonebins and N % rotatorlen == 0";
@@ -979,10 +984,21 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
       CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
    } else {
-      // four-step tables, each entry rounded once from double
-      std::vector<float2> t1, t2, tA, tB;
-      make_twiddles(bplan.N1, bplan.N1, t1);
-      make_twiddles(bplan.N2, bplan.N2, t2);
+      // four-step tables, each entry rounded once from double: W_N1 and
+      // W_N2 of every candidate split (one buffer), W_N^(2048 h), W_N^l
+      std::vector<float2> t1, tA, tB;
+      {
+         BigPlan cand[16];
+         const int nc = big_plan_candidates(cfg->fft_points, cand, 16);
+         for (int k = 0; k < nc; k++) {
+            std::vector<float2> a1, a2;
+            make_twiddles(cand[k].N1, cand[k].N1, a1);
+            make_twiddles(cand[k].N2, cand[k].N2, a2);
+            h->tw_off.push_back(make_int2((int)t1.size(), (int)(t1.size() + a1.size())));
+            t1.insert(t1.end(), a1.begin(), a1.end());
+            t1.insert(t1.end(), a2.begin(), a2.end());
+         }
+      }
       make_twiddles(cfg->fft_points, 2048, tB);
       const int nA = (cfg->fft_points + 2047) / 2048;
       tA.resize(nA);
@@ -990,8 +1006,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
          const double ang = -2.0 * M_PI * (double)((long long)k * 2048) / (double)cfg->fft_points;
          tA[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
       }
-      const std::pair<DevBuf *, std::vector<float2> *> tabs[4] = {
-          {&h->d_tw1, &t1}, {&h->d_tw2, &t2}, {&h->d_twA, &tA}, {&h->d_twB, &tB}};
+      const std::pair<DevBuf *, std::vector<float2> *> tabs[3] = {
+          {&h->d_tw1, &t1}, {&h->d_twA, &tA}, {&h->d_twB, &tB}};
       for (const auto &t : tabs) {
          CKB(t.first->ensure(sizeof(float2) * t.second->size()));
          CKB(cudaMemcpy(t.first->p, t.second->data(), sizeof(float2) * t.second->size(), cudaMemcpyHostToDevice));
@@ -1003,6 +1019,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       CKB(cudaMemcpy(h->d_chans[s].p, h->chans_of[s].data(), sizeof(int) * h->chans_of[s].size(),
                      cudaMemcpyHostToDevice));
    }
+   CKB(h->d_status.ensure(sizeof(int)));
+   CKB(cudaMemset(h->d_status.p, 0, sizeof(int)));
    CKB(h->d_code_stream.ensure(sizeof(int) * h->code_stream.size()));
    CKB(cudaMemcpy(h->d_code_stream.p, h->code_stream.data(), sizeof(int) * h->code_stream.size(),
                   cudaMemcpyHostToDevice));
@@ -1015,9 +1033,17 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
          h->big_cands = big_plan_candidates(cfg->fft_points, cand, 16);
          // a split tuned earlier in this process for the same length and bits
          const int t = tuned_choice(cfg->fft_points, nbit);
-         if (t >= 0 && t < h->big_cands) {
+         if (cfg->plan_candidate > 0 && !cfg->autotune) {
+            if (cfg->plan_candidate >= h->big_cands) {
+               h->err = "plan_candidate beyond the candidates of this length";
+               return bail(SWSGPU_EINVAL);
+            }
+            h->bplan = cand[cfg->plan_candidate];
+            h->cand = cfg->plan_candidate;
+         } else if (t >= 0 && t < h->big_cands) {
             h->bplan = cand[t];
             h->tuned = t;
+            h->cand = t;
          }
       }
       CKB(cudaFuncSetAttribute((const void *)h->bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1076,7 +1102,7 @@ void swsgpu_destroy(swsgpu_handle *h)
                      &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
                      &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
                      &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal, &h->d_out_tones,
-                     &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs,
+                     &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs, &h->d_status,
                      &h->d_bitems};
    for (DevBuf *b : bufs) b->release();
    drop_schedules(h);
@@ -1235,7 +1261,16 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
       std::this_thread::sleep_for(std::chrono::microseconds(50));
    }
    h->pending = false;
+   const bool had_out = h->pending_out;
    h->pending_out = false;
+   if (had_out && h->d_status.p) {
+      int st = 0;
+      CK(h, cudaMemcpy(&st, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (st) {
+         cudaMemset(h->d_status.p, 0, sizeof(int));
+         return fail(h, SWSGPU_ECUDA, "a device-side wait for cluster data gave up; the spectra are invalid");
+      }
+   }
    if (nspectra) *nspectra = h->pending_nspec;
    return SWSGPU_OK;
 }
@@ -1403,6 +1438,7 @@ static int autotune_big(swsgpu_handle *h, int iters)
          continue;
       }
       h->bplan = cand[k];
+      h->cand = k;
       int nspec = 0, rc = SWSGPU_OK;
       for (int it = 0; it <= iters && rc == SWSGPU_OK; it++) {
          if (it == 1) cudaEventRecord(e0, h->stream);
@@ -1427,6 +1463,7 @@ static int autotune_big(swsgpu_handle *h, int iters)
    if (best < 0) return fail(h, SWSGPU_ECUDA, "autotune: no candidate ran");
    h->bplan = cand[best];
    h->tuned = best;
+   h->cand = best;
    CK(h, set_big_attrs(h, h->bplan));
    std::lock_guard<std::mutex> lk(g_tune_mu);
    g_tuned[std::make_pair(c.fft_points, nbit)] = best;
@@ -1580,7 +1617,8 @@ int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len)
    if (!h || !buf || len == 0) return SWSGPU_EINVAL;
    if (h->big) {
       snprintf(buf, len, "four-step %d x %d, %d columns per CTA, candidate %d of %d%s", h->bplan.N1, h->bplan.N2,
-               h->bplan.C, h->tuned < 0 ? 0 : h->tuned, h->big_cands, h->tuned < 0 ? " (default)" : " (tuned)");
+               h->bplan.C, h->cand, h->big_cands,
+               h->tuned >= 0 ? " (tuned)" : (h->cand > 0 ? " (pinned)" : " (default)"));
    } else {
       snprintf(buf, len, "cluster %d x %d (CTAs x points), radices %d/%d/%d, %s form", h->plan.P, h->plan.Q,
                h->plan.R1, h->plan.R2, h->plan.R3,

@@ -61,6 +61,7 @@ struct SpecArgs {
    float *partial;               // [nitems][4][S]
    int N, S;
    float4 levels;                // level table for 1/2-bit codes
+   int *status;                  // set to 1 when a bounded wait gave up (null: not reported)
 };
 
 // Reduction of item partial sums into output spectra.

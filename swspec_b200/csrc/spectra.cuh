@@ -83,6 +83,39 @@ __device__ __forceinline__ void dsmem_st2(uint32_t addr, float2 v)
    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};\n" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
 
+// Asynchronous remote store whose 8 bytes are counted on the destination
+// CTA's mbarrier (both addresses shared::cluster): the receiver learns of
+// the data from its own barrier, the sender neither waits nor fences.
+__device__ __forceinline__ void dsmem_st2_async(uint32_t addr, float2 v, uint32_t mbar)
+{
+   asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];\n"
+                ::"r"(addr), "f"(v.x), "f"(v.y), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint32_t mbar, int count)
+{
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
+   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint32_t mbar, uint32_t bytes)
+{
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+// Waits for the completion of phase `parity` with a bounded number of
+// polls; returns false when it gave up (the caller reports it and goes on,
+// so that every cluster barrier is still reached).
+__device__ __forceinline__ bool mbar_wait_parity(uint32_t mbar, uint32_t parity)
+{
+   for (int it = 0; it < (1 << 18); it++) {
+      uint32_t done;
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+                   " selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+      if (done) return true;
+      if (it > 64) __nanosleep(64);
+   }
+   return false;
+}
+
 // Twiddle table of a pass: tw[(r-1)*Ns + k] = W_{Ns R}^{k r}, k < Ns, 0 < r < R.
 template <int Q, int R, int Ns>
 __device__ __forceinline__ void fill_pass_twiddles(float2 *tw, const float2 *__restrict__ twQ, int T)
@@ -431,11 +464,18 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    // shared::cluster address (mapped once instead of per pushed value)
    __shared__ float2 pair_lut[NBIT <= 2 ? (1 << (2 * NBIT)) : 1];
    __shared__ uint32_t rbase[P];
+   __shared__ uint32_t rbar[P];                   // every CTA's receive barrier (shared::cluster)
+   __shared__ __align__(8) unsigned long long rx_bar;  // this CTA's: Q values received per job
+   const uint32_t rx_bar_addr = (uint32_t)__cvta_generic_to_shared(&rx_bar);
+   if (tid == 0) mbar_init(rx_bar_addr, 1);
    if constexpr (NBIT <= 2)
       for (int i = tid; i < (1 << (2 * NBIT)); i += T)
          pair_lut[i] = make_float2(decode_level<NBIT>((uint32_t)i & MASK, a.levels),
                                    decode_level<NBIT>((uint32_t)i >> NBIT, a.levels));
-   for (int i = tid; i < P; i += T) rbase[i] = dsmem_addr(rbuf_addr, (uint32_t)i);
+   for (int i = tid; i < P; i += T) {
+      rbase[i] = dsmem_addr(rbuf_addr, (uint32_t)i);
+      rbar[i] = dsmem_addr(rx_bar_addr, (uint32_t)i);
+   }
 
    // ---- job sequence of this cluster: items cid, cid+ncl, ...; jobs 0..nfr-1 ----
    struct JobPos {
@@ -469,8 +509,135 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       }
    };
 
+   // pass 1 (Ns = 1) of job jp from staging slot `slot`: decode + window + radix-R1
+   auto pass1 = [&](const JobPos &jp, int slot) {
+      const Item item = a.items[jp.it];
+      const int mode = item.mode;
+      const bool has_b = mode != MODE_SINGLE;
+      const long long sa = item.start + (long long)jp.j * item.step;
+      const long long sb = (mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
+      const int offa = (int)(((sa + rank) / P) % SPW);
+      const int offb = (int)(((sb + rank) / P) % SPW);
+      const uint32_t *sta = stage + slot * 2 * NSLOT;
+      const uint32_t *stb = sta + NSLOT;
+      const int stream_a = a.code_stream[item.src_a];
+      const int src_b = (mode == MODE_AUTOSUM) ? item.src_a : item.src_b;
+      const int stream_b = has_b ? a.code_stream[src_b] : 0;
+      const uint32_t *blank_a = a.blank_any[stream_a] ? a.blank + (long long)stream_a * a.blank_words : nullptr;
+      const uint32_t *blank_b = (has_b && a.blank_any[stream_b]) ? a.blank + (long long)stream_b * a.blank_words : nullptr;
+      constexpr int nb1 = Q / R1;
+      constexpr int BPT1 = (nb1 + T - 1) / T;
+      float2 v[BPT1][R1];
+#pragma unroll
+      for (int b = 0; b < BPT1; b++) {
+         const int jj = tid + b * T;
+         if (nb1 % T == 0 || jj < nb1) {
+            uint32_t wa[R1], wb[R1];
+            if constexpr (PERM) {
+               // this thread's R1 words of each source, contiguous after the permutation
+               const int ga = (offa + jj) / SPW, gb = (offb + jj) / SPW;
+               const int sa0 = (ga % ST) * GS + ga / ST, sb0 = (gb % ST) * GS + gb / ST;
+               if ((sa0 & 3) == 0) {
+#pragma unroll
+                  for (int r = 0; r < R1; r += 4) {
+                     const uint4 t4 = *reinterpret_cast<const uint4 *>(sta + sa0 + r);
+                     wa[r] = t4.x; wa[r + 1] = t4.y; wa[r + 2] = t4.z; wa[r + 3] = t4.w;
+                  }
+               } else {
+#pragma unroll
+                  for (int r = 0; r < R1; r++) wa[r] = sta[sa0 + r];
+               }
+               if (has_b) {
+                  if ((sb0 & 3) == 0) {
+#pragma unroll
+                     for (int r = 0; r < R1; r += 4) {
+                        const uint4 t4 = *reinterpret_cast<const uint4 *>(stb + sb0 + r);
+                        wb[r] = t4.x; wb[r + 1] = t4.y; wb[r + 2] = t4.z; wb[r + 3] = t4.w;
+                     }
+                  } else {
+#pragma unroll
+                     for (int r = 0; r < R1; r++) wb[r] = stb[sb0 + r];
+                  }
+               }
+            }
+            if constexpr (PERM && NBIT <= 2) {
+               if (has_b) {
+                  // both sources' codes of sample q index one table entry
+                  // holding both levels; nb1 % SPW == 0, so the bit offset
+                  // within the word is the same for all r
+                  const int sha = NBIT * ((offa + jj) % SPW), shb = NBIT * ((offb + jj) % SPW);
+#pragma unroll
+                  for (int r = 0; r < R1; r++) {
+                     const int q = jj + r * nb1;
+                     const float w = wsl[q];
+                     const uint32_t ca = (wa[r] >> sha) & MASK, cb = (wb[r] >> shb) & MASK;
+                     float2 lv = pair_lut[(cb << NBIT) | ca];
+                     if (blank_a) {
+                        const long long smp = sa + rank + (long long)P * q;
+                        if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) lv.x = 0.0f;
+                     }
+                     if (blank_b) {
+                        const long long smp = sb + rank + (long long)P * q;
+                        if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) lv.y = 0.0f;
+                     }
+                     v[b][r] = make_float2(lv.x * w, lv.y * w);
+                  }
+                  DFT<R1>::run(v[b]);
+                  continue;
+               }
+            }
+#pragma unroll
+            for (int r = 0; r < R1; r++) {
+               const int q = jj + r * nb1;
+               const float w = wsl[q];
+               const int ia = offa + q;
+               const uint32_t worda = PERM ? wa[r] : sta[ia / SPW];
+               float xa = decode_level<NBIT>((worda >> (NBIT * (ia % SPW))) & MASK, a.levels);
+               if (blank_a) {
+                  const long long smp = sa + rank + (long long)P * q;
+                  if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) xa = 0.0f;
+               }
+               float xb = 0.0f;
+               if (has_b) {
+                  const int ib = offb + q;
+                  const uint32_t wordb = PERM ? wb[r] : stb[ib / SPW];
+                  xb = decode_level<NBIT>((wordb >> (NBIT * (ib % SPW))) & MASK, a.levels);
+                  if (blank_b) {
+                     const long long smp = sb + rank + (long long)P * q;
+                     if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) xb = 0.0f;
+                  }
+               }
+               v[b][r] = make_float2(xa * w, xb * w);
+            }
+            DFT<R1>::run(v[b]);
+         }
+      }
+      if constexpr (PREC == 0) {
+#pragma unroll
+         for (int b = 0; b < BPT1; b++) {
+            const int jj = tid + b * T;
+            if (nb1 % T == 0 || jj < nb1) {
+#pragma unroll
+               for (int r = 0; r < R1; r++)
+                  buf[(R1 == 16) ? jj * 17 + r : pidx(jj * R1 + r)] = v[b][r];  // pidx(16 jj + r), r < 16
+            }
+         }
+      } else {
+         // four-step twiddle W_Q^{q2 k1} (q2 = tid, k1 = r), then rows y[k1][q2];
+         // tw3 holds W_Q^{2^i q2}, the same bases the FP32 form's last pass uses
+         float2 base[nbases(R3)];
+#pragma unroll
+         for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
+         twiddle_by_powers<R1>(v[0], base);
+#pragma unroll
+         for (int r = 0; r < R1; r++) buf[r * TC_ROW + ridx(tid)] = v[0][r];
+      }
+   };
+
    JobPos cur{cid, 0};
    if (job_valid(cur)) prefetch(cur, 0);
+   cp_async_commit();
+   if (job_valid(cur) && job_valid(next_job(cur))) prefetch(next_job(cur), 1);
    cp_async_commit();
    __syncthreads();      // tables visible
    cluster_arrive();     // pairs with the wait before the first job's pushes
@@ -483,139 +650,20 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 #pragma unroll
          for (int c = 0; c < 4; c++) acc[u][x][c] = 0.0f;
 
-   int n = 0;  // job counter (staging slot parity)
+   int n = 0;  // job counter (staging slot parity, receive-barrier phase)
+   bool gave_up = false;
+   if (job_valid(cur)) {
+      cp_async_wait1();  // the first job's codes have landed
+      __syncthreads();
+      pass1(cur, 0);
+   }
    while (job_valid(cur)) {
       const Item item = a.items[cur.it];
       const int mode = item.mode;
       const bool has_b = mode != MODE_SINGLE;
+      (void)has_b;
       const JobPos nxt = next_job(cur);
-      if (job_valid(nxt)) prefetch(nxt, (n + 1) & 1);
-      cp_async_commit();
-      cp_async_wait1();     // this job's codes have landed
-      __syncthreads();
-
-      // ---- pass 1 (Ns = 1): decode + window + radix-R1 ----
-      {
-         const long long sa = item.start + (long long)cur.j * item.step;
-         const long long sb = (mode == MODE_AUTOSUM) ? sa + item.offset_b : sa;
-         const int offa = (int)(((sa + rank) / P) % SPW);
-         const int offb = (int)(((sb + rank) / P) % SPW);
-         const uint32_t *sta = stage + (n & 1) * 2 * NSLOT;
-         const uint32_t *stb = sta + NSLOT;
-         const int stream_a = a.code_stream[item.src_a];
-         const int src_b = (mode == MODE_AUTOSUM) ? item.src_a : item.src_b;
-         const int stream_b = has_b ? a.code_stream[src_b] : 0;
-         const uint32_t *blank_a = a.blank_any[stream_a] ? a.blank + (long long)stream_a * a.blank_words : nullptr;
-         const uint32_t *blank_b = (has_b && a.blank_any[stream_b]) ? a.blank + (long long)stream_b * a.blank_words : nullptr;
-         constexpr int nb1 = Q / R1;
-         constexpr int BPT1 = (nb1 + T - 1) / T;
-         float2 v[BPT1][R1];
-#pragma unroll
-         for (int b = 0; b < BPT1; b++) {
-            const int jj = tid + b * T;
-            if (nb1 % T == 0 || jj < nb1) {
-               uint32_t wa[R1], wb[R1];
-               if constexpr (PERM) {
-                  // this thread's R1 words of each source, contiguous after the permutation
-                  const int ga = (offa + jj) / SPW, gb = (offb + jj) / SPW;
-                  const int sa0 = (ga % ST) * GS + ga / ST, sb0 = (gb % ST) * GS + gb / ST;
-                  if ((sa0 & 3) == 0) {
-#pragma unroll
-                     for (int r = 0; r < R1; r += 4) {
-                        const uint4 t4 = *reinterpret_cast<const uint4 *>(sta + sa0 + r);
-                        wa[r] = t4.x; wa[r + 1] = t4.y; wa[r + 2] = t4.z; wa[r + 3] = t4.w;
-                     }
-                  } else {
-#pragma unroll
-                     for (int r = 0; r < R1; r++) wa[r] = sta[sa0 + r];
-                  }
-                  if (has_b) {
-                     if ((sb0 & 3) == 0) {
-#pragma unroll
-                        for (int r = 0; r < R1; r += 4) {
-                           const uint4 t4 = *reinterpret_cast<const uint4 *>(stb + sb0 + r);
-                           wb[r] = t4.x; wb[r + 1] = t4.y; wb[r + 2] = t4.z; wb[r + 3] = t4.w;
-                        }
-                     } else {
-#pragma unroll
-                        for (int r = 0; r < R1; r++) wb[r] = stb[sb0 + r];
-                     }
-                  }
-               }
-               if constexpr (PERM && NBIT <= 2) {
-                  if (has_b) {
-                     // both sources' codes of sample q index one table entry
-                     // holding both levels; nb1 % SPW == 0, so the bit offset
-                     // within the word is the same for all r
-                     const int sha = NBIT * ((offa + jj) % SPW), shb = NBIT * ((offb + jj) % SPW);
-#pragma unroll
-                     for (int r = 0; r < R1; r++) {
-                        const int q = jj + r * nb1;
-                        const float w = wsl[q];
-                        const uint32_t ca = (wa[r] >> sha) & MASK, cb = (wb[r] >> shb) & MASK;
-                        float2 lv = pair_lut[(cb << NBIT) | ca];
-                        if (blank_a) {
-                           const long long smp = sa + rank + (long long)P * q;
-                           if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) lv.x = 0.0f;
-                        }
-                        if (blank_b) {
-                           const long long smp = sb + rank + (long long)P * q;
-                           if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) lv.y = 0.0f;
-                        }
-                        v[b][r] = make_float2(lv.x * w, lv.y * w);
-                     }
-                     DFT<R1>::run(v[b]);
-                     continue;
-                  }
-               }
-#pragma unroll
-               for (int r = 0; r < R1; r++) {
-                  const int q = jj + r * nb1;
-                  const float w = wsl[q];
-                  const int ia = offa + q;
-                  const uint32_t worda = PERM ? wa[r] : sta[ia / SPW];
-                  float xa = decode_level<NBIT>((worda >> (NBIT * (ia % SPW))) & MASK, a.levels);
-                  if (blank_a) {
-                     const long long smp = sa + rank + (long long)P * q;
-                     if ((__ldg(blank_a + (smp >> 5)) >> (smp & 31)) & 1u) xa = 0.0f;
-                  }
-                  float xb = 0.0f;
-                  if (has_b) {
-                     const int ib = offb + q;
-                     const uint32_t wordb = PERM ? wb[r] : stb[ib / SPW];
-                     xb = decode_level<NBIT>((wordb >> (NBIT * (ib % SPW))) & MASK, a.levels);
-                     if (blank_b) {
-                        const long long smp = sb + rank + (long long)P * q;
-                        if ((__ldg(blank_b + (smp >> 5)) >> (smp & 31)) & 1u) xb = 0.0f;
-                     }
-                  }
-                  v[b][r] = make_float2(xa * w, xb * w);
-               }
-               DFT<R1>::run(v[b]);
-            }
-         }
-         if constexpr (PREC == 0) {
-#pragma unroll
-            for (int b = 0; b < BPT1; b++) {
-               const int jj = tid + b * T;
-               if (nb1 % T == 0 || jj < nb1) {
-#pragma unroll
-                  for (int r = 0; r < R1; r++)
-                     buf[(R1 == 16) ? jj * 17 + r : pidx(jj * R1 + r)] = v[b][r];  // pidx(16 jj + r), r < 16
-               }
-            }
-         } else {
-            // four-step twiddle W_Q^{q2 k1} (q2 = tid, k1 = r), then rows y[k1][q2];
-            // tw3 holds W_Q^{2^i q2}, the same bases the FP32 form's last pass uses
-            float2 base[nbases(R3)];
-#pragma unroll
-            for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
-            twiddle_by_powers<R1>(v[0], base);
-#pragma unroll
-            for (int r = 0; r < R1; r++) buf[r * TC_ROW + ridx(tid)] = v[0][r];
-         }
-      }
-      __syncthreads();
+      __syncthreads();  // this job's pass-1 output is visible
       // push F_rank[k1] to the CTA that owns pair min(k1, Q-k1); receive layout [p][hi][u]
       auto push = [&](int k1, float2 val) {
          int u, hi;
@@ -625,7 +673,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          else { u = Q - k1; hi = 1; }
          const int owner = u / UC;
          const int slot = hi * UC + (u - owner * UC);
-         dsmem_st2(dsmem_addr(rbuf_addr + 8u * (uint32_t)(rank * SIDES + slot), owner), val);
+         dsmem_st2_async(rbase[owner] + 8u * (uint32_t)(rank * SIDES + slot), val, rbar[owner]);
       };
       if constexpr (PREC == 0) {
          // ---- pass 2 in shared memory, pass 3 into registers ----
@@ -648,7 +696,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                      const int k1 = j + r * NS3;
                      const int uu = (r < R3 / 2) ? k1 : ((Q - k1) & (Q / 2 - 1));
                      const int slot = ((r < R3 / 2) ? 0 : UC) + (uu & (UC - 1));
-                     dsmem_st2(rbase[uu / UC] + self + 8u * (uint32_t)slot, v3[b][r]);
+                     dsmem_st2_async(rbase[uu / UC] + self + 8u * (uint32_t)slot, v3[b][r], rbar[uu / UC]);
                   }
                } else {
 #pragma unroll
@@ -717,7 +765,22 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                   push((2 * warp + rr) + 16 * (16 * m1 + m2), make_float2(ore[rr][tp][e], oim[rr][tp][e]));
                }
       }
-      cluster.sync();  // every CTA's pushes have landed
+      // ---- the next job's pass 1 while this job's values are in flight ----
+      if (job_valid(nxt)) {
+         cp_async_wait0();  // its codes have landed
+         __syncthreads();   // and this job's last reads of buf are done
+         pass1(nxt, (n + 1) & 1);
+         const JobPos nn = next_job(nxt);
+         if (job_valid(nn)) prefetch(nn, n & 1);  // the slot this job's codes used
+         cp_async_commit();
+      }
+      // this CTA's Q values of the job have landed (counted in bytes on
+      // its barrier; one arrival per phase, from thread 0)
+      if (tid == 0) mbar_arrive_expect(rx_bar_addr, (uint32_t)(Q * 8));
+      if (!gave_up && !mbar_wait_parity(rx_bar_addr, (uint32_t)(n & 1))) {
+         gave_up = true;  // report once; later jobs do not wait again
+         if (a.status) atomicExch(a.status, 1);
+      }
 
       // ---- radix-P stage across the cluster + pair separation ----
 #pragma unroll

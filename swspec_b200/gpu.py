@@ -40,7 +40,8 @@ class Config(C.Structure):
                 ("pcal_tonebins", C.c_int), ("pcal_rotatorlen", C.c_int),
                 ("samplingfreq", C.c_double), ("pcal_offset_hz", C.c_double),
                 ("max_run_bytes", C.c_size_t), ("runs_per_output", C.c_int),
-                ("pcal_ntones", C.c_int), ("autotune", C.c_int), ("plan_family", C.c_int)]
+                ("pcal_ntones", C.c_int), ("autotune", C.c_int), ("plan_family", C.c_int),
+                ("plan_candidate", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -119,7 +120,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
                 extract_pcal=False, pcal_tonebins=0, pcal_rotatorlen=0, samplingfreq=32e6,
                 pcal_offset_hz=10e3, layout2: Layout | None = None,
                 runs_per_output: int = 1, pcal_ntones: int = 0, autotune: bool = False,
-                plan_family: int = 0) -> Config:
+                plan_family: int = 0, plan_candidate: int = 0) -> Config:
     c = Config()
     c.layout[0] = lay
     c.layout[1] = layout2 if layout2 is not None else lay
@@ -147,6 +148,7 @@ def make_config(lay: Layout, N: int, window="hann", overlap=1, core_overlapped_f
     c.pcal_ntones = pcal_ntones
     c.autotune = int(bool(autotune))
     c.plan_family = plan_family
+    c.plan_candidate = plan_candidate
     return c
 
 

@@ -153,3 +153,29 @@ def test_spacecraft_tone_3p2M_cosine2_pcal(gpu):
         got = core.tones[0, k]
         assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-6
         assert np.max(np.abs(np.angle(got * np.conj(ref)))) < 1e-5
+
+
+# candidate splits per length, as the autotuner numbers them
+CANDIDATES = {1 << 16: 3, 1 << 18: 3, 1 << 19: 2, 1 << 20: 4, 1 << 21: 2, 1 << 22: 3, 3_200_000: 4}
+
+
+@pytest.mark.parametrize("N,k", [(N, k) for N, n in CANDIDATES.items() for k in range(n)])
+def test_every_four_step_candidate(gpu, N, k):
+    """Each candidate split the autotuner may choose, pinned through
+    plan_candidate: two frames of a 2-bit single-channel stream (one
+    packed frame pair) against the FP64 oracle."""
+    from swspec_b200.workloads import StreamSpec, stream_payload
+    spec = StreamSpec(k, N, 2, 16e6, 1.0, 1, (2.7e6,), (N * 2 * 2 // 8 + 7) // 8 * 8, 2, 1)
+    pay = stream_payload(spec)
+    lay = gpu.layout("vdif:8000", 1, 2, framed=False)
+    cfg = gpu.make_config(lay, N, "hann", 1, 2, max_run_bytes=len(pay), samplingfreq=32e6,
+                          plan_family=gpu.PLAN_FOURSTEP, plan_candidate=k)
+    core = gpu.Core(cfg)
+    info = core.plan_info()
+    assert f"of {CANDIDATES[N]}" in info and "four-step" in info, info
+    auto, _, _, ns = core.run([pay])
+    x = O.decode(O.FMT_VDIF, 1, 2, pay, spec.samples_per_run, 0, payload_bytes=8000)
+    ra, _, _, nref = oracle_run([x], N, "hann", 1, 2)
+    r32, _, _, _ = _fp32_run([x], N, "hann", 1, 2)
+    assert ns == nref == 1
+    _check_auto(auto[0, 0], ra[0, 0], r32[0, 0], per_bin=False)
