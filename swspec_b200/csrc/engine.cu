@@ -139,6 +139,16 @@ struct swsgpu_handle {
    cudaEvent_t slot_free[2] = {nullptr, nullptr};  // kernels finished reading the slot
    int next_slot = 0;
    cudaEvent_t last_h2d = nullptr;    // input copy of the last submitted run
+   // runs of one output group collected into device chunks of up to chunk_max
+   // runs (header-free streams, equal sizes, consecutive payload offsets) and
+   // processed by one launch per chunk: one run per launch leaves most of the
+   // cluster kernel's CTAs idle at the end of each launch
+   DevBuf d_region[2][SWSGPU_MAX_STREAMS];
+   cudaEvent_t region_free[2] = {nullptr, nullptr};
+   int chunk_max = 1, chunk_n = 0, chunk_region = 0;
+   bool chunk_group_first = false;
+   size_t chunk_run_bytes = 0;
+   long long chunk_off0[SWSGPU_MAX_STREAMS] = {0, 0};
    bool pending_out = false;          // the pending run completes spectra
    bool pending = false;
    int pending_nspec = 0;
@@ -795,6 +805,38 @@ static void drop_prof_events(swsgpu_handle *h)
    h->prof_events.clear();
 }
 
+// Launches the open chunk of collected runs as one multi-run chunk whose
+// spectra are summed into the group's FP64 running sums (group_end: and
+// written out).
+static int flush_chunk(swsgpu_handle *h, bool group_end, int *nspec)
+{
+   const swsgpu_config &c = h->cfg;
+   if (h->chunk_n == 0) return SWSGPU_OK;
+   const int region = h->chunk_region;
+   const void *d_raw[SWSGPU_MAX_STREAMS];
+   size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   long long grid_off[SWSGPU_MAX_STREAMS];
+   for (int s = 0; s < c.num_streams; s++) {
+      d_raw[s] = h->d_region[region][s].p;
+      raw_bytes[s] = h->chunk_run_bytes * (size_t)h->chunk_n;
+      grid_off[s] = h->chunk_off0[s] % payload_bytes(c.layout[s]);
+   }
+   const bool first = h->chunk_group_first;
+   const int acc_mode = group_end ? (first ? 0 : 3) : (first ? 1 : 2);
+   CK(h, cudaStreamWaitEvent(h->stream, h->last_h2d, 0));
+   const int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, h->chunk_run_bytes, h->chunk_n, h->chunk_n,
+                               (float *)h->d_out_auto.p, c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
+                               c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, nspec, acc_mode,
+                               first ? 1 : 0, group_end ? 1 : 0,
+                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
+   if (rc) return rc;
+   CK(h, cudaEventRecord(h->region_free[region], h->stream));
+   h->chunk_region ^= 1;
+   h->chunk_n = 0;
+   h->chunk_group_first = false;
+   return SWSGPU_OK;
+}
+
 static int autotune_big(swsgpu_handle *h, int iters);
 static std::mutex &tune_mutex();
 static int tuned_choice(int N, int nbit);
@@ -955,7 +997,10 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    bool ev_ok = cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) == cudaSuccess;
    for (int k = 0; k < 2 && ev_ok; k++)
       ev_ok = cudaEventCreateWithFlags(&h->slot_h2d[k], cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&h->slot_free[k], cudaEventDisableTiming) == cudaSuccess;
+              cudaEventCreateWithFlags(&h->slot_free[k], cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&h->region_free[k], cudaEventDisableTiming) == cudaSuccess;
+   h->chunk_max = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(1, cfg->runs_per_output),
+                                                            ((size_t)32 << 20) / std::max<size_t>(1, cfg->max_run_bytes)));
    if (!ev_ok || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
        cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming) != cudaSuccess) {
       h->err = "stream/event creation failed";
@@ -1111,6 +1156,8 @@ void swsgpu_destroy(swsgpu_handle *h)
       for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) h->d_slot[k][s].release();
       if (h->slot_h2d[k]) cudaEventDestroy(h->slot_h2d[k]);
       if (h->slot_free[k]) cudaEventDestroy(h->slot_free[k]);
+      if (h->region_free[k]) cudaEventDestroy(h->region_free[k]);
+      for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) h->d_region[k][s].release();
    }
    for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) {
       h->d_raw[s].release();
@@ -1144,18 +1191,16 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       return fail(h, SWSGPU_ESTATE, "submit while a run's spectra are pending (wait and fetch first)");
    const swsgpu_config &c = h->cfg;
    CK(h, cudaSetDevice(h->device));
-   // input slot: its previous run's kernels must have finished reading it
-   const int slot = h->next_slot;
-   CK(h, cudaStreamWaitEvent(h->cstream, h->slot_free[slot], 0));
    // payload bytes per stream: the reference walks min over sources
    size_t payload_min = (size_t)-1;
    long long grid_off[SWSGPU_MAX_STREAMS];
-   size_t raw_bytes[SWSGPU_MAX_STREAMS];
-   const void *d_raw[SWSGPU_MAX_STREAMS];
+   long long offs[SWSGPU_MAX_STREAMS];
+   bool framed = false, equal = true;
    for (int s = 0; s < c.num_streams; s++) {
       const swsgpu_layout &L = c.layout[s];
       const int pb = payload_bytes(L);
-      long long off = stream_payload_offset ? (long long)(stream_payload_offset[s] % pb) : 0;
+      offs[s] = stream_payload_offset ? (long long)stream_payload_offset[s] : 0;
+      long long off = offs[s] % pb;
       if (off % 4) return fail(h, SWSGPU_EINVAL, "payload offset must be a multiple of 4 bytes");
       size_t pay;
       if (L.header_bytes == 0) {
@@ -1167,18 +1212,13 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
          size_t rem = nbytes[s] - nfr * L.frame_bytes;
          pay = nfr * pb + (rem > (size_t)L.header_bytes ? rem - L.header_bytes : 0);
          grid_off[s] = 0;
+         framed = true;
       }
       if (nbytes[s] > c.max_run_bytes + (size_t)c.max_run_bytes / 8 + 1024 + 64)
          return fail(h, SWSGPU_EINVAL, "buffer larger than max_run_bytes");
+      if (nbytes[s] != nbytes[0]) equal = false;
       payload_min = std::min(payload_min, pay);
-      CK(h, cudaMemcpyAsync(h->d_slot[slot][s].p, raw[s], nbytes[s], cudaMemcpyHostToDevice, h->cstream));
-      raw_bytes[s] = nbytes[s];
-      d_raw[s] = h->d_slot[slot][s].p;
    }
-   CK(h, cudaEventRecord(h->slot_h2d[slot], h->cstream));
-   CK(h, cudaStreamWaitEvent(h->stream, h->slot_h2d[slot], 0));
-   h->last_h2d = h->slot_h2d[slot];
-   h->next_slot ^= 1;
    RunShape rs = run_shape(c, samples_of(c.layout[0], payload_min));
    const int S = h->S;
    const int nsp = std::max(rs.nspec, 0);
@@ -1206,16 +1246,71 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       pcal_zero = first ? 1 : 0;
       pcal_write = group_end ? 1 : 0;
    }
-   if (nsp > 0) {
-      int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, payload_min, 1, 1, (float *)h->d_out_auto.p,
-                            c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
-                            c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec,
-                            acc_mode, pcal_zero, pcal_write,
-                            h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
+   // collect the runs of a group into device chunks when they continue the
+   // recording (equal header-free buffers at consecutive payload offsets)
+   const bool chunkable = rpo > 1 && h->chunk_max > 1 && !framed && equal && nsp == 1;
+   bool continues = chunkable && h->chunk_n > 0 && nbytes[0] == h->chunk_run_bytes;
+   for (int s = 0; continues && s < c.num_streams; s++)
+      if (offs[s] != h->chunk_off0[s] + (long long)h->chunk_n * (long long)h->chunk_run_bytes) continues = false;
+   if (h->chunk_n > 0 && !continues) {
+      int ns = 0;
+      const int rc = flush_chunk(h, false, &ns);
       if (rc) return rc;
-      if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
    }
-   CK(h, cudaEventRecord(h->slot_free[slot], h->stream));
+   if (chunkable) {
+      const int region = h->chunk_region;
+      if (h->chunk_n == 0) {
+         for (int k = 0; k < 2; k++)
+            for (int s = 0; s < c.num_streams; s++)
+               CK(h, h->d_region[k][s].ensure((size_t)h->chunk_max * c.max_run_bytes + 64));
+         CK(h, cudaStreamWaitEvent(h->cstream, h->region_free[region], 0));
+         for (int s = 0; s < c.num_streams; s++) h->chunk_off0[s] = offs[s];
+         h->chunk_run_bytes = nbytes[0];
+         h->chunk_group_first = h->group_pos == 0;
+      }
+      for (int s = 0; s < c.num_streams; s++)
+         CK(h, cudaMemcpyAsync((char *)h->d_region[region][s].p + (size_t)h->chunk_n * h->chunk_run_bytes, raw[s],
+                               nbytes[s], cudaMemcpyHostToDevice, h->cstream));
+      const int ev = h->next_slot;
+      CK(h, cudaEventRecord(h->slot_h2d[ev], h->cstream));
+      h->last_h2d = h->slot_h2d[ev];
+      h->next_slot ^= 1;
+      h->chunk_n++;
+      h->group_pos = group_end ? 0 : h->group_pos + 1;
+      if (h->chunk_n == h->chunk_max || group_end) {
+         const int rc = flush_chunk(h, group_end, &nspec);
+         if (rc) return rc;
+      } else {
+         h->last_launches = 0;
+      }
+   } else {
+      // one run per launch through the two input slots
+      const int slot = h->next_slot;
+      CK(h, cudaStreamWaitEvent(h->cstream, h->slot_free[slot], 0));
+      const void *d_raw[SWSGPU_MAX_STREAMS];
+      size_t raw_bytes[SWSGPU_MAX_STREAMS];
+      for (int s = 0; s < c.num_streams; s++) {
+         CK(h, cudaMemcpyAsync(h->d_slot[slot][s].p, raw[s], nbytes[s], cudaMemcpyHostToDevice, h->cstream));
+         raw_bytes[s] = nbytes[s];
+         d_raw[s] = h->d_slot[slot][s].p;
+      }
+      CK(h, cudaEventRecord(h->slot_h2d[slot], h->cstream));
+      CK(h, cudaStreamWaitEvent(h->stream, h->slot_h2d[slot], 0));
+      h->last_h2d = h->slot_h2d[slot];
+      h->next_slot ^= 1;
+      if (nsp > 0) {
+         int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, payload_min, 1, 1, (float *)h->d_out_auto.p,
+                               c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
+                               c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec,
+                               acc_mode, pcal_zero, pcal_write,
+                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
+         if (rc) return rc;
+         if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
+      } else {
+         h->last_launches = 0;
+      }
+      CK(h, cudaEventRecord(h->slot_free[slot], h->stream));
+   }
    h->fetch_ready = group_end;
    if (nsp > 0 && group_end) {
       char *hp = (char *)h->h_out.p;
@@ -1229,8 +1324,6 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       if (h->h_tones_bytes)
          CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->d_out_tones.p,
                                h->h_tones_bytes, cudaMemcpyDeviceToHost, h->stream));
-   } else {
-      h->last_launches = 0;
    }
    CK(h, cudaEventRecord(h->done, h->stream));
    h->pending = true;
@@ -1254,11 +1347,14 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
          h->pending = false;
          return fail(h, SWSGPU_ECUDA, std::string("run failed: ") + cudaGetErrorString(e));
       }
-      if (timeout_ms >= 0) {
-         auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
-         if (ms >= timeout_ms) return fail(h, SWSGPU_ETIMEOUT, "run not complete within timeout");
-      }
-      std::this_thread::sleep_for(std::chrono::microseconds(50));
+      const auto us = std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+      if (timeout_ms >= 0 && us >= 1000ll * timeout_ms)
+         return fail(h, SWSGPU_ETIMEOUT, "run not complete within timeout");
+      // a run's copy or kernels finish within a few hundred microseconds:
+      // poll tightly at first (a sleep costs a scheduler quantum per run),
+      // then back off
+      if (us < 2000) std::this_thread::yield();
+      else std::this_thread::sleep_for(std::chrono::microseconds(50));
    }
    h->pending = false;
    const bool had_out = h->pending_out;

@@ -314,3 +314,53 @@ def test_pcal_tones_known_answer(gpu):
     assert np.max(np.abs(tones - ref)) / np.max(np.abs(ref)) < 1e-6
     # phasor = amplitude / 2 in decoded units: 0.5 / 2 * 24 / 256
     assert np.allclose(np.abs(tones), 0.25 * 24.0 / 256.0, rtol=2e-2)
+
+
+def test_group_runs_chunked_and_per_run(gpu):
+    """A 10-run output group submitted run by run: header-free runs at
+    consecutive payload offsets are collected into one device chunk per
+    launch; a break in the offsets flushes the open chunk (4 + 6 runs);
+    framed runs go one per launch.  All three give the FP64 oracle's
+    combined spectrum."""
+    import oracle as O
+    N, cof, nrun, frames_per_run = 4096, 12, 10, 20
+    run_pay = frames_per_run * 10000          # 50000 sample-times: 12 whole FFTs
+    data, info = synth.c3_stream(123, N=N)
+    pay = np.frombuffer(payload_of(data, info["fmt"]), dtype=np.uint8)
+    fr = np.frombuffer(data, dtype=np.uint8).reshape(-1, 10016)
+    S = N // 2 + 1
+
+    def core_for(framed):
+        lay = gpu.layout("mark5b", 16, 2, framed=framed)
+        cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 1), (0, 9)), xpols=((0, 1),),
+                              max_run_bytes=frames_per_run * 10016, samplingfreq=64e6, runs_per_output=nrun)
+        return gpu.Core(cfg)
+
+    def collect(core, runs, offsets):
+        auto = np.zeros((1, 2, S), np.float32)
+        xp = np.zeros((1, 1, S, 2), np.float32)
+        for r, (buf, off) in enumerate(zip(runs, offsets)):
+            core.set_sizes([len(buf)])
+            core.submit([np.frombuffer(buf, dtype=np.uint8)], payload_offsets=[off])
+            assert core.wait() == (1 if r == len(runs) - 1 else 0)
+        core.fetch_into(auto, xp)
+        return auto[0], xp[0, 0, :, 0] + 1j * xp[0, 0, :, 1]
+
+    runs = [pay[r * run_pay:(r + 1) * run_pay].tobytes() for r in range(nrun)]
+    a1, x1 = collect(core_for(False), runs, [r * run_pay for r in range(nrun)])
+    # a jump after run 3 (a multiple of the 10000-byte payload keeps the frame phase)
+    a2, x2 = collect(core_for(False), runs, [r * run_pay + (0 if r < 4 else 10_000_000) for r in range(nrun)])
+    framed = [fr[r * frames_per_run:(r + 1) * frames_per_run].tobytes() for r in range(nrun)]
+    a3, x3 = collect(core_for(True), framed, [0] * nrun)
+    ra = np.zeros((2, S))
+    rx = np.zeros(S, complex)
+    for r in range(nrun):
+        s = [O.decode(O.FMT_MARK5B, 16, 2, runs[r], run_pay // 4, c, payload_bytes=10000) for c in (1, 9)]
+        aa, xx, _, n = oracle_run(s, N, "hann", 1, cof, nxpols=1)
+        assert n == 1
+        ra += aa[0]
+        rx += xx[0, 0]
+    for a, x in ((a1, x1), (a2, x2), (a3, x3)):
+        assert np.max(np.abs(a - ra) / ra) < REL_TOL
+        assert np.max(np.abs(x - rx) / np.sqrt(ra[0] * ra[1])) < REL_TOL
+    assert np.max(np.abs(a1 - a2) / a1) < 1e-6 and np.max(np.abs(a1 - a3) / a1) < 1e-6
