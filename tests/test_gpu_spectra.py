@@ -8,7 +8,7 @@ TaskCoreIPP::doMaths on the same decoded samples.
 import numpy as np
 import pytest
 
-from helpers import REL_TOL, decode_channels, oracle_run, rel_err_auto, rel_err_xpol
+from helpers import REL_TOL, decode_channels, oracle_run, payload_of, rel_err_auto, rel_err_xpol
 from swspec_b200 import synth
 
 pytestmark = pytest.mark.gpu
