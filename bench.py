@@ -506,6 +506,101 @@ def c4_arm(args) -> None:
     reps.close()
 
 
+# one integration per step, device-resident header-free payload, the
+# reference's buffer plan (runs of core_ffts FFTs combined on the device)
+SPEC_WORKLOADS = {
+    "c1": dict(desc="plain method: Mark5B-1024-16-2, channel 1 only, N=32768 Hann, 1 s (976 FFTs), "
+                    "2 MiB runs x 61", fmt="mark5b", nchan=16, nbit=2, N=32768, window="hann", fs=32e6,
+               core_ffts=16, run_bytes=2 << 20, runs=61, sources=((0, 0),), xpols=(), pcal=None),
+    "c2": dict(desc="spacecraft-tone tracking: Mark5B-1024-16-2, 16 channels, N=3,200,000 cosine2, 10 s "
+                    "(100 FFTs), 51.2 MB runs x 25, phase-cal 32 bins / 3200 rotator, 16 tones",
+               fmt="mark5b", nchan=16, nbit=2, N=3_200_000, window="cosine2", fs=32e6, core_ffts=4,
+               run_bytes=51_200_000, runs=25, sources=tuple((0, c) for c in range(16)), xpols=(),
+               pcal=dict(tonebins=32, rotatorlen=3200, offset=10e3, ntones=16)),
+    "c5": dict(desc="dynamic range: VDIF 8-bit 1 channel 64 Msps, N=2^22 Blackman-Harris, 5 s (76 FFTs), "
+                    "16 MiB runs x 19", fmt="vdif:8000", nchan=1, nbit=8, N=1 << 22, window="blackmanharris",
+               fs=64e6, core_ffts=4, run_bytes=16 << 20, runs=19, sources=((0, 0),), xpols=(), pcal=None),
+}
+
+
+def spec_arm(args) -> None:
+    import torch
+
+    from swspec_b200 import gpu
+    from swspec_b200.replicas import Replicas
+    w = SPEC_WORKLOADS[args.workload]
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    reps = Replicas("nccl")
+    lay = gpu.layout(w["fmt"], w["nchan"], w["nbit"], framed=False)
+    pc = w["pcal"] or {}
+    cfg = gpu.make_config(lay, w["N"], w["window"], 1, w["core_ffts"], sources=w["sources"], xpols=w["xpols"],
+                          max_run_bytes=w["run_bytes"], samplingfreq=w["fs"], runs_per_output=w["runs"],
+                          extract_pcal=bool(pc), pcal_tonebins=pc.get("tonebins", 0),
+                          pcal_rotatorlen=pc.get("rotatorlen", 0), pcal_offset_hz=pc.get("offset", 10e3),
+                          pcal_ntones=pc.get("ntones", 0), autotune=True)
+    core = gpu.Core(cfg, device=local)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1000 + reps.rank)
+    raw = torch.randint(0, 256, (w["run_bytes"] * w["runs"],), dtype=torch.uint8, device="cuda", generator=g)
+    S = w["N"] // 2 + 1
+    ns = len(w["sources"])
+    d_auto = torch.zeros(ns, S, dtype=torch.float32, device="cuda")
+    d_pcal = torch.zeros(ns, max(pc.get("tonebins", 1), 1), 2, dtype=torch.float32, device="cuda")
+    d_tones = torch.zeros(ns, max(pc.get("ntones", 1), 1), 2, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+
+    def step():
+        core.process_device([raw.data_ptr()], w["run_bytes"], w["runs"], w["runs"], d_auto.data_ptr(), 0,
+                            d_pcal.data_ptr() if pc else 0, st.cuda_stream, d_tones.data_ptr() if pc else 0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    reps.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as cs:
+        ev0.record(st)
+        for _ in range(args.steps):
+            step()
+        ev1.record(st)
+        st.synchronize()
+    reps.barrier()
+    ms = reps.max(ev0.elapsed_time(ev1)) / args.steps
+    launches = core.last_launches()
+    core.profile(True)
+    for _ in range(3):
+        step()
+    nk, kms = core.profile_read()
+    core.profile(False)
+    samples = w["runs"] * w["core_ffts"] * w["N"] * ns
+    value = samples * reps.world / (ms * 1e-3) / 1e9
+    if reps.rank == 0:
+        peaks = measured_peaks()
+        kern_s = kms / max(nk, 1) * 1e-3
+        bytes_in = w["run_bytes"] * w["runs"]
+        flops = 5.0 * w["N"] * math.log2(w["N"]) * w["core_ffts"] * w["runs"] * ns
+        p32 = fp32_peak(local)
+        line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": reps.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (random codes)",
+                "config": {"workload": w["desc"], "fft_points": w["N"], "sources": ns,
+                           "samples_per_step": samples, "bytes_per_step": bytes_in,
+                           "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_in / 1e6),
+                           "plan": core.plan_info()},
+                "clocks": cs.summary(), "gpu_launches": launches * args.steps, "e2e": None,
+                "roofline": {"bound": "hbm", "achieved": bytes_in / kern_s / 1e9, "peak": peaks["hbm_gbs"],
+                             "unit": "GB/s", "frac": bytes_in / kern_s / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                             "compute": {"achieved_tflops": flops / kern_s / 1e12, "fp32_peak_tflops": p32,
+                                         "frac_fp32": flops / kern_s / 1e12 / p32 if p32 else None},
+                             "kernel_ms": kern_s * 1e3},
+                "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    core.close()
+    reps.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -517,13 +612,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plan", default="auto", choices=["auto", "cluster", "fourstep"],
                     help="FFT path for the cross-spectra workload (auto: cluster kernel)")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4"],
-                    help="c3: dual-pol cross-spectra (default line); c4: batched uneven streams")
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c3: dual-pol cross-spectra (the default line); c1: plain single channel; "
+                         "c2: 3.2M-point spectra with phase-cal tones; c4: batched uneven streams; "
+                         "c5: 2^22-point 8-bit dynamic range")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload == "c4":
         c4_arm(args)
+    elif args.workload in SPEC_WORKLOADS:
+        spec_arm(args)
     else:
         gpu_arm(args)
 
