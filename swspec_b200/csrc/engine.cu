@@ -106,6 +106,7 @@ struct SchedEntry {
    Schedule sc;
    DevBuf d_items, d_entries, d_outs, d_pcal_jobs, d_bjobs, d_bitems;
    std::vector<int4> batches;  // four-step: {job0, njobs, item0, nitems}
+   int pcal_word_fold = 0;     // phase-cal jobs allow the word-wise fold
    void release()
    {
       d_items.release();
@@ -600,6 +601,13 @@ static int get_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int rpo, 
       return cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice);
    };
    cudaError_t err;
+   {
+      // word-wise phase-cal fold: periods and job starts on code-word boundaries
+      const long long unit = (long long)(32 / h->cfg.layout[0].nbit) * (h->big ? 1 : h->plan.P);
+      bool ok = h->cfg.extract_pcal && h->cfg.pcal_rotatorlen % unit == 0;
+      for (const PcalJob &pj : sc.pcal_jobs) ok = ok && (pj.start % unit == 0);
+      e->pcal_word_fold = ok ? 1 : 0;
+   }
    if ((err = upload(e->d_items, sc.items.data(), sizeof(Item) * sc.items.size())) != cudaSuccess ||
        (err = upload(e->d_entries, sc.entries.data(), sizeof(RedEntry) * sc.entries.size())) != cudaSuccess ||
        (err = upload(e->d_outs, sc.outs.data(), sizeof(OutVec) * sc.outs.size())) != cudaSuccess ||
@@ -786,6 +794,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          pa.nout = nout;
          pa.zero_acc = pcal_zero;
          pa.write_out = pcal_write;
+         pa.word_fold = se->pcal_word_fold;
          int rc = launch_pcal(pa, nbit, st);
          if (rc) return fail(h, SWSGPU_ECUDA, std::string("pcal launch: ") + cudaGetErrorString(cudaGetLastError()));
          launches += 2;

@@ -97,6 +97,85 @@ __global__ void k_pcal_tones(PcalArgs a)
    a.tones[2 * t + 1] = si * inv;
 }
 
+// Word-wise fold, for rotator periods and job starts that are multiples of
+// SPW * D: thread t of a job owns code word wi = t mod wpd of phase array
+// ph = t / wpd in every period, i.e. the SPW sample positions
+// i_k = (wi SPW + k) D + ph of the period, and sums them over its block's
+// periods -- one coalesced load and a table decode per sample, FP32 partial
+// sums flushed to FP64 every 64 periods; the FP64 rotator is applied once
+// per position at the end.
+template <int NBIT>
+__global__ void k_pcal_fold_words(PcalArgs a)
+{
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   extern __shared__ double pc_smem[];  // [tonebins][2]
+   __shared__ float lut[4];
+   const PcalJob job = a.jobs[blockIdx.y];
+   for (int i = threadIdx.x; i < 2 * a.tonebins; i += blockDim.x) pc_smem[i] = 0.0;
+   if (threadIdx.x < 4) {
+      const float lv[4] = {a.levels.x, a.levels.y, a.levels.z, a.levels.w};
+      lut[threadIdx.x] = lv[threadIdx.x];
+   }
+   __syncthreads();
+   const int D = a.D, rot = a.rotatorlen;
+   const int wpd = rot / (SPW * D);
+   const int nper = a.N / rot;
+   const int p0 = (int)((long long)nper * blockIdx.x / gridDim.x);
+   const int p1 = (int)((long long)nper * (blockIdx.x + 1) / gridDim.x);
+   const bool chk = a.blank_any[a.code_stream[job.src]] != 0;
+   const uint32_t *blank = a.blank + (long long)a.code_stream[job.src] * a.blank_words;
+   for (int t = threadIdx.x; t < wpd * D; t += blockDim.x) {
+      const int ph = t / wpd, wi = t % wpd;
+      const uint32_t *base = a.codes + (long long)job.src * a.code_words + (long long)ph * a.wpp +
+                             job.start / ((long long)D * SPW) + wi;
+      float s[SPW];
+      double sd[SPW];
+#pragma unroll
+      for (int k = 0; k < SPW; k++) {
+         s[k] = 0.0f;
+         sd[k] = 0.0;
+      }
+      for (int p = p0; p < p1; p++) {
+         const uint32_t w = __ldg(base + (long long)p * wpd);
+#pragma unroll
+         for (int k = 0; k < SPW; k++) {
+            const uint32_t code = (w >> (NBIT * k)) & MASK;
+            float v = (NBIT == 8) ? (float)((int)code * 2 - 255) * (1.0f / 256.0f) : lut[code & 3];
+            if (chk) {
+               const long long smp = job.start + (long long)p * rot + (long long)(wi * SPW + k) * D + ph;
+               if ((__ldg(blank + (smp >> 5)) >> (smp & 31)) & 1u) v = 0.0f;
+            }
+            s[k] += v;
+         }
+         if (((p - p0) & 63) == 63) {
+#pragma unroll
+            for (int k = 0; k < SPW; k++) {
+               sd[k] += (double)s[k];
+               s[k] = 0.0f;
+            }
+         }
+      }
+#pragma unroll
+      for (int k = 0; k < SPW; k++) {
+         const double tot = sd[k] + (double)s[k];
+         const int i = (wi * SPW + k) * D + ph;  // position within the period
+         if (i < a.used) {
+            double sn, cs;
+            sincos(a.dphi * (double)i, &sn, &cs);
+            const int b = i % a.tonebins;
+            atomicAdd(&pc_smem[2 * b], tot * cs);
+            atomicAdd(&pc_smem[2 * b + 1], tot * sn);
+         }
+      }
+   }
+   __syncthreads();
+   double *dst = a.acc + (long long)job.out * 2 * a.tonebins;
+   for (int i = threadIdx.x; i < 2 * a.tonebins; i += blockDim.x) atomicAdd(&dst[i], pc_smem[i]);
+   if (threadIdx.x == 0)
+      atomicAdd(a.acc + (long long)a.nout * 2 * a.tonebins + job.out, (double)(p1 - p0) * (double)a.used);
+}
+
 __global__ void k_pcal_out(PcalArgs a)
 {
    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -107,14 +186,23 @@ int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
 {
    const size_t n = (size_t)a.nout * 2 * a.tonebins;
    if (a.zero_acc) cudaMemsetAsync(a.acc, 0, sizeof(double) * (n + a.nout), st);
-   const int T = 256;
    const int nper = a.N / a.rotatorlen;
    int bpj = nper < 8 ? nper : 8;
    dim3 grid(bpj, a.njobs);
    size_t sm = sizeof(double) * 2 * a.tonebins;
-   if (nbit == 1) k_pcal_fold<1><<<grid, T, sm, st>>>(a);
-   else if (nbit == 2) k_pcal_fold<2><<<grid, T, sm, st>>>(a);
-   else k_pcal_fold<8><<<grid, T, sm, st>>>(a);
+   const int spw = 32 / nbit;
+   if (a.word_fold) {
+      const int nw = a.rotatorlen / spw;  // threads' words per job (all phases)
+      const int T = nw >= 256 ? 256 : ((nw + 31) / 32) * 32;
+      if (nbit == 1) k_pcal_fold_words<1><<<grid, T, sm, st>>>(a);
+      else if (nbit == 2) k_pcal_fold_words<2><<<grid, T, sm, st>>>(a);
+      else k_pcal_fold_words<8><<<grid, T, sm, st>>>(a);
+   } else {
+      const int T = 256;
+      if (nbit == 1) k_pcal_fold<1><<<grid, T, sm, st>>>(a);
+      else if (nbit == 2) k_pcal_fold<2><<<grid, T, sm, st>>>(a);
+      else k_pcal_fold<8><<<grid, T, sm, st>>>(a);
+   }
    if (a.write_out) {
       k_pcal_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
       if (a.tones && a.ntones > 0) {

@@ -36,6 +36,7 @@ struct PcalArgs {
    int nout;
    int zero_acc;       // clear acc first (start of an output group)
    int write_out;      // round acc into out (end of an output group)
+   int word_fold;      // rotatorlen and every job start are multiples of (32/nbit) * D
 };
 
 // Queues zeroing, folding and conversion on `st`; returns 0 or a CUDA error.
