@@ -35,6 +35,14 @@ __host__ __device__ constexpr int big_col_stride(int M)
 }
 __device__ __forceinline__ int bpad(int i) { return i + (i >> 4); }
 
+// Staged code words per column in the column pass: N1 samples from an
+// arbitrary position within their first word.
+template <int N1, int NBIT>
+__host__ __device__ constexpr int big_col_words()
+{
+   return (N1 + 32 / NBIT - 1) / (32 / NBIT) + 1;
+}
+
 // One Stockham pass (radix R, span NS) over C columns of M points held in
 // shared memory, in place through registers.  Butterfly j of column c reads
 // x[j + i M/R], twiddles by W_(NS R)^(k i) (k = j mod NS) from the W_M table
@@ -110,6 +118,32 @@ __global__ void __launch_bounds__(T) k_big_cols(BigArgs a)
       blank_b = a.blank_any[stb] ? a.blank + (long long)stb * a.blank_words : nullptr;
    }
 
+   // Column layout: column n2 of a frame starting at sample s0 is the run
+   // idx0 .. idx0 + N1 - 1 of phase array (s0 + n2) % N2, idx0 = (s0 + n2) / N2.
+   // The runs of the CTA's C columns (both frames of the pair) are staged in
+   // shared memory with coalesced loads, WPC words each from the word holding
+   // idx0; soff = idx0 % SPW.
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   constexpr int WPC = big_col_words<N1, NBIT>();
+   uint32_t *stg = reinterpret_cast<uint32_t *>(tw1 + N1);  // [2][C][WPC]
+   __shared__ int soff[2][C];
+   if (a.col_layout) {
+      const int nside = has_b ? 2 : 1;
+      for (int t = tid; t < nside * C * WPC; t += T) {
+         const int side = t / (C * WPC), c = (t / WPC) % C, w = t % WPC;
+         const long long s = (side ? jb.sb : jb.sa) + c0 + c;
+         const long long wi = (s / N2) / SPW + w;
+         const uint32_t *src = a.codes + (long long)(side ? jb.code_b : jb.code_a) * a.code_words + (s % N2) * a.wpp;
+         stg[t] = wi < a.wpp ? __ldg(src + wi) : 0u;
+      }
+      if (tid < nside * C) {
+         const long long s = ((tid / C) ? jb.sb : jb.sa) + c0 + tid % C;
+         soff[tid / C][tid % C] = (int)((s / N2) % SPW);
+      }
+      __syncthreads();
+   }
+
    // pass 1 (span 1): decode + window + radix R1
    {
       constexpr int NB = N1 / R1, TOT = C * NB, BPT = (TOT + T - 1) / T;
@@ -119,13 +153,31 @@ __global__ void __launch_bounds__(T) k_big_cols(BigArgs a)
          if (TOT % T == 0 || idx < TOT) {
             const int c = idx % C, j = idx / C;
             float2 v[R1];
+            if (a.col_layout) {
+               const int oa = soff[0][c] + j, ob = has_b ? soff[1][c] + j : 0;
 #pragma unroll
-            for (int i = 0; i < R1; i++) {
-               const long long n = (long long)(j + i * NB) * N2 + c0 + c;
-               const float w = __ldg(a.window + n);
-               const float xa = big_sample<NBIT>(a, jb.code_a, jb.sa + n, blank_a);
-               const float xb = has_b ? big_sample<NBIT>(a, jb.code_b, jb.sb + n, blank_b) : 0.0f;
-               v[i] = make_float2(xa * w, xb * w);
+               for (int i = 0; i < R1; i++) {
+                  const long long n = (long long)(j + i * NB) * N2 + c0 + c;
+                  const float w = __ldg(a.window + n);
+                  const int pa = oa + i * NB, pb = ob + i * NB;
+                  float xa = decode_level<NBIT>((stg[c * WPC + pa / SPW] >> (NBIT * (pa % SPW))) & MASK, a.levels);
+                  float xb = 0.0f;
+                  if (has_b)
+                     xb = decode_level<NBIT>((stg[(C + c) * WPC + pb / SPW] >> (NBIT * (pb % SPW))) & MASK,
+                                             a.levels);
+                  if (blank_a && ((__ldg(blank_a + ((jb.sa + n) >> 5)) >> ((jb.sa + n) & 31)) & 1u)) xa = 0.0f;
+                  if (blank_b && ((__ldg(blank_b + ((jb.sb + n) >> 5)) >> ((jb.sb + n) & 31)) & 1u)) xb = 0.0f;
+                  v[i] = make_float2(xa * w, xb * w);
+               }
+            } else {
+#pragma unroll
+               for (int i = 0; i < R1; i++) {
+                  const long long n = (long long)(j + i * NB) * N2 + c0 + c;
+                  const float w = __ldg(a.window + n);
+                  const float xa = big_sample<NBIT>(a, jb.code_a, jb.sa + n, blank_a);
+                  const float xb = has_b ? big_sample<NBIT>(a, jb.code_b, jb.sb + n, blank_b) : 0.0f;
+                  v[i] = make_float2(xa * w, xb * w);
+               }
             }
             DFT<R1>::run(v);
 #pragma unroll
@@ -223,7 +275,8 @@ __global__ void __launch_bounds__(T) k_big_rows(BigArgs a)
 template <int N1, int N2, int C, int T, int R1, int R2, int R3>
 constexpr size_t big_cols_smem()
 {
-   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1);
+   // columns, the W_N1 table and the staged code words (sized for 8-bit codes)
+   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1) + sizeof(uint32_t) * 2 * C * big_col_words<N1, 8>();
 }
 template <int N2>
 constexpr size_t big_rows_smem()

@@ -21,8 +21,14 @@ struct BigItem {
 };
 
 struct BigArgs {
-   const uint32_t *codes;      // D = 1 layout: codes[code * code_words + s / SPW]
+   // col_layout 0: codes[code * code_words + s / SPW] (no decimation);
+   // col_layout 1: decimated by N2, codes[code * code_words + (s % N2) * wpp +
+   // (s / N2) / SPW], so that every column of the column pass is one
+   // contiguous run of one phase array
+   const uint32_t *codes;
    long long code_words;
+   long long wpp;
+   int col_layout;
    const uint32_t *blank;      // per stream blank bitmap (1 bit per sample-time)
    long long blank_words;
    const int *blank_any;

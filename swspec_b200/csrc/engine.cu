@@ -28,7 +28,8 @@ namespace sws {
 __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any);
 cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, const int *chans, int nch,
                                 uint32_t *codes, int D, long long wpp, const int2 *valid,
-                                const int *blank_any, uint32_t *blank);
+                                const int *blank_any, uint32_t *blank, int &launches);
+bool unpack_decimation_ok(int D, int nchan, int nbit);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
 __global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
@@ -166,6 +167,7 @@ struct swsgpu_handle {
    // per-call buffers
    DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
    DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
+   DevBuf d_codes1;   // undecimated copy for phase-cal when the four-step path uses the column layout
    DevBuf d_pcal_jobs, d_pcal_part, d_pcal_entries, d_pcal_outs;
    DevBuf d_out_auto, d_out_xpol, d_out_pcal, d_out_tones;
    HostBuf h_out;   // pinned staging of one run's outputs
@@ -481,7 +483,8 @@ static void big_batches(const swsgpu_handle *h, const Schedule &sc, std::vector<
    }
 }
 
-static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_words, long long blank_words,
+static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_words, long long wpp, bool col,
+                      long long blank_words,
                       cudaStream_t st, int &launches)
 {
    const swsgpu_config &c = h->cfg;
@@ -495,6 +498,8 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    BigArgs a;
    a.codes = (const uint32_t *)h->d_codes.p;
    a.code_words = code_words;
+   a.wpp = wpp;
+   a.col_layout = col ? 1 : 0;
    a.blank = (const uint32_t *)h->d_blank.p;
    a.blank_words = blank_words;
    a.blank_any = (const int *)h->d_blank_any.p;
@@ -649,13 +654,25 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    const int nbit = c.layout[0].nbit;
    const int spw = 32 / nbit;
    const long long nsamp = sc.nsamp;
-   const int D = h->big ? 1 : h->plan.P;         // phase decimation of the code arrays
+   // phase decimation of the code arrays: the cluster size, or N2 on the
+   // four-step path (the column layout) when every stream's corner turn
+   // supports it
+   bool col = h->big;
+   for (int s = 0; s < c.num_streams && col; s++)
+      if (!h->chans_of[s].empty())
+         col = unpack_decimation_ok(h->bplan.N2, c.layout[s].nchan, c.layout[s].nbit);
+   const int D = h->big ? (col ? h->bplan.N2 : 1) : h->plan.P;
    const long long per_phase = (nsamp + D - 1) / D;
    const long long wpp = (per_phase + spw - 1) / spw + 2;  // +2: prefetch may touch one word past
    const long long code_words = (long long)D * wpp;
    const long long blank_words = (nsamp + 31) / 32;
+   // phase-cal folds read undecimated codes (word-wise when the rotator
+   // period allows); with the column layout they get their own copy
+   const bool pcal_copy = col && c.extract_pcal && d_pcal && !sc.pcal_jobs.empty();
+   const long long wpp1 = (nsamp + spw - 1) / spw + 2;
 
    CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 64));
+   if (pcal_copy) CK(h, h->d_codes1.ensure(sizeof(uint32_t) * (size_t)wpp1 * ncode + 64));
    CK(h, h->d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
    CK(h, h->d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
    // the blank bitmap is written by K1 and read by K2/PCal only for streams
@@ -686,8 +703,12 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)h->first_code[s] * code_words;
       uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
       CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(), codes, D, wpp,
-                                (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank));
-      launches++;
+                                (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank, launches));
+      if (pcal_copy)
+         CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(),
+                                   (uint32_t *)h->d_codes1.p + (size_t)h->first_code[s] * wpp1, 1, wpp1,
+                                   (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank,
+                                   launches));
    }
    CK(h, cudaGetLastError());
 
@@ -696,7 +717,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    if (nitems > 0) {
       CK(h, h->d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
       if (h->big) {
-         int rc = launch_big(h, *se, code_words, blank_words, st, launches);
+         int rc = launch_big(h, *se, code_words, wpp, col, blank_words, st, launches);
          if (rc != SWSGPU_OK) return rc;
       } else {
          SpecArgs a;
@@ -771,10 +792,10 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          CK(h, h->d_pcal_part.ensure(sizeof(double) * (2 * c.pcal_tonebins + 1) * (size_t)nout));
          int njobs = (int)sc.pcal_jobs.size();
          PcalArgs pa;
-         pa.codes = (const uint32_t *)h->d_codes.p;
-         pa.code_words = code_words;
-         pa.wpp = wpp;
-         pa.D = D;
+         pa.codes = (const uint32_t *)(pcal_copy ? h->d_codes1.p : h->d_codes.p);
+         pa.code_words = pcal_copy ? wpp1 : code_words;
+         pa.wpp = pcal_copy ? wpp1 : wpp;
+         pa.D = pcal_copy ? 1 : D;
          pa.blank = (const uint32_t *)h->d_blank.p;
          pa.blank_words = blank_words;
          pa.blank_any = (const int *)h->d_blank_any.p;
@@ -1152,7 +1173,7 @@ void swsgpu_destroy(swsgpu_handle *h)
    if (!h) return;
    cudaSetDevice(h->device);
    if (h->stream) cudaStreamSynchronize(h->stream);
-   DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes,
+   DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes, &h->d_codes1,
                      &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
                      &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
                      &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal, &h->d_out_tones,

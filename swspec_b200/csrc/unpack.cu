@@ -162,6 +162,13 @@ struct UnpackGeom {
    int D, G, SW, nw;   // decimation, code words per CTA, payload words per block, per chunk
    int vec16;          // 16-byte payload loads allowed
    long long wpp, words_total, blank_words;
+   // Phase blocks (decimations whose D * nchan payload words per code word
+   // exceed shared memory): CTA (x, y) owns phases [y Dt, (y + 1) Dt) and
+   // reads, per code word, SPW pieces of PW = Dt nchan nbit / 32 payload
+   // words RS = D nchan nbit / 32 words apart; SW = Dt nchan.  Without
+   // phase blocks Dt = D and the pieces are contiguous.
+   int pblock, Dt, PW;
+   long long RS;
 };
 
 template <int NBIT>
@@ -172,7 +179,8 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
    extern __shared__ uint32_t sm[];
-   const int SW = g.SW, SWp = g.SW + 1, nw = g.nw, D = g.D;
+   const int SW = g.SW, SWp = g.SW + 1, nw = g.nw, D = g.D, Dt = g.Dt;
+   const int ph0 = blockIdx.y * Dt;
    uint32_t *vbits = sm + (size_t)g.G * SWp;          // invalid-word flags, nw / 32 words
    int *pos = reinterpret_cast<int *>(vbits + nw / 32);  // channel -> output slot (transpose path)
    int *sch = pos + SPW;                                 // requested channels
@@ -193,7 +201,61 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
 
    // 1. payload words -> shared memory
    const int pb = s.payload_bytes;
-   if (g.vec16) {
+   if (g.pblock) {
+      // piece q / nq (code word iw = piece / SPW, sample offset k = piece % SPW)
+      // covers sample-times ((x G + iw) SPW + k) D + y Dt + [0, Dt)
+      constexpr int UNR = 4;
+      const int wpl = g.vec16 ? 4 : 1;
+      const int nq = g.PW / wpl, nload = g.G * SPW * nq;
+      const long long row0 = (long long)blockIdx.x * g.G * SPW, col0 = (long long)blockIdx.y * g.PW;
+      for (int qb = threadIdx.x; qb < nload; qb += UNR * blockDim.x) {
+         uint32_t val[UNR][4];
+         long long fu[UNR];
+         int ou[UNR];
+#pragma unroll
+         for (int u = 0; u < UNR; u++) {
+            const int q = qb + u * blockDim.x;
+            const int piece = q / nq;
+            const long long gw = (row0 + piece) * g.RS + col0 + (long long)(q - piece * nq) * wpl;
+            const long long v = s.grid_offset + 4 * gw;
+            fu[u] = v / pb;
+            ou[u] = (int)(v - fu[u] * pb);
+#pragma unroll
+            for (int i = 0; i < 4; i++) val[u][i] = 0u;
+            if (q < nload && gw < g.words_total) {
+               const long long a = s.header_bytes ? fu[u] * s.frame_bytes + s.header_bytes + ou[u] : 4 * gw;
+               if (wpl == 4 && a + 16 <= s.nbytes) {
+                  const uint4 t = __ldg(reinterpret_cast<const uint4 *>(s.data + a));
+                  val[u][0] = t.x;
+                  val[u][1] = t.y;
+                  val[u][2] = t.z;
+                  val[u][3] = t.w;
+               } else {
+                  for (int i = 0; i < wpl; i++)
+                     if (a + 4 * i + 4 <= s.nbytes) val[u][i] = __ldg(reinterpret_cast<const uint32_t *>(s.data + a + 4 * i));
+               }
+            }
+         }
+#pragma unroll
+         for (int u = 0; u < UNR; u++) {
+            const int q = qb + u * blockDim.x;
+            if (q >= nload) break;
+            const int piece = q / nq;
+            const long long gw = (row0 + piece) * g.RS + col0 + (long long)(q - piece * nq) * wpl;
+            const int jl = piece * g.PW + (q - piece * nq) * wpl;
+            for (int i = 0; i < wpl; i++) {
+               uint32_t x = val[u][i];
+               if (gw + i >= g.words_total) x = 0u;
+               else if (any) {
+                  const int2 vr = valid[fu[u]];
+                  const int oi = ou[u] + 4 * i;
+                  if (!(oi >= vr.x && oi < vr.y)) x = 0u;
+               }
+               sm[jl + i + (jl + i) / SW] = x;
+            }
+         }
+      }
+   } else if (g.vec16) {
       // UNR 16-byte loads in flight per thread before any shared store
       constexpr int UNR = 4;
       const int step = 16 * blockDim.x;
@@ -284,22 +346,22 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
    // 2. code words, one warp task = 32 consecutive words of one phase
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
    const long long code_words = (long long)D * g.wpp;
-   const int ntask = D * (g.G / 32);
+   const int ntask = Dt * (g.G / 32);
    for (int t = warp; t < ntask; t += nwarp) {
-      const int ph = t % D;
-      const int iw = (t / D) * 32 + lane;
+      const int ph = t % Dt;
+      const int iw = (t / Dt) * 32 + lane;
       const long long iwg = (long long)blockIdx.x * g.G + iw;
       const uint32_t *blk = sm + (size_t)iw * SWp;
       if (tpath) {
          uint32_t x[SPW];
 #pragma unroll
-         for (int k = 0; k < SPW; k++) x[k] = blk[k * D + ph];
+         for (int k = 0; k < SPW; k++) x[k] = blk[k * Dt + ph];
          transpose_codes<NBIT>(x);
          if (iwg < g.wpp) {
 #pragma unroll
             for (int c = 0; c < SPW; c++) {
                const int p = pos[c];
-               if (p >= 0) codes[(long long)p * code_words + (long long)ph * g.wpp + iwg] = x[c];
+               if (p >= 0) codes[(long long)p * code_words + (long long)(ph0 + ph) * g.wpp + iwg] = x[c];
             }
          }
       } else {
@@ -312,7 +374,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             int cached_idx = -1;
             uint32_t cached = 0u;
             for (int k = 0; k < SPW; k++) {
-               const int bit0 = (k * D + ph) * stride;
+               const int bit0 = (k * Dt + ph) * stride;
 #pragma unroll
                for (int c = 0; c < 16; c++) {
                   if (c < cn) {
@@ -329,14 +391,15 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             if (iwg < g.wpp) {
 #pragma unroll
                for (int c = 0; c < 16; c++)
-                  if (c < cn) codes[(long long)(c0 + c) * code_words + (long long)ph * g.wpp + iwg] = acc[c];
+                  if (c < cn) codes[(long long)(c0 + c) * code_words + (long long)(ph0 + ph) * g.wpp + iwg] = acc[c];
             }
          }
       }
    }
 
-   // 3. blank bitmap words of the chunk's sample-times
-   if (any) {
+   // 3. blank bitmap words of the chunk's sample-times (k_blank_bits with
+   // phase blocks, whose sample-times are not contiguous)
+   if (any && !g.pblock) {
       const int stride = s.nchan * NBIT;
       const int nbw = g.G * SPW * D / 32;
       const long long b0 = (long long)blockIdx.x * nbw;
@@ -351,6 +414,31 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
          blank[b0 + j] = m;
       }
    }
+}
+
+// Blank bitmap for phase-blocked corner turns, with the rule of step 3
+// above: sample-time t is blanked when the payload word holding its first
+// bit lies outside its frame's valid byte range.
+__global__ void k_blank_bits(StreamIn s, long long nsamp, long long words_total, long long blank_words,
+                             const int2 *valid, const int *blank_any, uint32_t *blank)
+{
+   if (*blank_any == 0) return;
+   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (j >= blank_words) return;
+   const int stride = s.nchan * s.nbit;
+   uint32_t m = 0u;
+   for (int i = 0; i < 32; i++) {
+      const long long t = 32 * j + i;
+      if (t >= nsamp) break;
+      const long long w = (t * stride) >> 5;
+      if (w >= words_total) continue;
+      const long long v = s.grid_offset + 4 * w;
+      const long long f = v / s.payload_bytes;
+      const int o = (int)(v - f * s.payload_bytes);
+      const int2 vr = valid[f];
+      if (!(o >= vr.x && o < vr.y)) m |= 1u << i;
+   }
+   blank[j] = m;
 }
 
 // Decoded float samples of one channel (test path; same rules as above).
@@ -378,19 +466,48 @@ __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 lev
    out[t] = val;
 }
 
+// Largest phase block Dt | D whose pieces are whole 16-byte loads (else
+// whole words) with at most kMaxBlockWords payload words per code word;
+// 0 when there is none.
+static constexpr int kMaxBlockWords = 512;
+static int phase_block(int D, int nchan, int nbit, bool *whole16)
+{
+   for (int unit : {128, 32}) {
+      int best = 0;
+      for (int dt = 1; dt <= D && dt * nchan <= kMaxBlockWords; dt++)
+         if (D % dt == 0 && ((long long)dt * nchan * nbit) % unit == 0) best = dt;
+      if (best) {
+         if (whole16) *whole16 = unit == 128;
+         return best;
+      }
+   }
+   return 0;
+}
+
+bool unpack_decimation_ok(int D, int nchan, int nbit)
+{
+   return D * nchan <= kMaxBlockWords || phase_block(D, nchan, nbit, nullptr) > 0;
+}
+
 UnpackGeom unpack_geometry(const StreamIn &s, long long nsamp, int D, long long wpp)
 {
    UnpackGeom g;
    g.D = D;
-   g.SW = D * s.nchan;
-   g.G = 32 * std::max(1, (8192 / g.SW) / 32);
-   g.nw = g.G * g.SW;
    g.wpp = wpp;
    g.words_total = (nsamp * s.nchan * s.nbit + 31) / 32;
    g.blank_words = (nsamp + 31) / 32;
    const bool frames16 = (s.payload_bytes % 16 == 0) &&
                          (s.header_bytes == 0 || (s.header_bytes % 16 == 0 && s.frame_bytes % 16 == 0));
    g.vec16 = frames16 && (s.grid_offset % 16 == 0) && ((uintptr_t)s.data % 16 == 0);
+   bool whole16 = false;
+   g.pblock = D * s.nchan > kMaxBlockWords;
+   g.Dt = g.pblock ? phase_block(D, s.nchan, s.nbit, &whole16) : D;
+   g.SW = g.Dt * s.nchan;
+   g.G = g.pblock ? 32 : 32 * std::max(1, (8192 / std::max(g.SW, 1)) / 32);
+   g.nw = g.G * g.SW;
+   g.PW = (int)(((long long)g.Dt * s.nchan * s.nbit) / 32);
+   g.RS = ((long long)D * s.nchan * s.nbit) / 32;
+   if (g.pblock) g.vec16 = g.vec16 && whole16 && g.RS % 4 == 0;
    return g;
 }
 
@@ -410,19 +527,30 @@ static cudaError_t launch_codes_t(const UnpackGeom &g, cudaStream_t st, StreamIn
       if (e != cudaSuccess) return e;
    }
    const unsigned nblk = (unsigned)((g.wpp + g.G - 1) / g.G);
-   k_unpack_codes<NBIT><<<nblk, 256, smem, st>>>(s, nsamp, chans, nch, codes, g, valid, blank_any, blank);
+   k_unpack_codes<NBIT><<<dim3(nblk, (unsigned)(g.D / g.Dt)), 256, smem, st>>>(s, nsamp, chans, nch, codes, g, valid,
+                                                                                blank_any, blank);
    return cudaGetLastError();
 }
 
 cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, const int *chans, int nch,
                                 uint32_t *codes, int D, long long wpp, const int2 *valid,
-                                const int *blank_any, uint32_t *blank)
+                                const int *blank_any, uint32_t *blank, int &launches)
 {
    const UnpackGeom g = unpack_geometry(s, nsamp, D, wpp);
-   if (unpack_smem_bytes(g, nch) > 227 * 1024) return cudaErrorInvalidValue;
-   if (s.nbit == 1) return launch_codes_t<1>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
-   if (s.nbit == 2) return launch_codes_t<2>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
-   return launch_codes_t<8>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   if (g.Dt <= 0 || unpack_smem_bytes(g, nch) > 227 * 1024) return cudaErrorInvalidValue;
+   cudaError_t e;
+   if (s.nbit == 1) e = launch_codes_t<1>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   else if (s.nbit == 2) e = launch_codes_t<2>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   else e = launch_codes_t<8>(g, st, s, nsamp, chans, nch, codes, valid, blank_any, blank);
+   if (e != cudaSuccess) return e;
+   launches++;
+   if (g.pblock) {
+      k_blank_bits<<<(unsigned)((g.blank_words + 255) / 256), 256, 0, st>>>(s, nsamp, g.words_total, g.blank_words,
+                                                                            valid, blank_any, blank);
+      launches++;
+      e = cudaGetLastError();
+   }
+   return e;
 }
 
 }  // namespace sws
