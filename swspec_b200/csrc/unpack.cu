@@ -207,6 +207,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
       constexpr int UNR = 4;
       const int wpl = g.vec16 ? 4 : 1;
       const int nq = g.PW / wpl, nload = g.G * SPW * nq;
+      const bool need_f = s.header_bytes != 0 || any;  // frame position for headers / validity
       const long long row0 = (long long)blockIdx.x * g.G * SPW, col0 = (long long)blockIdx.y * g.PW;
       for (int qb = threadIdx.x; qb < nload; qb += UNR * blockDim.x) {
          uint32_t val[UNR][4];
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             const int piece = q / nq;
             const long long gw = (row0 + piece) * g.RS + col0 + (long long)(q - piece * nq) * wpl;
             const long long v = s.grid_offset + 4 * gw;
-            fu[u] = v / pb;
+            fu[u] = need_f ? v / pb : 0;
             ou[u] = (int)(v - fu[u] * pb);
 #pragma unroll
             for (int i = 0; i < 4; i++) val[u][i] = 0u;
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
                   const int oi = ou[u] + 4 * i;
                   if (!(oi >= vr.x && oi < vr.y)) x = 0u;
                }
-               sm[jl + i + (jl + i) / SW] = x;
+               sm[jl + i + piece / SPW] = x;  // one pad word per code word's block
             }
          }
       }
@@ -298,6 +299,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             if (j >= nw) break;
             const long long w = w0 + j;
             uint32_t val[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+            const int pj = j / SW, rj = j - pj * SW;  // block and offset of word j
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                if (w + i >= g.words_total) val[i] = 0u;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
                      atomicOr(&vbits[(j + i) >> 5], 1u << ((j + i) & 31));
                   }
                }
-               sm[j + i + (j + i) / SW] = val[i];
+               sm[j + i + pj + (SW >= 4 ? (int)(rj + i >= SW) : (rj + i) / SW)] = val[i];
             }
          }
       }
@@ -346,6 +348,33 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
    // 2. code words, one warp task = 32 consecutive words of one phase
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
    const long long code_words = (long long)D * g.wpp;
+   if (s.nchan == 1 && Dt % SPW == 0) {
+      // One channel: payload word wc of sample index iw SPW + k (row k of
+      // the block) holds phases wc SPW + m at bits NBIT m, so the SPW x SPW
+      // transpose gives SPW phases' code words at once.
+      const int PWs = Dt / SPW;
+      const int nt1 = PWs * (g.G / 32);
+      for (int t = warp; t < nt1; t += nwarp) {
+         const int wc = t % PWs;
+         const int iw = (t / PWs) * 32 + lane;
+         const long long iwg = (long long)blockIdx.x * g.G + iw;
+         const uint32_t *blk = sm + (size_t)iw * SWp;
+         uint32_t x[SPW];
+#pragma unroll
+         for (int k = 0; k < SPW; k++) x[k] = blk[k * PWs + wc];
+         transpose_codes<NBIT>(x);
+         if (iwg < g.wpp) {
+#pragma unroll
+            for (int m = 0; m < SPW; m++) codes[(long long)(ph0 + wc * SPW + m) * g.wpp + iwg] = x[m];
+         }
+      }
+   } else if (s.nchan == 1 && Dt == 1) {
+      // one channel, no decimation: the code words are the payload words
+      for (int iw = threadIdx.x; iw < g.G; iw += blockDim.x) {
+         const long long iwg = (long long)blockIdx.x * g.G + iw;
+         if (iwg < g.wpp) codes[iwg] = sm[(size_t)iw * SWp];
+      }
+   } else {
    const int ntask = Dt * (g.G / 32);
    for (int t = warp; t < ntask; t += nwarp) {
       const int ph = t % Dt;
@@ -395,6 +424,8 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             }
          }
       }
+   }
+
    }
 
    // 3. blank bitmap words of the chunk's sample-times (k_blank_bits with
