@@ -200,25 +200,48 @@ __global__ void __launch_bounds__(T) k_big_cols(BigArgs a)
    }
 }
 
-// Row pass: grid (N1 / 2 + 1 row pairs, items of the batch).
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Row pass: a persistent grid over the units u = item * NP + rp of the
+// batch (row pair rp = (k1, N1 - k1), NP = N1 / 2 + 1).  A CTA walks its
+// units' jobs in order; while it transforms one job's row pair, the next
+// one streams into the other shared-memory slot (cp.async), and the W_N2
+// table is loaded once per CTA.
 template <int N1, int N2, int T, int R1, int R2, int R3>
-__global__ void __launch_bounds__(T) k_big_rows(BigArgs a)
+__global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
 {
    static_assert(R1 * R2 * R3 == N2, "radices must multiply to N2");
    static_assert(N1 % 2 == 0, "row pairs need an even N1");
    constexpr int CS = big_col_stride(N2);
    constexpr int KPT = (N2 + T - 1) / T;
+   constexpr int NP = N1 / 2 + 1;
    extern __shared__ float2 smf[];
-   float2 *buf = smf;
-   float2 *tw2 = smf + 2 * CS;
+   float2 *tw2 = smf + 4 * CS;  // two slots of two rows, then the table
    const int tid = threadIdx.x;
+   const int nunits = NP * a.nbitems;
+   int u = blockIdx.x;
+   if (u >= nunits) return;
    for (int i = tid; i < N2; i += T) tw2[i] = a.tw2[i];
-
-   const int rp = blockIdx.x;
-   const int k1a = rp, k1b = (N1 - rp) % N1;
-   const bool two = k1a != k1b;
-   const BigItem bi = a.bitems[blockIdx.y];
    const long long N = (long long)N1 * N2;
+
+   auto stage = [&](int uu, int jj, int sl) {
+      const BigItem si = a.bitems[uu / NP];
+      const int rp = uu % NP;
+      const int k1b = (N1 - rp) % N1;
+      const float2 *ra = a.scratch + ((long long)(si.job0 + jj) * N1 + rp) * N2;
+      const float2 *rb = a.scratch + ((long long)(si.job0 + jj) * N1 + k1b) * N2;
+      float2 *dst = smf + sl * 2 * CS;
+      for (int i = tid; i < N2; i += T) {
+         cp_async8(dst + bpad(i), ra + i);
+         if (k1b != rp) cp_async8(dst + CS + bpad(i), rb + i);
+      }
+   };
 
    float acc[KPT][4];
 #pragma unroll
@@ -226,14 +249,25 @@ __global__ void __launch_bounds__(T) k_big_rows(BigArgs a)
 #pragma unroll
       for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
 
-   for (int j = 0; j < bi.nfr; j++) {
-      const float2 *ra = a.scratch + ((long long)(bi.job0 + j) * N1 + k1a) * N2;
-      const float2 *rb = a.scratch + ((long long)(bi.job0 + j) * N1 + k1b) * N2;
-      for (int i = tid; i < N2; i += T) {
-         buf[bpad(i)] = __ldcs(ra + i);
-         buf[CS + bpad(i)] = two ? __ldcs(rb + i) : make_float2(0.0f, 0.0f);
+   int j = 0, slot = 0;
+   BigItem bi = a.bitems[u / NP];
+   stage(u, 0, 0);
+   cp_async_commit();
+   while (true) {
+      int un = u, jn = j + 1;
+      if (jn >= bi.nfr) {
+         un = u + gridDim.x;
+         jn = 0;
       }
+      const bool more = un < nunits;
+      if (more) stage(un, jn, slot ^ 1);
+      cp_async_commit();
+      cp_async_wait1();
       __syncthreads();
+
+      float2 *buf = smf + slot * 2 * CS;
+      const int rp = u % NP;
+      const bool two = rp != (N1 - rp) % N1;
       big_pass<N2, 2, T, R1, 1>(buf, tw2);
       big_pass<N2, 2, T, R2, R1>(buf, tw2);
       if constexpr (R3 > 1) big_pass<N2, 2, T, R3, R1 * R2>(buf, tw2);
@@ -249,26 +283,34 @@ __global__ void __launch_bounds__(T) k_big_rows(BigArgs a)
             acc_bin(acc[q], bi.mode, zk, zm);
          }
       }
-      __syncthreads();
-   }
 
-   // bin k = k1 + N1 k2 of row k1, or its mirror N - k (conjugate cross
-   // product) when k lies above N/2; self-paired rows keep k <= N/2 only
-   float *part = a.partial + (long long)bi.item * 4 * a.S;
-   const int nprod = (bi.mode == MODE_XPOL) ? 4 : 1;
+      if (j == bi.nfr - 1) {
+         // bin k = k1 + N1 k2 of row k1, or its mirror N - k (conjugate cross
+         // product) when k lies above N/2; self-paired rows keep k <= N/2 only
+         float *part = a.partial + (long long)bi.item * 4 * a.S;
+         const int nprod = (bi.mode == MODE_XPOL) ? 4 : 1;
 #pragma unroll
-   for (int q = 0; q < KPT; q++) {
-      const int k2 = tid + q * T;
-      if (!(N2 % T == 0 || k2 < N2)) continue;
-      const long long k = rp + (long long)N1 * k2;
-      long long bin = k;
-      bool conj = false;
-      if (k > N / 2) {
-         if (!two) continue;
-         bin = N - k;
-         conj = true;
+         for (int q = 0; q < KPT; q++) {
+            const int k2 = tid + q * T;
+            if (N2 % T == 0 || k2 < N2) {
+               const long long k = rp + (long long)N1 * k2;
+               if (k <= N / 2 || two) {
+                  const bool conj = k > N / 2;
+                  const long long bin = conj ? N - k : k;
+                  for (int c = 0; c < nprod; c++)
+                     part[(long long)c * a.S + bin] = (c == 3 && conj) ? -acc[q][c] : acc[q][c];
+               }
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
+         }
       }
-      for (int c = 0; c < nprod; c++) part[(long long)c * a.S + bin] = (c == 3 && conj) ? -acc[q][c] : acc[q][c];
+      __syncthreads();  // this slot is restaged two iterations on
+      if (!more) break;
+      if (un != u) bi = a.bitems[un / NP];
+      u = un;
+      j = jn;
+      slot ^= 1;
    }
 }
 
@@ -281,7 +323,8 @@ constexpr size_t big_cols_smem()
 template <int N2>
 constexpr size_t big_rows_smem()
 {
-   return sizeof(float2) * ((size_t)2 * big_col_stride(N2) + N2);
+   // two slots of a row pair, then the W_N2 table
+   return sizeof(float2) * ((size_t)4 * big_col_stride(N2) + N2);
 }
 
 #define SWS_BIG_C(N1_, C_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)                                 \

@@ -42,6 +42,7 @@ struct BigArgs {
    const float2 *twB;          // W_N^l, l < 2048
    float2 *scratch;            // [job][N1][N2] column FFTs, twiddled
    float *partial;
+   int nbitems;                // items of this batch (row pass)
    int N, S;
    float4 levels;
 };

@@ -131,6 +131,8 @@ struct swsgpu_handle {
    std::vector<int2> tw_off;  // per candidate: offsets of its W_N1 and W_N2 tables in d_tw1
    int S = 0;
    int max_clusters = 1;
+   const void *rows_fn = nullptr;   // row-pass kernel the persistent grid was sized for
+   int rows_grid = 0;
    std::string err;
    cudaStream_t stream = nullptr;     // kernels and result copies
    cudaStream_t cstream = nullptr;    // input copies of submit()
@@ -514,6 +516,14 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.N = c.fft_points;
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
+   if (h->rows_fn != (const void *)bp.rows) {
+      // persistent row pass: as many CTAs as fit on the device at once
+      int occ = 0, nsm = 0;
+      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bp.rows, bp.TB, bp.smem_rows));
+      CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+      h->rows_grid = std::max(1, occ) * nsm;
+      h->rows_fn = (const void *)bp.rows;
+   }
    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
    if (h->profiling) {
       CK(h, cudaEventCreate(&ev0));
@@ -524,7 +534,9 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
       a.jobs = (const BigJob *)se.d_bjobs.p + b.x;
       a.bitems = (const BigItem *)se.d_bitems.p + b.z;
       bp.cols[nbi]<<<dim3(bp.N2 / bp.C, (unsigned)b.y), bp.TA, bp.smem_cols, st>>>(a);
-      bp.rows<<<dim3(bp.N1 / 2 + 1, (unsigned)b.w), bp.TB, bp.smem_rows, st>>>(a);
+      a.nbitems = b.w;
+      const int units = (bp.N1 / 2 + 1) * b.w;
+      bp.rows<<<(unsigned)std::min(units, h->rows_grid), bp.TB, bp.smem_rows, st>>>(a);
       CK(h, cudaGetLastError());
       launches += 2;
    }
