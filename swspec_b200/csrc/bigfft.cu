@@ -94,112 +94,11 @@ __device__ __forceinline__ float big_sample(const BigArgs &a, int code, long lon
    return x;
 }
 
-// Column pass: grid (N2 / C, jobs of the batch).
-template <int N1, int N2, int C, int T, int R1, int R2, int R3, int NBIT>
-__global__ void __launch_bounds__(T) k_big_cols(BigArgs a)
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
 {
-   static_assert(R1 * R2 * R3 == N1, "radices must multiply to N1");
-   static_assert(N2 % C == 0, "columns per CTA must divide N2");
-   constexpr int CS = big_col_stride(N1);
-   extern __shared__ float2 smf[];
-   float2 *buf = smf;
-   float2 *tw1 = smf + C * CS;
-   const int tid = threadIdx.x;
-   for (int i = tid; i < N1; i += T) tw1[i] = a.tw1[i];
-
-   const int c0 = blockIdx.x * C;
-   const BigJob jb = a.jobs[blockIdx.y];
-   const bool has_b = jb.mode != MODE_SINGLE;
-   const int sta = a.code_stream[jb.code_a];
-   const uint32_t *blank_a = a.blank_any[sta] ? a.blank + (long long)sta * a.blank_words : nullptr;
-   const uint32_t *blank_b = nullptr;
-   if (has_b) {
-      const int stb = a.code_stream[jb.code_b];
-      blank_b = a.blank_any[stb] ? a.blank + (long long)stb * a.blank_words : nullptr;
-   }
-
-   // Column layout: column n2 of a frame starting at sample s0 is the run
-   // idx0 .. idx0 + N1 - 1 of phase array (s0 + n2) % N2, idx0 = (s0 + n2) / N2.
-   // The runs of the CTA's C columns (both frames of the pair) are staged in
-   // shared memory with coalesced loads, WPC words each from the word holding
-   // idx0; soff = idx0 % SPW.
-   constexpr int SPW = 32 / NBIT;
-   constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   constexpr int WPC = big_col_words<N1, NBIT>();
-   uint32_t *stg = reinterpret_cast<uint32_t *>(tw1 + N1);  // [2][C][WPC]
-   __shared__ int soff[2][C];
-   if (a.col_layout) {
-      const int nside = has_b ? 2 : 1;
-      for (int t = tid; t < nside * C * WPC; t += T) {
-         const int side = t / (C * WPC), c = (t / WPC) % C, w = t % WPC;
-         const long long s = (side ? jb.sb : jb.sa) + c0 + c;
-         const long long wi = (s / N2) / SPW + w;
-         const uint32_t *src = a.codes + (long long)(side ? jb.code_b : jb.code_a) * a.code_words + (s % N2) * a.wpp;
-         stg[t] = wi < a.wpp ? __ldg(src + wi) : 0u;
-      }
-      if (tid < nside * C) {
-         const long long s = ((tid / C) ? jb.sb : jb.sa) + c0 + tid % C;
-         soff[tid / C][tid % C] = (int)((s / N2) % SPW);
-      }
-      __syncthreads();
-   }
-
-   // pass 1 (span 1): decode + window + radix R1
-   {
-      constexpr int NB = N1 / R1, TOT = C * NB, BPT = (TOT + T - 1) / T;
-#pragma unroll
-      for (int b = 0; b < BPT; b++) {
-         const int idx = tid + b * T;
-         if (TOT % T == 0 || idx < TOT) {
-            const int c = idx % C, j = idx / C;
-            float2 v[R1];
-            if (a.col_layout) {
-               const int oa = soff[0][c] + j, ob = has_b ? soff[1][c] + j : 0;
-#pragma unroll
-               for (int i = 0; i < R1; i++) {
-                  const long long n = (long long)(j + i * NB) * N2 + c0 + c;
-                  const float w = __ldg(a.window + n);
-                  const int pa = oa + i * NB, pb = ob + i * NB;
-                  float xa = decode_level<NBIT>((stg[c * WPC + pa / SPW] >> (NBIT * (pa % SPW))) & MASK, a.levels);
-                  float xb = 0.0f;
-                  if (has_b)
-                     xb = decode_level<NBIT>((stg[(C + c) * WPC + pb / SPW] >> (NBIT * (pb % SPW))) & MASK,
-                                             a.levels);
-                  if (blank_a && ((__ldg(blank_a + ((jb.sa + n) >> 5)) >> ((jb.sa + n) & 31)) & 1u)) xa = 0.0f;
-                  if (blank_b && ((__ldg(blank_b + ((jb.sb + n) >> 5)) >> ((jb.sb + n) & 31)) & 1u)) xb = 0.0f;
-                  v[i] = make_float2(xa * w, xb * w);
-               }
-            } else {
-#pragma unroll
-               for (int i = 0; i < R1; i++) {
-                  const long long n = (long long)(j + i * NB) * N2 + c0 + c;
-                  const float w = __ldg(a.window + n);
-                  const float xa = big_sample<NBIT>(a, jb.code_a, jb.sa + n, blank_a);
-                  const float xb = has_b ? big_sample<NBIT>(a, jb.code_b, jb.sb + n, blank_b) : 0.0f;
-                  v[i] = make_float2(xa * w, xb * w);
-               }
-            }
-            DFT<R1>::run(v);
-#pragma unroll
-            for (int i = 0; i < R1; i++) buf[c * CS + bpad(j * R1 + i)] = v[i];
-         }
-      }
-   }
-   __syncthreads();
-   big_pass<N1, C, T, R2, R1>(buf, tw1);
-   if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1);
-
-   // four-step twiddle and the 32-byte row segments of scratch
-   float2 *dst = a.scratch + (long long)blockIdx.y * N1 * N2 + c0;
-   for (int idx = tid; idx < C * N1; idx += T) {
-      const int c = idx % C, k1 = idx / C;
-      const float2 x = buf[c * CS + bpad(k1)];
-      const int m = (c0 + c) * k1;  // < N
-      const float2 w = cmul(__ldg(a.twA + (m >> 11)), __ldg(a.twB + (m & 2047)));
-      dst[(long long)k1 * N2 + c] = cmul(x, w);
-   }
+   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 {
    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -207,6 +106,164 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Shared memory of the column pass: C columns, the W_N1 table and `slots`
+// staging slots of code words (both frames of the pair).
+template <int N1, int C, int NBIT>
+__host__ __device__ constexpr size_t big_cols_smem_slots(int slots)
+{
+   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1) +
+          sizeof(uint32_t) * (size_t)slots * 2 * C * big_col_words<N1, NBIT>();
+}
+template <int N1, int C, int NBIT>
+__host__ __device__ constexpr int big_cols_slots()
+{
+   return big_cols_smem_slots<N1, C, NBIT>(2) <= 227 * 1024 ? 2 : 1;
+}
+
+// Column pass: a persistent grid over the units u = job * (N2 / C) + g of
+// the batch (columns gC .. gC + C - 1 of one pair job).  With the column
+// layout -- column n2 of a frame starting at sample s0 is the run idx0 ..
+// idx0 + N1 - 1 of phase array (s0 + n2) % N2, idx0 = (s0 + n2) / N2 -- the
+// unit's code runs (WPC words per column and frame from the word holding
+// idx0, soff = idx0 % SPW) are staged in shared memory by cp.async, the next
+// unit's into a second slot while the current one is transformed.  The W_N1
+// table is loaded once per CTA.
+template <int N1, int N2, int C, int T, int R1, int R2, int R3, int NBIT>
+__global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
+{
+   static_assert(R1 * R2 * R3 == N1, "radices must multiply to N1");
+   static_assert(N2 % C == 0, "columns per CTA must divide N2");
+   constexpr int CS = big_col_stride(N1);
+   constexpr int SPW = 32 / NBIT;
+   constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   constexpr int WPC = big_col_words<N1, NBIT>();
+   constexpr int SLOT = 2 * C * WPC;
+   constexpr int NS = big_cols_slots<N1, C, NBIT>();
+   constexpr int NG = N2 / C;
+   extern __shared__ float2 smf[];
+   float2 *buf = smf;
+   float2 *tw1 = smf + C * CS;
+   uint32_t *stg = reinterpret_cast<uint32_t *>(tw1 + N1);  // [NS][2][C][WPC]
+   __shared__ int soff[2][2][C];
+   const int tid = threadIdx.x;
+   const int nunits = NG * a.nbjobs;
+   int u = blockIdx.x;
+   if (u >= nunits) return;
+   for (int i = tid; i < N1; i += T) tw1[i] = a.tw1[i];
+
+   auto stage = [&](int uu, int sl) {
+      const BigJob sj = a.jobs[uu / NG];
+      const int sc0 = (uu % NG) * C;
+      const int nside = sj.mode != MODE_SINGLE ? 2 : 1;
+      uint32_t *dst = stg + sl * SLOT;
+      for (int t = tid; t < nside * C * WPC; t += T) {
+         const int side = t / (C * WPC), c = (t / WPC) % C, w = t % WPC;
+         const long long s = (side ? sj.sb : sj.sa) + sc0 + c;
+         const long long wi = (s / N2) / SPW + w;
+         const uint32_t *src = a.codes + (long long)(side ? sj.code_b : sj.code_a) * a.code_words + (s % N2) * a.wpp;
+         if (wi < a.wpp) cp_async4(dst + t, src + wi);
+         else dst[t] = 0u;
+      }
+      if (tid < nside * C) {
+         const long long s = ((tid / C) ? sj.sb : sj.sa) + sc0 + tid % C;
+         soff[sl][tid / C][tid % C] = (int)((s / N2) % SPW);
+      }
+   };
+
+   int slot = 0;
+   if (a.col_layout) stage(u, 0);
+   cp_async_commit();
+   while (true) {
+      const int un = u + gridDim.x;
+      const bool more = un < nunits;
+      if constexpr (NS == 2) {
+         if (a.col_layout && more) stage(un, slot ^ 1);
+         cp_async_commit();
+         cp_async_wait1();
+      } else {
+         cp_async_wait0();
+      }
+      __syncthreads();
+
+      const int job = u / NG, c0 = (u % NG) * C;
+      const BigJob jb = a.jobs[job];
+      const bool has_b = jb.mode != MODE_SINGLE;
+      const int sta = a.code_stream[jb.code_a];
+      const uint32_t *blank_a = a.blank_any[sta] ? a.blank + (long long)sta * a.blank_words : nullptr;
+      const uint32_t *blank_b = nullptr;
+      if (has_b) {
+         const int stb = a.code_stream[jb.code_b];
+         blank_b = a.blank_any[stb] ? a.blank + (long long)stb * a.blank_words : nullptr;
+      }
+      const uint32_t *sg = stg + slot * SLOT;
+
+      // pass 1 (span 1): decode + window + radix R1
+      {
+         constexpr int NB = N1 / R1, TOT = C * NB, BPT = (TOT + T - 1) / T;
+#pragma unroll
+         for (int b = 0; b < BPT; b++) {
+            const int idx = tid + b * T;
+            if (TOT % T == 0 || idx < TOT) {
+               const int c = idx % C, j = idx / C;
+               float2 v[R1];
+               if (a.col_layout) {
+                  const int oa = soff[slot][0][c] + j, ob = has_b ? soff[slot][1][c] + j : 0;
+#pragma unroll
+                  for (int i = 0; i < R1; i++) {
+                     const long long n = (long long)(j + i * NB) * N2 + c0 + c;
+                     const float w = __ldg(a.window + n);
+                     const int pa = oa + i * NB, pb = ob + i * NB;
+                     float xa = decode_level<NBIT>((sg[c * WPC + pa / SPW] >> (NBIT * (pa % SPW))) & MASK, a.levels);
+                     float xb = 0.0f;
+                     if (has_b)
+                        xb = decode_level<NBIT>((sg[(C + c) * WPC + pb / SPW] >> (NBIT * (pb % SPW))) & MASK,
+                                                a.levels);
+                     if (blank_a && ((__ldg(blank_a + ((jb.sa + n) >> 5)) >> ((jb.sa + n) & 31)) & 1u)) xa = 0.0f;
+                     if (blank_b && ((__ldg(blank_b + ((jb.sb + n) >> 5)) >> ((jb.sb + n) & 31)) & 1u)) xb = 0.0f;
+                     v[i] = make_float2(xa * w, xb * w);
+                  }
+               } else {
+#pragma unroll
+                  for (int i = 0; i < R1; i++) {
+                     const long long n = (long long)(j + i * NB) * N2 + c0 + c;
+                     const float w = __ldg(a.window + n);
+                     const float xa = big_sample<NBIT>(a, jb.code_a, jb.sa + n, blank_a);
+                     const float xb = has_b ? big_sample<NBIT>(a, jb.code_b, jb.sb + n, blank_b) : 0.0f;
+                     v[i] = make_float2(xa * w, xb * w);
+                  }
+               }
+               DFT<R1>::run(v);
+#pragma unroll
+               for (int i = 0; i < R1; i++) buf[c * CS + bpad(j * R1 + i)] = v[i];
+            }
+         }
+      }
+      __syncthreads();
+      big_pass<N1, C, T, R2, R1>(buf, tw1);
+      if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1);
+
+      // four-step twiddle and the 32-byte row segments of scratch
+      float2 *dst = a.scratch + (long long)job * N1 * N2 + c0;
+      for (int idx = tid; idx < C * N1; idx += T) {
+         const int c = idx % C, k1 = idx / C;
+         const float2 x = buf[c * CS + bpad(k1)];
+         const int m = (c0 + c) * k1;  // < N
+         const float2 w = cmul(__ldg(a.twA + (m >> 11)), __ldg(a.twB + (m & 2047)));
+         dst[(long long)k1 * N2 + c] = cmul(x, w);
+      }
+      if (!more) break;
+      __syncthreads();  // the columns and this staging slot are reused
+      u = un;
+      if constexpr (NS == 2) {
+         slot ^= 1;
+      } else {
+         if (a.col_layout) stage(u, 0);
+         cp_async_commit();
+      }
+   }
+}
 
 // Row pass: a persistent grid over the units u = item * NP + rp of the
 // batch (row pair rp = (k1, N1 - k1), NP = N1 / 2 + 1).  A CTA walks its
@@ -314,12 +371,6 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
    }
 }
 
-template <int N1, int N2, int C, int T, int R1, int R2, int R3>
-constexpr size_t big_cols_smem()
-{
-   // columns, the W_N1 table and the staged code words (sized for 8-bit codes)
-   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1) + sizeof(uint32_t) * 2 * C * big_col_words<N1, 8>();
-}
 template <int N2>
 constexpr size_t big_rows_smem()
 {
@@ -331,7 +382,10 @@ constexpr size_t big_rows_smem()
    {N1_ * N2_, N1_, N2_, C_, TA_, TB_,                                                            \
     {k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 1>, k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 2>,  \
      k_big_cols<N1_, N2_, C_, TA_, A1, A2, A3, 8>},                                               \
-    k_big_rows<N1_, N2_, TB_, B1, B2, B3>, big_cols_smem<N1_, N2_, C_, TA_, A1, A2, A3>(),        \
+    k_big_rows<N1_, N2_, TB_, B1, B2, B3>,                                                        \
+    {big_cols_smem_slots<N1_, C_, 1>(big_cols_slots<N1_, C_, 1>()),                               \
+     big_cols_smem_slots<N1_, C_, 2>(big_cols_slots<N1_, C_, 2>()),                               \
+     big_cols_smem_slots<N1_, C_, 8>(big_cols_slots<N1_, C_, 8>())},                              \
     big_rows_smem<N2_>()}
 #define SWS_BIG(N1_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3) SWS_BIG_C(N1_, 4, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)
 

@@ -42,6 +42,7 @@ struct BigArgs {
    const float2 *twB;          // W_N^l, l < 2048
    float2 *scratch;            // [job][N1][N2] column FFTs, twiddled
    float *partial;
+   int nbjobs;                 // jobs of this batch (column pass)
    int nbitems;                // items of this batch (row pass)
    int N, S;
    float4 levels;
@@ -55,7 +56,7 @@ struct BigPlan {
    int TA, TB;                  // threads of the column / row kernels
    BigColsKernel cols[3];       // nbit 1, 2, 8
    BigRowsKernel rows;
-   size_t smem_cols, smem_rows;
+   size_t smem_cols[3], smem_rows;  // column pass per bit depth (1, 2, 8)
 };
 
 bool find_big_plan(int N, BigPlan *out);

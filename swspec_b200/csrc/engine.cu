@@ -131,8 +131,9 @@ struct swsgpu_handle {
    std::vector<int2> tw_off;  // per candidate: offsets of its W_N1 and W_N2 tables in d_tw1
    int S = 0;
    int max_clusters = 1;
-   const void *rows_fn = nullptr;   // row-pass kernel the persistent grid was sized for
-   int rows_grid = 0;
+   const void *rows_fn = nullptr;   // four-step kernels the persistent grids were sized for
+   const void *cols_fn = nullptr;
+   int rows_grid = 0, cols_grid = 0;
    std::string err;
    cudaStream_t stream = nullptr;     // kernels and result copies
    cudaStream_t cstream = nullptr;    // input copies of submit()
@@ -516,13 +517,16 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.N = c.fft_points;
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
-   if (h->rows_fn != (const void *)bp.rows) {
-      // persistent row pass: as many CTAs as fit on the device at once
-      int occ = 0, nsm = 0;
-      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bp.rows, bp.TB, bp.smem_rows));
+   if (h->rows_fn != (const void *)bp.rows || h->cols_fn != (const void *)bp.cols[nbi]) {
+      // persistent passes: as many CTAs as fit on the device at once
+      int occ_r = 0, occ_c = 0, nsm = 0;
+      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, bp.rows, bp.TB, bp.smem_rows));
+      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, bp.cols[nbi], bp.TA, bp.smem_cols[nbi]));
       CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-      h->rows_grid = std::max(1, occ) * nsm;
+      h->rows_grid = std::max(1, occ_r) * nsm;
+      h->cols_grid = std::max(1, occ_c) * nsm;
       h->rows_fn = (const void *)bp.rows;
+      h->cols_fn = (const void *)bp.cols[nbi];
    }
    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
    if (h->profiling) {
@@ -533,7 +537,8 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    for (const int4 &b : se.batches) {
       a.jobs = (const BigJob *)se.d_bjobs.p + b.x;
       a.bitems = (const BigItem *)se.d_bitems.p + b.z;
-      bp.cols[nbi]<<<dim3(bp.N2 / bp.C, (unsigned)b.y), bp.TA, bp.smem_cols, st>>>(a);
+      a.nbjobs = b.y;
+      bp.cols[nbi]<<<(unsigned)std::min((bp.N2 / bp.C) * b.y, h->cols_grid), bp.TA, bp.smem_cols[nbi], st>>>(a);
       a.nbitems = b.w;
       const int units = (bp.N1 / 2 + 1) * b.w;
       bp.rows<<<(unsigned)std::min(units, h->rows_grid), bp.TB, bp.smem_rows, st>>>(a);
@@ -1134,7 +1139,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
          }
       }
       CKB(cudaFuncSetAttribute((const void *)h->bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)h->bplan.smem_cols));
+                               (int)h->bplan.smem_cols[nbi]));
       CKB(cudaFuncSetAttribute((const void *)h->bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)h->bplan.smem_rows));
       for (int k = 0; k < 2; k++)
@@ -1517,7 +1522,7 @@ static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
    const int nbit = h->cfg.layout[0].nbit;
    const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
    cudaError_t e = cudaFuncSetAttribute((const void *)bp.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)bp.smem_cols);
+                                        (int)bp.smem_cols[nbi]);
    if (e != cudaSuccess) return e;
    return cudaFuncSetAttribute((const void *)bp.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)bp.smem_rows);
