@@ -45,14 +45,13 @@ __host__ __device__ constexpr int big_col_words()
 
 // One Stockham pass (radix R, span NS) over C columns of M points held in
 // shared memory, in place through registers.  Butterfly j of column c reads
-// x[j + i M/R], twiddles by W_(NS R)^(k i) (k = j mod NS) from the W_M table
-// and writes d + i NS, d = (j / NS) NS R + k.
+// x[j + i M/R], twiddles by W_(NS R)^(k i) (k = j mod NS) from the pass's
+// table tw[(i - 1) NS + k] and writes d + i NS, d = (j / NS) NS R + k.
 template <int M, int C, int T, int R, int NS>
 __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
 {
    constexpr int CS = big_col_stride(M);
    constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
-   constexpr int TS = M / (NS * R);
    const int tid = threadIdx.x;
    float2 v[BPT][R];
 #pragma unroll
@@ -63,7 +62,7 @@ __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
 #pragma unroll
          for (int i = 0; i < R; i++) {
             float2 x = buf[c * CS + bpad(j + i * NB)];
-            if (NS > 1 && i > 0) x = cmul(x, tw[k * i * TS]);
+            if (NS > 1 && i > 0) x = cmul(x, tw[(i - 1) * NS + k]);
             v[b][i] = x;
          }
          DFT<R>::run(v[b]);
@@ -81,6 +80,25 @@ __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
       }
    }
    __syncthreads();
+}
+
+// Twiddle tables of the passes of span R1 (radix R2) and R1 R2 (radix R3),
+// laid out [i - 1][k] so that the lanes of a warp (consecutive k) read
+// consecutive entries: W_M^(k i M / (R1 R2)) then W_M^(k i), from the W_M
+// table wm in global memory.  M - R1 entries.
+template <int M, int T, int R1, int R2, int R3>
+__device__ __forceinline__ void load_pass_twiddles(float2 *tab, const float2 *wm)
+{
+   constexpr int NA = (R2 - 1) * R1, NBT = (R3 - 1) * R1 * R2;
+   for (int e = threadIdx.x; e < NA + NBT; e += T) {
+      if (e < NA) {
+         const int i = e / R1 + 1, k = e % R1;
+         tab[e] = wm[k * i * (M / (R1 * R2))];
+      } else {
+         const int f = e - NA, i = f / (R1 * R2) + 1, k = f % (R1 * R2);
+         tab[e] = wm[k * i];
+      }
+   }
 }
 
 template <int NBIT>
@@ -151,7 +169,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
    const int nunits = NG * a.nbjobs;
    int u = blockIdx.x;
    if (u >= nunits) return;
-   for (int i = tid; i < N1; i += T) tw1[i] = a.tw1[i];
+   load_pass_twiddles<N1, T, R1, R2, R3>(tw1, a.tw1);
 
    auto stage = [&](int uu, int sl) {
       const BigJob sj = a.jobs[uu / NG];
@@ -242,7 +260,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
       }
       __syncthreads();
       big_pass<N1, C, T, R2, R1>(buf, tw1);
-      if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1);
+      if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1 + (R2 - 1) * R1);
 
       // four-step twiddle and the 32-byte row segments of scratch
       float2 *dst = a.scratch + (long long)job * N1 * N2 + c0;
@@ -284,7 +302,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
    const int nunits = NP * a.nbitems;
    int u = blockIdx.x;
    if (u >= nunits) return;
-   for (int i = tid; i < N2; i += T) tw2[i] = a.tw2[i];
+   load_pass_twiddles<N2, T, R1, R2, R3>(tw2, a.tw2);
    const long long N = (long long)N1 * N2;
 
    auto stage = [&](int uu, int jj, int sl) {
@@ -327,7 +345,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
       const bool two = rp != (N1 - rp) % N1;
       big_pass<N2, 2, T, R1, 1>(buf, tw2);
       big_pass<N2, 2, T, R2, R1>(buf, tw2);
-      if constexpr (R3 > 1) big_pass<N2, 2, T, R3, R1 * R2>(buf, tw2);
+      if constexpr (R3 > 1) big_pass<N2, 2, T, R3, R1 * R2>(buf, tw2 + (R2 - 1) * R1);
 #pragma unroll
       for (int q = 0; q < KPT; q++) {
          const int k2 = tid + q * T;
@@ -396,23 +414,23 @@ static const BigPlan kBigPlans[] = {
     SWS_BIG_C(256, 32, 512, 16, 16, 1, 256, 128, 16, 16, 1),
     SWS_BIG_C(128, 32, 256, 16, 8, 1, 512, 256, 16, 16, 2),
     SWS_BIG(512, 256, 16, 16, 2, 512, 256, 16, 16, 2),        // 2^18
-    SWS_BIG(256, 256, 16, 16, 1, 1024, 512, 16, 16, 4),
+    SWS_BIG(256, 256, 16, 16, 1, 1024, 128, 16, 16, 4),
     SWS_BIG(1024, 256, 16, 16, 4, 256, 256, 16, 16, 1),
-    SWS_BIG(512, 256, 16, 16, 2, 1024, 512, 16, 16, 4),       // 2^19
+    SWS_BIG(512, 256, 16, 16, 2, 1024, 128, 16, 16, 4),       // 2^19
     SWS_BIG(1024, 256, 16, 16, 4, 512, 256, 16, 16, 2),
-    SWS_BIG(1024, 256, 16, 16, 4, 1024, 512, 16, 16, 4),      // 2^20
-    SWS_BIG_C(1024, 8, 512, 16, 16, 4, 1024, 512, 16, 16, 4),
-    SWS_BIG(512, 256, 16, 16, 2, 2048, 512, 16, 16, 8),
+    SWS_BIG(1024, 256, 16, 16, 4, 1024, 128, 16, 16, 4),      // 2^20
+    SWS_BIG_C(1024, 8, 512, 16, 16, 4, 1024, 128, 16, 16, 4),
+    SWS_BIG(512, 256, 16, 16, 2, 2048, 256, 16, 16, 8),
     SWS_BIG(2048, 512, 16, 16, 8, 512, 256, 16, 16, 2),
-    SWS_BIG(1024, 256, 16, 16, 4, 2048, 512, 16, 16, 8),      // 2^21
-    SWS_BIG(2048, 512, 16, 16, 8, 1024, 512, 16, 16, 4),
-    SWS_BIG(2048, 512, 16, 16, 8, 2048, 512, 16, 16, 8),      // 2^22
+    SWS_BIG(1024, 256, 16, 16, 4, 2048, 256, 16, 16, 8),      // 2^21
+    SWS_BIG(2048, 512, 16, 16, 8, 1024, 128, 16, 16, 4),
+    SWS_BIG(2048, 512, 16, 16, 8, 2048, 256, 16, 16, 8),      // 2^22
     SWS_BIG(1024, 256, 16, 16, 4, 4096, 512, 16, 16, 16),
-    SWS_BIG(4096, 512, 16, 16, 16, 1024, 512, 16, 16, 4),
-    SWS_BIG(1600, 512, 16, 4, 25, 2000, 512, 16, 5, 25),      // 3,200,000 = 2^10 5^5
-    SWS_BIG(2000, 512, 16, 5, 25, 1600, 512, 16, 4, 25),
-    SWS_BIG(3200, 512, 16, 8, 25, 1000, 512, 8, 5, 25),
-    SWS_BIG(1280, 512, 16, 16, 5, 2500, 512, 4, 25, 25),
+    SWS_BIG(4096, 512, 16, 16, 16, 1024, 128, 16, 16, 4),
+    SWS_BIG(3200, 512, 16, 8, 25, 1000, 256, 8, 5, 25),       // 3,200,000 = 2^10 5^5
+    SWS_BIG(1600, 512, 16, 4, 25, 2000, 256, 16, 5, 25),
+    SWS_BIG(2000, 512, 16, 5, 25, 1600, 256, 16, 4, 25),
+    SWS_BIG(1280, 512, 16, 16, 5, 2500, 256, 4, 25, 25),
 };
 
 bool find_big_plan(int N, BigPlan *out)
