@@ -10,6 +10,8 @@
 // sums are FP64, so folding 1e5 samples per bin per FFT loses nothing; the
 // folded bins are rounded to FP32 once, at the output.
 #include "pcal.cuh"
+#include "bins.cuh"
+#include "dft.cuh"
 
 namespace sws {
 
@@ -109,14 +111,21 @@ __global__ void k_pcal_fold_words(PcalArgs a)
 {
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
+   constexpr int NPAIR = SPW / 2;                 // code pairs per word
+   constexpr int PB = 2 * NBIT;                   // bits per pair
+   constexpr int NLUT = NBIT < 8 ? 1 << PB : 1;   // pair table (1/2-bit codes)
    extern __shared__ double pc_smem[];  // [tonebins][2]
    __shared__ float lut[4];
+   __shared__ float2 plut[NLUT];
    const PcalJob job = a.jobs[blockIdx.y];
    for (int i = threadIdx.x; i < 2 * a.tonebins; i += blockDim.x) pc_smem[i] = 0.0;
    if (threadIdx.x < 4) {
       const float lv[4] = {a.levels.x, a.levels.y, a.levels.z, a.levels.w};
       lut[threadIdx.x] = lv[threadIdx.x];
    }
+   if (NBIT < 8)
+      for (int i = threadIdx.x; i < NLUT; i += blockDim.x)
+         plut[i] = make_float2(decode_level<NBIT>(i & MASK, a.levels), decode_level<NBIT>((i >> NBIT) & MASK, a.levels));
    __syncthreads();
    const int D = a.D, rot = a.rotatorlen;
    const int wpd = rot / (SPW * D);
@@ -136,23 +145,63 @@ __global__ void k_pcal_fold_words(PcalArgs a)
          s[k] = 0.0f;
          sd[k] = 0.0;
       }
-      for (int p = p0; p < p1; p++) {
-         const uint32_t w = __ldg(base + (long long)p * wpd);
+      if (!chk) {
+         // four periods' words in flight, two codes per table lookup and
+         // packed add; the FP32 sums of each position run in period order
+         // and are flushed after the same 64-period groups as below
+         float2 s2[NPAIR];
 #pragma unroll
-         for (int k = 0; k < SPW; k++) {
-            const uint32_t code = (w >> (NBIT * k)) & MASK;
-            float v = (NBIT == 8) ? (float)((int)code * 2 - 255) * (1.0f / 256.0f) : lut[code & 3];
-            if (chk) {
-               const long long smp = job.start + (long long)p * rot + (long long)(wi * SPW + k) * D + ph;
-               if ((__ldg(blank + (smp >> 5)) >> (smp & 31)) & 1u) v = 0.0f;
+         for (int q = 0; q < NPAIR; q++) s2[q] = make_float2(0.0f, 0.0f);
+         for (int p = p0; p < p1; p += 4) {
+            uint32_t w[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) w[v] = p + v < p1 ? __ldg(base + (long long)(p + v) * wpd) : 0u;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+               if (p + v < p1) {
+#pragma unroll
+                  for (int q = 0; q < NPAIR; q++) {
+                     float2 x;
+                     if constexpr (NBIT == 8)
+                        x = make_float2(decode_level<8>((w[v] >> (PB * q)) & 0xffu, a.levels),
+                                        decode_level<8>((w[v] >> (PB * q + 8)) & 0xffu, a.levels));
+                     else
+                        x = plut[(w[v] >> (PB * q)) & ((1u << PB) - 1u)];
+                     s2[q] = padd(s2[q], x);
+                  }
+               }
             }
-            s[k] += v;
+            if (((p - p0) & 63) == 60) {
+#pragma unroll
+               for (int q = 0; q < NPAIR; q++) {
+                  sd[2 * q] += (double)s2[q].x;
+                  sd[2 * q + 1] += (double)s2[q].y;
+                  s2[q] = make_float2(0.0f, 0.0f);
+               }
+            }
          }
-         if (((p - p0) & 63) == 63) {
+#pragma unroll
+         for (int q = 0; q < NPAIR; q++) {
+            s[2 * q] = s2[q].x;
+            s[2 * q + 1] = s2[q].y;
+         }
+      } else {
+         for (int p = p0; p < p1; p++) {
+            const uint32_t w = __ldg(base + (long long)p * wpd);
 #pragma unroll
             for (int k = 0; k < SPW; k++) {
-               sd[k] += (double)s[k];
-               s[k] = 0.0f;
+               const uint32_t code = (w >> (NBIT * k)) & MASK;
+               float v = (NBIT == 8) ? (float)((int)code * 2 - 255) * (1.0f / 256.0f) : lut[code & 3];
+               const long long smp = job.start + (long long)p * rot + (long long)(wi * SPW + k) * D + ph;
+               if ((__ldg(blank + (smp >> 5)) >> (smp & 31)) & 1u) v = 0.0f;
+               s[k] += v;
+            }
+            if (((p - p0) & 63) == 63) {
+#pragma unroll
+               for (int k = 0; k < SPW; k++) {
+                  sd[k] += (double)s[k];
+                  s[k] = 0.0f;
+               }
             }
          }
       }
