@@ -538,7 +538,9 @@ def spec_arm(args) -> None:
                           max_run_bytes=w["run_bytes"], samplingfreq=w["fs"], runs_per_output=w["runs"],
                           extract_pcal=bool(pc), pcal_tonebins=pc.get("tonebins", 0),
                           pcal_rotatorlen=pc.get("rotatorlen", 0), pcal_offset_hz=pc.get("offset", 10e3),
-                          pcal_ntones=pc.get("ntones", 0), autotune=True)
+                          pcal_ntones=pc.get("ntones", 0), autotune=args.candidate < 0,
+                          plan_family=gpu.PLAN_FOURSTEP if args.candidate >= 0 else gpu.PLAN_DEFAULT,
+                          plan_candidate=max(args.candidate, 0))
     core = gpu.Core(cfg, device=local)
     g = torch.Generator(device="cuda")
     g.manual_seed(1000 + reps.rank)
@@ -612,6 +614,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plan", default="auto", choices=["auto", "cluster", "fourstep"],
                     help="FFT path for the cross-spectra workload (auto: cluster kernel)")
+    ap.add_argument("--candidate", type=int, default=-1,
+                    help="c2/c5: pin four-step split k of the length's candidates instead of autotuning")
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c3: dual-pol cross-spectra (the default line); c1: plain single channel; "
                          "c2: 3.2M-point spectra with phase-cal tones; c4: batched uneven streams; "

@@ -208,8 +208,9 @@ int swsgpu_host_unregister(void *p);
 /* Autotuner (no counterpart in the reference, whose IPP core has one FFT
  * plan per length): for a length on the four-step path, times every
  * candidate split N = N1 x N2 and columns-per-CTA width on a hash-filled run
- * of two frames per source with this core's sources, pairs and window, and
- * keeps the fastest; later cores of the same length and bit depth in this
+ * with this core's sources, pairs and window (enough frames for about 16
+ * pair FFTs), and keeps the one with the shortest of `iterations` (at most
+ * 16) timed iterations; later cores of the same length and bit depth in this
  * process start with that choice.  Cluster lengths have one plan and return
  * at once.  Synchronous; call it with no run pending. */
 int swsgpu_autotune(swsgpu_handle *h, int iterations);

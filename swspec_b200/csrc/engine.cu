@@ -1528,8 +1528,10 @@ static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
                                (int)bp.smem_rows);
 }
 
-// Times every candidate split on a hash-filled run of two frames per source
-// (the handle's own sources, pairs and window) and keeps the fastest.
+// Times every candidate split on a hash-filled run (the handle's own
+// sources, pairs and window) of enough frames for about 16 pair FFTs, so
+// that both passes fill the device as a full run does, and keeps the one
+// with the shortest single iteration.
 static int autotune_big(swsgpu_handle *h, int iters)
 {
    const swsgpu_config &c = h->cfg;
@@ -1538,7 +1540,8 @@ static int autotune_big(swsgpu_handle *h, int iters)
    h->big_cands = nc;
    if (nc <= 1) return SWSGPU_OK;
    const int nbit = c.layout[0].nbit;
-   const long long nsamp = 2ll * c.fft_points;
+   const int frames = 2 * std::max(1, (16 + c.num_sources - 1) / std::max(1, c.num_sources));
+   const long long nsamp = (long long)frames * c.fft_points;
    const int pb = payload_bytes(c.layout[0]);
    size_t pay = (size_t)((nsamp * c.layout[0].nchan * nbit + 7) / 8);
    pay = ((pay + pb - 1) / pb) * pb;
@@ -1565,16 +1568,16 @@ static int autotune_big(swsgpu_handle *h, int iters)
       k_fill_hash<<<(unsigned)((nw + 255) / 256), 256, 0, h->stream>>>((uint32_t *)raw[s].p, nw, 1234u + s);
       d_raw[s] = raw[s].p;
    }
-   if (oa.ensure(sizeof(float) * (size_t)h->S * c.num_sources * 2 + 64) != cudaSuccess ||
-       ox.ensure(sizeof(float) * 2 * (size_t)h->S * std::max(c.num_xpols, 1) * 2 + 64) != cudaSuccess) {
+   if (oa.ensure(sizeof(float) * (size_t)h->S * c.num_sources * (frames + 1) + 64) != cudaSuccess ||
+       ox.ensure(sizeof(float) * 2 * (size_t)h->S * std::max(c.num_xpols, 1) * (frames + 1) + 64) != cudaSuccess) {
       cleanup();
       return fail(h, SWSGPU_ECUDA, "autotune: allocation failed");
    }
    int best = -1;
    float best_ms = 0.0f;
-   cudaEvent_t e0, e1;
-   cudaEventCreate(&e0);
-   cudaEventCreate(&e1);
+   const int nit = std::max(1, std::min(iters, 16));
+   cudaEvent_t ev[17];
+   for (int i = 0; i <= nit; i++) cudaEventCreate(&ev[i]);
    for (int k = 0; k < nc; k++) {
       if (set_big_attrs(h, cand[k]) != cudaSuccess) {
          cudaGetLastError();
@@ -1583,25 +1586,29 @@ static int autotune_big(swsgpu_handle *h, int iters)
       h->bplan = cand[k];
       h->cand = k;
       int nspec = 0, rc = SWSGPU_OK;
-      for (int it = 0; it <= iters && rc == SWSGPU_OK; it++) {
-         if (it == 1) cudaEventRecord(e0, h->stream);
+      // one untimed iteration, then nit timed ones
+      for (int it = 0; it <= nit && rc == SWSGPU_OK; it++) {
+         if (it >= 1) cudaEventRecord(ev[it - 1], h->stream);
          rc = launch_chunk(h, d_raw, raw_bytes, grid_off, pay, 1, 1, (float *)oa.p,
                            c.num_xpols ? (float *)ox.p : nullptr, nullptr, h->stream, &nspec);
       }
-      cudaEventRecord(e1, h->stream);
-      if (rc != SWSGPU_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaEventRecord(ev[nit], h->stream);
+      if (rc != SWSGPU_OK || cudaEventSynchronize(ev[nit]) != cudaSuccess) {
          cudaGetLastError();
          continue;
       }
       float ms = 0.0f;
-      cudaEventElapsedTime(&ms, e0, e1);
+      for (int i = 0; i < nit; i++) {
+         float t = 0.0f;
+         cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+         if (i == 0 || t < ms) ms = t;
+      }
       if (best < 0 || ms < best_ms) {
          best = k;
          best_ms = ms;
       }
    }
-   cudaEventDestroy(e0);
-   cudaEventDestroy(e1);
+   for (int i = 0; i <= nit; i++) cudaEventDestroy(ev[i]);
    cleanup();
    if (best < 0) return fail(h, SWSGPU_ECUDA, "autotune: no candidate ran");
    h->bplan = cand[best];
