@@ -392,7 +392,12 @@ def gpu_arm(args) -> None:
         achieved = bytes_per_launch / kern_s / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": f"HBM copy, {peaks['source']}"}
-    roof["traffic"] = None
+    # DRAM bytes of one FP32 k_spectra launch on this workload, from an ncu
+    # capture (dram__bytes_read.sum + dram__bytes_write.sum): the 2-bit codes
+    # read plus the per-item partial spectra that k_reduce combines
+    roof["traffic"] = (256476672 + 208978176) if headline == gpu.PREC_FP32 else None
+    roof["traffic_source"] = ("ncu capture of k_spectra<16, 4096, 256, 16, 16, 16, 2, 2, 0>, this workload"
+                              if headline == gpu.PREC_FP32 else None)
     roof["kernel"] = "k_spectra (cluster FFT + accumulate)"
     roof["compute"] = {"achieved_tflops": flops_per_launch / kern_s / 1e12,
                        "fp32_peak_tflops": p32,

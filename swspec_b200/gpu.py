@@ -191,13 +191,21 @@ class Core:
 
     def submit(self, raws: list, payload_offsets=None) -> None:
         n = len(raws)
-        ptrs = (C.c_void_p * n)(*[int(r) if isinstance(r, int) else r.ctypes.data for r in raws])
-        sizes = (C.c_size_t * n)(*self._sizes)
-        offs = (C.c_int64 * n)(*(payload_offsets or [0] * n))
-        _check(lib().swsgpu_submit(self.h, ptrs, sizes, offs), self.h)
+        # argument arrays kept across calls: a run's submit is on the
+        # per-run critical path of the host loop
+        if getattr(self, "_sub_n", 0) != n:
+            self._sub_n = n
+            self._sub_ptrs = (C.c_void_p * n)()
+            self._sub_sizes = (C.c_size_t * n)(*self._sizes)
+            self._sub_offs = (C.c_int64 * n)()
+        for i, r in enumerate(raws):
+            self._sub_ptrs[i] = int(r) if isinstance(r, int) else r.ctypes.data
+            self._sub_offs[i] = payload_offsets[i] if payload_offsets else 0
+        _check(lib().swsgpu_submit(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs), self.h)
 
     def set_sizes(self, sizes: list[int]) -> None:
         self._sizes = list(sizes)
+        self._sub_n = 0
 
     def wait(self, timeout_ms: int = 60000) -> int:
         ns = C.c_int()
