@@ -82,6 +82,41 @@ __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
    __syncthreads();
 }
 
+// The column pass's last Stockham pass, with the four-step twiddle applied
+// in registers: output k1 = d + i NS of column c goes straight to scratch
+// row k1 as x W_N^((c0 + c) k1), W_N^m = W_N^(2048 (m >> 11)) W_N^(m & 2047).
+template <int M, int C, int T, int R, int NS>
+__device__ __forceinline__ void big_pass_out(const float2 *buf, const float2 *tw, float2 *dst, int N2, int c0,
+                                             const float2 *twA, const float2 *twB)
+{
+   constexpr int CS = big_col_stride(M);
+   constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
+   const int tid = threadIdx.x;
+#pragma unroll
+   for (int b = 0; b < BPT; b++) {
+      const int idx = tid + b * T;
+      if (TOT % T == 0 || idx < TOT) {
+         const int c = idx % C, j = idx / C, k = j % NS;
+         float2 v[R];
+#pragma unroll
+         for (int i = 0; i < R; i++) {
+            float2 x = buf[c * CS + bpad(j + i * NB)];
+            if (NS > 1 && i > 0) x = cmul(x, tw[(i - 1) * NS + k]);
+            v[i] = x;
+         }
+         DFT<R>::run(v);
+         const int d = (j / NS) * NS * R + k;
+#pragma unroll
+         for (int i = 0; i < R; i++) {
+            const int k1 = d + i * NS;
+            const int m = (c0 + c) * k1;  // < N
+            const float2 w = cmul(__ldg(twA + (m >> 11)), __ldg(twB + (m & 2047)));
+            dst[(long long)k1 * N2 + c] = cmul(v[i], w);
+         }
+      }
+   }
+}
+
 // Twiddle tables of the passes of span R1 (radix R2) and R1 R2 (radix R3),
 // laid out [i - 1][k] so that the lanes of a warp (consecutive k) read
 // consecutive entries: W_M^(k i M / (R1 R2)) then W_M^(k i), from the W_M
@@ -259,17 +294,14 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
          }
       }
       __syncthreads();
-      big_pass<N1, C, T, R2, R1>(buf, tw1);
-      if constexpr (R3 > 1) big_pass<N1, C, T, R3, R1 * R2>(buf, tw1 + (R2 - 1) * R1);
-
-      // four-step twiddle and the 32-byte row segments of scratch
+      // remaining passes; the last writes the twiddled 32-byte row segments
+      // of scratch itself
       float2 *dst = a.scratch + (long long)job * N1 * N2 + c0;
-      for (int idx = tid; idx < C * N1; idx += T) {
-         const int c = idx % C, k1 = idx / C;
-         const float2 x = buf[c * CS + bpad(k1)];
-         const int m = (c0 + c) * k1;  // < N
-         const float2 w = cmul(__ldg(a.twA + (m >> 11)), __ldg(a.twB + (m & 2047)));
-         dst[(long long)k1 * N2 + c] = cmul(x, w);
+      if constexpr (R3 > 1) {
+         big_pass<N1, C, T, R2, R1>(buf, tw1);
+         big_pass_out<N1, C, T, R3, R1 * R2>(buf, tw1 + (R2 - 1) * R1, dst, N2, c0, a.twA, a.twB);
+      } else {
+         big_pass_out<N1, C, T, R2, R1>(buf, tw1, dst, N2, c0, a.twA, a.twB);
       }
       if (!more) break;
       __syncthreads();  // the columns and this staging slot are reused
