@@ -27,11 +27,13 @@
 
 namespace sws {
 
-__host__ __device__ constexpr int big_col_stride(int M)
+__host__ __device__ constexpr int big_col_stride(int M, int C)
 {
-   // column stride in float2: one pad per 16 entries, rounded to 16, + 4
-   // (a stride of 4 mod 16 spreads four columns over distinct banks)
-   return ((M + M / 16 + 15) / 16) * 16 + 4;
+   // column stride in float2: one pad per 16 entries, rounded to 16, plus
+   // 16 / min(C, 16): the 16 lanes of a half-warp (one shared-memory
+   // wavefront of 8-byte accesses) cover min(C, 16) columns at 16 / min(C, 16)
+   // consecutive points each, which this offset puts in distinct banks
+   return ((M + M / 16 + 15) / 16) * 16 + 16 / (C < 16 ? C : 16);
 }
 __device__ __forceinline__ int bpad(int i) { return i + (i >> 4); }
 
@@ -50,7 +52,7 @@ __host__ __device__ constexpr int big_col_words()
 template <int M, int C, int T, int R, int NS>
 __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
 {
-   constexpr int CS = big_col_stride(M);
+   constexpr int CS = big_col_stride(M, C);
    constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
    const int tid = threadIdx.x;
    float2 v[BPT][R];
@@ -89,7 +91,7 @@ template <int M, int C, int T, int R, int NS>
 __device__ __forceinline__ void big_pass_out(const float2 *buf, const float2 *tw, float2 *dst, int N2, int c0,
                                              const float2 *twA, const float2 *twB)
 {
-   constexpr int CS = big_col_stride(M);
+   constexpr int CS = big_col_stride(M, C);
    constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
    const int tid = threadIdx.x;
 #pragma unroll
@@ -166,7 +168,7 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 template <int N1, int C, int NBIT>
 __host__ __device__ constexpr size_t big_cols_smem_slots(int slots)
 {
-   return sizeof(float2) * ((size_t)C * big_col_stride(N1) + N1) +
+   return sizeof(float2) * ((size_t)C * big_col_stride(N1, C) + N1) +
           sizeof(uint32_t) * (size_t)slots * 2 * C * big_col_words<N1, NBIT>();
 }
 template <int N1, int C, int NBIT>
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
 {
    static_assert(R1 * R2 * R3 == N1, "radices must multiply to N1");
    static_assert(N2 % C == 0, "columns per CTA must divide N2");
-   constexpr int CS = big_col_stride(N1);
+   constexpr int CS = big_col_stride(N1, C);
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
    constexpr int WPC = big_col_words<N1, NBIT>();
@@ -325,7 +327,7 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
 {
    static_assert(R1 * R2 * R3 == N2, "radices must multiply to N2");
    static_assert(N1 % 2 == 0, "row pairs need an even N1");
-   constexpr int CS = big_col_stride(N2);
+   constexpr int CS = big_col_stride(N2, 2);
    constexpr int KPT = (N2 + T - 1) / T;
    constexpr int NP = N1 / 2 + 1;
    extern __shared__ float2 smf[];
@@ -425,7 +427,7 @@ template <int N2>
 constexpr size_t big_rows_smem()
 {
    // two slots of a row pair, then the W_N2 table
-   return sizeof(float2) * ((size_t)4 * big_col_stride(N2) + N2);
+   return sizeof(float2) * ((size_t)4 * big_col_stride(N2, 2) + N2);
 }
 
 #define SWS_BIG_C(N1_, C_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)                                 \
