@@ -53,6 +53,7 @@ int load_ini(Settings &s, const std::string &inifile, std::string &err)
       s.gpu_precision = (strcasecmp(keyval.c_str(), "TCSPLIT") == 0) ? SWSGPU_PREC_TCSPLIT : SWSGPU_PREC_FP32;
    ini.getKeyValue("GpuDevice", s.gpu_device);
    ini.getKeyValue("GpuCombineOnDevice", s.gpu_combine_on_device);
+   ini.getKeyValue("GpuAutotune", s.gpu_autotune);
    ini.getKeyValue("FixXpolLength", s.fix_xpol_length);
    return 0;
 }
@@ -205,7 +206,7 @@ std::string settings_json(const Settings &s)
      << ", \"source_channels\": " << s.source_channels << ", \"bits_per_sample\": " << s.bits_per_sample
      << ", \"calc_Xpol\": " << (s.calc_Xpol ? 1 : 0) << ", \"sinkformat\": \"" << (s.sinkformat == Ascii ? "ascii" : "binary")
      << "\", \"basefilename1\": \"" << s.basefilename1 << "\", \"basefilename2\": \"" << s.basefilename2
-     << "\", \"gpu_precision\": " << s.gpu_precision << "}";
+     << "\", \"gpu_precision\": " << s.gpu_precision << ", \"gpu_autotune\": " << (s.gpu_autotune ? 1 : 0) << "}";
    return o.str();
 }
 

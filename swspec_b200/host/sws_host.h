@@ -107,6 +107,7 @@ struct Settings {
    int gpu_precision = SWSGPU_PREC_FP32;  // GpuPrecision = FP32 | TCSPLIT
    int gpu_device = 0;                    // GpuDevice
    bool gpu_combine_on_device = true;     // GpuCombineOnDevice
+   bool gpu_autotune = false;             // GpuAutotune: time the four-step splits of the length at prepare
    bool fix_xpol_length = false;          // FixXpolLength (reference quirk: half of XY* written)
    // counts
    int num_sources = 0, num_sinks = 0, num_xpols = 0;

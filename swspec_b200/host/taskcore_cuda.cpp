@@ -64,6 +64,7 @@ void TaskCoreCUDA::prepare(Settings *s)
    c.pcal_offset_hz = s->pcaloffsethz;
    c.max_run_bytes = s->rawbuf_size;
    c.runs_per_output = (s->gpu_combine_on_device && s->max_buffers_per_spectrum > 1) ? s->max_buffers_per_spectrum : 1;
+   c.autotune = s->gpu_autotune ? 1 : 0;
    int rc = swsgpu_create(&c, s->gpu_device, &h_);
    if (rc != SWSGPU_OK) {
       *s->tlog << "CUDA core " << rank_ << ": " << swsgpu_last_error(nullptr) << std::endl;

@@ -41,6 +41,7 @@ WindowType = Hann
 BaseFilename1 = out_%fftpoints%_%channel%
 """)
     s = _settings(ini)
+    assert s["gpu_autotune"] == 0            # off unless asked for
     py = from_ini_values(fft_points=65536, fft_integ_seconds=1.0, fft_overlap_factor=1,
                          BandwidthHz=32e6, bits_per_sample=2, source_channels=16)
     for k in ["averaged_ffts", "raw_fullfft_bytes", "rawbuf_size", "max_buffers_per_spectrum",
@@ -64,9 +65,11 @@ WindowType = Triangle
 ExtractPCal = yes
 PCalOffsetHz = 15625
 MaxSourceBufferMB = 64
+GpuAutotune = yes
 BaseFilename1 = plain
 """)
     s = _settings(ini)
+    assert s["gpu_autotune"] == 1            # GPU-core key, absent from the reference's settings
     assert s["fft_points"] == 32768          # 'FFT points' == 'FFTpoints', first wins
     assert s["wf_type"] == 2                 # unknown -> Cosine2
     py = from_ini_values(fft_points=32768, fft_integ_seconds=0.5, fft_overlap_factor=2,
