@@ -45,3 +45,12 @@ def rel_err_auto(gpu: np.ndarray, ref: np.ndarray) -> float:
 
 def rel_err_xpol(gpu: np.ndarray, ref: np.ndarray, ai: np.ndarray, aj: np.ndarray) -> float:
     return float(np.max(np.abs(gpu.astype(np.complex128) - ref) / np.sqrt(ai * aj)))
+
+
+def fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hdr: int) -> bytes:
+    """Overwrite payload bytes [start, end) of a frame with the mark5 fill
+    pattern 0x11223344 (little-endian words), as a recorder marks lost data."""
+    a = bytearray(raw)
+    base = frame * frame_bytes + hdr
+    a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
+    return bytes(a)

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import REL_TOL, decode_channels, oracle_run
+from helpers import REL_TOL, decode_channels, fill_zone, oracle_run
 from swspec_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -83,6 +83,43 @@ def test_four_step_cross_pair(gpu, N, nbit):
     # partial spectrum: one unscaled FFT
     for k in range(2):
         _check_auto(auto[1, k], ra[1, k], a32[1, k], per_bin=False)
+
+
+def test_four_step_blanked_mark5b_pcal(gpu):
+    """Fill-pattern zones (trailing, whole frame, leading, interior, all
+    but the edges) in a framed Mark5B 16 x 2-bit stream at N = 2^18: the
+    column-layout corner turn in phase blocks with its separate blank bitmap,
+    the undecimated phase-cal copy and the four-step FFT against the FP64
+    oracle of the blanked samples (blanker_mark5.c:126-200)."""
+    N, cof, fs, off = 1 << 18, 3, 32e6, 15625.0
+    spf = 2500
+    nfr = N * cof // spf + 3
+    rng = np.random.default_rng(406)
+    comb = synth.pcal_comb(nfr * spf, fs, 1e6, off, 0.05, rng.uniform(0, 6.28, 16))
+    data = synth.mark5b_stream(rng.standard_normal((16, nfr * spf)) + comb[None, :], 2, 1024)
+    for f, a, b in [(3, 6000, 10000), (40, 0, 10000), (101, 0, 4000), (150, 2000, 3000), (222, 4, 9996)]:
+        data = fill_zone(data, f, a, b, 10016, 16)
+    lay = gpu.layout("mark5b", 16, 2)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 2), (0, 9)), xpols=((0, 1),),
+                          max_run_bytes=len(data), extract_pcal=True, pcal_tonebins=32,
+                          pcal_rotatorlen=2048, samplingfreq=fs, pcal_offset_hz=off)
+    core = gpu.Core(cfg)
+    assert "four-step" in core.plan_info()
+    auto, xp, pc, ns = core.run([data])
+    s = decode_channels(data, "Mark5B-1024-16-2", 16, 2, [2, 9], nfr * spf)
+    assert np.count_nonzero(s[0][40 * spf:41 * spf]) == 0 and np.count_nonzero(s[0][150 * spf:151 * spf]) > 2000
+    ra, rx, rp, nref = oracle_run(s, N, "hann", 1, cof, nxpols=1,
+                                  pcal=dict(tonebins=32, rotatorlen=2048, fs=fs, offset=off))
+    a32, x32, _, _ = _fp32_run(s, N, "hann", 1, cof, nxpols=1)
+    assert ns == nref
+    for k in range(2):
+        _check_auto(auto[0, k], ra[0, k], a32[0, k])
+    norm = np.sqrt(ra[0, 0] * ra[0, 1])
+    floor = np.maximum(norm, np.median(norm))
+    e_x = float(np.max(np.abs(xp[0, 0] - rx[0, 0]) / floor))
+    c_x = float(np.max(np.abs(x32[0, 0] - rx[0, 0]) / floor))
+    assert e_x < max(REL_TOL, 2.0 * c_x), (e_x, c_x)
+    assert np.max(np.abs(pc - rp)) / np.max(np.abs(rp)) < 1e-6
 
 
 def test_dynamic_range_vdif_8bit_2p22(gpu):

@@ -8,7 +8,7 @@ TaskCoreIPP::doMaths on the same decoded samples.
 import numpy as np
 import pytest
 
-from helpers import REL_TOL, decode_channels, oracle_run, payload_of, rel_err_auto, rel_err_xpol
+from helpers import REL_TOL, decode_channels, fill_zone, oracle_run, payload_of, rel_err_auto, rel_err_xpol
 from swspec_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -211,13 +211,6 @@ def test_tcsplit_rejected_without_plan(gpu):
         gpu.Core(cfg)
 
 
-def _fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hdr: int) -> bytes:
-    a = bytearray(raw)
-    base = frame * frame_bytes + hdr
-    a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
-    return bytes(a)
-
-
 @pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
 def test_blanked_mark5b_frames(gpu, prec):
     """Fill-pattern zones (trailing, whole frame, leading, interior) through
@@ -229,7 +222,7 @@ def test_blanked_mark5b_frames(gpu, prec):
     comb = synth.pcal_comb(nfr * 2500, fs, 1e6, off, 0.05, rng.uniform(0, 6.28, 16))
     data = synth.mark5b_stream(rng.standard_normal((16, nfr * 2500)) + comb[None, :], 2, 1024)
     for f, a, b in [(2, 6000, 10000), (5, 0, 10000), (8, 0, 4000), (11, 2000, 3000), (20, 4, 9996)]:
-        data = _fill_zone(data, f, a, b, 10016, 16)
+        data = fill_zone(data, f, a, b, 10016, 16)
     lay = gpu.layout("mark5b", 16, 2)
     precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 2), (0, 9)), xpols=((0, 1),),
@@ -259,8 +252,8 @@ def test_blanked_vdif_frames(gpu):
     codes = synth.quantize_vdif_2bit(rng.standard_normal((4, nfr * spf)), 0.98)
     payload = synth.pack_codes(codes, 2)
     data = synth.vdif_frames(payload, 8000, 4, 2, 4000, invalid={3, 64})
-    data = _fill_zone(data, 5, 0, 8, 8032, 32)
-    data = _fill_zone(data, 90, 7992, 8000, 8032, 32)
+    data = fill_zone(data, 5, 0, 8, 8032, 32)
+    data = fill_zone(data, 90, 7992, 8000, 8032, 32)
     lay = gpu.layout("vdif:8000", 4, 2)
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 1), (0, 3)), xpols=((0, 1),),
                           max_run_bytes=len(data))

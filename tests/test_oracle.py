@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from helpers import fill_zone
 from swspec_b200 import synth
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -50,11 +51,6 @@ def test_decode_matches_golden_vdif():
     assert np.array_equal(mine.view(np.uint32), ref.view(np.uint32))
 
 
-def _fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hdr: int) -> bytes:
-    a = bytearray(raw)
-    base = frame * frame_bytes + hdr
-    a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
-    return bytes(a)
 
 
 @pytest.mark.skipif(O.ref() is None, reason="mark5access not built from the reference sources")
@@ -67,7 +63,7 @@ def test_blanker_matches_live_mark5access():
     zones = [(2, 6000, 10000), (5, 0, 10000), (8, 0, 4000), (11, 2000, 3000), (20, 4, 9996),
              (22, 8, 10000), (24, 0, 9992), (26, 0, 8), (27, 9992, 10000), (28, 0, 4004), (29, 5996, 10000)]
     for f, a, b in zones:
-        data = _fill_zone(data, f, a, b, 10016, 16)
+        data = fill_zone(data, f, a, b, 10016, 16)
     ref, _ = O.m5_decode("Mark5B-1024-16-2", data, 30 * 2500)
     pay = synth.strip_headers(data, 10016, 16)
     for c in range(16):
@@ -76,8 +72,8 @@ def test_blanker_matches_live_mark5access():
     spf = 8000
     codes = synth.quantize_vdif_2bit(rng.standard_normal((4, 8 * spf)), 0.98)
     vd = synth.vdif_frames(synth.pack_codes(codes, 2), 8000, 4, 2, 4000, invalid={3})
-    vd = _fill_zone(vd, 5, 0, 8, 8032, 32)
-    vd = _fill_zone(vd, 6, 7992, 8000, 8032, 32)
+    vd = fill_zone(vd, 5, 0, 8, 8032, 32)
+    vd = fill_zone(vd, 6, 7992, 8000, 8032, 32)
     vref, _ = O.m5_decode("VDIF_8000-64-4-2", vd, 8 * spf)
     inv = O.vdif_invalid_bits(vd, 8032)
     vpay = synth.strip_headers(vd, 8032, 32)
