@@ -93,6 +93,9 @@ struct Schedule {
    int nspec_total = 0;
    long long nsamp = 0;    // chunk sample-times
    int nffts = 0;
+   // cluster path: cluster c runs items [cl_first[c], cl_first[c + 1]), ncl clusters
+   std::vector<int> cl_first;
+   int ncl = 0;
 };
 
 // A schedule built once and kept on the device: runs of the same size and
@@ -105,12 +108,13 @@ struct SchedEntry {
    void *acc_base = nullptr;
    // value
    Schedule sc;
-   DevBuf d_items, d_entries, d_outs, d_pcal_jobs, d_bjobs, d_bitems;
+   DevBuf d_items, d_entries, d_outs, d_pcal_jobs, d_bjobs, d_bitems, d_cl_first;
    std::vector<int4> batches;  // four-step: {job0, njobs, item0, nitems}
    int pcal_word_fold = 0;     // phase-cal jobs allow the word-wise fold
    void release()
    {
       d_items.release();
+      d_cl_first.release();
       d_entries.release();
       d_outs.release();
       d_pcal_jobs.release();
@@ -293,6 +297,61 @@ static long long samples_of(const swsgpu_layout &l, size_t payload_bytes_n)
    return (long long)((payload_bytes_n * 8ull) / (unsigned long long)(l.nchan * l.nbit));
 }
 
+// Cluster path: cluster c gets the jobs [c J / ncl, (c + 1) J / ncl) of the
+// item sequence (J jobs in all), so that every cluster runs the same number
+// of jobs however few items there are (a run's spectrum is at most one item,
+// so a chunk of a few runs has few).  An item that straddles a boundary is
+// split into segments, each with copies of the item's reduction entries.
+static void balance_clusters(int max_clusters, Schedule &sc)
+{
+   long long J = 0;
+   for (const Item &it : sc.items) J += it.nfr;
+   if (J == 0) return;
+   const int ncl = (int)std::max<long long>(1, std::min<long long>(max_clusters, J));
+   std::vector<long long> bnd(ncl + 1);
+   for (int k = 0; k <= ncl; k++) bnd[k] = J * k / ncl;
+   std::vector<Item> items;
+   std::vector<std::vector<int>> parts(sc.items.size());
+   sc.cl_first.assign(ncl + 1, 0);
+   long long pos = 0;  // sequence index of the current item's first job
+   int cl = 0;         // cluster of the next segment
+   for (size_t i = 0; i < sc.items.size(); i++) {
+      const Item &it = sc.items[i];
+      int j = 0;
+      while (j < it.nfr) {
+         while (cl < ncl - 1 && pos + j >= bnd[cl + 1]) {
+            cl++;
+            sc.cl_first[cl] = (int)items.size();
+         }
+         const long long end = std::min<long long>(pos + it.nfr, bnd[cl + 1]);
+         const int n = (int)(end - (pos + j));
+         Item s = it;
+         s.start = it.start + (long long)j * it.step;
+         s.nfr = n;
+         parts[i].push_back((int)items.size());
+         items.push_back(s);
+         j += n;
+      }
+      pos += it.nfr;
+   }
+   for (int k = cl + 1; k <= ncl; k++) sc.cl_first[k] = (int)items.size();
+   std::vector<RedEntry> ents;
+   for (OutVec &o : sc.outs) {
+      const int first = (int)ents.size();
+      for (int k = o.first; k < o.first + o.count; k++)
+         for (int id : parts[sc.entries[k].item]) {
+            RedEntry e = sc.entries[k];
+            e.item = id;
+            ents.push_back(e);
+         }
+      o.first = first;
+      o.count = (int)ents.size() - first;
+   }
+   sc.entries.swap(ents);
+   sc.items.swap(items);
+   sc.ncl = ncl;
+}
+
 // Build items, reduction entries and output vectors for `nruns` runs.
 static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int runs_per_output,
                            float *d_auto, float *d_xpol, float *d_pcal, Schedule &sc)
@@ -442,6 +501,7 @@ static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int ru
       sc.entries.insert(sc.entries.end(), ents.begin(), ents.end());
       sc.outs.push_back(o);
    }
+   if (!h->big) balance_clusters(h->max_clusters, sc);
 }
 
 // ---------------------------------------------------------------------------
@@ -633,7 +693,8 @@ static int get_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int rpo, 
    if ((err = upload(e->d_items, sc.items.data(), sizeof(Item) * sc.items.size())) != cudaSuccess ||
        (err = upload(e->d_entries, sc.entries.data(), sizeof(RedEntry) * sc.entries.size())) != cudaSuccess ||
        (err = upload(e->d_outs, sc.outs.data(), sizeof(OutVec) * sc.outs.size())) != cudaSuccess ||
-       (err = upload(e->d_pcal_jobs, sc.pcal_jobs.data(), sizeof(PcalJob) * sc.pcal_jobs.size())) != cudaSuccess)
+       (err = upload(e->d_pcal_jobs, sc.pcal_jobs.data(), sizeof(PcalJob) * sc.pcal_jobs.size())) != cudaSuccess ||
+       (err = upload(e->d_cl_first, sc.cl_first.data(), sizeof(int) * sc.cl_first.size())) != cudaSuccess)
       return bail(err, "schedule upload");
    if (h->big) {
       std::vector<BigJob> jobs;
@@ -748,6 +809,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          a.code_stream = (const int *)h->d_code_stream.p;
          a.items = (const Item *)se->d_items.p;
          a.nitems = nitems;
+         a.cl_first = sc.cl_first.empty() ? nullptr : (const int *)se->d_cl_first.p;
          a.window = (const float *)h->d_window.p;
          a.twQ = (const float2 *)h->d_twQ.p;
          a.twN = (const float2 *)h->d_twN.p;
@@ -759,7 +821,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          const Plan &pl = h->plan;
          const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
          SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
-         const int ncl = std::max(1, std::min(nitems, h->max_clusters));
+         const int ncl = sc.cl_first.empty() ? std::max(1, std::min(nitems, h->max_clusters)) : sc.ncl;
          cudaLaunchConfig_t cfgl = {};
          cfgl.gridDim = dim3(ncl * pl.P);
          cfgl.blockDim = dim3(pl.T);

@@ -55,6 +55,7 @@ struct SpecArgs {
    const int *code_stream;       // stream of each code array
    const Item *items;
    int nitems;
+   const int *cl_first;          // [clusters + 1]: cluster c runs items [cl_first[c], cl_first[c + 1]) (null: every ncl-th item)
    const float *window;          // [N]
    const float2 *twQ;            // W_Q^m, m < Q
    const float2 *twN;            // W_N^m, m < N/2 (+1)

@@ -477,14 +477,18 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       rbar[i] = dsmem_addr(rx_bar_addr, (uint32_t)i);
    }
 
-   // ---- job sequence of this cluster: items cid, cid+ncl, ...; jobs 0..nfr-1 ----
+   // ---- job sequence of this cluster: its items in order, jobs 0..nfr-1 of each ----
    struct JobPos {
       int it, j;
    };
-   auto job_valid = [&](const JobPos &jp) { return jp.it < a.nitems; };
+   // this cluster's items: the contiguous range [cl_first[cid], cl_first[cid + 1])
+   // when the schedule balanced jobs across clusters, else every ncl-th item
+   const int it_end = a.cl_first ? a.cl_first[cid + 1] : a.nitems;
+   const int it_step = a.cl_first ? 1 : ncl;
+   auto job_valid = [&](const JobPos &jp) { return jp.it < it_end; };
    auto next_job = [&](JobPos jp) {
       if (jp.j + 1 < a.items[jp.it].nfr) return JobPos{jp.it, jp.j + 1};
-      return JobPos{jp.it + ncl, 0};
+      return JobPos{jp.it + it_step, 0};
    };
    // prefetch the codes of job jp into staging slot `slot`
    auto prefetch = [&](const JobPos &jp, int slot) {
@@ -634,7 +638,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       }
    };
 
-   JobPos cur{cid, 0};
+   JobPos cur{a.cl_first ? a.cl_first[cid] : cid, 0};
    if (job_valid(cur)) prefetch(cur, 0);
    cp_async_commit();
    if (job_valid(cur) && job_valid(next_job(cur))) prefetch(next_job(cur), 1);
