@@ -8,16 +8,20 @@
 // (Bailey) with the intermediate in HBM:
 //
 //   column pass  X1[k1][n2] = W_N^(n2 k1) sum_n1 z[n1 N2 + n2] W_N1^(n1 k1)
-//     one CTA per C adjacent columns n2 of one pair job: decode + window +
-//     first radix fused, the N1-point Stockham FFT in shared memory, the
-//     four-step twiddle from two small tables (W_N^(2048 h) W_N^l, both
-//     rounded once from double), 32-byte row segments written to scratch.
+//     a persistent grid over units of C adjacent columns n2 of one pair job.
+//     With codes decimated by N2 (the column layout) a column is one
+//     contiguous code run, staged by cp.async one unit ahead; decode +
+//     window + first radix fused, the N1-point Stockham FFT in shared
+//     memory, and the last pass applies the four-step twiddle (two small
+//     tables, W_N^(2048 h) W_N^l, both rounded once from double) in registers
+//     and writes 32-byte row segments of scratch.
 //   row pass     X[k1 + N1 k2] = sum_n2 X1[k1][n2] W_N2^(n2 k2)
-//     one CTA per row pair (k1, N1 - k1) of one work item: both rows'
-//     N2-point FFTs, the pair separation Z_k / Z_(N-k) -- bin N-k of row k1
-//     sits in row N1 - k1 at column N2 - 1 - k2 -- and the products of every
-//     job of the item accumulated in registers, written once per bin into the
-//     partial rows the reduction kernel scales and combines.
+//     a persistent grid over units (row pair (k1, N1 - k1), work item), the
+//     next job's rows prefetched by cp.async: both rows' N2-point FFTs, the
+//     pair separation Z_k / Z_(N-k) -- bin N-k of row k1 sits in row N1 - k1
+//     at column N2 - 1 - k2 -- and the products of every job of the item
+//     accumulated in registers, written once per bin into the partial rows
+//     the reduction kernel scales and combines.
 //
 // Traffic per pair job: the packed codes once, 8N bytes written and read
 // back; the window and twiddle tables stay in L2.
