@@ -247,8 +247,11 @@ void swsgpu_batch_destroy(swsgpu_batch *b);
 int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
                           int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream);
 
-/* Sizes (bytes) of device scratch and of per-call work for a process_device
- * call with these arguments. */
+/* Device memory (bytes) the core allocates for a process_device call of
+ * `nruns` runs of `run_bytes` as one output group, beyond the caller's
+ * inputs and outputs: code arrays, blank bitmaps, frame validity, per-item
+ * partial spectra, FP64 running sums for groups that span launches and,
+ * for four-step lengths, the column-pass scratch (an upper bound). */
 int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes);
 
 /* Unpack test entry: decode channel `chan` of `nsamp` samples from the

@@ -353,7 +353,7 @@ static void balance_clusters(int max_clusters, Schedule &sc)
 }
 
 // Build items, reduction entries and output vectors for `nruns` runs.
-static void build_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int runs_per_output,
+static void build_schedule(const swsgpu_handle *h, size_t run_bytes, int nruns, int runs_per_output,
                            float *d_auto, float *d_xpol, float *d_pcal, Schedule &sc)
 {
    const swsgpu_config &c = h->cfg;
@@ -709,6 +709,19 @@ static int get_schedule(swsgpu_handle *h, size_t run_bytes, int nruns, int rpo, 
    return SWSGPU_OK;
 }
 
+// Phase decimation of the code arrays: the cluster size, or N2 on the
+// four-step path (the column layout) when every stream's corner turn
+// supports it (*col), else 1.
+static int code_decimation(const swsgpu_handle *h, bool *col)
+{
+   const swsgpu_config &c = h->cfg;
+   bool cl = h->big;
+   for (int s = 0; s < c.num_streams && cl; s++)
+      if (!h->chans_of[s].empty()) cl = unpack_decimation_ok(h->bplan.N2, c.layout[s].nchan, c.layout[s].nbit);
+   *col = cl;
+   return h->big ? (cl ? h->bplan.N2 : 1) : h->plan.P;
+}
+
 // ---------------------------------------------------------------------------
 // pipeline launch for a chunk already in device memory
 // ---------------------------------------------------------------------------
@@ -732,14 +745,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    const int nbit = c.layout[0].nbit;
    const int spw = 32 / nbit;
    const long long nsamp = sc.nsamp;
-   // phase decimation of the code arrays: the cluster size, or N2 on the
-   // four-step path (the column layout) when every stream's corner turn
-   // supports it
-   bool col = h->big;
-   for (int s = 0; s < c.num_streams && col; s++)
-      if (!h->chans_of[s].empty())
-         col = unpack_decimation_ok(h->bplan.N2, c.layout[s].nchan, c.layout[s].nbit);
-   const int D = h->big ? (col ? h->bplan.N2 : 1) : h->plan.P;
+   bool col = false;
+   const int D = code_decimation(h, &col);
    const long long per_phase = (nsamp + D - 1) / D;
    const long long wpp = (per_phase + spw - 1) / spw + 2;  // +2: prefetch may touch one word past
    const long long code_words = (long long)D * wpp;
@@ -1718,13 +1725,38 @@ extern "C" {
 
 int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, size_t *bytes)
 {
-   if (!h || !bytes) return SWSGPU_EINVAL;
+   if (!h || !bytes || nruns < 1) return SWSGPU_EINVAL;
    const swsgpu_config &c = h->cfg;
-   long long nsamp = samples_of(c.layout[0], run_bytes) * nruns;
-   int spw = 32 / c.layout[0].nbit;
-   size_t code = sizeof(uint32_t) * ((nsamp + spw - 1) / spw) * h->code_stream.size();
-   size_t blank = sizeof(uint32_t) * ((nsamp + 31) / 32) * c.num_streams;
-   *bytes = code + blank;
+   const long long nsamp = samples_of(c.layout[0], run_bytes) * nruns;
+   const int spw = 32 / c.layout[0].nbit;
+   const size_t ncode = h->code_stream.size();
+   bool col = false;
+   const int D = code_decimation(h, &col);
+   const long long wpp = ((nsamp + D - 1) / D + spw - 1) / spw + 2;
+   size_t total = sizeof(uint32_t) * (size_t)D * (size_t)wpp * ncode + 64;       // codes
+   if (col && c.extract_pcal)                                                      // undecimated copy
+      total += sizeof(uint32_t) * (size_t)((nsamp + spw - 1) / spw + 2) * ncode + 64;
+   total += sizeof(uint32_t) * (size_t)((nsamp + 31) / 32) * c.num_streams + 16;  // blank bitmaps
+   for (int s = 0; s < c.num_streams; s++)                                         // frame validity
+      total += sizeof(int2) * (size_t)(run_bytes * (size_t)nruns / payload_bytes(c.layout[s]) + 2);
+   // the schedule's partial rows and, on the four-step path, its scratch;
+   // the output addresses are only recorded in the entries, never used here
+   Schedule sc;
+   float *unused = reinterpret_cast<float *>(alignof(float2));
+   build_schedule(h, run_bytes, nruns, nruns, unused, c.num_xpols ? unused : nullptr, nullptr, sc);
+   total += sizeof(float) * 4 * (size_t)h->S * sc.items.size();
+   // FP64 running sums, used when an output group spans launches
+   if (nruns > 1) total += sizeof(double) * (size_t)h->S * (sc.outs.size() + 1);
+   if (h->big) {
+      std::vector<BigJob> jobs;
+      std::vector<BigItem> bitems;
+      std::vector<int4> batches;
+      big_batches(h, sc, jobs, bitems, batches);
+      int max_jobs = 0;
+      for (const int4 &b : batches) max_jobs = std::max(max_jobs, b.y);
+      total += sizeof(float2) * (size_t)c.fft_points * (size_t)max_jobs;
+   }
+   *bytes = total;
    return SWSGPU_OK;
 }
 

@@ -254,6 +254,12 @@ class Core:
         _check(lib().swsgpu_autotune(self.h, iterations), self.h)
         return self.plan_info()
 
+    def workspace_size(self, run_bytes: int, nruns: int) -> int:
+        """Device bytes the core allocates for process_device of nruns runs."""
+        n = C.c_size_t()
+        _check(lib().swsgpu_workspace_size(self.h, run_bytes, nruns, C.byref(n)), self.h)
+        return n.value
+
     def process_device(self, d_raw_ptrs: list[int], run_bytes: int, nruns: int,
                        runs_per_output: int, d_auto: int, d_xpol: int = 0, d_pcal: int = 0,
                        stream: int = 0, d_tones: int = 0) -> None:

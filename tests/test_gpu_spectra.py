@@ -357,3 +357,33 @@ def test_group_runs_chunked_and_per_run(gpu):
         assert np.max(np.abs(a - ra) / ra) < REL_TOL
         assert np.max(np.abs(x - rx) / np.sqrt(ra[0] * ra[1])) < REL_TOL
     assert np.max(np.abs(a1 - a2) / a1) < 1e-6 and np.max(np.abs(a1 - a3) / a1) < 1e-6
+
+
+@pytest.mark.parametrize("N,nbit,fmt,nchan", [(65536, 2, "mark5b", 16), (1 << 20, 8, "vdif:8000", 1)])
+def test_workspace_size_covers_allocations(gpu, N, nbit, fmt, nchan):
+    """swsgpu_workspace_size predicts the device memory a first
+    process_device call takes (codes, bitmaps, partial spectra, four-step
+    scratch): within 10 % + 64 MB above and at least half of it."""
+    import torch
+    lay = gpu.layout(fmt, nchan, nbit, framed=False)
+    run_bytes, nruns = 8 << 20, 4
+    src = ((0, 0), (0, 1)) if nchan > 1 else ((0, 0),)
+    xp = ((0, 1),) if nchan > 1 else ()
+    cfg = gpu.make_config(lay, N, "hann", 1, 1, sources=src, xpols=xp, max_run_bytes=run_bytes,
+                          samplingfreq=32e6, runs_per_output=nruns)
+    core = gpu.Core(cfg)
+    ws = core.workspace_size(run_bytes, nruns)
+    raw = torch.randint(0, 256, (run_bytes * nruns,), dtype=torch.uint8, device="cuda")
+    per_run = run_bytes * 8 // (nchan * nbit) // N
+    S = N // 2 + 1
+    d_auto = torch.zeros(max(1, per_run) * len(src), S, device="cuda")
+    d_xpol = torch.zeros(max(1, per_run) * max(1, len(xp)), S, 2, device="cuda")
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    core.process_device([raw.data_ptr()], run_bytes, nruns, nruns, d_auto.data_ptr(),
+                        d_xpol.data_ptr() if xp else 0)
+    torch.cuda.synchronize()
+    used = free0 - torch.cuda.mem_get_info()[0]
+    core.close()
+    assert used <= ws * 1.1 + (64 << 20), (used, ws)
+    assert ws >= used // 2, (used, ws)
