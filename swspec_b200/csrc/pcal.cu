@@ -107,14 +107,14 @@ __global__ void k_pcal_tones(PcalArgs a)
 // sums flushed to FP64 every 64 periods; the FP64 rotator is applied once
 // per position at the end.
 template <int NBIT>
-__global__ void k_pcal_fold_words(PcalArgs a)
+__global__ void __launch_bounds__(256, 4) k_pcal_fold_words(PcalArgs a)
 {
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
    constexpr int NPAIR = SPW / 2;                 // code pairs per word
    constexpr int PB = 2 * NBIT;                   // bits per pair
    constexpr int NLUT = NBIT < 8 ? 1 << PB : 1;   // pair table (1/2-bit codes)
-   extern __shared__ double pc_smem[];  // [tonebins][2]
+   extern __shared__ double pc_smem[];  // [tonebins][2], then the FP64 sums [SPW][blockDim.x]
    __shared__ float lut[4];
    __shared__ float2 plut[NLUT];
    const PcalJob job = a.jobs[blockIdx.y];
@@ -138,12 +138,14 @@ __global__ void k_pcal_fold_words(PcalArgs a)
       const int ph = t / wpd, wi = t % wpd;
       const uint32_t *base = a.codes + (long long)job.src * a.code_words + (long long)ph * a.wpp +
                              job.start / ((long long)D * SPW) + wi;
+      // per-position FP64 sums in shared memory ([k][thread]: a warp's
+      // accesses are consecutive), leaving the registers to the FP32 sums
+      double *sd = pc_smem + 2 * a.tonebins + threadIdx.x;
       float s[SPW];
-      double sd[SPW];
 #pragma unroll
       for (int k = 0; k < SPW; k++) {
          s[k] = 0.0f;
-         sd[k] = 0.0;
+         sd[k * blockDim.x] = 0.0;
       }
       if (!chk) {
          // four periods' words in flight, two codes per table lookup and
@@ -174,8 +176,8 @@ __global__ void k_pcal_fold_words(PcalArgs a)
             if (((p - p0) & 63) == 60) {
 #pragma unroll
                for (int q = 0; q < NPAIR; q++) {
-                  sd[2 * q] += (double)s2[q].x;
-                  sd[2 * q + 1] += (double)s2[q].y;
+                  sd[2 * q * blockDim.x] += (double)s2[q].x;
+                  sd[(2 * q + 1) * blockDim.x] += (double)s2[q].y;
                   s2[q] = make_float2(0.0f, 0.0f);
                }
             }
@@ -199,7 +201,7 @@ __global__ void k_pcal_fold_words(PcalArgs a)
             if (((p - p0) & 63) == 63) {
 #pragma unroll
                for (int k = 0; k < SPW; k++) {
-                  sd[k] += (double)s[k];
+                  sd[k * blockDim.x] += (double)s[k];
                   s[k] = 0.0f;
                }
             }
@@ -207,7 +209,7 @@ __global__ void k_pcal_fold_words(PcalArgs a)
       }
 #pragma unroll
       for (int k = 0; k < SPW; k++) {
-         const double tot = sd[k] + (double)s[k];
+         const double tot = sd[k * blockDim.x] + (double)s[k];
          const int i = (wi * SPW + k) * D + ph;  // position within the period
          if (i < a.used) {
             double sn, cs;
@@ -243,6 +245,11 @@ int launch_pcal(PcalArgs a, int nbit, cudaStream_t st)
    if (a.word_fold) {
       const int nw = a.rotatorlen / spw;  // threads' words per job (all phases)
       const int T = nw >= 256 ? 256 : ((nw + 31) / 32) * 32;
+      sm += sizeof(double) * (size_t)spw * T;  // per-thread FP64 sums
+      const void *kf = nbit == 1 ? (const void *)k_pcal_fold_words<1>
+                                 : nbit == 2 ? (const void *)k_pcal_fold_words<2> : (const void *)k_pcal_fold_words<8>;
+      if (sm > 48 * 1024 && cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+         return 1;
       if (nbit == 1) k_pcal_fold_words<1><<<grid, T, sm, st>>>(a);
       else if (nbit == 2) k_pcal_fold_words<2><<<grid, T, sm, st>>>(a);
       else k_pcal_fold_words<8><<<grid, T, sm, st>>>(a);
