@@ -103,9 +103,10 @@ __global__ void k_pcal_tones(PcalArgs a)
 // SPW * D: thread t of a job owns code word wi = t mod wpd of phase array
 // ph = t / wpd in every period, i.e. the SPW sample positions
 // i_k = (wi SPW + k) D + ph of the period, and sums them over its block's
-// periods -- one coalesced load and a table decode per sample, FP32 partial
-// sums flushed to FP64 every 64 periods; the FP64 rotator is applied once
-// per position at the end.
+// periods -- one coalesced load per code word (four periods in flight), two
+// codes per pair-table lookup and packed FP32 add, FP32 partial sums
+// flushed every 64 periods into FP64 sums held in shared memory; the FP64
+// rotator is applied once per position at the end.
 template <int NBIT>
 __global__ void __launch_bounds__(256, 4) k_pcal_fold_words(PcalArgs a)
 {
