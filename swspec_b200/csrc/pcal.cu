@@ -7,8 +7,9 @@
 // tonebins; only the first (rotatorlen / tonebins) * tonebins samples of each
 // block are folded (the reference's integer division).  The rotator phase is
 // evaluated in FP64 from the integer position in the period, and products and
-// sums are FP64, so folding 1e5 samples per bin per FFT loses nothing; the
-// folded bins are rounded to FP32 once, at the output.
+// sums are FP64 (the word-wise fold first adds at most 64 samples of a
+// position in FP32), so folding 1e5 samples per bin per FFT loses nothing;
+// the folded bins are rounded to FP32 once, at the output.
 #include "pcal.cuh"
 #include "bins.cuh"
 #include "dft.cuh"
