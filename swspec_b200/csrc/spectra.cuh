@@ -912,12 +912,28 @@ __global__ void k_reduce(const float *__restrict__ partial, int S, const RedEntr
    const OutVec o = ov[blockIdx.y];
    if (k >= S) return;
    float sum = 0.0f, comp = 0.0f;
-   for (int e = o.first; e < o.first + o.count; e++) {
-      const RedEntry r = ent[e];
-      float x = __ldg(partial + ((long long)r.item * 4 + r.prod) * S + k) * r.scale - comp;
-      float t = sum + x;
+   auto add = [&](float v) {
+      const float x = v - comp;
+      const float t = sum + x;
       comp = (t - sum) - x;
       sum = t;
+   };
+   // eight entries' partials in flight, then their Kahan updates in order
+   const int end = o.first + o.count;
+   int e = o.first;
+   for (; e + 8 <= end; e += 8) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+         const RedEntry r = ent[e + u];
+         v[u] = __ldg(partial + ((long long)r.item * 4 + r.prod) * S + k) * r.scale;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) add(v[u]);
+   }
+   for (; e < end; e++) {
+      const RedEntry r = ent[e];
+      add(__ldg(partial + ((long long)r.item * 4 + r.prod) * S + k) * r.scale);
    }
    if (o.acc_mode == 0) {
       o.dst[(long long)k * o.stride] = sum;
