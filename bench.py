@@ -134,7 +134,7 @@ def measured_peaks() -> dict:
 
 def fp32_peak(device: int) -> float | None:
     try:
-        L = C.CDLL(os.path.join(ROOT, "swspec_b200", "libswsprobe.so"))
+        L = C.CDLL(os.path.join(ROOT, "libfp32probe.so"))
         v = C.c_double()
         if L.sws_probe_fp32_tflops(device, C.byref(v)) == 0:
             return v.value

@@ -70,7 +70,10 @@ extern "C" {
 #define SWSGPU_PLAN_FOURSTEP 2
 
 #define SWSGPU_PREC_FP32 0       /* plain FP32 throughout */
-#define SWSGPU_PREC_TCSPLIT 1    /* inner DFT stages on tensor cores, FP16 hi+lo split, FP32 accumulate */
+#define SWSGPU_PREC_TCSPLIT 1    /* the CTA's inner radix-16 levels 2-3 as tcgen05 GEMMs (FP16 hi+lo
+                                    split operands, FP32 accumulators in tensor memory); level 1
+                                    in FP32 registers fused with the decode */
+#define SWSGPU_PREC_TCSPLIT_ALL 2 /* as TCSPLIT with level 1 on the tensor cores too */
 
 #define SWSGPU_MAX_SOURCES 64
 #define SWSGPU_MAX_STREAMS 2
@@ -246,6 +249,26 @@ void swsgpu_batch_destroy(swsgpu_batch *b);
  * spectrum slots.  `cuda_stream` is a cudaStream_t (NULL: the handle's). */
 int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
                           int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream);
+
+/* swsgpu_process_device and swsgpu_batch_launch only queue work.  This waits
+ * for cuda_stream (NULL: the handle's stream) and then reads and clears the
+ * handle's device status word: SWSGPU_ECUDA when a kernel of an earlier call
+ * on this handle gave up a bounded device-side wait (its spectra are
+ * invalid; the GPU context stays usable) or the stream reports a CUDA
+ * error.  swsgpu_wait performs the same check for submitted runs.  No
+ * counterpart in the reference (its join() has no failure path). */
+int swsgpu_sync(swsgpu_handle *h, void *cuda_stream);
+
+/* Fault injection for tests, on the host side of the launch (no device
+ * fault): SWSGPU_INJECT_DROP_EXCHANGE makes the next cluster-kernel launch
+ * of this handle skip the distributed-shared-memory pushes of each
+ * cluster's last job, so every receiving CTA's bounded wait for that job
+ * runs out; the kernel finishes, sets the status word, and the next
+ * swsgpu_wait / swsgpu_sync returns SWSGPU_ECUDA.  One-shot;
+ * SWSGPU_INJECT_NONE cancels it.  SWSGPU_EINVAL on four-step plans. */
+#define SWSGPU_INJECT_NONE 0
+#define SWSGPU_INJECT_DROP_EXCHANGE 1
+int swsgpu_inject(swsgpu_handle *h, int kind);
 
 /* Device memory (bytes) the core allocates for a process_device call of
  * `nruns` runs of `run_bytes` as one output group, beyond the caller's

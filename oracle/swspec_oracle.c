@@ -611,7 +611,8 @@ typedef struct {
    const int *spec_of;
    int f0, f1;
    const float *win;
-   const plan32 *pl;
+   const plan32 *pl;   /* N-point plan (odd N) or the N/2-point plan of the real FFT */
+   const c32 *wn;      /* W_N^k, k < N/2: real-FFT post-processing twiddles (even N) */
    const c32 *rot;
    const int *pairs;
    int nspec;
@@ -626,6 +627,7 @@ static void *orc_worker32(void *arg)
    const int N = c->fft_points, S = N / 2 + 1;
    c32 *d0 = (c32 *)malloc(sizeof(c32) * (size_t)N);
    c32 *d1 = (c32 *)malloc(sizeof(c32) * (size_t)N);
+   const int H = N / 2;
    c32 **X = (c32 **)malloc(sizeof(c32 *) * (size_t)c->num_sources);
    for (int s = 0; s < c->num_sources; s++) X[s] = (c32 *)malloc(sizeof(c32) * (size_t)S);
    int curr = j->curr0;
@@ -643,13 +645,34 @@ static void *orc_worker32(void *arg)
                   pc[2 * b + 1] += x[n0 + i] * j->rot[i].im;
                }
          }
-         /* real FFT as a complex FFT of the windowed samples */
-         for (int n = 0; n < N; n++) {
-            d0[n].re = x[n] * j->win[n];
-            d0[n].im = 0.0f;
+         if (j->wn) {
+            /* real FFT of the windowed samples as one complex FFT of N/2
+             * points: z[n] = x[2n] + i x[2n+1], then
+             * X[k] = (Z[k] + conj Z[H-k])/2 + W_N^k (Z[k] - conj Z[H-k])/(2i) */
+            for (int n = 0; n < H; n++) {
+               d0[n].re = x[2 * n] * j->win[2 * n];
+               d0[n].im = x[2 * n + 1] * j->win[2 * n + 1];
+            }
+            const c32 *Z = fft32(j->pl, d0, d1);
+            X[s][0].re = Z[0].re + Z[0].im; X[s][0].im = 0.0f;
+            X[s][H].re = Z[0].re - Z[0].im; X[s][H].im = 0.0f;
+            for (int k = 1; k < H; k++) {
+               const c32 a = Z[k], b = Z[H - k];
+               const float er = 0.5f * (a.re + b.re), ei = 0.5f * (a.im - b.im);
+               const float o_r = 0.5f * (a.im + b.im), o_i = -0.5f * (a.re - b.re);
+               const c32 w = j->wn[k];
+               X[s][k].re = er + w.re * o_r - w.im * o_i;
+               X[s][k].im = ei + w.re * o_i + w.im * o_r;
+            }
+         } else {
+            /* odd N: complex FFT of the windowed samples */
+            for (int n = 0; n < N; n++) {
+               d0[n].re = x[n] * j->win[n];
+               d0[n].im = 0.0f;
+            }
+            c32 *r = fft32(j->pl, d0, d1);
+            memcpy(X[s], r, sizeof(c32) * (size_t)S);
          }
-         c32 *r = fft32(j->pl, d0, d1);
-         memcpy(X[s], r, sizeof(c32) * (size_t)S);
          curr++;
          float *oa = j->auto_acc + ((size_t)sp * c->num_sources + s) * S;
          for (int k = 0; k < S; k++) oa[k] += X[s][k].re * X[s][k].re + X[s][k].im * X[s][k].im;
@@ -686,7 +709,18 @@ int orc_domaths32(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
    orc_schedule(c, nsamp, starts, spec_of, nf, &nspec, &partial);
    float *win = (float *)malloc(sizeof(float) * (size_t)N);
    orc_window(c->window, N, win);
-   plan32 *pl = plan32_new(N);
+   /* even N: the real transform runs as an N/2-point complex FFT (the IPP
+    * core's ippsDFTFwd_RToPerm_32f is a real-input transform too) */
+   plan32 *pl = plan32_new(N % 2 == 0 ? N / 2 : N);
+   c32 *wn = NULL;
+   if (N % 2 == 0) {
+      wn = (c32 *)malloc(sizeof(c32) * (size_t)(N / 2));
+      for (int k = 0; k < N / 2; k++) {
+         double a = -2.0 * M_PI * (double)k / (double)N;
+         wn[k].re = (float)cos(a);
+         wn[k].im = (float)sin(a);
+      }
+   }
    int *pairs = (int *)malloc(sizeof(int) * 2 * (size_t)(c->num_xpols + 1));
    orc_xpol_pairs(c->num_sources, c->num_xpols, pairs);
    c32 *rot = NULL;
@@ -709,7 +743,7 @@ int orc_domaths32(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
       j->c = c; j->samples = samples; j->starts = starts; j->spec_of = spec_of;
       j->f0 = (int)((long long)nf * t / nt);
       j->f1 = (int)((long long)nf * (t + 1) / nt);
-      j->win = win; j->pl = pl; j->rot = rot; j->pairs = pairs; j->nspec = nspec;
+      j->win = win; j->pl = pl; j->wn = wn; j->rot = rot; j->pairs = pairs; j->nspec = nspec;
       j->auto_acc = (float *)calloc(na + 1, sizeof(float));
       j->xpol_acc = (float *)calloc(nx + 1, sizeof(float));
       j->pcal_acc = (float *)calloc(np + 1, sizeof(float));
@@ -730,7 +764,7 @@ int orc_domaths32(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
    float sc = (float)(1.0 / c->core_overlapped_ffts);
    for (size_t i = 0; i < (size_t)nfull * c->num_sources * S; i++) out_auto[i] *= sc;
    for (size_t i = 0; i < 2 * (size_t)nfull * c->num_xpols * S; i++) out_xpol[i] *= sc;
-   free(jobs); free(th); free(starts); free(spec_of); free(win); free(pairs); free(rot);
+   free(jobs); free(th); free(starts); free(spec_of); free(win); free(pairs); free(rot); free(wn);
    plan32_free(pl);
    return nspec;
 }

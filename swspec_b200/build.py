@@ -71,10 +71,11 @@ def build_cuda(verbose: bool = False) -> str:
 
 
 def build_probe() -> str:
-    """FP32 FMA probe used by the benchmark (not part of the C ABI)."""
+    """The benchmark's FP32 FMA peak probe (fp32_probe.cu beside bench.py;
+    not part of the library or its C ABI)."""
     os.makedirs(BUILD, exist_ok=True)
-    out = os.path.join(PKG, "libswsprobe.so")
-    src = os.path.join(CSRC, "probe_fp32.cu")
+    out = os.path.join(ROOT, "libfp32probe.so")
+    src = os.path.join(ROOT, "fp32_probe.cu")
     if os.path.exists(src) and _newer(out, [src]):
         _run([NVCC] + NVFLAGS + ["-shared", "-o", out, src])
     return out
@@ -100,6 +101,13 @@ def build_host() -> str:
     return out
 
 
+def build_refcore() -> None:
+    """The reference's own spectrometer program with TaskCoreCUDA as its core
+    (swspec_b200/refcore/Makefile); built only where the reference sources
+    are present, the result travels with the repository snapshot."""
+    subprocess.run(["make", "-s", "-C", os.path.join(PKG, "refcore")], check=True)
+
+
 def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
 
@@ -108,6 +116,7 @@ def build_all() -> None:
     build_cuda()
     build_probe()
     build_host()
+    build_refcore()
     build_oracle()
 
 

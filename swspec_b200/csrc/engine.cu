@@ -39,6 +39,18 @@ using namespace sws;
 
 static thread_local std::string g_create_error;
 
+// The kernel and shared-memory size of a cluster plan's form.
+static SpecKernel plan_kernel(const Plan &pl, int precision, int nbi)
+{
+   return precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi]
+          : precision == SWSGPU_PREC_TCSPLIT_ALL ? pl.kern_tc2[nbi] : pl.kern[nbi];
+}
+static size_t plan_smem(const Plan &pl, int precision, int nbi)
+{
+   return precision == SWSGPU_PREC_TCSPLIT ? pl.smem_tc[nbi]
+          : precision == SWSGPU_PREC_TCSPLIT_ALL ? pl.smem_tc2[nbi] : pl.smem[nbi];
+}
+
 
 struct DevBuf {
    void *p = nullptr;
@@ -162,6 +174,7 @@ struct swsgpu_handle {
    bool pending = false;
    int pending_nspec = 0;
    int last_launches = 0;
+   int inject = SWSGPU_INJECT_NONE;  // one-shot fault injection for the next cluster launch
    // code arrays: one per distinct (stream, channel)
    std::vector<int> code_stream, code_chan;
    std::vector<int> src_code;     // source -> code index
@@ -825,14 +838,16 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          a.S = S;
          a.levels = level_table(c.layout[0].format, nbit);
          a.status = (int *)h->d_status.p;
+         a.drop_last_exchange = h->inject == SWSGPU_INJECT_DROP_EXCHANGE;
+         h->inject = SWSGPU_INJECT_NONE;
          const Plan &pl = h->plan;
          const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
-         SpecKernel kern = c.precision == SWSGPU_PREC_TCSPLIT ? pl.kern_tc[nbi] : pl.kern[nbi];
+         SpecKernel kern = plan_kernel(pl, c.precision, nbi);
          const int ncl = sc.cl_first.empty() ? std::max(1, std::min(nitems, h->max_clusters)) : sc.ncl;
          cudaLaunchConfig_t cfgl = {};
          cfgl.gridDim = dim3(ncl * pl.P);
          cfgl.blockDim = dim3(pl.T);
-         cfgl.dynamicSmemBytes = c.precision == SWSGPU_PREC_TCSPLIT ? pl.smem_tc[nbi] : pl.smem[nbi];
+         cfgl.dynamicSmemBytes = plan_smem(pl, c.precision, nbi);
          cfgl.stream = st;
          cudaLaunchAttribute attr[1];
          attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1009,7 +1024,11 @@ static int validate_config(const swsgpu_config *c, std::string &why)
       for (int k = 0; k < 2; k++)
          if (c->xpol_pair[x][k] < 0 || c->xpol_pair[x][k] >= c->num_sources) { why = "xpol_pair out of range"; return 0; }
    if (c->window < 0 || c->window > SWSGPU_WIN_BLACKMANHARRIS) { why = "unknown window"; return 0; }
-   if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT) { why = "unknown precision"; return 0; }
+   if (c->precision != SWSGPU_PREC_FP32 && c->precision != SWSGPU_PREC_TCSPLIT &&
+       c->precision != SWSGPU_PREC_TCSPLIT_ALL) {
+      why = "unknown precision";
+      return 0;
+   }
    if (c->runs_per_output < 0) { why = "runs_per_output must be >= 0"; return 0; }
    if (c->plan_family < SWSGPU_PLAN_DEFAULT || c->plan_family > SWSGPU_PLAN_FOURSTEP) { why = "unknown plan_family"; return 0; }
    if (c->plan_candidate < 0) { why = "plan_candidate must be >= 0"; return 0; }
@@ -1049,7 +1068,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    }
    if (!cluster_plan && !four_step)
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
-   if (cfg->precision == SWSGPU_PREC_TCSPLIT && !(cluster_plan && plan.kern_tc[1]))
+   if (cfg->precision != SWSGPU_PREC_FP32 && !(cluster_plan && plan.kern_tc[1]))
       return fail(nullptr, SWSGPU_EINVAL,
                   "tensor-core split form not available for fft_points " + std::to_string(cfg->fft_points));
    int ndev = 0;
@@ -1221,8 +1240,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       *out = h;
       return SWSGPU_OK;
    }
-   SpecKernel kern = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.kern_tc[nbi] : plan.kern[nbi];
-   const size_t smem = cfg->precision == SWSGPU_PREC_TCSPLIT ? plan.smem_tc[nbi] : plan.smem[nbi];
+   SpecKernel kern = plan_kernel(plan, cfg->precision, nbi);
+   const size_t smem = plan_smem(plan, cfg->precision, nbi);
    CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
    if (plan.P > 8)
       CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1484,6 +1503,33 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
       }
    }
    if (nspectra) *nspectra = h->pending_nspec;
+   return SWSGPU_OK;
+}
+
+int swsgpu_sync(swsgpu_handle *h, void *cuda_stream)
+{
+   if (!h) return SWSGPU_EINVAL;
+   CK(h, cudaSetDevice(h->device));
+   CK(h, cudaStreamSynchronize(cuda_stream ? (cudaStream_t)cuda_stream : h->stream));
+   if (h->d_status.p) {
+      int st = 0;
+      CK(h, cudaMemcpy(&st, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (st) {
+         CK(h, cudaMemset(h->d_status.p, 0, sizeof(int)));
+         return fail(h, SWSGPU_ECUDA, "a device-side wait for cluster data gave up; the spectra are invalid");
+      }
+   }
+   return SWSGPU_OK;
+}
+
+int swsgpu_inject(swsgpu_handle *h, int kind)
+{
+   if (!h) return SWSGPU_EINVAL;
+   if (kind != SWSGPU_INJECT_NONE && kind != SWSGPU_INJECT_DROP_EXCHANGE)
+      return fail(h, SWSGPU_EINVAL, "unknown fault-injection kind");
+   if (kind == SWSGPU_INJECT_DROP_EXCHANGE && h->big)
+      return fail(h, SWSGPU_EINVAL, "the four-step path has no cluster exchange to drop");
+   h->inject = kind;
    return SWSGPU_OK;
 }
 
@@ -1866,7 +1912,9 @@ int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len)
    } else {
       snprintf(buf, len, "cluster %d x %d (CTAs x points), radices %d/%d/%d, %s form", h->plan.P, h->plan.Q,
                h->plan.R1, h->plan.R2, h->plan.R3,
-               h->cfg.precision == SWSGPU_PREC_TCSPLIT ? "tensor-core split" : "FP32");
+               h->cfg.precision == SWSGPU_PREC_TCSPLIT       ? "tensor-core split (tcgen05 levels 2-3)"
+               : h->cfg.precision == SWSGPU_PREC_TCSPLIT_ALL ? "tensor-core split (tcgen05 levels 1-3)"
+                                                             : "FP32");
    }
    return SWSGPU_OK;
 }

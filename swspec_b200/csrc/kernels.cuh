@@ -63,6 +63,7 @@ struct SpecArgs {
    int N, S;
    float4 levels;                // level table for 1/2-bit codes
    int *status;                  // set to 1 when a bounded wait gave up (null: not reported)
+   int drop_last_exchange;       // fault injection: the last job of each cluster pushes nothing
 };
 
 // Reduction of item partial sums into output spectra.

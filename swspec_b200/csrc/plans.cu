@@ -15,14 +15,17 @@ namespace sws {
 #define SWS_SMEM(P_, Q_, R1_, R2_, R3_, PREC_)                                                    \
    {spectra_smem<P_, Q_, R1_, R2_, R3_, 1, PREC_>(), spectra_smem<P_, Q_, R1_, R2_, R3_, 2, PREC_>(), \
     spectra_smem<P_, Q_, R1_, R2_, R3_, 8, PREC_>()}
-// plans with a tensor-core split form (Q = 4096 = 16 x 256, T = 256)
+// plans with tensor-core split forms (Q = 4096 = 16 x 16 x 16, T = 256):
+// levels 2-3 on tcgen05 (level 1 in FP32 with the decode), or all three
 #define SWS_PLAN_TC(N_, P_, MINB_)                                                                \
    {N_, P_, 4096, 256, 16, 16, 16, SWS_KERN(P_, 4096, 256, 16, 16, 16, MINB_, 0),                 \
     SWS_SMEM(P_, 4096, 16, 16, 16, 0), SWS_KERN(P_, 4096, 256, 16, 16, 16, MINB_, 1),            \
-    SWS_SMEM(P_, 4096, 16, 16, 16, 1)}
+    SWS_SMEM(P_, 4096, 16, 16, 16, 1), SWS_KERN(P_, 4096, 256, 16, 16, 16, MINB_, 2),            \
+    SWS_SMEM(P_, 4096, 16, 16, 16, 2)}
 #define SWS_PLAN(N_, P_, Q_, T_, R1_, R2_, R3_, MINB_)                                            \
    {N_, P_, Q_, T_, R1_, R2_, R3_, SWS_KERN(P_, Q_, T_, R1_, R2_, R3_, MINB_, 0),                 \
-    SWS_SMEM(P_, Q_, R1_, R2_, R3_, 0), {nullptr, nullptr, nullptr}, {0, 0, 0}}
+    SWS_SMEM(P_, Q_, R1_, R2_, R3_, 0), {nullptr, nullptr, nullptr}, {0, 0, 0},                  \
+    {nullptr, nullptr, nullptr}, {0, 0, 0}}
 
 static const Plan kPlans[] = {
     SWS_PLAN_TC(65536, 16, 2),

@@ -35,6 +35,7 @@
 #include <cuda_fp16.h>
 
 #include "dft.cuh"
+#include "tc.cuh"
 #include "kernels.cuh"
 #include "bins.cuh"
 
@@ -282,17 +283,32 @@ __host__ __device__ constexpr int stage_slots()
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-core split-precision stages (mma.sync m16n8k16, f16 x f16 -> f32)
+// Tensor-core split-precision stages (tcgen05.mma, FP16 x FP16 -> FP32 in TMEM)
 // ---------------------------------------------------------------------------
-// A 256-point DFT is done as 16 x 16: stage 1 DFT16 over n2 of x[n1 + 16 n2]
-// for the 16 columns n1, twiddle W_256^{n1 m2}, stage 2 DFT16 over n1, giving
-// X[16 m1 + m2].  Each complex DFT16 is the real block product
-//   [Re; Im] = [[Fr, -Fi], [Fi, Fr]] [Re; Im],
-// and every real product A.B is evaluated as Ah.Bh + Ah.Bl + Al.Bh with
-// FP16 hi/lo splits (hi = rn(x), lo = rn(x - hi)) and FP32 accumulation --
-// about 22 significant bits, FP32-level accuracy.  The D fragment of stage 1
-// (rows m2, columns n1) is exactly the B fragment stage 2 needs (rows n1,
-// columns m2), so the data never leaves registers between the two stages.
+// The CTA's Q = 4096-point transform is three radix-16 levels,
+// q = q0 + 16 q1 + 256 q2 and kappa = k0 + 16 k1 + 256 k2:
+//   level 1: DFT16 over q2 for each row r1 = q0 + 16 q1, then W_4096^{r1 k0};
+//   level 2: DFT16 over q1 for each row (k0, q0), then W_256^{q0 k1};
+//   level 3: DFT16 over q0 for each row (k1, k0) -> F[k0 + 16 k1 + 256 k2].
+// Each level is the real GEMM  D[row][n] = sum_k A[row][k] B[k][n]  with
+// 256 rows (two M = 128 tiles), K = 64 and N = 64:
+//   A = [Re x hi | Im x hi | Re x lo | Im x lo]          (16 values each)
+//   B = [[Mh | Ml]; [Mh | 0]],  M = s * [[C, -S]; [S, C]]-form of the DFT16
+// so that D[:, n] + D[:, n + 32] = Ah Mh + Al Mh + Ah Ml (n < 32): the
+// three products of an FP16 hi/lo split (hi = rn(x), lo = rn(x - hi)),
+// about 22 significant bits, accumulated in FP32.  s = 1/4 keeps the FP16
+// operands in range; the push multiplies the powers of 4 back (exact).
+// The accumulators land in tensor memory, one TMEM lane per row, which is
+// the thread's own row in the epilogue (warp w reads lanes 32 (w % 4) + i of
+// tile w / 4, so row = threadIdx.x).  The epilogue loads its row's 16
+// complex outputs, applies the next level's FP32 twiddle, splits them and
+// stores them as the next level's operand in MN-major order: the level's
+// output digit becomes the fastest row digit of the next level, so the
+// thread's 16 values are 16 consecutive rows of one K column (two 16-byte
+// core-matrix rows per K value and part).
+// Level 1 is either on the tensor cores (operand = decoded, windowed
+// samples, K-major rows) or an FP32 radix-16 in registers fused with the
+// decode (PREC 1).
 
 // hi/lo split of two floats into f16x2 words (lower half = first value)
 __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
@@ -304,82 +320,132 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
    lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+__device__ __forceinline__ void st_shared_v4(uint32_t saddr, const uint32_t (&v)[4])
 {
-   asm volatile(
-       "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-       "{%0,%1,%2,%3};\n"
-       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(saddr), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+                "r"(v[3])
+                : "memory");
 }
 
-// A fragments of the DFT16 matrix F[m][n] = W_16^{m n}: real part, imaginary
-// part and its negation, each split hi/lo.
-struct Dft16Frags {
-   uint32_t rh[4], rl[4], ih[4], il[4], nih[4], nil[4];
-};
+// Operand geometry: 256 rows x 64 K values of FP16.
+// MN-major (levels 2, 3): core matrices 8 K x 8 rows; rows step by SBO =
+// 144 bytes (16 bytes of padding per core matrix), K groups by LBO = 32 x 144.
+// K-major (level 1 on tensor cores): core matrices 8 rows x 8 K; K groups
+// step by 128 bytes, row groups by 1024.
+constexpr uint32_t TC_MN_SBO = 144, TC_MN_LBO = 32 * TC_MN_SBO;
+constexpr uint32_t TC_K_LBO = 128, TC_K_SBO = 1024;
+constexpr uint32_t TC_OPND_BYTES = 8 * TC_MN_LBO;  // 36864 >= 32768 (K-major)
+constexpr uint32_t TC_BMAT_BYTES = 64 * 64 * 2;
+constexpr uint32_t TC_TMEM_COLS = 128;             // two M = 128 tiles x N = 64 FP32 columns
 
-__device__ __forceinline__ void make_dft16_frags(Dft16Frags &f)
+// 16 complex values of rows m0 .. m0+15 (m0 % 16 == 0), K column kq of the
+// real part and kq + 16 of the imaginary part (hi parts; lo parts at +32),
+// into an MN-major operand.
+__device__ __forceinline__ void store_mn16(uint32_t opnd, int m0, int kq, const float2 (&v)[16])
 {
-   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-   // fragment element (row, col) pairs: a0 (g, 2t..2t+1), a1 (g+8, ...), a2 (g, 2t+8..), a3 (g+8, 2t+8..)
 #pragma unroll
-   for (int i = 0; i < 4; i++) {
-      const int row = g + ((i & 1) ? 8 : 0);
-      const int col = 2 * t + ((i & 2) ? 8 : 0);
-      float re[2], im[2];
+   for (int c = 0; c < 2; c++) {
 #pragma unroll
-      for (int e = 0; e < 2; e++) {
-         double sn, cs;
-         sincospi(-2.0 * (double)((row * (col + e)) & 15) / 16.0, &sn, &cs);
-         re[e] = (float)cs;
-         im[e] = (float)sn;
+      for (int g = 0; g < 2; g++) {
+         uint32_t hi[4], lo[4];
+#pragma unroll
+         for (int e = 0; e < 4; e++) {
+            const float2 x = v[8 * g + 2 * e], y = v[8 * g + 2 * e + 1];
+            split2(c ? x.y : x.x, c ? y.y : y.x, hi[e], lo[e]);
+         }
+         const int m = m0 + 8 * g;
+         st_shared_v4(opnd + tc::mnmajor_off(m, 16 * c + kq, TC_MN_LBO, TC_MN_SBO), hi);
+         st_shared_v4(opnd + tc::mnmajor_off(m, 32 + 16 * c + kq, TC_MN_LBO, TC_MN_SBO), lo);
       }
-      split2(re[0], re[1], f.rh[i], f.rl[i]);
-      split2(im[0], im[1], f.ih[i], f.il[i]);
-      split2(-im[0], -im[1], f.nih[i], f.nil[i]);
    }
 }
 
-// One complex DFT16 stage on an 8-column tile: inputs as B fragments
-// (re/im x hi/lo, b0 rows 2t..2t+1, b1 rows 2t+8..2t+9), outputs D (re, im).
-__device__ __forceinline__ void dft16_mma(const Dft16Frags &f, const uint32_t (&brh)[2],
-                                          const uint32_t (&brl)[2], const uint32_t (&bih)[2],
-                                          const uint32_t (&bil)[2], float (&dre)[4], float (&dim)[4])
+// Row `row` of the K-major level-1 operand from its 16 complex samples.
+__device__ __forceinline__ void store_k16(uint32_t opnd, int row, const float2 (&v)[16])
 {
-   // four independent accumulation chains of three products each
-   float are[4] = {0, 0, 0, 0}, bre[4] = {0, 0, 0, 0}, aim[4] = {0, 0, 0, 0}, bim[4] = {0, 0, 0, 0};
-   mma16816(are, f.rh, brl[0], brl[1]);
-   mma16816(bre, f.nih, bil[0], bil[1]);
-   mma16816(aim, f.ih, brl[0], brl[1]);
-   mma16816(bim, f.rh, bil[0], bil[1]);
-   mma16816(are, f.rl, brh[0], brh[1]);
-   mma16816(bre, f.nil, bih[0], bih[1]);
-   mma16816(aim, f.il, brh[0], brh[1]);
-   mma16816(bim, f.rl, bih[0], bih[1]);
-   mma16816(are, f.rh, brh[0], brh[1]);
-   mma16816(bre, f.nih, bih[0], bih[1]);
-   mma16816(aim, f.ih, brh[0], brh[1]);
-   mma16816(bim, f.rh, bih[0], bih[1]);
 #pragma unroll
-   for (int i = 0; i < 4; i++) {
-      dre[i] = are[i] + bre[i];
-      dim[i] = aim[i] + bim[i];
+   for (int c = 0; c < 2; c++) {
+#pragma unroll
+      for (int g = 0; g < 2; g++) {
+         uint32_t hi[4], lo[4];
+#pragma unroll
+         for (int e = 0; e < 4; e++) {
+            const float2 x = v[8 * g + 2 * e], y = v[8 * g + 2 * e + 1];
+            split2(c ? x.y : x.x, c ? y.y : y.x, hi[e], lo[e]);
+         }
+         st_shared_v4(opnd + tc::kmajor_off(row, 16 * c + 8 * g, TC_K_LBO, TC_K_SBO), hi);
+         st_shared_v4(opnd + tc::kmajor_off(row, 32 + 16 * c + 8 * g, TC_K_LBO, TC_K_SBO), lo);
+      }
    }
 }
 
-// Padded row layout of the 16 x 256 intermediate: 4 float2 of padding per 32
-// keeps the B-fragment loads (lanes at n1 = g, n2 = 2t..) bank-conflict free.
-__device__ __forceinline__ int ridx(int q2) { return q2 + 4 * (q2 >> 5); }
-constexpr int TC_ROW = 256 + 32;
+// The B operand (K-major: 64 rows n of 64 K values) of the scaled DFT16.
+__device__ __forceinline__ void fill_dft16_bmat(uint32_t bmat, int T)
+{
+   for (int i = threadIdx.x; i < 64 * 64; i += T) {
+      const int n = i >> 6, k = i & 63;
+      const int part = k >> 5, cin = (k >> 4) & 1, j = k & 15;
+      const int half = n >> 5, cout = (n >> 4) & 1, kk = n & 15;
+      double sn, cs;
+      sincospi(-2.0 * (double)((j * kk) & 15) / 16.0, &sn, &cs);  // W_16^{j kk} = cs + i sn
+      // y = x W: Re y = Re x cs - Im x sn, Im y = Re x sn + Im x cs
+      const double m = 0.25 * ((cin == cout) ? cs : (cin == 0 ? sn : -sn));
+      const __half h = __double2half(m);
+      const __half l = __double2half(m - (double)__half2float(h));
+      const __half val = (part == 0) ? (half == 0 ? h : l) : (half == 0 ? h : __double2half(0.0));
+      asm volatile("st.shared.b16 [%0], %1;\n" ::"r"(bmat + tc::kmajor_off(n, k, 128, 1024)),
+                   "h"(*reinterpret_cast<const unsigned short *>(&val))
+                   : "memory");
+   }
+}
+
+// Issue one level: two M = 128 tiles x four K = 16 steps into TMEM columns
+// [0, 64) and [64, 128); one thread.
+__device__ __forceinline__ void tc_issue_level(uint32_t tmem, uint32_t opnd, uint32_t bmat, bool kmajor,
+                                               uint32_t mbar)
+{
+   tc::fence_after();
+   const uint32_t id = tc::idesc_f16(128, 64, !kmajor, false);
+#pragma unroll
+   for (int t = 0; t < 2; t++) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+         const uint32_t a0 = kmajor ? opnd + (uint32_t)t * 16u * TC_K_SBO + (uint32_t)kk * 2u * TC_K_LBO
+                                    : opnd + (uint32_t)t * 16u * TC_MN_SBO + (uint32_t)kk * 2u * TC_MN_LBO;
+         const uint64_t ad = kmajor ? tc::smem_desc(a0, TC_K_LBO, TC_K_SBO) : tc::smem_desc(a0, TC_MN_LBO, TC_MN_SBO);
+         const uint64_t bd = tc::smem_desc(bmat + (uint32_t)kk * 256u, 128u, 1024u);
+         tc::mma_f16(tmem + 64u * (uint32_t)t, ad, bd, id, kk > 0);
+      }
+   }
+   tc::commit(mbar);
+}
+
+// The calling thread's row (= threadIdx.x) of a level's output: 16 complex values.
+__device__ __forceinline__ void tc_load_row(uint32_t tmem, float2 (&y)[16])
+{
+   const int w = threadIdx.x >> 5;
+   const uint32_t ta = tmem + ((uint32_t)(32 * (w & 3)) << 16) + 64u * (uint32_t)(w >> 2);
+   float a[16], b[16];
+   tc::ld16(ta, a);
+   tc::ld16(ta + 32, b);
+   tc::ld_wait();
+#pragma unroll
+   for (int i = 0; i < 16; i++) y[i].x = a[i] + b[i];
+   tc::ld16(ta + 16, a);
+   tc::ld16(ta + 48, b);
+   tc::ld_wait();
+#pragma unroll
+   for (int i = 0; i < 16; i++) y[i].y = a[i] + b[i];
+}
 
 // Shared memory layout of a plan: byte offsets of every region, used both
 // for the kernel's pointers and for the host-side launch size.
 template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
 struct SmemLayout {
-   static constexpr size_t BUFN = PREC ? 16 * TC_ROW : (Q + Q / 16);
-   static constexpr size_t buf = 0;                                             // FFT buffer (float2)
-   static constexpr size_t w256 = buf + BUFN * 8;                               // W_256 table
+   static constexpr size_t BUFB = PREC ? (size_t)TC_OPND_BYTES : (size_t)(Q + Q / 16) * 8;
+   static constexpr size_t buf = 0;                                             // FFT buffer / operand
+   static constexpr size_t bmat = buf + BUFB;                                   // DFT16 B operand
+   static constexpr size_t w256 = bmat + (PREC ? TC_BMAT_BYTES : 0);            // W_256 table
    static constexpr size_t rbuf = w256 + (PREC ? 256 : 0) * 8;                  // receive [P][sides]
    static constexpr size_t wsl = rbuf + (size_t)P * (Q / P) * 8;                // window slice (float)
    static constexpr size_t tw2 = wsl + (size_t)Q * 4;                           // pass-2 twiddles
@@ -398,8 +464,9 @@ __host__ __device__ constexpr size_t spectra_smem()
 template <int P, int Q, int T, int R1, int R2, int R3, int NBIT, int MINB, int PREC>
 __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 {
-   // PREC 1: passes 2 and 3 (two radix-16 levels) as in-register 256-point
-   // DFTs on tensor cores; needs Q = 16 * 256 and one 256-row pair per warp.
+   // PREC 1: levels 2 and 3 of the CTA's 4096-point transform on tensor
+   // cores (tcgen05), level 1 in FP32 registers fused with the decode;
+   // PREC 2: all three levels on tensor cores.  One operand row per thread.
    static_assert(PREC == 0 || (Q == 4096 && R1 == 16 && R2 == 16 && R3 == 16 && T == 256),
                  "tensor-core form plan");
    static_assert(R1 * R2 * R3 == Q, "radix plan must multiply to Q");
@@ -448,10 +515,18 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    for (int q = tid; q < Q; q += T) wsl[q] = __ldg(a.window + rank + (long long)P * q);
    if constexpr (PREC == 0) fill_pass_twiddles2<Q, R2, R1>(tw2, a.twQ, T);
    fill_pass_bases<Q, R3, NS3>(tw3, a.twQ, T);
-   if constexpr (PREC == 1)
+   const uint32_t opnd_addr = (uint32_t)__cvta_generic_to_shared(smem + L::buf);
+   const uint32_t bmat_addr = (uint32_t)__cvta_generic_to_shared(smem + L::bmat);
+   __shared__ uint32_t tmem_holder;
+   __shared__ __align__(8) unsigned long long mma_bar;
+   const uint32_t mma_bar_addr = (uint32_t)__cvta_generic_to_shared(&mma_bar);
+   if constexpr (PREC >= 1) {
       for (int i = tid; i < 256; i += T) w256[i] = __ldg(a.twQ + 16 * i);  // W_256^i = W_4096^{16 i}
-   Dft16Frags F16;
-   if constexpr (PREC == 1) make_dft16_frags(F16);
+      fill_dft16_bmat(bmat_addr, T);
+      tc::fence_async_smem();
+      if (tid < 32) tc::tmem_alloc((uint32_t)__cvta_generic_to_shared(&tmem_holder), TC_TMEM_COLS);
+      if (tid == 0) tc::mbar_init_cta(mma_bar_addr, 1);
+   }
    // twc[i*UC + u_local] = W_N^{2^i u}, read by both sides of pair u
    for (int idx = tid; idx < nbases(P) * UC; idx += T) {
       const int i = idx / UC, uu = idx % UC;
@@ -586,7 +661,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                      }
                      v[b][r] = make_float2(lv.x * w, lv.y * w);
                   }
-                  DFT<R1>::run(v[b]);
+                  if constexpr (PREC != 2) DFT<R1>::run(v[b]);
                   continue;
                }
             }
@@ -613,7 +688,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                }
                v[b][r] = make_float2(xa * w, xb * w);
             }
-            DFT<R1>::run(v[b]);
+            if constexpr (PREC != 2) DFT<R1>::run(v[b]);
          }
       }
       if constexpr (PREC == 0) {
@@ -626,15 +701,22 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                   buf[(R1 == 16) ? jj * 17 + r : pidx(jj * R1 + r)] = v[b][r];  // pidx(16 jj + r), r < 16
             }
          }
-      } else {
-         // four-step twiddle W_Q^{q2 k1} (q2 = tid, k1 = r), then rows y[k1][q2];
-         // tw3 holds W_Q^{2^i q2}, the same bases the FP32 form's last pass uses
+      } else if constexpr (PREC == 1) {
+         // level 1 done in registers: row r1 = tid holds k0 = r; twiddle
+         // W_4096^{r1 k0} (tw3 holds W_Q^{2^i r1}, the bases the FP32 form's
+         // last pass uses) and store as level 2's operand, rows k0 + 16 q0,
+         // K column q1 (r1 = q0 + 16 q1)
          float2 base[nbases(R3)];
 #pragma unroll
          for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
          twiddle_by_powers<R1>(v[0], base);
-#pragma unroll
-         for (int r = 0; r < R1; r++) buf[r * TC_ROW + ridx(tid)] = v[0][r];
+         store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, v[0]);
+         tc::fence_async_smem();
+      } else {
+         // the decoded, windowed samples z[r1 + 256 q2] as row r1 = tid of
+         // level 1's K-major operand
+         store_k16(opnd_addr, tid, v[0]);
+         tc::fence_async_smem();
       }
    };
 
@@ -643,7 +725,14 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    cp_async_commit();
    if (job_valid(cur) && job_valid(next_job(cur))) prefetch(next_job(cur), 1);
    cp_async_commit();
+   if constexpr (PREC >= 1) tc::fence_before();
    __syncthreads();      // tables visible
+   uint32_t tmem_base = 0, mma_par = 0;
+   bool tc_gave_up = false;
+   if constexpr (PREC >= 1) {
+      tc::fence_after();
+      tmem_base = tmem_holder;
+   }
    cluster_arrive();     // pairs with the wait before the first job's pushes
 
    float acc[SPT][NB][4];
@@ -667,6 +756,9 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       const bool has_b = mode != MODE_SINGLE;
       (void)has_b;
       const JobPos nxt = next_job(cur);
+      // fault injection (tests): the cluster's last job sends nothing, so
+      // every receiver's bounded wait for it runs out
+      const bool send = !(a.drop_last_exchange && !job_valid(nxt));
       __syncthreads();  // this job's pass-1 output is visible
       // push F_rank[k1] to the CTA that owns pair min(k1, Q-k1); receive layout [p][hi][u]
       auto push = [&](int k1, float2 val) {
@@ -692,7 +784,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 #pragma unroll
          for (int b = 0; b < BPT3; b++) {
             const int j = tid + b * T;
-            if (nb3 % T == 0 || j < nb3) {
+            if ((nb3 % T == 0 || j < nb3) && send) {
                if constexpr (FASTPUSH) {
                   const uint32_t self = 8u * (uint32_t)(rank * SIDES);
 #pragma unroll
@@ -709,65 +801,62 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
             }
          }
       } else {
-         // ---- two radix-16 levels per warp on tensor cores: rows k1 = 2w, 2w+1 ----
-         const int lane = tid & 31, g = lane >> 2, t = lane & 3, warp = tid >> 5;
-         float ore[2][2][4], oim[2][2][4];  // [row][tile][frag]
-#pragma unroll
-         for (int rr = 0; rr < 2; rr++) {
-            const float2 *row = buf + (2 * warp + rr) * TC_ROW;
-            // stage 1: B[n2][n1] = x[n1 + 16 n2], n1 = g (+8 for tile 1), n2 = 2t, 2t+1, 2t+8, 2t+9
-            float d1re[2][4], d1im[2][4];
-#pragma unroll
-            for (int tile = 0; tile < 2; tile++) {
-               const int n1 = g + 8 * tile;
-               const float2 x0 = row[ridx(n1 + 16 * (2 * t))];
-               const float2 x1 = row[ridx(n1 + 16 * (2 * t + 1))];
-               const float2 x2 = row[ridx(n1 + 16 * (2 * t + 8))];
-               const float2 x3 = row[ridx(n1 + 16 * (2 * t + 9))];
-               uint32_t brh[2], brl[2], bih[2], bil[2];
-               split2(x0.x, x1.x, brh[0], brl[0]);
-               split2(x2.x, x3.x, brh[1], brl[1]);
-               split2(x0.y, x1.y, bih[0], bil[0]);
-               split2(x2.y, x3.y, bih[1], bil[1]);
-               dft16_mma(F16, brh, brl, bih, bil, d1re[tile], d1im[tile]);
+         // ---- levels (1,) 2 and 3 on tensor cores; this thread owns row tid ----
+         // the operand was stored and fenced by pass 1; the barrier at the top
+         // of the loop made it visible to the issuing thread
+         constexpr float COMP = (PREC == 2) ? 64.0f : 16.0f;  // (1/s)^levels, exact
+         auto level = [&](bool kmajor) {
+            if (tid == 0) tc_issue_level(tmem_base, opnd_addr, bmat_addr, kmajor, mma_bar_addr);
+            if (!tc_gave_up && !tc::mbar_wait(mma_bar_addr, mma_par)) {
+               tc_gave_up = true;  // report once; later levels do not wait again
+               if (a.status) atomicExch(a.status, 1);
             }
-            // twiddle W_256^{n1 m2}: D1 element (m2 = g (+8 for frags 2,3), n1 = 2t (+1 for odd frags) + 8*tile)
+            mma_par ^= 1u;
+            tc::fence_after();
+         };
+         // hand the next operand to the tensor core: loads of TMEM done,
+         // generic stores visible to the async proxy, then one barrier
+         auto handoff = [&]() {
+            tc::fence_before();
+            tc::fence_async_smem();
+            __syncthreads();
+         };
+         float2 y[16];
+         if constexpr (PREC == 2) {
+            // level 1: row r1 = tid = q0 + 16 q1, outputs k0; twiddle W_4096^{r1 k0}
+            level(true);
+            tc_load_row(tmem_base, y);
+            float2 base[nbases(R3)];
 #pragma unroll
-            for (int tile = 0; tile < 2; tile++)
-#pragma unroll
-               for (int e = 0; e < 4; e++) {
-                  const int m2 = g + ((e & 2) ? 8 : 0);
-                  const int n1 = 2 * t + (e & 1) + 8 * tile;
-                  const float2 w = w256[(n1 * m2) & 255];
-                  const float2 y = cmul(make_float2(d1re[tile][e], d1im[tile][e]), w);
-                  d1re[tile][e] = y.x;
-                  d1im[tile][e] = y.y;
-               }
-            // stage 2: B2[n1][m2] from D1: tile' 0 (m2 = g): b0 = tile0 (c0, c1), b1 = tile1 (c0, c1);
-            //                               tile' 1 (m2 = g+8): b0 = tile0 (c2, c3), b1 = tile1 (c2, c3)
-#pragma unroll
-            for (int tp = 0; tp < 2; tp++) {
-               const int e0 = 2 * tp;
-               uint32_t brh[2], brl[2], bih[2], bil[2];
-               split2(d1re[0][e0], d1re[0][e0 + 1], brh[0], brl[0]);
-               split2(d1re[1][e0], d1re[1][e0 + 1], brh[1], brl[1]);
-               split2(d1im[0][e0], d1im[0][e0 + 1], bih[0], bil[0]);
-               split2(d1im[1][e0], d1im[1][e0 + 1], bih[1], bil[1]);
-               dft16_mma(F16, brh, brl, bih, bil, ore[rr][tp], oim[rr][tp]);
-            }
+            for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
+            twiddle_by_powers<16>(y, base);
+            handoff();  // every thread has read its TMEM row before the operand is overwritten
+            store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, y);
+            handoff();
          }
+         // level 2: row tid = k0 + 16 q0, outputs k1; twiddle W_256^{q0 k1};
+         // level 3's operand rows k1 + 16 k0, K column q0
+         level(false);
+         tc_load_row(tmem_base, y);
+         {
+            const int q0 = tid >> 4;
+#pragma unroll
+            for (int k1 = 1; k1 < 16; k1++) y[k1] = cmul(y[k1], w256[(q0 * k1) & 255]);
+         }
+         handoff();
+         store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, y);
+         handoff();
+         // level 3: row tid = k1 + 16 k0, outputs k2: F[k0 + 16 k1 + 256 k2]
+         level(false);
+         tc_load_row(tmem_base, y);
+         tc::fence_before();
          cluster_wait();  // owners have finished reading their receive buffers
-         // D2 element (m1 = g (+8 for frags 2,3), m2 = 2t (+1) + 8*tile') -> X[16 m1 + m2] = F[k1 + 16 X-index]
+         if (send) {
+            const int kap = (tid >> 4) + 16 * (tid & 15);
 #pragma unroll
-         for (int rr = 0; rr < 2; rr++)
-#pragma unroll
-            for (int tp = 0; tp < 2; tp++)
-#pragma unroll
-               for (int e = 0; e < 4; e++) {
-                  const int m1 = g + ((e & 2) ? 8 : 0);
-                  const int m2 = 2 * t + (e & 1) + 8 * tp;
-                  push((2 * warp + rr) + 16 * (16 * m1 + m2), make_float2(ore[rr][tp][e], oim[rr][tp][e]));
-               }
+            for (int k2 = 0; k2 < 16; k2++)
+               push(kap + 256 * k2, make_float2(y[k2].x * COMP, y[k2].y * COMP));
+         }
       }
       // ---- the next job's pass 1 while this job's values are in flight ----
       if (job_valid(nxt)) {
@@ -902,6 +991,14 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    }
    cp_async_wait0();
    cluster_wait();  // pairs with the last arrive: no one still reads a receive buffer
+   if constexpr (PREC >= 1) {
+      tc::fence_before();
+      __syncthreads();
+      if (tid < 32) {
+         tc::fence_after();
+         tc::tmem_dealloc(tmem_base, TC_TMEM_COLS);
+      }
+   }
 }
 
 // K3: out[o][k] = sum over entries of scale * partial[item][prod][k], Kahan.

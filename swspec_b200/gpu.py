@@ -16,8 +16,9 @@ LIB_PATH = os.path.join(PKG, "libswsgpu.so")
 FMT_MARK5B, FMT_VDIF = 0, 1
 WIN = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
        "blackmanharris": 6}
-PREC_FP32, PREC_TCSPLIT = 0, 1
+PREC_FP32, PREC_TCSPLIT, PREC_TCSPLIT_ALL = 0, 1, 2
 PLAN_DEFAULT, PLAN_CLUSTER, PLAN_FOURSTEP = 0, 1, 2
+INJECT_NONE, INJECT_DROP_EXCHANGE = 0, 1
 MAX_SOURCES = 64
 MAX_STREAMS = 2
 
@@ -97,6 +98,8 @@ def lib():
         L.swsgpu_batch_destroy.restype = None
         L.swsgpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
         L.swsgpu_host_unregister.argtypes = [C.c_void_p]
+        L.swsgpu_sync.argtypes = [C.c_void_p, C.c_void_p]
+        L.swsgpu_inject.argtypes = [C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -244,6 +247,15 @@ class Core:
         xp = xpol[:, : c.num_xpols, :, 0] + 1j * xpol[:, : c.num_xpols, :, 1]
         pc = pcal[:, :, : c.pcal_tonebins, 0] + 1j * pcal[:, :, : c.pcal_tonebins, 1]
         return auto, xp, pc, nspec
+
+    def sync(self, stream: int = 0) -> None:
+        """Wait for the stream and raise if a kernel of an earlier call on
+        this core gave up a bounded device-side wait (swsgpu_sync)."""
+        _check(lib().swsgpu_sync(self.h, C.c_void_p(stream or None)), self.h)
+
+    def inject(self, kind: int) -> None:
+        """One-shot host-side fault injection for the next launch (swsgpu_inject)."""
+        _check(lib().swsgpu_inject(self.h, kind), self.h)
 
     def plan_info(self) -> str:
         buf = C.create_string_buffer(256)

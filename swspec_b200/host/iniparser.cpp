@@ -3,61 +3,94 @@
 // / ' # starts a comment anywhere on a line, "[name]" opens a section,
 // "key=value" (key of at least two characters) adds an entry, a duplicate
 // key keeps the first value, integers are read through atof.
+#include <cctype>
 #include <cstdlib>
 #include <cstring>
-#include <sstream>
 #include <strings.h>
 
 #include "sws_host.h"
 
 namespace swshost {
 
+namespace {
+
+// What one line of the file holds once the parsing rules are applied.
+enum class LineKind { Empty, Section, Entry, Malformed };
+
+struct ParsedLine {
+   LineKind kind = LineKind::Empty;
+   std::string a, b;  // section name, or key and value
+};
+
+// The reference's rules, applied in order: drop every whitespace character,
+// cut at the first comment character, then "[name]..." is a section header
+// (non-empty name), "kk...=value" an entry (key of two or more characters).
+ParsedLine classify(const std::string &raw)
+{
+   std::string t;
+   t.reserve(raw.size());
+   for (char ch : raw) {
+      if (ch == '/' || ch == '\'' || ch == '#') break;
+      if (!std::isspace(static_cast<unsigned char>(ch))) t.push_back(ch);
+   }
+   ParsedLine pl;
+   if (t.empty()) return pl;
+   if (t.front() == '[') {
+      const size_t close = t.find(']');
+      if (close != std::string::npos && close >= 2) {
+         pl.kind = LineKind::Section;
+         pl.a = t.substr(1, close - 1);
+      } else {
+         pl.kind = LineKind::Malformed;
+      }
+      return pl;
+   }
+   const size_t eq = t.find('=');
+   if (eq != std::string::npos && eq >= 2) {
+      pl.kind = LineKind::Entry;
+      pl.a = t.substr(0, eq);
+      pl.b = t.substr(eq + 1);
+      return pl;
+   }
+   pl.kind = LineKind::Malformed;
+   pl.a = t;
+   return pl;
+}
+
+}  // namespace
+
 IniParser::IniParser(const std::string &filename)
 {
-   std::ifstream file(filename.c_str());
-   if (!file.is_open()) {
-      std::cerr << "Error: Could not open INI file " << filename << std::endl;
+   std::ifstream in(filename.c_str());
+   if (!in) {
+      std::cerr << "INI file '" << filename << "' cannot be opened" << std::endl;
       return;
    }
    opened_ = true;
-   std::string line;
-   int linenr = -1;
-   while (!std::getline(file, line).fail()) {
-      linenr++;
-      std::string mline, element;
-      std::istringstream istr(line);
-      while (istr >> element) mline += element;
-      size_t cpos = mline.find_first_of("/'#", 0);
-      if (cpos != std::string::npos) mline.resize(cpos);
-      if (mline.empty()) continue;
-      if (mline[0] == '[') {
-         cpos = mline.find_first_of("]", 0);
-         if (cpos == std::string::npos || cpos <= 1) {
-            std::cerr << "INI section line " << linenr << " '" << line << "' incorrectly formed'" << std::endl;
-            continue;
-         }
-         Section sec;
-         sec.name = mline.substr(1, cpos - 1);
-         sections_.push_back(sec);
+   std::string raw;
+   for (int number = 0; std::getline(in, raw); number++) {
+      const ParsedLine pl = classify(raw);
+      switch (pl.kind) {
+      case LineKind::Empty:
+         break;
+      case LineKind::Section:
+         sections_.push_back(Section{pl.a, {}});
          section_index_ = (int)sections_.size() - 1;
-         continue;
-      }
-      cpos = mline.find_first_of("=", 0);
-      if (cpos != std::string::npos && cpos > 1) {
-         if (section_index_ < 0) continue;
-         KV kv;
-         kv.key = mline.substr(0, cpos);
-         kv.value = mline.substr(cpos + 1);
-         if (hasKey(kv.key)) {
-            std::cerr << "Warning: INI section contains duplicate key '" << kv.key << "'! "
-                      << "Not assigning new value '" << kv.value << "'." << std::endl;
-            continue;
+         break;
+      case LineKind::Entry:
+         if (section_index_ < 0) break;  // entries before the first section are dropped
+         if (hasKey(pl.a)) {
+            std::cerr << "INI key '" << pl.a << "' repeated in section '" << sections_[section_index_].name
+                      << "': the first value stays, '" << pl.b << "' is ignored" << std::endl;
+            break;
          }
-         sections_[section_index_].entries.push_back(kv);
-         continue;
+         sections_[section_index_].entries.push_back(KV{pl.a, pl.b});
+         break;
+      case LineKind::Malformed:
+         std::cerr << "INI line " << number << " ignored (neither a [section] nor key=value): '" << raw << "'"
+                   << std::endl;
+         break;
       }
-      std::cerr << "INI has malformed line " << linenr << " '" << line << "' (parsed as '" << mline << "') "
-                << std::endl;
    }
 }
 

@@ -13,6 +13,11 @@ from swspec_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
+# the plain FP32 form and the two tensor-core split forms (tcgen05 levels
+# 2-3 with an FP32 level 1, or all three local levels)
+PRECS = ["fp32", "tcsplit", "tcsplit_all"]
+PREC_OF = {"fp32": 0, "tcsplit": 1, "tcsplit_all": 2}
+
 
 def _mark5b_noise(nchan, nbit, nframes_m5b, seed, mbps=1024):
     spf = synth.mark5b_samples_per_frame(nchan, nbit)
@@ -22,12 +27,12 @@ def _mark5b_noise(nchan, nbit, nframes_m5b, seed, mbps=1024):
     return synth.mark5b_stream(sig, nbit, mbps), T
 
 
-@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+@pytest.mark.parametrize("prec", PRECS)
 def test_c1_like_auto_single_channel(gpu, prec):
     """16 ch x 2 bit Mark5B, channel 1 only, N=32768 Hann, 16 FFTs per spectrum
     (the default buffer plan's core run), tone at +3.1 MHz; both FFT forms."""
     N, cof = 32768, 16
-    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
+    precision = PREC_OF[prec]
     data, info = synth.c1_stream(0, frames=int(np.ceil(N * cof / 2500)) + 1, N=N)
     lay = gpu.layout("mark5b", 16, 2)
     run_bytes_payload = N * cof * 4
@@ -44,12 +49,12 @@ def test_c1_like_auto_single_channel(gpu, prec):
     assert err < REL_TOL, err
 
 
-@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+@pytest.mark.parametrize("prec", PRECS)
 def test_c3_like_dual_pol_cross(gpu, prec):
     """Mark5B-2048-16-2, 8 subband pairs (c, c+8), N=65536, XX/YY/XY*; both
     the plain FP32 form and the tensor-core split form meet the bar."""
     N, cof, nfft = 65536, 16, 16
-    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
+    precision = PREC_OF[prec]
     data, info = synth.c3_stream(nfft, N=N)
     lay = gpu.layout("mark5b", 16, 2)
     pairs = [(c, c + 8) for c in range(8)]
@@ -186,15 +191,16 @@ def test_short_integration_level_relative(gpu):
     assert err <= max(np.sqrt(2.0) * 1.1 * err_cpu32, 1e-6), (err, err_cpu32)
 
 
+@pytest.mark.parametrize("prec", ["tcsplit", "tcsplit_all"])
 @pytest.mark.parametrize("N", [8192, 16384])
-def test_tcsplit_two_files_overlap(gpu, N):
-    """Tensor-core form on the remaining Q=4096 plans, overlapped FFTs, two files."""
+def test_tcsplit_two_files_overlap(gpu, N, prec):
+    """Tensor-core forms on the remaining Q=4096 plans, overlapped FFTs, two files."""
     d1, T = _mark5b_noise(8, 2, 40, 51)
     d2, _ = _mark5b_noise(8, 2, 40, 52)
     lay = gpu.layout("mark5b", 8, 2)
     cof = 2 * (T // N) - 1
     cfg = gpu.make_config(lay, N, "hann", 2, cof, sources=((0, 1), (1, 6)), xpols=((0, 1),),
-                          max_run_bytes=len(d1), precision=gpu.PREC_TCSPLIT)
+                          max_run_bytes=len(d1), precision=PREC_OF[prec])
     core = gpu.Core(cfg)
     auto, xp, _, ns = core.run([d1, d2])
     s1 = decode_channels(d1, "Mark5B-1024-8-2", 8, 2, [1], T)[0]
@@ -211,7 +217,7 @@ def test_tcsplit_rejected_without_plan(gpu):
         gpu.Core(cfg)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "tcsplit"])
+@pytest.mark.parametrize("prec", PRECS)
 def test_blanked_mark5b_frames(gpu, prec):
     """Fill-pattern zones (trailing, whole frame, leading, interior) through
     the whole path: blanked sample-times enter the FFTs and the phase-cal
@@ -224,7 +230,7 @@ def test_blanked_mark5b_frames(gpu, prec):
     for f, a, b in [(2, 6000, 10000), (5, 0, 10000), (8, 0, 4000), (11, 2000, 3000), (20, 4, 9996)]:
         data = fill_zone(data, f, a, b, 10016, 16)
     lay = gpu.layout("mark5b", 16, 2)
-    precision = gpu.PREC_TCSPLIT if prec == "tcsplit" else gpu.PREC_FP32
+    precision = PREC_OF[prec]
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 2), (0, 9)), xpols=((0, 1),),
                           max_run_bytes=len(data), extract_pcal=True, pcal_tonebins=32,
                           pcal_rotatorlen=2048, samplingfreq=fs, pcal_offset_hz=off, precision=precision)
