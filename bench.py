@@ -143,55 +143,94 @@ def fp32_peak(device: int) -> float | None:
     return None
 
 
-def cpu_baseline(seconds_budget: float = 12.0) -> dict:
-    """FP32 CPU restatement of the IPP core (oracle port) on host cores:
-    whole core runs (16 FFTs x 16 channels, 8 cross pairs) until the budget."""
+def cpu_payload(seed: int = 5):
+    """One integration's packed Mark5B payload (61 runs of 4 MiB): random
+    2-bit codes; the CPU core's speed does not depend on their values."""
     import numpy as np
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 256, RUNS_PER_SPECTRUM * RUN_BYTES, dtype=np.uint8)
+
+
+def cpu_step(O, payload, pool, cores: int, npairs: int = NPAIRS) -> int:
+    """One step of the workload on the CPU restatement of the reference core
+    (TaskCoreIPP::doMaths, src/IA-32/TaskCoreIPP.cpp:355-560): decode the used
+    channels from the packed payload (mark5access tables, one channel per
+    thread), then for every 4 MiB run and subband pair the FP32 doMaths of 16
+    FFTs (windowed real-input FFT, |X|^2 and X.Y* accumulation).  As the
+    reference's NumCPUCores cores do, each thread takes whole core runs.
+    Returns the input samples processed."""
+    nsamp = RUNS_PER_SPECTRUM * RUN_BYTES // 4          # 16 ch x 2 bit = 4 bytes per sample-time
+    chans = [c for p in range(npairs) for c in (p, p + NPAIRS)]
+    dec = dict(zip(chans, pool.map(lambda c: O.decode(O.FMT_MARK5B, NCHAN, 2, payload, nsamp, c), chans)))
+    cfg = O.make_cfg(N, core_overlapped_ffts=CORE_FFTS, num_sources=2, num_xpols=1,
+                     window=O.W_HANN, nthreads=1)
+    per_run = CORE_FFTS * N
+
+    def core_run(task):
+        r, p = task
+        O.domaths(cfg, [dec[p][r * per_run:(r + 1) * per_run], dec[p + NPAIRS][r * per_run:(r + 1) * per_run]],
+                  fp64=False)
+
+    list(pool.map(core_run, [(r, p) for r in range(RUNS_PER_SPECTRUM) for p in range(npairs)]))
+    return len(chans) * RUNS_PER_SPECTRUM * per_run
+
+
+def cpu_baseline(seconds_budget: float = 12.0) -> dict:
+    """The CPU restatement on all host cores over whole steps of the
+    workload (packed payload in, spectra out) until the budget is spent."""
+    from concurrent.futures import ThreadPoolExecutor
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
-    rng = np.random.default_rng(5)
-    lv = np.array([-3.3359, -1.0, 1.0, 3.3359], dtype=np.float32)
-    nsamp = CORE_FFTS * N
-    chans = [lv[rng.integers(0, 4, nsamp)] for _ in range(NCHAN)]
-    cfg = O.make_cfg(N, core_overlapped_ffts=CORE_FFTS, num_sources=2, num_xpols=1,
-                     window=O.W_HANN, nthreads=cores)
-    runs = 0
-    t0 = time.perf_counter()
-    while True:
-        for p in range(NPAIRS):
-            O.domaths(cfg, [chans[p], chans[p + NPAIRS]], fp64=False)
-        runs += 1
-        if time.perf_counter() - t0 > seconds_budget:
-            break
-    dt = time.perf_counter() - t0
-    samples = runs * CORE_FFTS * N * NCHAN
+    payload = cpu_payload()
+    samples = 0
+    steps = 0
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        t0 = time.perf_counter()
+        while True:
+            samples += cpu_step(O, payload, pool, cores)
+            steps += 1
+            if time.perf_counter() - t0 > seconds_budget:
+                break
+        dt = time.perf_counter() - t0
     return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "port",
-            "sample": f"{runs} core runs of the workload (16 FFTs x 16 channels each, "
-                      f"{samples / 1e6:.0f} Msamples), FP32 restatement of TaskCoreIPP::doMaths",
+            "sample": f"{steps} whole step(s) of the workload (1 s integration, 16 channels, "
+                      f"{samples / 1e6:.0f} Msamples) from packed Mark5B bytes: mark5access decode + "
+                      "FP32 restatement of TaskCoreIPP::doMaths (real-input FFT), one core run per thread",
             "seconds": dt}
 
 
 def reference_arm(args) -> None:
+    """The reference's CPU core, restated (its IPP build cannot be compiled:
+    Intel IPP is closed and absent), on all host cores: every step is one
+    whole step of the workload, timed as it runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
     cores = os.cpu_count() or 1
-    # each step: one bounded sample of the workload (about 3 s of CPU work)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(seconds_budget=3.0)
-        if i >= args.warmup:
-            vals.append(r["value"])
-    v = sum(vals) / len(vals)
+    payload = cpu_payload()
+    times = []
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            n = cpu_step(O, payload, pool, cores)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+    ms = 1e3 * sum(times) / len(times)
+    v = n / (ms * 1e-3) / 1e9
     line = {"metric": METRIC, "value": v, "unit": "Gsamples/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": SAMPLES_PER_STEP / (v * 1e9) * 1e3, "higher_is_better": True,
+            "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": CONFIG,
             "cpu_baseline": {"value": v, "unit": "Gsamples/s", "cores": cores, "kind": "port",
-                             "sample": "per step ~3 s of core runs (16 FFTs x 16 channels), "
-                                       "FP32 C restatement of TaskCoreIPP::doMaths, all host threads"},
+                             "sample": "every step is one whole step of the workload (1 s integration, "
+                                       "16 channels) from packed Mark5B bytes: mark5access decode + FP32 C "
+                                       "restatement of TaskCoreIPP::doMaths (real-input FFT), all host threads"},
             "e2e": {"value": v, "unit": "Gsamples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -250,9 +289,14 @@ def gpu_arm(args) -> None:
     reps = Replicas("nccl")
     world, rank = reps.world, reps.rank
 
+    names = {gpu.PREC_FP32: "fp32", gpu.PREC_TCSPLIT: "tcsplit", gpu.PREC_TCSPLIT_ALL: "tcsplit_all"}
     precisions = [gpu.PREC_FP32]
-    if args.precision in ("tcsplit", "auto") and args.plan != "fourstep" and tc_available(gpu):
-        precisions = [gpu.PREC_TCSPLIT, gpu.PREC_FP32]
+    if args.plan != "fourstep" and tc_available(gpu):
+        if args.precision == "auto":
+            precisions = [gpu.PREC_TCSPLIT_ALL, gpu.PREC_TCSPLIT, gpu.PREC_FP32]
+        elif args.precision != "fp32":
+            precisions = [{"tcsplit": gpu.PREC_TCSPLIT, "tcsplit_all": gpu.PREC_TCSPLIT_ALL}[args.precision],
+                          gpu.PREC_FP32]
     headline = precisions[0]
 
     # ---- input: one integration of framed Mark5B on the device ----
@@ -290,7 +334,7 @@ def gpu_arm(args) -> None:
     launches_per_step = 0
     clocks = None
     for prec in precisions:
-        name = "tcsplit" if prec == gpu.PREC_TCSPLIT else "fp32"
+        name = names[prec]
         core = make_core(prec)
         plan_desc = core.plan_info()
         for _ in range(args.warmup):
@@ -317,6 +361,7 @@ def gpu_arm(args) -> None:
             step(core)
         nk, kms = core.profile_read()
         core.profile(False)
+        core.sync(stream.cuda_stream)   # raises if a bounded device wait of any step gave up
         core.close()
         value = SAMPLES_PER_STEP * args.steps * world / (ms * 1e-3) / 1e9
         forms[name] = {"value": value, "ms_per_step": ms / args.steps, "plan": plan_desc,
@@ -327,10 +372,9 @@ def gpu_arm(args) -> None:
         log(f"[{name}] {value:.3f} Gsamples/s, {ms / args.steps:.3f} ms/step, "
             f"FFT kernel {kms / max(nk, 1):.3f} ms/launch")
 
-    # the headline is the faster form (both meet the parity bar; both are reported)
-    if len(forms) > 1:
-        headline = gpu.PREC_TCSPLIT if forms["tcsplit"]["value"] > forms["fp32"]["value"] else gpu.PREC_FP32
-        clocks = forms["tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32"]["clocks"]
+    # the headline is the fastest form (every form meets the parity bar; all are reported)
+    headline = max(precisions, key=lambda p: forms[names[p]]["value"])
+    clocks = forms[names[headline]]["clocks"]
 
     # ---- e2e: TaskCore path, host buffers, per-run submit/wait ----
     pay_dev = d_raw.view(nfr, 10016)[:, 16:].reshape(-1)[:payload_needed]
@@ -375,45 +419,60 @@ def gpu_arm(args) -> None:
         reps.close()
         return
 
-    hl = forms["tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32"]
+    hl = forms[names[headline]]
     peaks = measured_peaks()
-    # roofline of the dominant kernel: 5 N log2 N flops per channel-FFT
+    # the roofline of the dominant kernel (k_spectra: FFT + accumulate) is the
+    # slower of the packed-input-plus-spectra bytes at HBM bandwidth and the
+    # 5 N log2 N flops per channel FFT at the form's arithmetic peak
     flops_per_launch = 5.0 * N * math.log2(N) * NCHAN * FFTS_PER_STEP
     bytes_per_launch = (SAMPLES_PER_STEP * 2 / 8            # packed 2-bit input
                         + (NCHAN + 2 * NPAIRS) * 4 * (N // 2 + 1))  # spectra written
     kern_s = hl["kernel_ms_per_launch"] * 1e-3
     p32 = fp32_peak(local)
-    if headline == gpu.PREC_TCSPLIT:
-        achieved = flops_per_launch / kern_s / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
-                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
-                "peak_source": f"bf16 dense burst, {peaks['source']}"}
+    achieved_tf = flops_per_launch / kern_s / 1e12
+    hbm = {"achieved_gbs": bytes_per_launch / kern_s / 1e9, "peak_gbs": peaks["hbm_gbs"],
+           "frac": bytes_per_launch / kern_s / 1e9 / peaks["hbm_gbs"],
+           "t_min_ms": bytes_per_launch / (peaks["hbm_gbs"] * 1e9) * 1e3,
+           "peak_source": f"HBM copy, {peaks['source']}"}
+    if headline == gpu.PREC_FP32:
+        roof = {"bound": "fp32", "achieved": achieved_tf, "peak": p32, "unit": "TFLOP/s",
+                "frac": achieved_tf / p32 if p32 else None,
+                "t_min_ms": flops_per_launch / (p32 * 1e12) * 1e3 if p32 else None,
+                "peak_source": "FP32 FMA issue, measured on this GPU by fp32_probe.cu "
+                               "(MEASURED_PEAKS.json holds no FP32 figure)"}
     else:
-        achieved = bytes_per_launch / kern_s / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "peak_source": f"HBM copy, {peaks['source']}"}
-    # DRAM bytes of one FP32 k_spectra launch on this workload, from an ncu
-    # capture (dram__bytes_read.sum + dram__bytes_write.sum): the 2-bit codes
-    # read plus the per-item partial spectra that k_reduce combines
-    roof["traffic"] = (256476672 + 208978176) if headline == gpu.PREC_FP32 else None
-    roof["traffic_source"] = ("ncu capture of k_spectra<16, 4096, 256, 16, 16, 16, 2, 2, 0>, this workload"
-                              if headline == gpu.PREC_FP32 else None)
-    roof["kernel"] = "k_spectra (cluster FFT + accumulate)"
-    roof["compute"] = {"achieved_tflops": flops_per_launch / kern_s / 1e12,
-                       "fp32_peak_tflops": p32,
-                       "frac_fp32": (flops_per_launch / kern_s / 1e12 / p32) if p32 else None,
-                       "flops_per_launch": flops_per_launch,
-                       "convention": "5 N log2 N per channel FFT"}
+        tp = peaks["bf16_tflops"]
+        levels = 3 if headline == gpu.PREC_TCSPLIT_ALL else 2
+        # tcgen05.mma work actually issued: per pair FFT, 16 CTAs x levels x
+        # 2 tiles x 4 K-steps of M=128, N=64, K=16
+        mma_flops = FFTS_PER_STEP * NPAIRS * 16 * levels * 8 * 2.0 * 128 * 64 * 16
+        roof = {"bound": "tensor", "achieved": achieved_tf, "peak": tp, "unit": "TFLOP/s",
+                "frac": achieved_tf / tp, "t_min_ms": flops_per_launch / (tp * 1e12) * 1e3,
+                "peak_source": f"dense bf16/f16 tensor burst, {peaks['source']}",
+                "mma_issued": {"tflops": mma_flops / kern_s / 1e12, "frac": mma_flops / kern_s / 1e12 / tp,
+                               "flops_per_launch": mma_flops,
+                               "note": "split-precision GEMM work issued (hi/lo operands, K = 64)"}}
+    roof["hbm"] = hbm
+    # DRAM bytes of one k_spectra launch on this workload, from ncu captures
+    # (dram__bytes_read.sum + dram__bytes_write.sum): the 2-bit codes read
+    # plus the per-item partial spectra that k_reduce combines
+    traffic = {gpu.PREC_FP32: (256476672 + 208978176, "profiles/k_spectra_c3_fp32.md")}
+    t = traffic.get(headline)
+    roof["traffic"] = t[0] if t else None
+    roof["traffic_source"] = t[1] if t else None
+    roof["kernel"] = "k_spectra (cluster FFT + accumulate), " + names[headline] + " form"
+    roof["flops_per_launch"] = flops_per_launch
     roof["algorithmic_bytes_per_launch"] = bytes_per_launch
+    roof["fp32_peak_tflops"] = p32
     cpu = cpu_baseline() if (world == 1 and not args.no_cpu) else None
     line = {"metric": METRIC, "value": hl["value"], "unit": "Gsamples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": hl["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if headline == gpu.PREC_FP32 else "f16x2-split/f32",
             "data": "synthetic", "config": CONFIG,
-            "precision": "tcsplit" if headline == gpu.PREC_TCSPLIT else "fp32",
+            "precision": names[headline],
             "forms": forms, "clocks": clocks,
-            "tc_over_fp32": (forms["tcsplit"]["value"] / forms["fp32"]["value"]) if len(forms) > 1 else None,
+            "tc_over_fp32": {n: forms[n]["value"] / forms["fp32"]["value"] for n in forms if n != "fp32"} or None,
             "e2e": {"value": e2e_val, "unit": "Gsamples/s",
                     "h2d_bytes_per_step": RUNS_PER_SPECTRUM * RUN_BYTES,
                     "d2h_bytes_per_step": d2h,
@@ -581,6 +640,7 @@ def spec_arm(args) -> None:
         step()
     nk, kms = core.profile_read()
     core.profile(False)
+    core.sync(st.cuda_stream)   # raises if a bounded device wait of any step gave up
     samples = w["runs"] * w["core_ffts"] * w["N"] * ns
     value = samples * reps.world / (ms * 1e-3) / 1e9
     if reps.rank == 0:
@@ -597,11 +657,13 @@ def spec_arm(args) -> None:
                            "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_in / 1e6),
                            "plan": core.plan_info()},
                 "clocks": cs.summary(), "gpu_launches": launches * args.steps, "e2e": None,
-                "roofline": {"bound": "hbm", "achieved": bytes_in / kern_s / 1e9, "peak": peaks["hbm_gbs"],
-                             "unit": "GB/s", "frac": bytes_in / kern_s / 1e9 / peaks["hbm_gbs"], "traffic": None,
-                             "compute": {"achieved_tflops": flops / kern_s / 1e12, "fp32_peak_tflops": p32,
-                                         "frac_fp32": flops / kern_s / 1e12 / p32 if p32 else None},
-                             "kernel_ms": kern_s * 1e3},
+                "roofline": {"bound": "fp32", "achieved": flops / (ms * 1e-3) / 1e12, "peak": p32,
+                             "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / p32 if p32 else None,
+                             "traffic": None, "scope": "whole step (every kernel of the step)",
+                             "peak_source": "FP32 FMA issue, measured on this GPU by fp32_probe.cu",
+                             "hbm": {"achieved_gbs": bytes_in / (ms * 1e-3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                                     "frac": bytes_in / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"]},
+                             "fft_kernel_ms_per_launch": kern_s * 1e3, "fft_kernel_launches_per_step": nk / 3},
                 "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     core.close()
@@ -614,7 +676,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "tcsplit"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "tcsplit", "tcsplit_all"])
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plan", default="auto", choices=["auto", "cluster", "fourstep"],

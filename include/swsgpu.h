@@ -51,6 +51,16 @@ extern "C" {
 /* Sample tables (level values) of the stream. */
 #define SWSGPU_FMT_MARK5B 0      /* Mark5B: 2-bit {-H,+1,-1,+H}[s+2m], 1-bit {+1,-1} */
 #define SWSGPU_FMT_VDIF 1        /* VDIF: 2-bit {-H,-1,+1,+H}, 1-bit {-1,+1}, 8-bit (2b-255)/256 */
+/* Raw sampler data, the reference's RawSigned / RawUnsigned formats
+ * (src/IA-32/DataUnpackerFactory.h:44-67): 8-bit samples byte-interleaved by
+ * channel, signed (int8) or unsigned (b - 128) (DataUnpackers.cpp:68-171);
+ * 2-bit with nchan % 4 == 0: channel c's code at bit 2c of the sample-time's
+ * nchan/4 bytes (:191-249; ChannelOrderIncreasing = no is channel
+ * nchan-1-c); 2-bit with one channel: four samples per byte, the oldest in
+ * the two most significant bits (:261-310).  2-bit codes map to
+ * {+1, -1, +H, -H}.  No fill-pattern blanking. */
+#define SWSGPU_FMT_RAW_SIGNED 2
+#define SWSGPU_FMT_RAW_UNSIGNED 3
 
 /* Window functions: the reference's WindowFunctionType (src/Settings.h:45)
  * plus BlackmanHarris (4-term Harris 1978), which the reference lacks. */

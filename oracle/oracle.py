@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None
 _ref = None
+_uref = None
 
 W_NONE, W_COSINE, W_COSINE2, W_HAMMING, W_HANN, W_BLACKMAN, W_BLACKMANHARRIS = range(7)
 WINDOW_NAMES = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
@@ -82,7 +83,7 @@ def ref():
 # decoding
 # ----------------------------------------------------------------------------
 
-FMT_MARK5B, FMT_VDIF = 0, 1
+FMT_MARK5B, FMT_VDIF, FMT_RAW_SIGNED, FMT_RAW_UNSIGNED = 0, 1, 2, 3
 
 
 def decode(fmt: int, nchan: int, nbit: int, payload: bytes, nsamp: int, chan: int,
@@ -111,6 +112,37 @@ def vdif_invalid_bits(framed: bytes, frame_bytes: int) -> np.ndarray:
     a = np.frombuffer(framed, dtype=np.uint8).reshape(-1, frame_bytes)
     w0 = a[:, :4].copy().view(np.uint32)[:, 0]
     return ((w0 >> 31) & 1).astype(np.uint8)
+
+
+def ref_unpack():
+    """The reference's raw-data unpackers (src/IA-32/DataUnpackers.cpp, built
+    with oracle/unpack_shim.cpp into _ref/libunpackref.so), or None."""
+    global _uref
+    if _uref is None:
+        path = os.path.join(HERE, "_ref", "libunpackref.so")
+        if not os.path.exists(path):
+            return None
+        _uref = C.CDLL(path)
+        _uref.refunpack_raw.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_long, C.c_int]
+        _uref.refunpack_raw.restype = C.c_long
+    return _uref
+
+
+RAW_SIGNED_8, RAW_UNSIGNED_8, RAW_TWOBIT, RAW_TWOBIT_1CH = range(4)
+
+
+def ref_unpack_raw(kind: int, nbit: int, nchan: int, payload: bytes, count: int, chan: int,
+                   increasing: bool = True) -> np.ndarray:
+    """count samples of channel chan through the reference's own unpacker of
+    the given kind (count is rounded up to the unpackers' 8/16-sample unroll)."""
+    L = ref_unpack()
+    buf = np.frombuffer(payload, dtype=np.uint8)
+    n = (count + 15) // 16 * 16
+    out = np.zeros(n + 16, dtype=np.float32)
+    got = L.refunpack_raw(kind, nbit, nchan, int(increasing), buf.ctypes.data, out.ctypes.data, n, chan)
+    assert got == n, got
+    return out[:count]
 
 
 def m5_format_info(fmt: str) -> dict:

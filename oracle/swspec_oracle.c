@@ -47,6 +47,8 @@
 
 #define ORC_FMT_MARK5B 0
 #define ORC_FMT_VDIF 1
+#define ORC_FMT_RAW_SIGNED 2
+#define ORC_FMT_RAW_UNSIGNED 3
 
 static const float ORC_HIMAG = 3.3359f; /* OPTIMAL_2BIT_HIGH, mark5_stream.h:72 */
 
@@ -74,6 +76,47 @@ static float orc_level(int fmt, int nbit, unsigned code)
    return 0.0f;
 }
 
+/* The reference's raw unpackers (src/IA-32/DataUnpackers.cpp):
+ * SignedUnpacker 8-bit: (signed char) byte (:68-90); UnsignedUnpacker
+ * 8-bit: byte - 128 (:125-147); TwoBitUnpacker and the single-channel one:
+ * map_rev[code] = {1, -1, 3.3359, -3.3359} (:214, :280). */
+static float orc_raw_level(int fmt, int nbit, unsigned code)
+{
+   if (nbit == 8) return fmt == ORC_FMT_RAW_SIGNED ? (float)(signed char)code : (float)code - 128.0f;
+   static const float map_rev[4] = {1.0f, -1.0f, 3.3359f, -3.3359f};
+   return map_rev[code & 3];
+}
+
+/* Raw sampler data, channel `chan` (0-based, as the unpacker sees it):
+ *  8-bit: byte t*nchan + chan (SignedUnpacker / UnsignedUnpacker :74-78);
+ *  2-bit, nchan % 4 == 0: byte t*nchan/4 + chan/4, bits 2*(chan%4) .. +1
+ *    (TwoBitUnpacker :207-243 with ChannelOrderIncreasing; the decreasing
+ *    order is channel nchan-1-chan);
+ *  2-bit, one channel: byte t/4, bits 6-2*(t%4) .. +1, the oldest sample
+ *    in the most significant bits (TwoBitSinglechannelUnpacker :261-265;
+ *    its table lookup at :280-284 masks with the top two bits for every
+ *    sample position, so only the first sample of each byte reads a
+ *    defined table entry there: this restates the layout the function
+ *    documents). */
+static int orc_decode_raw(int fmt, int nchan, int nbit, const uint8_t *payload, int64_t nsamp, int chan,
+                          float *out)
+{
+   if (nbit == 8) {
+      for (int64_t t = 0; t < nsamp; t++) out[t] = orc_raw_level(fmt, 8, payload[t * nchan + chan]);
+      return 0;
+   }
+   if (nbit != 2) return -1;
+   if (nchan == 1) {
+      for (int64_t t = 0; t < nsamp; t++) out[t] = orc_raw_level(fmt, 2, (payload[t >> 2] >> (6 - 2 * (t & 3))) & 3u);
+      return 0;
+   }
+   if (nchan % 4) return -1;
+   const int64_t step = nchan / 4;
+   for (int64_t t = 0; t < nsamp; t++)
+      out[t] = orc_raw_level(fmt, 2, (payload[t * step + chan / 4] >> (2 * (chan % 4))) & 3u);
+   return 0;
+}
+
 /* Decode channel `chan` of a header-free payload byte stream: sample-time t
  * occupies nchan*nbit consecutive bits starting at bit t*nchan*nbit, channel c
  * at bit offset c*nbit inside it, bits numbered LSB-first within each byte.
@@ -83,6 +126,8 @@ int orc_decode(int fmt, int nchan, int nbit, const uint8_t *payload, int64_t nsa
                float *out)
 {
    if (chan < 0 || chan >= nchan) return -1;
+   if (fmt == ORC_FMT_RAW_SIGNED || fmt == ORC_FMT_RAW_UNSIGNED)
+      return orc_decode_raw(fmt, nchan, nbit, payload, nsamp, chan, out);
    const int64_t stride = (int64_t)nchan * nbit;
    for (int64_t t = 0; t < nsamp; t++) {
       int64_t bit = t * stride + (int64_t)chan * nbit;

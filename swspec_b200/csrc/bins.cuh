@@ -14,7 +14,7 @@ template <int NBIT>
 __device__ __forceinline__ float decode_level(uint32_t code, float4 lv)
 {
    if constexpr (NBIT == 8) {
-      return (float)((int)code * 2 - 255) * (1.0f / 256.0f);
+      return fmaf(lv.x, (float)(code ^ __float_as_uint(lv.z)), lv.y);
    } else if constexpr (NBIT == 2) {
       float lo = (code & 1u) ? lv.y : lv.x;
       float hi = (code & 1u) ? lv.w : lv.z;

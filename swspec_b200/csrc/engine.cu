@@ -39,6 +39,11 @@ using namespace sws;
 
 static thread_local std::string g_create_error;
 
+namespace sws {
+// The message swsgpu_last_error(NULL) returns on this thread.
+void record_create_error(const std::string &msg) { g_create_error = msg; }
+}  // namespace sws
+
 // The kernel and shared-memory size of a cluster plan's form.
 static SpecKernel plan_kernel(const Plan &pl, int precision, int nbi)
 {
@@ -262,18 +267,14 @@ static void make_twiddles(int n, int count, std::vector<float2> &t)
    }
 }
 
-static float4 level_table(int format, int nbit)
-{
-   const float H = 3.3359f;  // OPTIMAL_2BIT_HIGH
-   if (format == SWSGPU_FMT_MARK5B) {
-      if (nbit == 2) return make_float4(-H, 1.0f, -1.0f, H);
-      return make_float4(1.0f, -1.0f, 0.0f, 0.0f);
-   }
-   if (nbit == 2) return make_float4(-H, -1.0f, 1.0f, H);
-   return make_float4(-1.0f, 1.0f, 0.0f, 0.0f);
-}
 
 static int payload_bytes(const swsgpu_layout &l) { return l.frame_bytes - l.header_bytes; }
+
+// Raw single-channel 2-bit data stores the oldest sample in the byte's MSBs.
+static int is_msb2(const swsgpu_layout &l)
+{
+   return (l.format >= SWSGPU_FMT_RAW_SIGNED && l.nbit == 2 && l.nchan == 1) ? 1 : 0;
+}
 
 // ---------------------------------------------------------------------------
 // doMaths frame schedule of one run (TaskCoreIPP.cpp:394-524)
@@ -790,6 +791,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       si.nchan = L.nchan;
       si.nbit = L.nbit;
       si.format = L.format;
+      si.msb2 = is_msb2(L);
       const long long last_v = si.grid_offset + ((nsamp * (long long)L.nchan * L.nbit - 1) >> 3);
       si.nframes = last_v / si.payload_bytes + 1;
       CK(h, h->d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes));
@@ -998,7 +1000,15 @@ static int validate_config(const swsgpu_config *c, std::string &why)
       const swsgpu_layout &l = c->layout[s];
       if (l.nbit != 1 && l.nbit != 2 && l.nbit != 8) { why = "nbit must be 1, 2 or 8"; return 0; }
       if (l.nchan < 1 || l.nchan * l.nbit > 64) { why = "nchan*nbit must be 1..64"; return 0; }
-      if (l.format != SWSGPU_FMT_MARK5B && l.format != SWSGPU_FMT_VDIF) { why = "unknown format"; return 0; }
+      if (l.format < SWSGPU_FMT_MARK5B || l.format > SWSGPU_FMT_RAW_UNSIGNED) { why = "unknown format"; return 0; }
+      if (l.format >= SWSGPU_FMT_RAW_SIGNED) {
+         // the reference's raw unpackers (DataUnpackerFactory.h:44-67)
+         if (l.nbit == 1) { why = "raw formats have no 1-bit unpacker"; return 0; }
+         if (l.nbit == 2 && !(l.nchan == 1 || l.nchan % 4 == 0)) {
+            why = "raw 2-bit data needs one channel or a multiple of 4";
+            return 0;
+         }
+      }
       if (l.header_bytes < 0 || l.frame_bytes <= l.header_bytes) { why = "bad frame layout"; return 0; }
       if ((l.frame_bytes % 8) || (l.header_bytes % 4) || ((l.frame_bytes - l.header_bytes) % 8)) {
          why = "frame, header and payload sizes must be multiples of 8, 4 and 8 bytes";
@@ -1826,6 +1836,7 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    si.nchan = lay->nchan;
    si.nbit = lay->nbit;
    si.format = lay->format;
+   si.msb2 = is_msb2(*lay);
    if (nsamp == 0) {
       if (nvalid) *nvalid = 0;
       return SWSGPU_OK;

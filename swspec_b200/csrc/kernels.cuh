@@ -2,7 +2,10 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
+
+#include "../../include/swsgpu.h"
 
 namespace sws {
 
@@ -23,9 +26,39 @@ struct StreamIn {
    int payload_bytes;
    int nchan;
    int nbit;
-   int format;   // 0 Mark5B, 1 VDIF
+   int format;   // SWSGPU_FMT_*
    long long nframes;  // frames touched by the chunk
+   int msb2;     // 2-bit samples stored oldest-first from the byte's MSB (raw single channel)
 };
+
+// Level table of a format, as decode_level reads it: 1-bit {x, y}; 2-bit
+// {x, y, z, w} for codes 0..3; 8-bit v = x * (code ^ bits(z)) + y (exact
+// for every 8-bit table: VDIF (2b - 255)/256, raw b - 128 and (int8)b).
+__host__ __device__ inline float4 level_table(int format, int nbit)
+{
+   const float H = 3.3359f;  // OPTIMAL_2BIT_HIGH (mark5access) = the reference's 2-bit high level
+   if (format == SWSGPU_FMT_MARK5B) {
+      if (nbit == 2) return make_float4(-H, 1.0f, -1.0f, H);
+      return make_float4(1.0f, -1.0f, 0.0f, 0.0f);
+   }
+   if (format == SWSGPU_FMT_RAW_SIGNED || format == SWSGPU_FMT_RAW_UNSIGNED) {
+      if (nbit == 2) return make_float4(1.0f, -1.0f, H, -H);
+      float x;
+      const uint32_t xm = format == SWSGPU_FMT_RAW_SIGNED ? 0x80u : 0u;
+      memcpy(&x, &xm, 4);
+      return make_float4(1.0f, -128.0f, x, 0.0f);
+   }
+   if (nbit == 2) return make_float4(-H, -1.0f, 1.0f, H);
+   if (nbit == 8) return make_float4(1.0f / 128.0f, -255.0f / 256.0f, 0.0f, 0.0f);
+   return make_float4(-1.0f, 1.0f, 0.0f, 0.0f);
+}
+
+// Reverses the order of the four 2-bit fields of every byte of w.
+__host__ __device__ inline uint32_t swap2_in_bytes(uint32_t w)
+{
+   return ((w & 0x03030303u) << 6) | ((w & 0x0C0C0C0Cu) << 2) | ((w & 0x30303030u) >> 2) |
+          ((w & 0xC0C0C0C0u) >> 6);
+}
 
 // A run of consecutive FFT jobs that share their accumulators.
 // mode 0 (XPOL):    job j packs A = source a, B = source b, both starting at

@@ -13,11 +13,13 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <string>
 
 #include "../../include/swsgpu.h"
 #include "kernels.cuh"
 
 namespace sws {
+void record_create_error(const std::string &msg);
 __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
@@ -58,16 +60,6 @@ static int scratch_for_current_device(unsigned char **out)
    return SWSGPU_OK;
 }
 
-static float4 noalloc_levels(int format, int nbit)
-{
-   const float H = 3.3359f;  // OPTIMAL_2BIT_HIGH
-   if (format == SWSGPU_FMT_MARK5B) {
-      if (nbit == 2) return make_float4(-H, 1.0f, -1.0f, H);
-      return make_float4(1.0f, -1.0f, 0.0f, 0.0f);
-   }
-   if (nbit == 2) return make_float4(-H, -1.0f, 1.0f, H);
-   return make_float4(-1.0f, 1.0f, 0.0f, 0.0f);
-}
 
 extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void *d_raw,
                                             size_t nbytes, int64_t payload_offset, int chan,
@@ -93,6 +85,7 @@ extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void
    si.nchan = lay->nchan;
    si.nbit = lay->nbit;
    si.format = lay->format;
+   si.msb2 = (lay->format >= SWSGPU_FMT_RAW_SIGNED && lay->nbit == 2 && lay->nchan == 1) ? 1 : 0;
    const long long last_v = si.grid_offset + ((nsamp * (long long)lay->nchan * lay->nbit - 1) >> 3);
    si.nframes = last_v / pb + 1;
    // the fixed scratch holds one valid range per frame
@@ -116,12 +109,15 @@ extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void
       return SWSGPU_ECUDA;
    k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(si, valid, flag);
    k_unpack_float<<<(unsigned)((nsamp + 255) / 256), 256, 0, st>>>(
-       si, nsamp, chan, noalloc_levels(lay->format, lay->nbit), d_out, valid, counter);
-   if (cudaGetLastError() != cudaSuccess) return SWSGPU_ECUDA;
+       si, nsamp, chan, level_table(lay->format, lay->nbit), d_out, valid, counter);
+   cudaError_t e = cudaGetLastError();
    unsigned long long cnt = 0;
-   if (cudaMemcpyAsync(&cnt, counter, sizeof(cnt), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+   if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, counter, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+   if (e != cudaSuccess) {
+      record_create_error(std::string("swsgpu_unpack_device_noalloc: ") + cudaGetErrorString(e));
       return SWSGPU_ECUDA;
-   if (cudaStreamSynchronize(st) != cudaSuccess) return SWSGPU_ECUDA;
+   }
    if (nvalid) *nvalid = (int64_t)cnt;
    return SWSGPU_OK;
 }

@@ -83,7 +83,9 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
    const int big = 1 << 30;
    int vs = 0, ve = big;
    const int nword = s.payload_bytes / 8;
-   if (s.format == 1) {
+   if (s.format >= SWSGPU_FMT_RAW_SIGNED) {
+      // raw sampler data: the reference's raw unpackers blank nothing
+   } else if (s.format == SWSGPU_FMT_VDIF) {
       // VDIF: invalid bit in header word 0 (framed layouts only), then fill check
       bool bad = false;
       if (s.header_bytes > 0) {
@@ -246,6 +248,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             const int jl = piece * g.PW + (q - piece * nq) * wpl;
             for (int i = 0; i < wpl; i++) {
                uint32_t x = val[u][i];
+               if (s.msb2) x = swap2_in_bytes(x);
                if (gw + i >= g.words_total) x = 0u;
                else if (any) {
                   const int2 vr = valid[fu[u]];
@@ -299,6 +302,8 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             if (j >= nw) break;
             const long long w = w0 + j;
             uint32_t val[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+            if (s.msb2)
+               for (int i = 0; i < 4; i++) val[i] = swap2_in_bytes(val[i]);
             const int pj = j / SW, rj = j - pj * SW;  // block and offset of word j
 #pragma unroll
             for (int i = 0; i < 4; i++) {
@@ -326,6 +331,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
          if (w < g.words_total) {
             const long long a = s.header_bytes ? f * s.frame_bytes + s.header_bytes + o : v - s.grid_offset;
             if (a + 4 <= s.nbytes) val = __ldg(reinterpret_cast<const uint32_t *>(s.data + a));
+            if (s.msb2) val = swap2_in_bytes(val);
             if (any) {
                const int2 vr = valid[f];
                if (!(o >= vr.x && o < vr.y)) {
@@ -488,8 +494,9 @@ __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 lev
    if (o >= vr.x && o < vr.y) {
       long long widx = bit >> 5;
       uint32_t word = *reinterpret_cast<const uint32_t *>(s.data + payload_addr(s, s.grid_offset + 4 * widx));
+      if (s.msb2) word = swap2_in_bytes(word);
       uint32_t code = (word >> (bit & 31)) & ((nbit == 8) ? 0xffu : ((1u << nbit) - 1u));
-      if (nbit == 8) val = (float)((int)code * 2 - 255) * (1.0f / 256.0f);
+      if (nbit == 8) val = fmaf(levels.x, (float)(code ^ __float_as_uint(levels.z)), levels.y);
       else if (nbit == 2) val = (code == 0) ? levels.x : (code == 1) ? levels.y : (code == 2) ? levels.z : levels.w;
       else val = code ? levels.y : levels.x;
       atomicAdd(nvalid, 1ull);

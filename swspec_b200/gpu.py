@@ -13,7 +13,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libswsgpu.so")
 
-FMT_MARK5B, FMT_VDIF = 0, 1
+FMT_MARK5B, FMT_VDIF, FMT_RAW_SIGNED, FMT_RAW_UNSIGNED = 0, 1, 2, 3
 WIN = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
        "blackmanharris": 6}
 PREC_FP32, PREC_TCSPLIT, PREC_TCSPLIT_ALL = 0, 1, 2
@@ -111,7 +111,11 @@ def _check(rc: int, h=None) -> None:
 
 
 def layout(fmt: str, nchan: int, nbit: int, framed: bool = True) -> Layout:
-    """Layout of a Mark5B or VDIF stream ("mark5b" / "vdif:<payload>")."""
+    """Layout of a Mark5B or VDIF stream ("mark5b" / "vdif:<payload>"), or of
+    header-free raw sampler data ("raw_signed" / "raw_unsigned")."""
+    if fmt.lower().startswith("raw"):
+        code = FMT_RAW_SIGNED if fmt.lower() == "raw_signed" else FMT_RAW_UNSIGNED
+        return Layout(code, nchan, nbit, 8192, 0)
     if fmt.lower().startswith("mark5b"):
         return Layout(FMT_MARK5B, nchan, nbit, 10016 if framed else 10000, 16 if framed else 0)
     payload = int(fmt.split(":")[1]) if ":" in fmt else 8000

@@ -19,7 +19,10 @@ int FileSource::open(const std::string &uri)
 {
    const Settings &s = *cfg_;
    const bool mark5b = (s.sourceformat == Mark5B || s.sourceformat == Mk5B);
-   header_bytes_ = mark5b ? 16 : (s.sourceformat_str.size() > 4 && s.sourceformat_str[4] == '_' ? 32 : 16);
+   const bool raw = (s.sourceformat == RawSigned || s.sourceformat == RawUnsigned);
+   if (raw) header_bytes_ = 0;
+   else if (s.sourceformat == iBOB) header_bytes_ = 4;  // packet sequence header (src/FileSource.cpp:53-57)
+   else header_bytes_ = mark5b ? 16 : (s.sourceformat_str.size() > 4 && s.sourceformat_str[4] == '_' ? 32 : 16);
    frame_bytes_ = header_bytes_ + s.layout.frame_bytes;
    ifile_.open(uri.c_str(), std::ios::binary | std::ios::in);
    if (!ifile_.is_open()) {
@@ -65,9 +68,15 @@ int FileSource::open(const std::string &uri)
    int64_t seek = first_frame_;
    if (s.seconds_to_skip > 0) {
       const double smp_bytes = (double)s.bits_per_sample * s.source_channels * s.samplingfreq / 8.0 * s.seconds_to_skip;
-      const int64_t frames = (int64_t)std::ceil(smp_bytes / (double)s.layout.frame_bytes);
-      seek += frames * frame_bytes_;
-      *cfg_->tlog << "Skipping " << s.seconds_to_skip << " sample-seconds: " << frames << " frames" << std::endl;
+      if (header_bytes_ == 0) {
+         seek += (int64_t)smp_bytes;  // unframed data: a plain byte offset
+         *cfg_->tlog << "Skipping " << s.seconds_to_skip << " sample-seconds: " << (int64_t)smp_bytes << " bytes"
+                     << std::endl;
+      } else {
+         const int64_t frames = (int64_t)std::ceil(smp_bytes / (double)s.layout.frame_bytes);
+         seek += frames * frame_bytes_;
+         *cfg_->tlog << "Skipping " << s.seconds_to_skip << " sample-seconds: " << frames << " frames" << std::endl;
+      }
    }
    ifile_.clear();
    ifile_.seekg(seek, std::ios::beg);

@@ -100,8 +100,20 @@ int parse_format(Settings &s, std::string &err)
       // the reference's framed VDIF: 16-byte legacy headers, 8000-byte payloads
       s.sourceformat = VDIF;
       s.layout = {SWSGPU_FMT_VDIF, s.source_channels, s.bits_per_sample, 8000, 0};
+   } else if (strcasecmp(f.c_str(), "RawSigned") == 0 || strcasecmp(f.c_str(), "RawUnsigned") == 0) {
+      // header-free sampler data (the reference's default format); the frame
+      // size only delimits blanking zones, and raw data has none
+      const bool sgn = strcasecmp(f.c_str(), "RawSigned") == 0;
+      s.sourceformat = sgn ? RawSigned : RawUnsigned;
+      s.layout = {sgn ? SWSGPU_FMT_RAW_SIGNED : SWSGPU_FMT_RAW_UNSIGNED, s.source_channels, s.bits_per_sample, 8192, 0};
+   } else if (strcasecmp(f.c_str(), "iBob") == 0) {
+      // iBOB UDP captures: 4-byte sequence headers, 4096-byte payloads of
+      // signed samples (src/FileSource.cpp:53-57, DataUnpackerFactory.h:91-95)
+      s.sourceformat = iBOB;
+      s.layout = {SWSGPU_FMT_RAW_SIGNED, s.source_channels, s.bits_per_sample, 4096, 0};
    } else {
-      err = "source format '" + f + "' is not decoded by the GPU core (Mark5B-*, VDIF_*, Mk5B, VDIF)";
+      err = "source format '" + f + "' is not decoded by the GPU core (Mark5B-*, VDIF_*, Mk5B, VDIF, RawSigned, "
+            "RawUnsigned, iBob)";
       return -1;
    }
    if (nbit != 0 && nbit != 1 && nbit != 2 && nbit != 8) {

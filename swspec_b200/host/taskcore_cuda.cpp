@@ -51,6 +51,11 @@ void TaskCoreCUDA::prepare(Settings *s)
    for (int i = 0; i < s->num_sources; i++) {
       c.source_stream[i] = i;
       c.source_channel[i] = (i == 0) ? s->use_channel_file1 : s->use_channel_file2;
+      // raw 2-bit multi-channel data with ChannelOrderIncreasing = no keeps
+      // channel 0 in the highest bits (TwoBitUnpacker, DataUnpackers.cpp:201-211)
+      if (s->layout.format >= SWSGPU_FMT_RAW_SIGNED && s->layout.nbit == 2 && s->layout.nchan % 4 == 0 &&
+          !s->channelorder_increasing)
+         c.source_channel[i] = s->layout.nchan - 1 - c.source_channel[i];
    }
    c.num_xpols = s->num_xpols;
    if (s->num_xpols) {

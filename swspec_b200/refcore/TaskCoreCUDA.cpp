@@ -48,7 +48,19 @@ bool layout_of(const swspect_settings_t *s, swsgpu_layout &l, std::string &why)
       l.frame_bytes = 8000;
       return true;
    }
-   why = "source format '" + s->sourceformat_str + "' is not decoded by the GPU core (Mk5B, VDIF)";
+   if (s->sourceformat == RawSigned || s->sourceformat == RawUnsigned) {
+      // header-free sampler data; the frame size only delimits blanking zones
+      l.format = s->sourceformat == RawSigned ? SWSGPU_FMT_RAW_SIGNED : SWSGPU_FMT_RAW_UNSIGNED;
+      l.frame_bytes = 8192;
+      return true;
+   }
+   if (s->sourceformat == iBOB) {
+      l.format = SWSGPU_FMT_RAW_SIGNED;  // 4-byte headers stripped by FileSource, signed samples
+      l.frame_bytes = 4096;
+      return true;
+   }
+   why = "source format '" + s->sourceformat_str + "' is not decoded by the GPU core (Mk5B, VDIF, RawSigned, "
+         "RawUnsigned, iBob)";
    return false;
 }
 
@@ -90,6 +102,11 @@ void TaskCoreCUDA::prepare(swspect_settings_t *s)
    for (int i = 0; i < s->num_sources; i++) {
       c.source_stream[i] = i;
       c.source_channel[i] = (i == 0) ? s->use_channel_file1 : s->use_channel_file2;  // 0-based after main
+      // raw 2-bit multi-channel data with ChannelOrderIncreasing = no keeps
+      // channel 0 in the highest bits (TwoBitUnpacker, DataUnpackers.cpp:201-211)
+      if (c.layout[0].format >= SWSGPU_FMT_RAW_SIGNED && c.layout[0].nbit == 2 && c.layout[0].nchan % 4 == 0 &&
+          !s->channelorder_increasing)
+         c.source_channel[i] = c.layout[0].nchan - 1 - c.source_channel[i];
    }
    c.num_xpols = s->num_xpols;
    if (s->num_xpols) {

@@ -121,3 +121,23 @@ def test_golden_decode_fixture(gpu):
     for c in range(int(z["nchan"])):
         got, _ = _gpu_decode(gpu, lay, raw, c, int(z["nsamp"]))
         assert np.array_equal(got.view(np.uint32), z["decoded"][c].view(np.uint32))
+
+
+@pytest.mark.parametrize("fmt,nchan,nbit", [("raw_signed", 1, 8), ("raw_signed", 4, 8), ("raw_unsigned", 2, 8),
+                                            ("raw_signed", 16, 2), ("raw_unsigned", 4, 2),
+                                            ("raw_signed", 1, 2)])
+def test_raw_formats_bit_exact(gpu, fmt, nchan, nbit):
+    """The reference's raw unpackers (RawSigned / RawUnsigned: 8-bit signed or
+    offset, 2-bit multi-channel, 2-bit single channel oldest-in-MSB) as the
+    oracle restates them (pinned to the reference's own DataUnpackers.cpp in
+    test_oracle.py); no blanking."""
+    rng = np.random.default_rng(nchan * 10 + nbit)
+    nsamp = 100_000
+    raw = rng.integers(0, 256, nsamp * nchan * nbit // 8 + 64, dtype=np.uint8).tobytes()
+    lay = gpu.layout(fmt, nchan, nbit)
+    ofmt = O.FMT_RAW_SIGNED if fmt == "raw_signed" else O.FMT_RAW_UNSIGNED
+    for c in sorted({0, nchan // 2, nchan - 1}):
+        got, nv = _gpu_decode(gpu, lay, raw, c, nsamp)
+        ref = O.decode(ofmt, nchan, nbit, raw, nsamp, c)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (fmt, nchan, nbit, c)
+        assert nv == nsamp
