@@ -566,6 +566,74 @@ int orc_schedule(const orc_cfg *c, int64_t nsamp, int64_t *starts, int *spec_of,
  * out_xpol     : [nspec][num_xpols][N/2+1][2]
  * out_pcal     : [nspec][num_sources][tonebins][2]
  * Returns number of spectra (incl. a trailing partial one). */
+typedef struct {
+   const orc_cfg *c;
+   const float *const *samples;
+   const int64_t *starts;
+   const int *spec_of;
+   int f0, f1;
+   const float *win;
+   const c64 *rot;
+   const int *pairs;
+   double *auto_acc, *xpol_acc, *pcal_acc; /* [nspec][...] (thread-private when threaded) */
+} orc_job64;
+
+static void *orc_worker64(void *arg)
+{
+   orc_job64 *j = (orc_job64 *)arg;
+   const orc_cfg *c = j->c;
+   const int N = c->fft_points, S = N / 2 + 1;
+   double *in = (double *)malloc(sizeof(double) * 2 * (size_t)N);
+   double **X = (double **)malloc(sizeof(double *) * (size_t)c->num_sources);
+   for (int s = 0; s < c->num_sources; s++) X[s] = (double *)malloc(sizeof(double) * 2 * (size_t)N);
+   /* curr_ffts counts source FFTs in doMaths order (TaskCoreIPP.cpp:633) */
+   int curr_ffts = j->f0 * c->num_sources;
+   for (int f = j->f0; f < j->f1; f++) {
+      int sp = j->spec_of[f];
+      for (int s = 0; s < c->num_sources; s++) {
+         const float *x = j->samples[s] + j->starts[f];
+         if (c->extract_pcal && (curr_ffts % c->overlap) == 0) {
+            double *pc = j->pcal_acc + 2 * ((size_t)sp * c->num_sources + s) * c->pcal_tonebins;
+            /* only whole tone periods of each rotator block are folded
+             * (the reference's integer division rotatorlen/tonebins) */
+            int used = (c->pcal_rotatorlen / c->pcal_tonebins) * c->pcal_tonebins;
+            for (int n = 0; n < N; n++) {
+               int ph = n % c->pcal_rotatorlen;
+               if (ph >= used) continue;
+               int b = ph % c->pcal_tonebins;
+               pc[2 * b] += (double)x[n] * j->rot[ph].re;
+               pc[2 * b + 1] += (double)x[n] * j->rot[ph].im;
+            }
+         }
+         for (int n = 0; n < N; n++) {
+            in[2 * n] = (double)x[n] * (double)j->win[n];
+            in[2 * n + 1] = 0.0;
+         }
+         orc_fft64(N, in, X[s]);
+         curr_ffts++;
+         double *oa = j->auto_acc + ((size_t)sp * c->num_sources + s) * S;
+         for (int k = 0; k < S; k++) oa[k] += X[s][2 * k] * X[s][2 * k] + X[s][2 * k + 1] * X[s][2 * k + 1];
+      }
+      for (int xp = 0; xp < c->num_xpols; xp++) {
+         const double *A = X[j->pairs[2 * xp]], *B = X[j->pairs[2 * xp + 1]];
+         double *ox = j->xpol_acc + 2 * ((size_t)sp * c->num_xpols + xp) * S;
+         for (int k = 0; k < S; k++) {
+            ox[2 * k] += A[2 * k] * B[2 * k] + A[2 * k + 1] * B[2 * k + 1];
+            ox[2 * k + 1] += A[2 * k + 1] * B[2 * k] - A[2 * k] * B[2 * k + 1];
+         }
+         ox[1] = 0.0;
+         ox[2 * (S - 1) + 1] = 0.0;
+      }
+   }
+   free(in);
+   for (int s = 0; s < c->num_sources; s++) free(X[s]);
+   free(X);
+   return NULL;
+}
+
+/* FP64 oracle over one buffer (doMaths, TaskCoreIPP.cpp:355-560).  With
+ * c->nthreads > 1 the FFTs are split into contiguous ranges, one per
+ * thread, and the thread-private FP64 sums are added in thread order. */
 int orc_domaths64(const orc_cfg *c, const float *const *samples, int64_t nsamp, double *out_auto,
                   double *out_xpol, double *out_pcal)
 {
@@ -578,9 +646,6 @@ int orc_domaths64(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
 
    float *win = (float *)malloc(sizeof(float) * (size_t)N);
    orc_window(c->window, N, win);
-   double *in = (double *)malloc(sizeof(double) * 2 * (size_t)N);
-   double **X = (double **)malloc(sizeof(double *) * (size_t)c->num_sources);
-   for (int s = 0; s < c->num_sources; s++) X[s] = (double *)malloc(sizeof(double) * 2 * (size_t)N);
    int *pairs = (int *)malloc(sizeof(int) * 2 * (size_t)(c->num_xpols + 1));
    orc_xpol_pairs(c->num_sources, c->num_xpols, pairs);
    c64 *rot = NULL;
@@ -592,47 +657,39 @@ int orc_domaths64(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
          rot[i].im = sin(dphi * (double)i);
       }
    }
-   memset(out_auto, 0, sizeof(double) * (size_t)nspec * c->num_sources * S);
-   if (c->num_xpols) memset(out_xpol, 0, sizeof(double) * 2 * (size_t)nspec * c->num_xpols * S);
-   if (c->extract_pcal)
-      memset(out_pcal, 0, sizeof(double) * 2 * (size_t)nspec * c->num_sources * c->pcal_tonebins);
+   size_t na = (size_t)nspec * c->num_sources * S, nx = 2 * (size_t)nspec * c->num_xpols * S,
+          np = 2 * (size_t)nspec * c->num_sources * (c->extract_pcal ? c->pcal_tonebins : 0);
+   memset(out_auto, 0, sizeof(double) * na);
+   if (nx) memset(out_xpol, 0, sizeof(double) * nx);
+   if (np) memset(out_pcal, 0, sizeof(double) * np);
 
-   int curr_ffts = 0;
-   for (int f = 0; f < nf; f++) {
-      int sp = spec_of[f];
-      for (int s = 0; s < c->num_sources; s++) {
-         const float *x = samples[s] + starts[f];
-         if (c->extract_pcal && (curr_ffts % c->overlap) == 0) {
-            double *pc = out_pcal + 2 * ((size_t)sp * c->num_sources + s) * c->pcal_tonebins;
-            /* only whole tone periods of each rotator block are folded
-             * (the reference's integer division rotatorlen/tonebins) */
-            int used = (c->pcal_rotatorlen / c->pcal_tonebins) * c->pcal_tonebins;
-            for (int n = 0; n < N; n++) {
-               int ph = n % c->pcal_rotatorlen;
-               if (ph >= used) continue;
-               int b = ph % c->pcal_tonebins;
-               pc[2 * b] += (double)x[n] * rot[ph].re;
-               pc[2 * b + 1] += (double)x[n] * rot[ph].im;
-            }
-         }
-         for (int n = 0; n < N; n++) {
-            in[2 * n] = (double)x[n] * (double)win[n];
-            in[2 * n + 1] = 0.0;
-         }
-         orc_fft64(N, in, X[s]);
-         curr_ffts++;
-         double *oa = out_auto + ((size_t)sp * c->num_sources + s) * S;
-         for (int k = 0; k < S; k++) oa[k] += X[s][2 * k] * X[s][2 * k] + X[s][2 * k + 1] * X[s][2 * k + 1];
+   int nt = c->nthreads < 1 ? 1 : c->nthreads;
+   if (nt > nf) nt = nf > 0 ? nf : 1;
+   orc_job64 *jobs = (orc_job64 *)calloc((size_t)nt, sizeof(orc_job64));
+   pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nt);
+   for (int t = 0; t < nt; t++) {
+      orc_job64 *j = &jobs[t];
+      j->c = c; j->samples = samples; j->starts = starts; j->spec_of = spec_of;
+      j->f0 = (int)((long long)nf * t / nt);
+      j->f1 = (int)((long long)nf * (t + 1) / nt);
+      j->win = win; j->rot = rot; j->pairs = pairs;
+      if (nt == 1) {
+         j->auto_acc = out_auto; j->xpol_acc = out_xpol; j->pcal_acc = out_pcal;
+         orc_worker64(j);
+      } else {
+         j->auto_acc = (double *)calloc(na + 1, sizeof(double));
+         j->xpol_acc = (double *)calloc(nx + 1, sizeof(double));
+         j->pcal_acc = (double *)calloc(np + 1, sizeof(double));
+         pthread_create(&th[t], NULL, orc_worker64, j);
       }
-      for (int xp = 0; xp < c->num_xpols; xp++) {
-         const double *A = X[pairs[2 * xp]], *B = X[pairs[2 * xp + 1]];
-         double *ox = out_xpol + 2 * ((size_t)sp * c->num_xpols + xp) * S;
-         for (int k = 0; k < S; k++) {
-            ox[2 * k] += A[2 * k] * B[2 * k] + A[2 * k + 1] * B[2 * k + 1];
-            ox[2 * k + 1] += A[2 * k + 1] * B[2 * k] - A[2 * k] * B[2 * k + 1];
-         }
-         ox[1] = 0.0;
-         ox[2 * (S - 1) + 1] = 0.0;
+   }
+   if (nt > 1) {
+      for (int t = 0; t < nt; t++) {
+         pthread_join(th[t], NULL);
+         for (size_t i = 0; i < na; i++) out_auto[i] += jobs[t].auto_acc[i];
+         for (size_t i = 0; i < nx; i++) out_xpol[i] += jobs[t].xpol_acc[i];
+         for (size_t i = 0; i < np; i++) out_pcal[i] += jobs[t].pcal_acc[i];
+         free(jobs[t].auto_acc); free(jobs[t].xpol_acc); free(jobs[t].pcal_acc);
       }
    }
    /* scale completed spectra; a trailing partial spectrum stays unscaled */
@@ -641,9 +698,7 @@ int orc_domaths64(const orc_cfg *c, const float *const *samples, int64_t nsamp, 
    for (size_t i = 0; i < (size_t)nfull * c->num_sources * S; i++) out_auto[i] *= sc;
    for (size_t i = 0; i < 2 * (size_t)nfull * c->num_xpols * S; i++) out_xpol[i] *= sc;
 
-   free(starts); free(spec_of); free(win); free(in);
-   for (int s = 0; s < c->num_sources; s++) free(X[s]);
-   free(X); free(pairs); free(rot);
+   free(jobs); free(th); free(starts); free(spec_of); free(win); free(pairs); free(rot);
    return nspec;
 }
 

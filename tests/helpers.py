@@ -1,6 +1,8 @@
 """Shared test helpers: oracle runs and error metrics."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 import oracle as O
@@ -31,7 +33,7 @@ def decode_channels(framed: bytes, fmt: str, nchan: int, nbit: int, chans, nsamp
 
 def oracle_run(samples, N, window, overlap, cof, nxpols=0, pcal=None):
     cfg = O.make_cfg(N, overlap=overlap, core_overlapped_ffts=cof, num_sources=len(samples),
-                     num_xpols=nxpols, window=O.WINDOW_NAMES[window])
+                     num_xpols=nxpols, window=O.WINDOW_NAMES[window], nthreads=os.cpu_count() or 1)
     if pcal:
         cfg.extract_pcal = 1
         cfg.pcal_tonebins, cfg.pcal_rotatorlen = pcal["tonebins"], pcal["rotatorlen"]

@@ -6,8 +6,16 @@ mark5access), FileSink, Buffer, IniParser and LogFile, compiled from the
 reference sources -- with TaskDispatcher.h selecting TaskCoreCUDA
 (swspec_b200/refcore/TaskCoreCUDA.cpp), a subclass of the reference's
 abstract TaskCore (src/TaskCore.h:36-89) over libswsgpu.so.  These tests run
-that program on Mark5B files and compare the spectrum files it writes with
+that program on recordings and compare the spectrum files it writes with
 the FP64 oracle over the same core-run schedule.
+
+The reference's framed FileSource::read (src/FileSource.cpp:185-210) always
+reads the rest of the current frame, however little room the buffer has
+left: a raw buffer that is not a whole number of frame payloads is overrun
+(heap memory past it is overwritten) and the next buffer starts at the next
+frame.  The settings below therefore give buffers of whole frames: Mk5B at
+N = 20000 (640000-byte buffers, 64 payloads of 10000 bytes) and iBOB at
+N = 8192 (393216-byte buffers, 96 payloads of 4096 bytes).
 """
 import os
 import subprocess
@@ -15,7 +23,8 @@ import subprocess
 import numpy as np
 import pytest
 
-from test_host import PCAL, _ini, _model_runs, _pcal_signal_files
+import oracle as O
+from test_host import _ini, _model_runs, _pcal_signal_files, _settings
 from swspec_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -33,18 +42,17 @@ def _run(tmp_path, ini, files, precision):
     return r
 
 
-@pytest.mark.parametrize("precision", ["fp32", "tcsplit"])
-def test_reference_dispatcher_drives_gpu_core(tmp_path, gpu, precision):
+def test_reference_dispatcher_mk5b_combined_spectra(tmp_path, gpu):
     """Two Mk5B files (channels 3 and 12 of 16, 2-bit), cross-pol and PCal,
-    each spectrum summed over 3 core runs (MaxSourceBufferMB = 1): the
-    reference's dispatcher loop writes 2 spectra per file, the cross spectrum
-    with the half length its combineResults sets, and phase-cal vectors."""
-    N, fs = 4096, 32e6
-    files = _pcal_signal_files(tmp_path, 197, fs, 77)
-    ini = _ini(tmp_path, f"""[Spectrometer]
+    each spectrum summed over 3 core runs: the reference's dispatcher writes
+    2 spectra per file, the cross spectrum with the half length its
+    combineResults sets (TaskCoreIPP.cpp:333), and phase-cal vectors."""
+    N, fs = 20000, 32e6
+    files = _pcal_signal_files(tmp_path, 450, fs, 77)
+    body = f"""[Spectrometer]
 NumCPUCores = 1
 FFTpoints = {N}
-FFTIntegrationTimeSec = 0.00615
+FFTIntegrationTimeSec = 0.015
 FFToverlapFactor = 1
 BandwidthHz = 16e6
 WindowType = Hann
@@ -55,22 +63,20 @@ UseFile1Channel = 3
 UseFile2Channel = 12
 DoCrossPolarization = yes
 ExtractPCal = yes
-PCalOffsetHz = 15625
+PCalOffsetHz = 200000
 MaxSourceBufferMB = 1
 BaseFilename1 = r_%channel%
-""")
-    if precision == "tcsplit":
-        # the split form exists for N = 8192 .. 65536
-        ini = _ini(tmp_path, open(ini).read().replace(f"FFTpoints = {N}", "FFTpoints = 8192")
-                   .replace("0.00615", "0.0123"))
-        N = 8192
-    _run(tmp_path, ini, files, precision)
-    rawbuf = 262144 if N == 4096 else 524288
-    cof = rawbuf * 8 // (2 * 16) // N
+"""
+    ini = _ini(tmp_path, body)
+    s = _settings(ini, 2)
+    rawbuf, cof = s["rawbuf_size"], s["core_overlapped_ffts"]
+    assert rawbuf % 10000 == 0 and s["max_buffers_per_spectrum"] == 3, s
+    _run(tmp_path, ini, files, "fp32")
     pays = [synth.strip_headers((tmp_path / f).read_bytes(), 10016, 16) for f in files]
-    runs = _model_runs(pays, rawbuf, N, 1, cof, [2, 11], 16, pcal=PCAL, xpol=True)
+    pcal = dict(tonebins=32, rotatorlen=160, fs=fs, offset=200e3)
+    runs = _model_runs(pays, rawbuf, N, 1, cof, [2, 11], 16, pcal=pcal, xpol=True)
     ngroup = len(runs) // 3
-    assert ngroup >= 1
+    assert ngroup == 2
     groups = [[sum(r[i][0] for r in runs[3 * g:3 * g + 3]) for i in range(3)] for g in range(ngroup)]
     S = N // 2 + 1
     a = [np.fromfile(tmp_path / f"r_{c}_swspec.bin", dtype=np.float32).reshape(-1, S) for c in (3, 12)]
@@ -88,3 +94,68 @@ BaseFilename1 = r_%channel%
         ni = np.repeat(norm, 2)[:S]
         assert np.max(np.abs(xp[g] - ri) / ni) < 2e-6
     assert (tmp_path / "r_3_runlog.txt").exists() and (tmp_path / "r_3_starttiming.txt").exists()
+
+
+def _ibob_file(path, nframes, seed, tone):
+    """iBOB capture: frames of a 4-byte header and 4096 bytes of signed 8-bit
+    samples, two channels interleaved (a tone in channel 0)."""
+    rng = np.random.default_rng(seed)
+    n = nframes * 2048
+    t = np.arange(n)
+    x = rng.standard_normal((n, 2)) * 20
+    x[:, 0] += tone * np.cos(2 * np.pi * 0.0711 * t)
+    q = np.clip(np.round(x), -128, 127).astype(np.int8).reshape(nframes, 4096).view(np.uint8)
+    hdr = np.zeros((nframes, 4), np.uint8)
+    hdr[:, 3] = np.arange(nframes) & 0xFF
+    path.write_bytes(np.concatenate([hdr, q], axis=1).tobytes())
+    return q.reshape(-1).tobytes()
+
+
+@pytest.mark.parametrize("precision", ["tcsplit", "tcsplit_all", "fp32"])
+def test_reference_dispatcher_ibob_spectra_per_buffer(tmp_path, gpu, precision):
+    """Two iBOB files (signed 8-bit, two channels; channel 1 of the first and
+    channel 2 of the second), cross-pol, N = 8192: one whole spectrum per
+    core run written straight from the cores' output buffers
+    (TaskDispatcher.cpp:172-191), on each GPU form."""
+    N = 8192
+    pays = [_ibob_file(tmp_path / f"in{k}.ibob", 400, 30 + k, 8.0 * (k + 1)) for k in range(2)]
+    ini = _ini(tmp_path, f"""[Spectrometer]
+FFTpoints = {N}
+FFTIntegrationTimeSec = 0.006144
+FFToverlapFactor = 1
+BandwidthHz = 16e6
+WindowType = Hann
+SourceFormat = iBob
+BitsPerSample = 8
+SourceChannels = 2
+UseFile1Channel = 1
+UseFile2Channel = 2
+DoCrossPolarization = yes
+MaxSourceBufferMB = 1
+BaseFilename1 = b_%channel%
+""")
+    s = _settings(ini, 2)
+    rawbuf, cof, nsp = s["rawbuf_size"], s["core_overlapped_ffts"], s["max_spectra_per_buffer"]
+    assert rawbuf % 4096 == 0 and nsp >= 1 and s["max_buffers_per_spectrum"] == 0, s
+    _run(tmp_path, ini, ["in0.ibob", "in1.ibob"], precision)
+    S = N // 2 + 1
+    nbuf = len(pays[0]) // rawbuf
+    ra_all, rx_all = [], []
+    for b in range(nbuf):
+        smp = [O.decode(O.FMT_RAW_SIGNED, 2, 8, p[b * rawbuf:(b + 1) * rawbuf], rawbuf // 2, c)
+               for p, c in zip(pays, (0, 1))]
+        cfg = O.make_cfg(N, core_overlapped_ffts=cof, num_sources=2, num_xpols=1, window=O.W_HANN,
+                         nthreads=os.cpu_count() or 1)
+        ra, rx, _, n = O.domaths(cfg, smp)
+        ra_all.append(ra[:nsp])
+        rx_all.append(rx[:nsp, 0])
+    ra = np.concatenate(ra_all)
+    rx = np.concatenate(rx_all)
+    a0 = np.fromfile(tmp_path / "b_1_swspec.bin", dtype=np.float32).reshape(-1, S)
+    a1 = np.fromfile(tmp_path / "b_2_swspec.bin", dtype=np.float32).reshape(-1, S)
+    xp = np.fromfile(tmp_path / "b_1_xpol_swspec.bin", dtype=np.float32).reshape(-1, S, 2)
+    assert a0.shape[0] == a1.shape[0] == xp.shape[0] == ra.shape[0] == nbuf * nsp
+    assert np.max(np.abs(a0 - ra[:, 0]) / ra[:, 0]) < 2e-6
+    assert np.max(np.abs(a1 - ra[:, 1]) / ra[:, 1]) < 2e-6
+    xc = xp[..., 0] + 1j * xp[..., 1]
+    assert np.max(np.abs(xc - rx) / np.sqrt(ra[:, 0] * ra[:, 1])) < 2e-6
