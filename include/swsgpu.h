@@ -305,12 +305,16 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
  * every device that loads the library holds it until the process exits.
  * Limit: at most SWSGPU_NOALLOC_MAX_FRAMES frames per call (about 160 MB of
  * Mark5B data); larger requests return SWSGPU_ETOOBIG.  The caller still
- * provides d_raw and d_out.  The first call on each device looks up the
- * scratch address for that device (cudaGetSymbolAddress), so make that first
- * call before any stream capture.  All calls share the one scratch array:
- * calls that overlap on the GPU (for example on two streams at once) race
- * and must be serialised by the caller.  Returns like swsgpu_unpack_device,
- * waiting for its own stream. */
+ * provides d_raw and d_out.  The first call on each device is the one that
+ * is not allocation-free: it looks up the scratch address for that device
+ * (cudaGetSymbolAddress), which loads the library's device code and
+ * allocates the array there; make one small warm-up call per device at
+ * start-up, outside the thread that must not allocate.  Every call
+ * synchronises its stream (it reads the sample count back), so it cannot
+ * be issued on a stream that is being captured.  All calls share the one
+ * scratch array: calls that overlap on the GPU (for example on two streams
+ * at once) race and must be serialised by the caller.  Returns like
+ * swsgpu_unpack_device; on a CUDA error swsgpu_last_error(NULL) describes it. */
 #define SWSGPU_NOALLOC_MAX_FRAMES 16384
 #define SWSGPU_NOALLOC_SCRATCH_BYTES (SWSGPU_NOALLOC_MAX_FRAMES * 8 + 256)
 int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,

@@ -111,6 +111,21 @@ int FileSource::read(Buffer *buf)
             memcpy(&sync, hdr.data(), 4);
             if (sync != kMark5BSync) *cfg_->tlog << "FileSource: Mark5B sync word mismatch" << std::endl;
          }
+         if (cfg_->sourceformat == VDIF && cfg_->vdif_thread >= 0) {
+            // multi-thread VDIF: the thread id is bits 16-25 of header word 3;
+            // frames of other threads are skipped whole, so the kept frames
+            // form one contiguous stream
+            uint32_t w3;
+            memcpy(&w3, hdr.data() + 12, 4);
+            if ((int)((w3 >> 16) & 0x3FFu) != cfg_->vdif_thread) {
+               ifile_.seekg(payload, std::ios::cur);
+               if (!ifile_.good()) {
+                  got_eof_ = true;
+                  break;
+               }
+               continue;
+            }
+         }
          pending_header_ = false;
          in_frame_ = 0;
       }

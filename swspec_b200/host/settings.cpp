@@ -50,8 +50,11 @@ int load_ini(Settings &s, const std::string &inifile, std::string &err)
    }
    // keys of the GPU core
    if (ini.getKeyValue("GpuPrecision", keyval))
-      s.gpu_precision = (strcasecmp(keyval.c_str(), "TCSPLIT") == 0) ? SWSGPU_PREC_TCSPLIT : SWSGPU_PREC_FP32;
+      s.gpu_precision = (strcasecmp(keyval.c_str(), "TCSPLIT") == 0)       ? SWSGPU_PREC_TCSPLIT
+                        : (strcasecmp(keyval.c_str(), "TCSPLIT_ALL") == 0) ? SWSGPU_PREC_TCSPLIT_ALL
+                                                                            : SWSGPU_PREC_FP32;
    ini.getKeyValue("GpuDevice", s.gpu_device);
+   ini.getKeyValue("VdifThread", s.vdif_thread);
    ini.getKeyValue("GpuCombineOnDevice", s.gpu_combine_on_device);
    ini.getKeyValue("GpuAutotune", s.gpu_autotune);
    ini.getKeyValue("FixXpolLength", s.fix_xpol_length);

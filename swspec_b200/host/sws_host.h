@@ -106,6 +106,7 @@ struct Settings {
    // GPU core keys (new; the reference's parser ignores unknown keys)
    int gpu_precision = SWSGPU_PREC_FP32;  // GpuPrecision = FP32 | TCSPLIT
    int gpu_device = 0;                    // GpuDevice
+   int vdif_thread = -1;                  // VdifThread: keep only the frames of this VDIF thread (-1: all)
    bool gpu_combine_on_device = true;     // GpuCombineOnDevice
    bool gpu_autotune = false;             // GpuAutotune: time the four-step splits of the length at prepare
    bool fix_xpol_length = false;          // FixXpolLength (reference quirk: half of XY* written)

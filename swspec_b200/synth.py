@@ -112,8 +112,9 @@ def mark5b_frames(payload: bytes, mbps: int, mjd: int = 57000, sec: int = 100) -
 
 
 def vdif_frames(payload: bytes, payload_bytes: int, nchan: int, nbit: int, frames_per_sec: int,
-                sec: int = 1000000, epoch: int = 30, invalid: set | None = None) -> bytes:
-    """Wrap a payload stream into VDIF frames with 32-byte headers."""
+                sec: int = 1000000, epoch: int = 30, invalid: set | None = None, thread: int = 0) -> bytes:
+    """Wrap a payload stream into VDIF frames with 32-byte headers (thread id
+    in bits 16-25 of word 3)."""
     assert len(payload) % payload_bytes == 0
     nfr = len(payload) // payload_bytes
     fb = VDIF_HEADER + payload_bytes
@@ -130,7 +131,7 @@ def vdif_frames(payload: bytes, payload_bytes: int, nchan: int, nbit: int, frame
         hdr[f, 0] = w0
         hdr[f, 1] = (epoch << 24) | (fn & 0xFFFFFF)
         hdr[f, 2] = (log2nchan << 24) | (fb // 8)
-        hdr[f, 3] = ((nbit - 1) << 26) | 0x4142  # station id "AB"
+        hdr[f, 3] = ((nbit - 1) << 26) | ((thread & 0x3FF) << 16) | 0x4142  # station id "AB"
     out[:, :VDIF_HEADER] = hdr.view(np.uint8).reshape(nfr, VDIF_HEADER)
     return out.tobytes()
 

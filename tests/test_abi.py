@@ -47,3 +47,11 @@ def test_create_rejects_bad_config():
     cfg = gpu.make_config(gpu.layout("mark5b", 16, 2), 32768, overlap=3)
     with pytest.raises(gpu.SwsError, match="EINVAL|ENODEV"):
         gpu.Core(cfg)
+
+
+def test_noalloc_source_names_no_allocation_call():
+    """The allocation-free decode entry's source file calls no allocator."""
+    src = open(os.path.join(ROOT, "swspec_b200", "csrc", "noalloc.cu")).read()
+    code = re.sub(r"//.*", "", src)
+    for name in ("cudaMalloc", "cudaMallocAsync", "cudaFree", "cudaMallocHost", "cudaMallocManaged"):
+        assert not re.search(rf"\b{name}\s*\(", code), name

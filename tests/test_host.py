@@ -231,3 +231,50 @@ BaseFilename1 = o_%fftpoints%
         ref = np.concatenate([flat[0:2 * npair:2], flat[1:2]])
         assert vals.shape == ref.shape
         assert np.max(np.abs(vals - ref) / ref) < 2e-6
+
+
+@pytest.mark.gpu
+def test_cli_multithread_vdif_selects_one_thread(tmp_path, gpu):
+    """A VDIF recording with two interleaved threads (frames alternate between
+    thread 0 and thread 1, each its own signal): VdifThread = 1 keeps that
+    thread's frames only, which then form one contiguous stream (two whole
+    512 KiB buffers of 32 spectra each; the third meets the end of file)."""
+    N, cof = 8192, 8
+    rng = np.random.default_rng(61)
+    nfr = 140
+    frames = []
+    codes_by_thread = []
+    for th in range(2):
+        pay = rng.integers(0, 256, nfr * 8000, dtype=np.uint8).tobytes()
+        codes_by_thread.append(pay)
+        frames.append(np.frombuffer(synth.vdif_frames(pay, 8000, 1, 2, 4000, thread=th),
+                                    dtype=np.uint8).reshape(nfr, -1))
+    inter = np.stack(frames, axis=1).reshape(-1).tobytes()   # t0 f0, t1 f0, t0 f1, ...
+    (tmp_path / "mt.vdif").write_bytes(inter)
+    ini = _ini(tmp_path, f"""[Spectrometer]
+FFTpoints = {N}
+FFTIntegrationTimeSec = 0.002048
+FFToverlapFactor = 1
+BandwidthHz = 16e6
+WindowType = Hann
+SourceFormat = VDIF_8000-64-1-2
+VdifThread = 1
+MaxSourceBufferMB = 1
+BaseFilename1 = v
+""")
+    s = _settings(ini, 1)
+    rawbuf = s["rawbuf_size"]
+    assert rawbuf == 524288 and s["max_spectra_per_buffer"] == 32, s
+    _run_cli(tmp_path, ini, ["mt.vdif"])
+    pay1 = codes_by_thread[1]
+    nbuf = len(pay1) // rawbuf
+    ref = []
+    for b in range(nbuf):
+        x = O.decode(O.FMT_VDIF, 1, 2, pay1[b * rawbuf:(b + 1) * rawbuf], rawbuf * 4, 0)
+        cfg = O.make_cfg(N, core_overlapped_ffts=s["core_overlapped_ffts"], num_sources=1, window=O.W_HANN)
+        ra, _, _, n = O.domaths(cfg, [x])
+        ref.append(ra[:, 0])
+    ref = np.concatenate(ref)
+    got = np.fromfile(tmp_path / "v_swspec.bin", dtype=np.float32).reshape(-1, N // 2 + 1)
+    assert got.shape == ref.shape == (64, N // 2 + 1), (got.shape, ref.shape)
+    assert np.max(np.abs(got - ref) / ref) < 2e-6

@@ -62,3 +62,22 @@ def test_noalloc_rejects_more_frames_than_its_scratch_holds(gpu):
     rc = lib.swsgpu_unpack_device_noalloc(C.byref(lay), d.data_ptr(), 2 ** 40, 0, 0, nsamp,
                                           out.data_ptr(), C.byref(nv), None)
     assert rc == -6  # SWSGPU_ETOOBIG
+
+
+def test_noalloc_allocates_nothing_after_the_warm_up_call(gpu):
+    """After one warm-up call per device (which loads the scratch array),
+    further calls leave the device's free memory unchanged."""
+    import torch
+    rng = np.random.default_rng(5)
+    raw = synth.mark5b_stream(rng.standard_normal((16, 2500 * 6)), 2, 1024)
+    d = torch.from_numpy(np.frombuffer(raw, dtype=np.uint8).copy()).cuda()
+    out = torch.empty(2500 * 5, dtype=torch.float32, device="cuda")
+    lay = gpu.layout("mark5b", 16, 2)
+    gpu.unpack_device_noalloc(lay, d.data_ptr(), d.numel(), 0, 3, 2500 * 5, out.data_ptr())
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for chan in range(16):
+        gpu.unpack_device_noalloc(lay, d.data_ptr(), d.numel(), 0, chan, 2500 * 5, out.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
