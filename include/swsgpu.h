@@ -321,6 +321,50 @@ int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void *d_raw, si
                                  int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
                                  int64_t *nvalid, void *cuda_stream);
 
+/* The reference's phase-cal extractor library (src/IA-32/PhaseCal/PCal.h,
+ * PCal.cpp) on the GPU: a stateful extractor over a stream of float samples
+ * in device memory (e.g. swsgpu_unpack_device output).
+ *   swsgpu_pcal_create      -> PCal::getNew (PCal.cpp:92-112); kind
+ *                              SWSGPU_PCAL_AUTO takes the factory's choice,
+ *                              the others force a class; the indices start
+ *                              from sampleoffset (the reference's
+ *                              constructors leave them unset)
+ *   swsgpu_pcal_info        -> getLength (tone count), plus class and bins
+ *   swsgpu_pcal_clear       -> clear (:229-241, :387-400, :575-587)
+ *   swsgpu_pcal_adjust_offset -> adjustSampleOffset (:243-247, :402-406, :589-592)
+ *   swsgpu_pcal_extract     -> extractAndIntegrate (:265-296, :424-487, :610-652);
+ *                              asynchronous on cuda_stream; SWSGPU_ESTATE
+ *                              after a final until clear, as the reference
+ *                              returns false
+ *   swsgpu_pcal_final       -> getFinalPCal (:298-318, :489-517, :654-678):
+ *                              ntones complex tones (re, im doubles) into
+ *                              host memory, *nsamples = samples integrated;
+ *                              waits for cuda_stream
+ * Sums and the DFT are FP64 (the reference's are FP32).  Shifting keeps the
+ * reference's per-period sample selection (only floor(R/N)*N rotated
+ * samples of every whole rotator period R are added). */
+#define SWSGPU_PCAL_AUTO 0
+#define SWSGPU_PCAL_TRIVIAL 1
+#define SWSGPU_PCAL_SHIFTING 2
+#define SWSGPU_PCAL_IMPLICIT 3
+typedef struct swsgpu_pcal swsgpu_pcal;
+int swsgpu_pcal_create(double bandwidth_hz, double spacing_hz, int offset_hz, int64_t sampleoffset, int kind,
+                       int device, swsgpu_pcal **out);
+int swsgpu_pcal_info(const swsgpu_pcal *p, int *kind, int *nbins, int *ntones);
+int swsgpu_pcal_clear(swsgpu_pcal *p);
+int swsgpu_pcal_adjust_offset(swsgpu_pcal *p, int64_t sampleoffset);
+int swsgpu_pcal_extract(swsgpu_pcal *p, const float *d_samples, int64_t len, void *cuda_stream);
+int swsgpu_pcal_final(swsgpu_pcal *p, double *tones_reim, uint64_t *nsamples, void *cuda_stream);
+void swsgpu_pcal_destroy(swsgpu_pcal *p);
+
+/* Tone-phase delay in ns from extracted tones: calcDelay of mark5access's
+ * pulse-cal tool (mark5access/examples/m5pcal.c:96-155) -- the mean slope
+ * of neighbouring tones' phase differences (radians, frequencies in MHz)
+ * within band_valid_mhz of band_center_mhz, each unwrapped against the
+ * difference at the middle of the list, folded into +- 500 / spacing. */
+double swsgpu_pcal_delay(int ntones, const int *tone_mhz, const double *phase, double band_center_mhz,
+                         double band_valid_mhz);
+
 /* Number of kernel launches the last submit / process_device call issued. */
 int swsgpu_last_launch_count(const swsgpu_handle *h);
 

@@ -145,6 +145,50 @@ def ref_unpack_raw(kind: int, nbit: int, nchan: int, payload: bytes, count: int,
     return out[:count]
 
 
+class PcalLib:
+    """The reference's PCal extractor classes (src/IA-32/PhaseCal/PCal.cpp)
+    as restated in C: kind 0 = PCal::getNew's choice, 1 Trivial, 2 Shifting,
+    3 ImplicitShift."""
+
+    def __init__(self, bandwidth_hz, spacing_hz, offset_hz, sampleoffset=0, kind=0):
+        L = lib()
+        L.orc_pcallib_new.restype = C.c_void_p
+        L.orc_pcallib_new.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int64, C.c_int]
+        L.orc_pcallib_free.argtypes = [C.c_void_p]
+        L.orc_pcallib_clear.argtypes = [C.c_void_p]
+        L.orc_pcallib_adjust.argtypes = [C.c_void_p, C.c_int64]
+        L.orc_pcallib_extract.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        L.orc_pcallib_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3
+        L.orc_pcallib_final.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_pcallib_final.restype = C.c_uint64
+        self.L = L
+        self.h = L.orc_pcallib_new(bandwidth_hz, spacing_hz, int(offset_hz), int(sampleoffset), kind)
+        k, nb, nt = C.c_int(), C.c_int(), C.c_int()
+        L.orc_pcallib_info(self.h, C.byref(k), C.byref(nb), C.byref(nt))
+        self.kind, self.nbins, self.ntones = k.value, nb.value, nt.value
+
+    def extract(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        self.L.orc_pcallib_extract(self.h, x.ctypes.data, len(x))
+
+    def adjust(self, sampleoffset):
+        self.L.orc_pcallib_adjust(self.h, int(sampleoffset))
+
+    def clear(self):
+        self.L.orc_pcallib_clear(self.h)
+
+    def final(self):
+        out = np.zeros(2 * self.ntones)
+        n = self.L.orc_pcallib_final(self.h, out.ctypes.data)
+        return out[0::2] + 1j * out[1::2], int(n)
+
+    def __del__(self):
+        try:
+            self.L.orc_pcallib_free(self.h)
+        except Exception:
+            pass
+
+
 def m5_format_info(fmt: str) -> dict:
     r = ref()
     vals = [C.c_int() for _ in range(6)]

@@ -895,3 +895,174 @@ int orc_pcal_tones(int tonebins, const double *bins_reim, double nfolded, int nt
    }
    return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The PCal extractor library (src/IA-32/PhaseCal/PCal.cpp)                 */
+/* ------------------------------------------------------------------------ */
+
+/* State of one extractor.  kind: 1 Trivial (:183-318), 2 Shifting
+ * (:321-517), 3 ImplicitShift (:521-678).  Sums are kept in FP64 here (the
+ * reference adds in FP32); the index bookkeeping and the tone selection are
+ * the reference's, quirks included: Shifting adds, per full rotator period,
+ * only the first floor(R/N)*N rotated samples (:451-462), and both indices
+ * start from the sample offset given at creation (the reference's
+ * constructors leave them unset until adjustSampleOffset). */
+typedef struct {
+   int kind;
+   double fs, spacing, offset;
+   int nbins, ntones, rotlen;
+   int64_t pcal_index, rotator_index;
+   uint64_t samplecount;
+   float *rot_re, *rot_im; /* FP32 oscillator table, 2 * rotlen entries (:350-355) */
+   double *acc;            /* [2 * nbins][re, im] */
+} orc_pcallib;
+
+static long long orc_gcdll(long long a, long long b)
+{
+   while (b) {
+      long long t = a % b;
+      a = b;
+      b = t;
+   }
+   return a < 0 ? -a : a;
+}
+
+void *orc_pcallib_new(double bandwidth_hz, double spacing_hz, int offset_hz, int64_t sampleoffset, int kind)
+{
+   orc_pcallib *p = (orc_pcallib *)calloc(1, sizeof(orc_pcallib));
+   const long long fs = (long long)(2.0 * bandwidth_hz);
+   p->fs = (double)fs;
+   p->spacing = spacing_hz;
+   p->offset = offset_hz;
+   if (kind == 0) { /* PCal::getNew (:92-112) */
+      if (offset_hz == 0) kind = 1;
+      else {
+         long long No = fs / orc_gcdll(offset_hz, fs), Np = fs / orc_gcdll((long long)spacing_hz, fs);
+         kind = (No % Np == 0) ? 3 : 2;
+      }
+   }
+   p->kind = kind;
+   if (kind == 3) {
+      p->nbins = (int)(fs / orc_gcdll(offset_hz, fs));
+      p->ntones = (int)floor((bandwidth_hz - offset_hz) / spacing_hz) + 1;
+   } else {
+      p->nbins = (int)(fs / orc_gcdll((long long)fabs(spacing_hz), fs));
+      p->ntones = kind == 1 ? (int)floor(bandwidth_hz / spacing_hz)
+                            : (int)floor((bandwidth_hz - offset_hz) / spacing_hz) + 1;
+   }
+   p->rotlen = kind == 2 ? (int)(fs / orc_gcdll((long long)abs(offset_hz), fs)) : p->nbins;
+   p->acc = (double *)calloc(4 * (size_t)p->nbins, sizeof(double));
+   if (kind == 2) {
+      p->rot_re = (float *)malloc(sizeof(float) * 2 * (size_t)p->rotlen);
+      p->rot_im = (float *)malloc(sizeof(float) * 2 * (size_t)p->rotlen);
+      double dphi = 2 * M_PI * (-(double)offset_hz / p->fs);
+      for (int n = 0; n < 2 * p->rotlen; n++) {
+         p->rot_re[n] = (float)cos(dphi * (double)n);
+         p->rot_im[n] = (float)sin(dphi * (double)n);
+      }
+   }
+   p->pcal_index = sampleoffset % p->nbins;
+   p->rotator_index = sampleoffset % p->rotlen;
+   return p;
+}
+
+void orc_pcallib_free(void *h)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   if (!p) return;
+   free(p->acc); free(p->rot_re); free(p->rot_im); free(p);
+}
+
+void orc_pcallib_clear(void *h)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   memset(p->acc, 0, sizeof(double) * 4 * (size_t)p->nbins);
+   p->samplecount = 0;
+}
+
+void orc_pcallib_adjust(void *h, int64_t sampleoffset)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   p->pcal_index = sampleoffset % p->nbins;
+   if (p->kind == 2) p->rotator_index = sampleoffset % p->rotlen;
+}
+
+static void orc_pcallib_add(orc_pcallib *p, int64_t slot, double re, double im)
+{
+   p->acc[2 * slot] += re;
+   p->acc[2 * slot + 1] += im;
+}
+
+void orc_pcallib_extract(void *h, const float *x, int64_t len)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   const int N = p->nbins;
+   if (p->kind != 2) {
+      /* real fold into nbins (:265-296, :610-652): sample n at slot pcal_index + n mod N */
+      int64_t tail = len % N, end = len - tail;
+      for (int64_t n = 0; n < len; n++) {
+         int64_t slot = n < end ? p->pcal_index + (n % N) : p->pcal_index + (n - end);
+         orc_pcallib_add(p, slot, (double)x[n], 0.0);
+      }
+      p->pcal_index = (p->pcal_index + tail) % N;
+   } else {
+      const int R = p->rotlen, P = R / N;
+      int64_t tail = len % R, end = len - tail;
+      for (int64_t n = 0; n < end; n++) {
+         int64_t j = n % R;
+         if (j >= (int64_t)P * N) continue; /* the samples past the last whole pulse */
+         int64_t r = p->rotator_index + j;
+         orc_pcallib_add(p, p->pcal_index + (j % N), (double)x[n] * p->rot_re[r], (double)x[n] * p->rot_im[r]);
+      }
+      for (int64_t m = 0; m < tail; m++) {
+         int64_t r = p->rotator_index + m;
+         orc_pcallib_add(p, p->pcal_index + (m % N), (double)x[end + m] * p->rot_re[r],
+                         (double)x[end + m] * p->rot_im[r]);
+      }
+      int64_t tail2 = tail % N;
+      p->rotator_index = (p->rotator_index + tail) % R;
+      p->pcal_index = (p->pcal_index + tail2) % N;
+   }
+   p->samplecount += (uint64_t)len;
+}
+
+int orc_pcallib_info(void *h, int *kind, int *nbins, int *ntones)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   *kind = p->kind; *nbins = p->nbins; *ntones = p->ntones;
+   return 0;
+}
+
+/* getFinalPCal: bins [0, N) += [N, 2N), forward DFT scaled by 1/N
+ * (IPP_FFT_DIV_FWD_BY_N), then the tone bins: Trivial the first ntones,
+ * Shifting every step-th, ImplicitShift every step-th from the offset bin;
+ * tones whose bin falls past N stay zero.  Returns the samples integrated. */
+uint64_t orc_pcallib_final(void *h, double *out_reim)
+{
+   orc_pcallib *p = (orc_pcallib *)h;
+   const int N = p->nbins;
+   double *b = (double *)malloc(sizeof(double) * 2 * (size_t)N);
+   for (int k = 0; k < N; k++) {
+      b[2 * k] = p->acc[2 * k] + p->acc[2 * (k + N)];
+      b[2 * k + 1] = p->acc[2 * k + 1] + p->acc[2 * (k + N) + 1];
+   }
+   const long long step = (long long)floor((double)N * (p->spacing / p->fs));
+   const long long off = p->kind == 3 ? (long long)floor((double)N * p->offset / p->fs) : 0;
+   for (int t = 0; t < p->ntones; t++) {
+      long long idx = p->kind == 1 ? t : off + (long long)t * step;
+      out_reim[2 * t] = out_reim[2 * t + 1] = 0.0;
+      if (idx >= N) continue;
+      long double sr = 0, si = 0;
+      for (int k = 0; k < N; k++) {
+         long long e = (idx * (long long)k) % N;
+         long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)N;
+         long double c = cosl(a), s = sinl(a);
+         sr += b[2 * k] * c - b[2 * k + 1] * s;
+         si += b[2 * k] * s + b[2 * k + 1] * c;
+      }
+      out_reim[2 * t] = (double)(sr / N);
+      out_reim[2 * t + 1] = (double)(si / N);
+   }
+   free(b);
+   return p->samplecount;
+}

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
            "-diag-suppress", "20281"] + ARCH
 
-CU_SOURCES = ["engine.cu", "unpack.cu", "pcal.cu", "plans.cu", "bigfft.cu", "noalloc.cu"]
+CU_SOURCES = ["engine.cu", "unpack.cu", "pcal.cu", "plans.cu", "bigfft.cu", "noalloc.cu", "pcallib.cu"]
 HOST_SOURCES = ["settings.cpp", "iniparser.cpp", "buffer.cpp", "filesource.cpp", "filesink.cpp",
                 "taskcore_cuda.cpp", "dispatcher.cpp"]
 

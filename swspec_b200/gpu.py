@@ -99,6 +99,17 @@ def lib():
         L.swsgpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
         L.swsgpu_host_unregister.argtypes = [C.c_void_p]
         L.swsgpu_sync.argtypes = [C.c_void_p, C.c_void_p]
+        L.swsgpu_pcal_create.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int64, C.c_int, C.c_int,
+                                         C.POINTER(C.c_void_p)]
+        L.swsgpu_pcal_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3
+        L.swsgpu_pcal_clear.argtypes = [C.c_void_p]
+        L.swsgpu_pcal_adjust_offset.argtypes = [C.c_void_p, C.c_int64]
+        L.swsgpu_pcal_extract.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.swsgpu_pcal_final.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p]
+        L.swsgpu_pcal_destroy.argtypes = [C.c_void_p]
+        L.swsgpu_pcal_destroy.restype = None
+        L.swsgpu_pcal_delay.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double]
+        L.swsgpu_pcal_delay.restype = C.c_double
         L.swsgpu_inject.argtypes = [C.c_void_p, C.c_int]
         _lib = L
     return _lib
@@ -338,3 +349,49 @@ def unpack_device_noalloc(lay: Layout, d_raw: int, nbytes: int, payload_offset: 
     if rc != 0:
         raise SwsError(f"{ERRORS.get(rc, rc)}: swsgpu_unpack_device_noalloc failed")
     return nv.value
+
+
+class PcalExtractor:
+    """The reference's PCal extractor library on the GPU (swsgpu_pcal_*)."""
+
+    def __init__(self, bandwidth_hz: float, spacing_hz: float, offset_hz: int, sampleoffset: int = 0,
+                 kind: int = 0, device: int = 0):
+        self.h = C.c_void_p()
+        _check(lib().swsgpu_pcal_create(bandwidth_hz, spacing_hz, int(offset_hz), int(sampleoffset), kind,
+                                        device, C.byref(self.h)))
+        k, nb, nt = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().swsgpu_pcal_info(self.h, C.byref(k), C.byref(nb), C.byref(nt)))
+        self.kind, self.nbins, self.ntones = k.value, nb.value, nt.value
+
+    def extract(self, d_samples: int, n: int, stream: int = 0) -> None:
+        _check(lib().swsgpu_pcal_extract(self.h, d_samples, n, C.c_void_p(stream or None)))
+
+    def adjust(self, sampleoffset: int) -> None:
+        _check(lib().swsgpu_pcal_adjust_offset(self.h, int(sampleoffset)))
+
+    def clear(self) -> None:
+        _check(lib().swsgpu_pcal_clear(self.h))
+
+    def final(self, stream: int = 0):
+        out = np.zeros(2 * self.ntones)
+        n = C.c_uint64()
+        _check(lib().swsgpu_pcal_final(self.h, out.ctypes.data, C.byref(n), C.c_void_p(stream or None)))
+        return out[0::2] + 1j * out[1::2], int(n.value)
+
+    def close(self) -> None:
+        if self.h:
+            lib().swsgpu_pcal_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pcal_delay(tone_mhz, phase, band_center_mhz: float, band_valid_mhz: float) -> float:
+    """swsgpu_pcal_delay: tone-phase delay in ns (m5pcal.c calcDelay)."""
+    f = np.ascontiguousarray(tone_mhz, dtype=np.int32)
+    ph = np.ascontiguousarray(phase, dtype=np.float64)
+    return lib().swsgpu_pcal_delay(len(f), f.ctypes.data, ph.ctypes.data, band_center_mhz, band_valid_mhz)

@@ -55,3 +55,19 @@ def test_noalloc_source_names_no_allocation_call():
     code = re.sub(r"//.*", "", src)
     for name in ("cudaMalloc", "cudaMallocAsync", "cudaFree", "cudaMallocHost", "cudaMallocManaged"):
         assert not re.search(rf"\b{name}\s*\(", code), name
+
+
+def test_pcal_delay_recovers_a_known_delay():
+    """swsgpu_pcal_delay (m5pcal.c calcDelay, host code): tones 1 MHz apart
+    with phases 2 pi f tau wrapped to (-pi, pi] give back tau in ns, and a
+    band-edge cut drops the tones outside the valid band."""
+    import numpy as np
+    from swspec_b200 import gpu
+    f = np.arange(1, 16, dtype=np.int32)
+    for tau_ns in (37.0, -120.5, 0.0):
+        ph = np.angle(np.exp(2j * np.pi * f * 1e6 * tau_ns * 1e-9))
+        assert abs(gpu.pcal_delay(f, ph, 8.0, 20.0) - tau_ns) < 1e-9
+    ph = np.angle(np.exp(2j * np.pi * f * 1e6 * 55e-9))
+    ph[0] += 1.0                                        # a corrupted edge tone, excluded below
+    assert abs(gpu.pcal_delay(f, ph, 8.0, 6.5) - 55.0) < 1e-9
+    assert gpu.pcal_delay(f[:1], ph[:1], 8.0, 20.0) == 0.0

@@ -256,3 +256,75 @@ def test_raw_2bit_single_channel_layout():
     t = np.arange(nsamp)
     want = lv[(raw[t // 4] >> (6 - 2 * (t % 4))) & 3]
     assert np.array_equal(ours, want)
+
+
+# ---- the PCal extractor library (src/IA-32/PhaseCal/PCal.cpp) ----
+
+def _pcal_test_signal(n, bw, spacing, offset, ntones, sampleoffset):
+    """The library's own test signal (PCal.cpp:896-906): tones at offset +
+    t*spacing with phases -90 deg + 5 deg * t."""
+    t = np.arange(n, dtype=np.float64) + sampleoffset
+    x = np.zeros(n)
+    for k in range(ntones):
+        x += np.sin(np.pi * t * (offset + k * spacing) / bw + k * np.pi * 5 / 180)
+    return x.astype(np.float32)
+
+
+@pytest.mark.parametrize("bw,spacing,offset,kind", [(8e6, 1e6, 0, 1), (8e6, 1e6, 10000, 3)])
+def test_pcallib_known_answer(bw, spacing, offset, kind):
+    """The library's known answer (PCal.cpp:879-948): tone phases -90 + 5 t
+    degrees, after a gap re-entered with adjustSampleOffset."""
+    import oracle as O
+    p = O.PcalLib(bw, spacing, offset, 0)
+    assert p.kind == kind
+    n, prime = 160000, 3
+    x = _pcal_test_signal(n, bw, spacing, offset, p.ntones, 0)
+    p.extract(x)
+    p.adjust(n + prime)
+    y = _pcal_test_signal(n, bw, spacing, offset, p.ntones, n + prime)   # the stream after the gap
+    p.extract(y)
+    tones, used = p.final()
+    assert used == 2 * n
+    first = 1 if offset == 0 else 0      # the DC tone of the zero-offset comb has no power
+    ph = np.rad2deg(np.angle(tones[first:]))
+    want = -90.0 + 5.0 * np.arange(first, p.ntones)
+    d = (ph - want + 180) % 360 - 180
+    assert np.max(np.abs(d)) < 0.5, d
+
+
+def test_pcallib_shifting_matches_direct_restatement():
+    """Shifting (chosen when the rotator period is not a multiple of the bin
+    count): per full rotator period only floor(R/N)*N rotated samples are
+    added (PCal.cpp:451-462); the restated C against a direct numpy model,
+    over a call with a tail and a second call."""
+    import oracle as O
+    bw, spacing, offset = 8e6, 1e6, 128000
+    p = O.PcalLib(bw, spacing, offset, 5)
+    assert p.kind == 2 and p.nbins == 16
+    R, N = 125, 16
+    rng = np.random.default_rng(3)
+    x1 = rng.standard_normal(R * 7 + 40).astype(np.float32)
+    x2 = rng.standard_normal(R * 3 + 70).astype(np.float32)
+    p.extract(x1)
+    p.extract(x2)
+    tones, used = p.final()
+    fs = 2 * bw
+    rot = np.exp(1j * 2 * np.pi * (-offset / fs) * np.arange(2 * R)).astype(np.complex64).astype(np.complex128)
+    acc = np.zeros(2 * N, complex)
+    pi, ri = 5 % N, 5 % R
+    for x in (x1, x2):
+        tail = len(x) % R
+        end = len(x) - tail
+        for n in range(end):
+            j = n % R
+            if j < (R // N) * N:
+                acc[pi + j % N] += x[n] * rot[ri + j]
+        for m in range(tail):
+            acc[pi + m % N] += x[end + m] * rot[ri + m]
+        ri = (ri + tail) % R
+        pi = (pi + tail % N) % N
+    b = acc[:N] + acc[N:]
+    dft = np.fft.fft(b) / N
+    want = dft[:p.ntones]
+    assert used == len(x1) + len(x2)
+    assert np.max(np.abs(tones - want)) < 1e-9 * np.max(np.abs(want))
