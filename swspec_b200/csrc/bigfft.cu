@@ -13,7 +13,8 @@
 //     contiguous code run, staged by cp.async one unit ahead; decode +
 //     window + first radix fused, the N1-point Stockham FFT in shared
 //     memory, and the last pass applies the four-step twiddle (two small
-//     tables, W_N^(2048 h) W_N^l, both rounded once from double) in registers
+//     tables of FP64 values, W_N^(2048 h) W_N^l, multiplied in FP64 and
+//     rounded once to FP32) in registers
 //     and writes 32-byte row segments of scratch.
 //   row pass     X[k1 + N1 k2] = sum_n2 X1[k1][n2] W_N2^(n2 k2)
 //     a persistent grid over units (row pair (k1, N1 - k1), work item), the
@@ -93,7 +94,7 @@ __device__ __forceinline__ void big_pass(float2 *buf, const float2 *tw)
 // row k1 as x W_N^((c0 + c) k1), W_N^m = W_N^(2048 (m >> 11)) W_N^(m & 2047).
 template <int M, int C, int T, int R, int NS>
 __device__ __forceinline__ void big_pass_out(const float2 *buf, const float2 *tw, float2 *dst, int N2, int c0,
-                                             const float2 *twA, const float2 *twB)
+                                             const double2 *twA, const double2 *twB)
 {
    constexpr int CS = big_col_stride(M, C);
    constexpr int NB = M / R, TOT = C * NB, BPT = (TOT + T - 1) / T;
@@ -116,7 +117,10 @@ __device__ __forceinline__ void big_pass_out(const float2 *buf, const float2 *tw
          for (int i = 0; i < R; i++) {
             const int k1 = d + i * NS;
             const int m = (c0 + c) * k1;  // < N
-            const float2 w = cmul(__ldg(twA + (m >> 11)), __ldg(twB + (m & 2047)));
+            // W_N^m = W_N^(2048 (m >> 11)) W_N^(m & 2047): the product of the two
+            // FP64 table entries, rounded once to FP32
+            const double2 A = __ldg(twA + (m >> 11)), B = __ldg(twB + (m & 2047));
+            const float2 w = make_float2((float)fma(A.x, B.x, -A.y * B.y), (float)fma(A.x, B.y, A.y * B.x));
             dst[(long long)k1 * N2 + c] = cmul(v[i], w);
          }
       }

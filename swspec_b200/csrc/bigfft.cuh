@@ -38,8 +38,8 @@ struct BigArgs {
    const float *window;        // N
    const float2 *tw1;          // W_N1^m, m < N1
    const float2 *tw2;          // W_N2^m, m < N2
-   const float2 *twA;          // W_N^(2048 h), h < ceil(N / 2048)
-   const float2 *twB;          // W_N^l, l < 2048
+   const double2 *twA;         // W_N^(2048 h), h < ceil(N / 2048), FP64
+   const double2 *twB;         // W_N^l, l < 2048, FP64
    float2 *scratch;            // [job][N1][N2] column FFTs, twiddled
    float *partial;
    int nbjobs;                 // jobs of this batch (column pass)

@@ -390,9 +390,10 @@ static void build_schedule(const swsgpu_handle *h, size_t run_bytes, int nruns, 
    }
    long long target_items = std::max<long long>(1, 4ll * h->max_clusters);
    int fper = (int)std::max<long long>(1, (total_jobs + target_items - 1) / target_items);
-   // the four-step row kernel accumulates a whole item per CTA: one item per
-   // source pair and spectrum
-   if (h->big) fper = 1 << 30;
+   // the four-step row kernel accumulates an item's jobs in FP32 registers
+   // per CTA: at most 16 jobs per item, so those sums stay short and the
+   // compensated reduction adds the items
+   if (h->big) fper = 16;
 
    // key -> output vector index
    std::map<long long, std::vector<RedEntry>> vec_entries;
@@ -584,8 +585,8 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.window = (const float *)h->d_window.p;
    a.tw1 = (const float2 *)h->d_tw1.p + h->tw_off[h->cand].x;
    a.tw2 = (const float2 *)h->d_tw1.p + h->tw_off[h->cand].y;
-   a.twA = (const float2 *)h->d_twA.p;
-   a.twB = (const float2 *)h->d_twB.p;
+   a.twA = (const double2 *)h->d_twA.p;
+   a.twB = (const double2 *)h->d_twB.p;
    a.scratch = (float2 *)h->d_scratch.p;
    a.partial = (float *)h->d_partial.p;
    a.N = c.fft_points;
@@ -1176,7 +1177,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    } else {
       // four-step tables, each entry rounded once from double: W_N1 and
       // W_N2 of every candidate split (one buffer), W_N^(2048 h), W_N^l
-      std::vector<float2> t1, tA, tB;
+      std::vector<float2> t1;
       {
          BigPlan cand[16];
          const int nc = big_plan_candidates(cfg->fft_points, cand, 16);
@@ -1189,18 +1190,24 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
             t1.insert(t1.end(), a2.begin(), a2.end());
          }
       }
-      make_twiddles(cfg->fft_points, 2048, tB);
+      // the four-step twiddle W_N^m = W_N^(2048 h) W_N^l from two FP64 tables
+      std::vector<double2> dA, dB(2048);
+      for (int l = 0; l < 2048; l++) {
+         const double ang = -2.0 * M_PI * (double)l / (double)cfg->fft_points;
+         dB[l] = make_double2(std::cos(ang), std::sin(ang));
+      }
       const int nA = (cfg->fft_points + 2047) / 2048;
-      tA.resize(nA);
+      dA.resize(nA);
       for (int k = 0; k < nA; k++) {
          const double ang = -2.0 * M_PI * (double)((long long)k * 2048) / (double)cfg->fft_points;
-         tA[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+         dA[k] = make_double2(std::cos(ang), std::sin(ang));
       }
-      const std::pair<DevBuf *, std::vector<float2> *> tabs[3] = {
-          {&h->d_tw1, &t1}, {&h->d_twA, &tA}, {&h->d_twB, &tB}};
+      CKB(h->d_tw1.ensure(sizeof(float2) * t1.size()));
+      CKB(cudaMemcpy(h->d_tw1.p, t1.data(), sizeof(float2) * t1.size(), cudaMemcpyHostToDevice));
+      const std::pair<DevBuf *, std::vector<double2> *> tabs[2] = {{&h->d_twA, &dA}, {&h->d_twB, &dB}};
       for (const auto &t : tabs) {
-         CKB(t.first->ensure(sizeof(float2) * t.second->size()));
-         CKB(cudaMemcpy(t.first->p, t.second->data(), sizeof(float2) * t.second->size(), cudaMemcpyHostToDevice));
+         CKB(t.first->ensure(sizeof(double2) * t.second->size()));
+         CKB(cudaMemcpy(t.first->p, t.second->data(), sizeof(double2) * t.second->size(), cudaMemcpyHostToDevice));
       }
    }
    for (int s = 0; s < cfg->num_streams; s++) {

@@ -303,9 +303,12 @@ __host__ __device__ constexpr int stage_slots()
 // tile w / 4, so row = threadIdx.x).  The epilogue loads its row's 16
 // complex outputs, applies the next level's FP32 twiddle, splits them and
 // stores them as the next level's operand in MN-major order: the level's
-// output digit becomes the fastest row digit of the next level, so the
-// thread's 16 values are 16 consecutive rows of one K column (two 16-byte
-// core-matrix rows per K value and part).
+// output digit d = d0 + 8 d1 becomes the row digits of the next level, row
+// (d0, g, d1) = d0 + 8 g + 128 d1 for the thread's remaining digit g < 16,
+// so the thread's values d < 8 and d >= 8 are the 8 rows of row groups g
+// and 16 + g of one K column (two 16-byte core-matrix rows per K value and
+// part), and the 8 lanes of a shared-memory wavefront, which differ in g,
+// write 8 distinct 16-byte bank groups (144-byte group stride).
 // Level 1 is either on the tensor cores (operand = decoded, windowed
 // samples, K-major rows) or an FP32 radix-16 in registers fused with the
 // decode (PREC 1).
@@ -338,10 +341,10 @@ constexpr uint32_t TC_OPND_BYTES = 8 * TC_MN_LBO;  // 36864 >= 32768 (K-major)
 constexpr uint32_t TC_BMAT_BYTES = 64 * 64 * 2;
 constexpr uint32_t TC_TMEM_COLS = 128;             // two M = 128 tiles x N = 64 FP32 columns
 
-// 16 complex values of rows m0 .. m0+15 (m0 % 16 == 0), K column kq of the
-// real part and kq + 16 of the imaginary part (hi parts; lo parts at +32),
-// into an MN-major operand.
-__device__ __forceinline__ void store_mn16(uint32_t opnd, int m0, int kq, const float2 (&v)[16])
+// 16 complex values into an MN-major operand: values 0-7 as the 8 rows of
+// row group g0, values 8-15 as row group g1, K column kq of the real part
+// and kq + 16 of the imaginary part (hi parts; lo parts at +32).
+__device__ __forceinline__ void store_mn16(uint32_t opnd, int g0, int g1, int kq, const float2 (&v)[16])
 {
 #pragma unroll
    for (int c = 0; c < 2; c++) {
@@ -353,7 +356,7 @@ __device__ __forceinline__ void store_mn16(uint32_t opnd, int m0, int kq, const 
             const float2 x = v[8 * g + 2 * e], y = v[8 * g + 2 * e + 1];
             split2(c ? x.y : x.x, c ? y.y : y.x, hi[e], lo[e]);
          }
-         const int m = m0 + 8 * g;
+         const int m = 8 * (g ? g1 : g0);
          st_shared_v4(opnd + tc::mnmajor_off(m, 16 * c + kq, TC_MN_LBO, TC_MN_SBO), hi);
          st_shared_v4(opnd + tc::mnmajor_off(m, 32 + 16 * c + kq, TC_MN_LBO, TC_MN_SBO), lo);
       }
@@ -710,7 +713,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 #pragma unroll
          for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
          twiddle_by_powers<R1>(v[0], base);
-         store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, v[0]);
+         store_mn16(opnd_addr, tid & 15, 16 + (tid & 15), tid >> 4, v[0]);
          tc::fence_async_smem();
       } else {
          // the decoded, windowed samples z[r1 + 256 q2] as row r1 = tid of
@@ -831,28 +834,31 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
             for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
             twiddle_by_powers<16>(y, base);
             handoff();  // every thread has read its TMEM row before the operand is overwritten
-            store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, y);
+            store_mn16(opnd_addr, tid & 15, 16 + (tid & 15), tid >> 4, y);
             handoff();
          }
-         // level 2: row tid = k0 + 16 q0, outputs k1; twiddle W_256^{q0 k1};
-         // level 3's operand rows k1 + 16 k0, K column q0
+         // level 2: row tid = (k0 & 7) + 8 q0 + 128 (k0 >> 3), outputs k1;
+         // twiddle W_256^{q0 k1}; level 3's operand rows (k1 & 7) + 8 k0 +
+         // 128 (k1 >> 3), K column q0
          level(false);
          tc_load_row(tmem_base, y);
+         const int k0 = (tid & 7) + 8 * (tid >> 7);
          {
-            const int q0 = tid >> 4;
+            const int q0 = (tid >> 3) & 15;
 #pragma unroll
             for (int k1 = 1; k1 < 16; k1++) y[k1] = cmul(y[k1], w256[(q0 * k1) & 255]);
+            handoff();
+            store_mn16(opnd_addr, k0, 16 + k0, q0, y);
+            handoff();
          }
-         handoff();
-         store_mn16(opnd_addr, 16 * (tid & 15), tid >> 4, y);
-         handoff();
-         // level 3: row tid = k1 + 16 k0, outputs k2: F[k0 + 16 k1 + 256 k2]
+         // level 3: row tid = (k1 & 7) + 8 k0 + 128 (k1 >> 3), outputs k2:
+         // F[k0 + 16 k1 + 256 k2]
          level(false);
          tc_load_row(tmem_base, y);
          tc::fence_before();
          cluster_wait();  // owners have finished reading their receive buffers
          if (send) {
-            const int kap = (tid >> 4) + 16 * (tid & 15);
+            const int kap = ((tid >> 3) & 15) + 16 * ((tid & 7) + 8 * (tid >> 7));
 #pragma unroll
             for (int k2 = 0; k2 < 16; k2++)
                push(kap + 256 * k2, make_float2(y[k2].x * COMP, y[k2].y * COMP));
