@@ -49,6 +49,13 @@ __host__ __device__ constexpr int big_col_words()
 {
    return (N1 + 32 / NBIT - 1) / (32 / NBIT) + 1;
 }
+// Their shared-memory region: the run is copied from the 16-byte boundary
+// at or below its first word, in whole 16-byte units.
+template <int N1, int NBIT>
+__host__ __device__ constexpr int big_col_region()
+{
+   return (big_col_words<N1, NBIT>() + 3 + 3) / 4 * 4;
+}
 
 // One Stockham pass (radix R, span NS) over C columns of M points held in
 // shared memory, in place through registers.  Butterfly j of column c reads
@@ -168,6 +175,39 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// Bulk copy global -> shared by the TMA engine (addresses 16-byte aligned,
+// size a multiple of 16), its bytes counted on an mbarrier of this CTA.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar)
+{
+   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                "l"(src), "r"(bytes), "r"(mbar)
+                : "memory");
+}
+__device__ __forceinline__ void big_mbar_init(uint32_t mbar, int count)
+{
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
+   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void big_mbar_expect(uint32_t mbar, uint32_t bytes)
+{
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+// Bounded wait for phase `parity`; false when it gave up.
+__device__ __forceinline__ bool big_mbar_wait(uint32_t mbar, uint32_t parity)
+{
+   for (int it = 0; it < (1 << 20); it++) {
+      uint32_t done;
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                   " selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done)
+                   : "r"(mbar), "r"(parity)
+                   : "memory");
+      if (done) return true;
+      if (it > 32) __nanosleep(32);
+   }
+   return false;
+}
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -176,8 +216,8 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 template <int N1, int C, int NBIT>
 __host__ __device__ constexpr size_t big_cols_smem_slots(int slots)
 {
-   return sizeof(float2) * ((size_t)C * big_col_stride(N1, C) + N1) +
-          sizeof(uint32_t) * (size_t)slots * 2 * C * big_col_words<N1, NBIT>();
+   return sizeof(float2) * ((size_t)C * big_col_stride(N1, C) + N1 + 1) +
+          sizeof(uint32_t) * (size_t)slots * 2 * C * big_col_region<N1, NBIT>();
 }
 template <int N1, int C, int NBIT>
 __host__ __device__ constexpr int big_cols_slots()
@@ -189,10 +229,12 @@ __host__ __device__ constexpr int big_cols_slots()
 // the batch (columns gC .. gC + C - 1 of one pair job).  With the column
 // layout -- column n2 of a frame starting at sample s0 is the run idx0 ..
 // idx0 + N1 - 1 of phase array (s0 + n2) % N2, idx0 = (s0 + n2) / N2 -- the
-// unit's code runs (WPC words per column and frame from the word holding
-// idx0, soff = idx0 % SPW) are staged in shared memory by cp.async, the next
-// unit's into a second slot while the current one is transformed.  The W_N1
-// table is loaded once per CTA.
+// unit's code runs (the 16-byte aligned span around the WPC words per
+// column and frame from the word holding idx0) are staged in shared memory
+// by bulk copies of the TMA engine, one per run, issued by warp 0 and
+// counted on the slot's mbarrier; the next unit's go into a second slot
+// while the current one is transformed.  The W_N1 table is loaded once per
+// CTA.
 template <int N1, int N2, int C, int T, int R1, int R2, int R3, int NBIT>
 __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
 {
@@ -201,53 +243,81 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
    constexpr int CS = big_col_stride(N1, C);
    constexpr int SPW = 32 / NBIT;
    constexpr uint32_t MASK = (NBIT == 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
-   constexpr int WPC = big_col_words<N1, NBIT>();
+   constexpr int WPC = big_col_region<N1, NBIT>();  // staged words per run (16-byte multiple)
    constexpr int SLOT = 2 * C * WPC;
+   constexpr int NIW = (2 * C + 31) / 32;  // warps issuing the bulk copies, one per run
+   static_assert(NIW * 32 <= T, "issuing warps within the block");
    constexpr int NS = big_cols_slots<N1, C, NBIT>();
    constexpr int NG = N2 / C;
    extern __shared__ float2 smf[];
    float2 *buf = smf;
    float2 *tw1 = smf + C * CS;
-   uint32_t *stg = reinterpret_cast<uint32_t *>(tw1 + N1);  // [NS][2][C][WPC]
+   // [NS][2][C][WPC], 16-byte aligned for the bulk copies
+   uint32_t *stg = reinterpret_cast<uint32_t *>(tw1 + N1 + ((C * CS + N1) & 1));
    __shared__ int soff[2][2][C];
+   __shared__ __align__(8) unsigned long long sbar[2];  // one per staging slot: its bulk copies' bytes
    const int tid = threadIdx.x;
    const int nunits = NG * a.nbjobs;
    int u = blockIdx.x;
    if (u >= nunits) return;
    load_pass_twiddles<N1, T, R1, R2, R3>(tw1, a.tw1);
+   const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&sbar[0]);
+   const uint32_t stg_addr = (uint32_t)__cvta_generic_to_shared(stg);
+   if (tid == 0) {
+      big_mbar_init(bar0, NIW);
+      big_mbar_init(bar0 + 8, NIW);
+   }
+   __syncthreads();
+   uint32_t par = 0u;  // bit s: the phase of slot s's barrier to wait for
+   bool gave_up = false;
 
+   // warps 0 .. NIW-1: thread l < nside*C copies run l (side l / C, column
+   // l % C) from the 16-byte boundary at or below its first word; each
+   // warp's lane 0 arrives on the slot's barrier announcing its warp's bytes
+   // before they are copied
    auto stage = [&](int uu, int sl) {
+      if (tid >= 32 * NIW) return;
       const BigJob sj = a.jobs[uu / NG];
       const int sc0 = (uu % NG) * C;
       const int nside = sj.mode != MODE_SINGLE ? 2 : 1;
-      uint32_t *dst = stg + sl * SLOT;
-      for (int t = tid; t < nside * C * WPC; t += T) {
-         const int side = t / (C * WPC), c = (t / WPC) % C, w = t % WPC;
-         const long long s = (side ? sj.sb : sj.sa) + sc0 + c;
-         const long long wi = (s / N2) / SPW + w;
-         const uint32_t *src = a.codes + (long long)(side ? sj.code_b : sj.code_a) * a.code_words + (s % N2) * a.wpp;
-         if (wi < a.wpp) cp_async4(dst + t, src + wi);
-         else dst[t] = 0u;
-      }
+      uint32_t bytes = 0;
+      const uint32_t *src = nullptr;
       if (tid < nside * C) {
-         const long long s = ((tid / C) ? sj.sb : sj.sa) + sc0 + tid % C;
-         soff[sl][tid / C][tid % C] = (int)((s / N2) % SPW);
+         const int side = tid / C, c = tid % C;
+         const long long s = (side ? sj.sb : sj.sa) + sc0 + c;
+         const long long wi = (s / N2) / SPW;
+         const long long w0 = wi & ~3ll;
+         const int extra = (int)(wi - w0);
+         const long long nw = min((long long)WPC, a.wpp - w0);  // wpp is a multiple of 4 words
+         src = a.codes + (long long)(side ? sj.code_b : sj.code_a) * a.code_words + (s % N2) * a.wpp + w0;
+         bytes = (uint32_t)(nw > 0 ? nw : 0) * 4u;
+         soff[sl][side][c] = extra * SPW + (int)((s / N2) % SPW);
       }
+      uint32_t total = bytes;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+      if ((tid & 31) == 0) big_mbar_expect(bar0 + 8u * (uint32_t)sl, total);
+      __syncwarp();
+      if (bytes)
+         bulk_g2s(stg_addr + 4u * (uint32_t)(sl * SLOT + tid * WPC), src, bytes, bar0 + 8u * (uint32_t)sl);
+   };
+   auto wait_slot = [&](int sl) {
+      if (!gave_up && !big_mbar_wait(bar0 + 8u * (uint32_t)sl, (par >> sl) & 1u)) {
+         gave_up = true;  // report once; the data of this unit are invalid
+         if (a.status) atomicExch(a.status, 1);
+      }
+      par ^= 1u << sl;
    };
 
    int slot = 0;
    if (a.col_layout) stage(u, 0);
-   cp_async_commit();
    while (true) {
       const int un = u + gridDim.x;
       const bool more = un < nunits;
       if constexpr (NS == 2) {
          if (a.col_layout && more) stage(un, slot ^ 1);
-         cp_async_commit();
-         cp_async_wait1();
-      } else {
-         cp_async_wait0();
       }
+      if (a.col_layout) wait_slot(slot);
       __syncthreads();
 
       const int job = u / NG, c0 = (u % NG) * C;
@@ -320,9 +390,10 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_cols(BigArgs a)
          slot ^= 1;
       } else {
          if (a.col_layout) stage(u, 0);
-         cp_async_commit();
       }
    }
+   // a unit staged but never waited for cannot exist: every stage is
+   // followed by the wait of the iteration that transforms it
 }
 
 // Row pass: a persistent grid over the units u = item * NP + rp of the

@@ -46,6 +46,7 @@ struct BigArgs {
    int nbitems;                // items of this batch (row pass)
    int N, S;
    float4 levels;
+   int *status;                // set to 1 when a bounded wait gave up (null: not reported)
 };
 
 typedef void (*BigColsKernel)(BigArgs);

@@ -592,6 +592,7 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.N = c.fft_points;
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
+   a.status = (int *)h->d_status.p;
    if (h->rows_fn != (const void *)bp.rows || h->cols_fn != (const void *)bp.cols[nbi]) {
       // persistent passes: as many CTAs as fit on the device at once
       int occ_r = 0, occ_c = 0, nsm = 0;
@@ -763,7 +764,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    bool col = false;
    const int D = code_decimation(h, &col);
    const long long per_phase = (nsamp + D - 1) / D;
-   const long long wpp = (per_phase + spw - 1) / spw + 2;  // +2: prefetch may touch one word past
+   // +2: prefetch may touch one word past; a multiple of 4 words, so every
+   // phase array starts on a 16-byte boundary (bulk copies of its runs)
+   const long long wpp = ((per_phase + spw - 1) / spw + 2 + 3) / 4 * 4;
    const long long code_words = (long long)D * wpp;
    const long long blank_words = (nsamp + 31) / 32;
    // phase-cal folds read undecimated codes (word-wise when the rotator
@@ -1795,7 +1798,7 @@ int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, s
    const size_t ncode = h->code_stream.size();
    bool col = false;
    const int D = code_decimation(h, &col);
-   const long long wpp = ((nsamp + D - 1) / D + spw - 1) / spw + 2;
+   const long long wpp = (((nsamp + D - 1) / D + spw - 1) / spw + 2 + 3) / 4 * 4;
    size_t total = sizeof(uint32_t) * (size_t)D * (size_t)wpp * ncode + 64;       // codes
    if (col && c.extract_pcal)                                                      // undecimated copy
       total += sizeof(uint32_t) * (size_t)((nsamp + spw - 1) / spw + 2) * ncode + 64;
