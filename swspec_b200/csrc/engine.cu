@@ -56,6 +56,27 @@ static size_t plan_smem(const Plan &pl, int precision, int nbi)
           : precision == SWSGPU_PREC_TCSPLIT_ALL ? pl.smem_tc2[nbi] : pl.smem[nbi];
 }
 
+// Launch attributes of the cluster kernel: P CTAs per cluster.  The FP32
+// form is placed with the load-balancing policy, which fits one more 16-CTA
+// cluster of two CTAs per SM on a B200 than the default spread policy (15
+// against 14: 120 SMs busy instead of 112; the FP32 kernel of the
+// dual-pol workload went from 4.84 to 4.53 ms).  The tensor-core forms keep
+// the spread policy: their grid of 15 load-balanced clusters ran as 14 plus
+// a straggler (10.5 ms against 6.9 ms for 14 spread clusters).  Returns the
+// number of attributes written.
+static unsigned cluster_attrs(cudaLaunchAttribute (&attr)[2], int P, int precision)
+{
+   attr[0].id = cudaLaunchAttributeClusterDimension;
+   attr[0].val.clusterDim.x = P;
+   attr[0].val.clusterDim.y = 1;
+   attr[0].val.clusterDim.z = 1;
+   attr[1].id = cudaLaunchAttributeClusterSchedulingPolicyPreference;
+   attr[1].val.clusterSchedulingPolicyPreference = precision == SWSGPU_PREC_FP32
+                                                       ? cudaClusterSchedulingPolicyLoadBalancing
+                                                       : cudaClusterSchedulingPolicySpread;
+   return 2;
+}
+
 
 struct DevBuf {
    void *p = nullptr;
@@ -855,13 +876,9 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          cfgl.blockDim = dim3(pl.T);
          cfgl.dynamicSmemBytes = plan_smem(pl, c.precision, nbi);
          cfgl.stream = st;
-         cudaLaunchAttribute attr[1];
-         attr[0].id = cudaLaunchAttributeClusterDimension;
-         attr[0].val.clusterDim.x = pl.P;
-         attr[0].val.clusterDim.y = 1;
-         attr[0].val.clusterDim.z = 1;
+         cudaLaunchAttribute attr[2];
+         cfgl.numAttrs = cluster_attrs(attr, pl.P, c.precision);
          cfgl.attrs = attr;
-         cfgl.numAttrs = 1;
          cudaEvent_t ev0 = nullptr, ev1 = nullptr;
          if (h->profiling) {
             CK(h, cudaEventCreate(&ev0));
@@ -1270,15 +1287,24 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       cfgl.gridDim = dim3(plan.P);
       cfgl.blockDim = dim3(plan.T);
       cfgl.dynamicSmemBytes = smem;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = plan.P;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
+      cudaLaunchAttribute attr[2];
+      cfgl.numAttrs = cluster_attrs(attr, plan.P, cfg->precision);
       cfgl.attrs = attr;
-      cfgl.numAttrs = 1;
+      // The occupancy query reports one resident CTA per SM for any kernel
+      // that allocates tensor memory, whatever its footprint; two 113 KB
+      // tensor-core CTAs (128 TMEM columns each, 512 per SM) do co-reside,
+      // and a grid sized for one CTA per SM runs at 0.69x the speed of one
+      // sized for two.  So the grid of a tensor-core form is sized by the
+      // FP32 form's kernel of the same plan (same threads and register cap)
+      // at the tensor-core form's shared-memory footprint.
+      const void *occ_kern = (const void *)kern;
+      if (cfg->precision != SWSGPU_PREC_FP32) {
+         occ_kern = (const void *)plan.kern[nbi];
+         CKB(cudaFuncSetAttribute(occ_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+         if (plan.P > 8) CKB(cudaFuncSetAttribute(occ_kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      }
       int ncl = 0;
-      CKB(cudaOccupancyMaxActiveClusters(&ncl, (const void *)kern, &cfgl));
+      CKB(cudaOccupancyMaxActiveClusters(&ncl, occ_kern, &cfgl));
       if (ncl < 1) {
          h->err = "cluster configuration does not fit on this device";
          return bail(SWSGPU_ECUDA);

@@ -340,6 +340,9 @@ constexpr uint32_t TC_K_LBO = 128, TC_K_SBO = 1024;
 constexpr uint32_t TC_OPND_BYTES = 8 * TC_MN_LBO;  // 36864 >= 32768 (K-major)
 constexpr uint32_t TC_BMAT_BYTES = 64 * 64 * 2;
 constexpr uint32_t TC_TMEM_COLS = 128;             // two M = 128 tiles x N = 64 FP32 columns
+// up to four resident CTAs of a tensor-core form share an SM's 512 columns,
+// so no CTA's allocation ever waits for another's release
+static_assert(4 * TC_TMEM_COLS <= 512, "tensor memory of the resident CTAs of one SM");
 
 // 16 complex values into an MN-major operand: values 0-7 as the 8 rows of
 // row group g0, values 8-15 as row group g1, K column kq of the real part
@@ -818,7 +821,11 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
             tc::fence_after();
          };
          // hand the next operand to the tensor core: loads of TMEM done,
-         // generic stores visible to the async proxy, then one barrier
+         // generic stores visible to the async proxy, then one barrier.
+         // Overwriting the operand needs no barrier before it: every thread
+         // has seen the level's commit arrive on mma_bar, and the commit
+         // arrives only after the MMAs, their operand reads included, have
+         // completed; no thread reads the operand through the generic proxy.
          auto handoff = [&]() {
             tc::fence_before();
             tc::fence_async_smem();
@@ -833,7 +840,6 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
 #pragma unroll
             for (int i = 0; i < nbases(R3); i++) base[i] = tw3[i * NS3 + tid];
             twiddle_by_powers<16>(y, base);
-            handoff();  // every thread has read its TMEM row before the operand is overwritten
             store_mn16(opnd_addr, tid & 15, 16 + (tid & 15), tid >> 4, y);
             handoff();
          }
@@ -847,7 +853,6 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
             const int q0 = (tid >> 3) & 15;
 #pragma unroll
             for (int k1 = 1; k1 < 16; k1++) y[k1] = cmul(y[k1], w256[(q0 * k1) & 255]);
-            handoff();
             store_mn16(opnd_addr, k0, 16 + k0, q0, y);
             handoff();
          }

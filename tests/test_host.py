@@ -278,3 +278,73 @@ BaseFilename1 = v
     got = np.fromfile(tmp_path / "v_swspec.bin", dtype=np.float32).reshape(-1, N // 2 + 1)
     assert got.shape == ref.shape == (64, N // 2 + 1), (got.shape, ref.shape)
     assert np.max(np.abs(got - ref) / ref) < 2e-6
+
+
+def _ibob_file(path, nframes, seed, tone):
+    """iBOB capture: frames of a 4-byte sequence header and 4096 bytes of
+    signed 8-bit samples, two channels interleaved (a tone in channel 0).
+    Returns the payload bytes."""
+    rng = np.random.default_rng(seed)
+    n = nframes * 2048
+    t = np.arange(n)
+    x = rng.standard_normal((n, 2)) * 20
+    x[:, 0] += tone * np.cos(2 * np.pi * 0.0711 * t)
+    q = np.clip(np.round(x), -128, 127).astype(np.int8).reshape(nframes, 4096).view(np.uint8)
+    hdr = np.zeros((nframes, 4), np.uint8)
+    hdr[:, 0] = 0x5E
+    hdr[:, 3] = (np.arange(nframes) + 1) & 0xFF
+    path.write_bytes(np.concatenate([hdr, q], axis=1).tobytes())
+    return q.reshape(-1).tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["tcsplit", "tcsplit_all", "fp32"])
+def test_cli_ibob_spectra_per_buffer(tmp_path, gpu, precision):
+    """Two iBOB files (signed 8-bit, two channels; channel 1 of the first and
+    channel 2 of the second), cross-pol, N = 8192, on each GPU form: the
+    4-byte headers are stripped (src/FileSource.cpp:53-57, 185-210) and the
+    payloads form one contiguous stream, whole spectra per buffer."""
+    N = 8192
+    pays = [_ibob_file(tmp_path / f"in{k}.ibob", 500, 30 + k, 8.0 * (k + 1)) for k in range(2)]
+    ini = _ini(tmp_path, f"""[Spectrometer]
+FFTpoints = {N}
+FFTIntegrationTimeSec = 0.006144
+FFToverlapFactor = 1
+BandwidthHz = 16e6
+WindowType = Hann
+SourceFormat = iBob
+BitsPerSample = 8
+SourceChannels = 2
+UseFile1Channel = 1
+UseFile2Channel = 2
+DoCrossPolarization = yes
+MaxSourceBufferMB = 1
+GpuPrecision = {precision}
+BaseFilename1 = b_%channel%
+""")
+    s = _settings(ini, 2)
+    rawbuf, cof, nsp = s["rawbuf_size"], s["core_overlapped_ffts"], s["max_spectra_per_buffer"]
+    assert nsp >= 1 and s["max_buffers_per_spectrum"] == 0, s
+    _run_cli(tmp_path, ini, ["in0.ibob", "in1.ibob"])
+    S = N // 2 + 1
+    nbuf = len(pays[0]) // rawbuf
+    assert nbuf >= 4
+    ra_all, rx_all = [], []
+    for b in range(nbuf):
+        smp = [O.decode(O.FMT_RAW_SIGNED, 2, 8, p[b * rawbuf:(b + 1) * rawbuf], rawbuf // 2, c)
+               for p, c in zip(pays, (0, 1))]
+        cfg = O.make_cfg(N, core_overlapped_ffts=cof, num_sources=2, num_xpols=1, window=O.W_HANN,
+                         nthreads=os.cpu_count() or 1)
+        ra, rx, _, n = O.domaths(cfg, smp)
+        ra_all.append(ra[:nsp])
+        rx_all.append(rx[:nsp, 0])
+    ra = np.concatenate(ra_all)
+    rx = np.concatenate(rx_all)
+    a0 = np.fromfile(tmp_path / "b_1_swspec.bin", dtype=np.float32).reshape(-1, S)
+    a1 = np.fromfile(tmp_path / "b_2_swspec.bin", dtype=np.float32).reshape(-1, S)
+    xp = np.fromfile(tmp_path / "b_1_xpol_swspec.bin", dtype=np.float32).reshape(-1, S, 2)
+    assert a0.shape[0] == a1.shape[0] == xp.shape[0] == ra.shape[0] == nbuf * nsp
+    assert np.max(np.abs(a0 - ra[:, 0]) / ra[:, 0]) < 2e-6
+    assert np.max(np.abs(a1 - ra[:, 1]) / ra[:, 1]) < 2e-6
+    xc = xp[..., 0] + 1j * xp[..., 1]
+    assert np.max(np.abs(xc - rx) / np.sqrt(ra[:, 0] * ra[:, 1])) < 2e-6
