@@ -51,17 +51,30 @@ int FileSource::open(const std::string &uri)
          return -1;
       }
       first_frame_ = found;
+      if (found > 0)
+         *cfg_->tlog << "FileSource: first Mark5B frame at byte " << found << " (" << found
+                     << " leading bytes skipped)" << std::endl;
       if (cfg_->startlog) {
+         // header word 2 holds the time as 8 BCD digits JJJSSSSS (MJD mod
+         // 1000, second of day); the reference reads it without checks
+         // (src/FileSource.cpp:338-339), here a digit above 9 is reported
          const unsigned char *h = &win[found + 8];
          int nib[8];
+         bool bcd_ok = true;
          for (int i = 0; i < 4; i++) {
             nib[2 * i] = h[3 - i] >> 4;
             nib[2 * i + 1] = h[3 - i] & 15;
          }
+         for (int i = 0; i < 8; i++) bcd_ok = bcd_ok && nib[i] <= 9;
          const int mjd3 = nib[0] * 100 + nib[1] * 10 + nib[2];
          const int sec = nib[3] * 10000 + nib[4] * 1000 + nib[5] * 100 + nib[6] * 10 + nib[7];
          *cfg_->startlog << "First frame at byte " << found << ": MJD(mod 1000) " << mjd3 << " second " << sec
                          << std::endl;
+         if (!bcd_ok || sec >= 86400) {
+            *cfg_->tlog << "FileSource: Mark5B time code of the first frame is not a valid BCD time (digits";
+            for (int i = 0; i < 8; i++) *cfg_->tlog << " " << nib[i];
+            *cfg_->tlog << ")" << std::endl;
+         }
       }
    }
    // skip whole seconds (FileSource.cpp:132-153)
@@ -106,10 +119,17 @@ int FileSource::read(Buffer *buf)
             got_eof_ = true;
             break;
          }
+         frames_++;
          if (cfg_->sourceformat == Mark5B || cfg_->sourceformat == Mk5B) {
+            // the reference logs a header without the sync word and keeps
+            // reading (src/FileSource.cpp:401-427); so does this reader
             uint32_t sync;
             memcpy(&sync, hdr.data(), 4);
-            if (sync != kMark5BSync) *cfg_->tlog << "FileSource: Mark5B sync word mismatch" << std::endl;
+            if (sync != kMark5BSync) {
+               bad_sync_++;
+               *cfg_->tlog << "FileSource: Mark5B sync word mismatch in frame " << frames_ - 1 << " at byte "
+                           << (int64_t)ifile_.tellg() - header_bytes_ << std::endl;
+            }
          }
          if (cfg_->sourceformat == VDIF && cfg_->vdif_thread >= 0) {
             // multi-thread VDIF: the thread id is bits 16-25 of header word 3;
@@ -137,6 +157,9 @@ int FileSource::read(Buffer *buf)
       in_frame_ += r;
       if (r < n) {
          got_eof_ = true;
+         if (r > 0 || in_frame_ > 0)
+            *cfg_->tlog << "FileSource: file ends inside frame " << frames_ - 1 << " after " << in_frame_ << " of "
+                        << payload << " payload bytes" << std::endl;
          break;
       }
       if (in_frame_ == payload) pending_header_ = true;

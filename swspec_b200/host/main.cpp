@@ -2,6 +2,7 @@
 // GPU core in place of the IPP core:
 //   swspectrometer_gpu <inifile> <infile1> [<infile2>]
 //   swspectrometer_gpu --print-settings <inifile> [ninputs]   (no GPU needed)
+//   swspectrometer_gpu --read-source <inifile> <infile> <outfile>  (no GPU needed)
 #include <cstring>
 #include <fstream>
 #include <streambuf>
@@ -38,6 +39,34 @@ int main(int argc, char *argv[])
          return 1;
       }
       std::cout << settings_json(s) << std::endl;
+      return 0;
+   }
+   if (argc == 5 && strcmp(argv[1], "--read-source") == 0) {
+      // the front end alone: read <infile> into buffers of the INI's raw
+      // buffer size, append the payload bytes to <outfile>, print one JSON
+      // line with the buffer lengths; messages go to stderr and the start
+      // timing to <outfile>.starttiming.txt (no GPU needed)
+      Settings s;
+      if (load_ini(s, argv[2], err) || parse_format(s, err) || derive(s, 1, err)) {
+         std::cerr << "Error: " << err << std::endl;
+         return 1;
+      }
+      std::ofstream st(std::string(argv[4]) + ".starttiming.txt");
+      s.tlog = &std::cerr;
+      s.startlog = &st;
+      FileSource f(&s);
+      if (f.open(argv[3])) return 2;
+      std::ofstream o(argv[4], std::ios::binary);
+      Buffer b(s.rawbuf_size);
+      std::cout << "{\"buffers\": [";
+      for (int k = 0; !f.eof(); k++) {
+         const int n = f.read(&b);
+         o.write(b.getData(), n);
+         std::cout << (k ? ", " : "") << n;
+      }
+      std::cout << "], \"frames\": " << f.frames_read() << ", \"bad_sync_frames\": " << f.bad_sync_frames() << "}"
+                << std::endl;
+      f.close();
       return 0;
    }
    std::cout << std::endl << "SWSpec GPU core (sm_100a)" << std::endl << std::endl;

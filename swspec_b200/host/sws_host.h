@@ -183,7 +183,13 @@ private:
    int64_t in_frame_ = 0;       // payload bytes of the current frame already consumed
    int64_t payload_total_ = 0;  // payload bytes delivered so far
    int64_t last_offset_ = 0;
+   int64_t frames_ = 0;         // frame headers consumed so far
+   int64_t bad_sync_ = 0;       // of them, Mark5B headers without the sync word
    bool pending_header_ = true;
+
+public:
+   int64_t frames_read() const { return frames_; }
+   int64_t bad_sync_frames() const { return bad_sync_; }
 };
 
 class DataSink {
