@@ -29,6 +29,7 @@
 #include "bigfft.cuh"
 #include "bins.cuh"
 #include "dft.cuh"
+#include "tcdft.cuh"
 
 namespace sws {
 
@@ -502,6 +503,175 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
    }
 }
 
+// Row pass of 4096-point rows on the tensor cores (the tensor-core split
+// form of the four-step path).  Each row's DFT is three radix-16 levels,
+// n2 = q0 + 16 q1 + 256 q2 and k2 = k0 + 16 k1 + 256 kk, on tcgen05 exactly
+// as the cluster kernel's all-levels form: level 1 over q2 for operand row
+// r1 = q0 + 16 q1 = threadIdx.x, twiddle W_4096^(r1 k0); level 2 over q1,
+// twiddle W_256^(q0 k1); level 3 over q0.  The scratch rows hold sums of N1
+// samples, so they enter scaled by 2^-e (tc_in_scale, exact) and the DFT16
+// operand carries 1/16 (exact): no level's output exceeds its input's
+// bound, so no FP16 operand overflows whatever the signal (a carrier
+// included); tc_out_comp = 16^3 2^e restores the scale.  Both rows of the
+// pair land in shared memory for the pair separation, which with the
+// accumulation and the partial write is the FP32 row pass's.  One unit at
+// a time per CTA, one CTA per SM (144 KB of shared memory).
+constexpr int kTcRowThreads = 256;
+
+template <int N1>
+__global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
+{
+   constexpr int N2 = 4096, T = kTcRowThreads, KPT = N2 / T;
+   static_assert(N1 % 2 == 0, "row pairs need an even N1");
+   constexpr int NP = N1 / 2 + 1;
+   constexpr int FS = N2 + N2 / 16;  // padded row in float2
+   extern __shared__ __align__(1024) unsigned char smb[];
+   float2 *w4096 = reinterpret_cast<float2 *>(smb + TC_OPND_BYTES + TC_BMAT_BYTES);
+   float2 *fa = w4096 + N2;
+   float2 *fb = fa + FS;
+   __shared__ uint32_t tmem_holder;
+   __shared__ __align__(8) unsigned long long mma_bar;
+   const int tid = threadIdx.x;
+   const int nunits = NP * a.nbitems;
+   int u = blockIdx.x;
+   if (u >= nunits) return;  // the whole CTA, before any barrier
+   const uint32_t opnd = (uint32_t)__cvta_generic_to_shared(smb);
+   const uint32_t bmat = opnd + TC_OPND_BYTES;
+   const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&mma_bar);
+   for (int i = tid; i < N2; i += T) w4096[i] = a.tw2[i];
+   fill_dft16_bmat(bmat, T, 1.0 / 16.0);
+   tc::fence_async_smem();
+   if (tid < 32) tc::tmem_alloc((uint32_t)__cvta_generic_to_shared(&tmem_holder), TC_TMEM_COLS);
+   if (tid == 0) tc::mbar_init_cta(mbar, 1);
+   tc::fence_before();
+   __syncthreads();
+   tc::fence_after();
+   const uint32_t tmem = tmem_holder;
+   uint32_t par = 0;
+   bool gave_up = false;
+   const long long N = (long long)N1 * N2;
+   const float in_scale = a.tc_in_scale, comp = a.tc_out_comp;
+
+   auto level = [&](bool kmajor) {
+      if (tid == 0) tc_issue_level(tmem, opnd, bmat, kmajor, mbar);
+      if (!gave_up && !tc::mbar_wait(mbar, par)) {
+         gave_up = true;  // report once; later levels do not wait again
+         if (a.status) atomicExch(a.status, 1);
+      }
+      par ^= 1u;
+      tc::fence_after();
+   };
+   auto handoff = [&]() {
+      tc::fence_before();
+      tc::fence_async_smem();
+      __syncthreads();
+   };
+   // the 4096-point DFT of one scratch row into out[bpad(k)]
+   auto transform = [&](const float2 *row, float2 *out) {
+      float2 y[16];
+#pragma unroll
+      for (int q2 = 0; q2 < 16; q2++) {
+         const float2 x = __ldg(row + tid + 256 * q2);
+         y[q2] = make_float2(x.x * in_scale, x.y * in_scale);
+      }
+      store_k16(opnd, tid, y);
+      handoff();
+      level(true);
+      tc_load_row(tmem, y);
+#pragma unroll
+      for (int k0 = 1; k0 < 16; k0++) y[k0] = cmul(y[k0], w4096[(tid * k0) & (N2 - 1)]);
+      store_mn16(opnd, tid & 15, 16 + (tid & 15), tid >> 4, y);
+      handoff();
+      level(false);
+      tc_load_row(tmem, y);
+      const int k0 = (tid & 7) + 8 * (tid >> 7), q0 = (tid >> 3) & 15;
+#pragma unroll
+      for (int k1 = 1; k1 < 16; k1++) y[k1] = cmul(y[k1], w4096[16 * ((q0 * k1) & 255)]);
+      store_mn16(opnd, k0, 16 + k0, q0, y);
+      handoff();
+      level(false);
+      tc_load_row(tmem, y);
+      const int kap = ((tid >> 3) & 15) + 16 * ((tid & 7) + 8 * (tid >> 7));
+#pragma unroll
+      for (int kk = 0; kk < 16; kk++) out[bpad(kap + 256 * kk)] = make_float2(y[kk].x * comp, y[kk].y * comp);
+   };
+
+   float acc[KPT][4];
+#pragma unroll
+   for (int q = 0; q < KPT; q++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
+   int j = 0;
+   BigItem bi = a.bitems[u / NP];
+   while (true) {
+      const int rp = u % NP;
+      const int k1b = (N1 - rp) % N1;
+      const bool two = rp != k1b;
+      transform(a.scratch + ((long long)(bi.job0 + j) * N1 + rp) * N2, fa);
+      if (two) transform(a.scratch + ((long long)(bi.job0 + j) * N1 + k1b) * N2, fb);
+      tc::fence_before();
+      __syncthreads();  // both rows' spectra visible
+#pragma unroll
+      for (int q = 0; q < KPT; q++) {
+         const int k2 = tid + q * T;
+         const float2 zk = fa[bpad(k2)];
+         float2 zm;
+         if (rp == 0) zm = fa[bpad((N2 - k2) % N2)];
+         else if (two) zm = fb[bpad(N2 - 1 - k2)];
+         else zm = fa[bpad(N2 - 1 - k2)];
+         acc_bin(acc[q], bi.mode, zk, zm);
+      }
+      if (j == bi.nfr - 1) {
+         // bin k = k1 + N1 k2 of row k1, or its mirror N - k (conjugate
+         // cross product) above N/2; self-paired rows keep k <= N/2 only
+         float *part = a.partial + (long long)bi.item * 4 * a.S;
+         const int nprod = (bi.mode == MODE_XPOL) ? 4 : 1;
+#pragma unroll
+         for (int q = 0; q < KPT; q++) {
+            const int k2 = tid + q * T;
+            const long long k = rp + (long long)N1 * k2;
+            if (k <= N / 2 || two) {
+               const bool conj = k > N / 2;
+               const long long bin = conj ? N - k : k;
+               for (int c = 0; c < nprod; c++)
+                  part[(long long)c * a.S + bin] = (c == 3 && conj) ? -acc[q][c] : acc[q][c];
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
+         }
+      }
+      __syncthreads();  // the row spectra are read before the next unit writes them
+      int un = u, jn = j + 1;
+      if (jn >= bi.nfr) {
+         un = u + gridDim.x;
+         jn = 0;
+      }
+      if (un >= nunits) break;
+      if (un != u) bi = a.bitems[un / NP];
+      u = un;
+      j = jn;
+   }
+   tc::fence_before();
+   __syncthreads();
+   if (tid < 32) {
+      tc::fence_after();
+      tc::tmem_dealloc(tmem, TC_TMEM_COLS);
+   }
+}
+
+constexpr size_t big_rows_tc_smem()
+{
+   return (size_t)TC_OPND_BYTES + TC_BMAT_BYTES + sizeof(float2) * (4096 + 2 * (4096 + 4096 / 16));
+}
+
+// The tensor-core row pass of a split, or null where rows are not 4096 points.
+template <int N1, int N2>
+constexpr BigRowsKernel big_rows_tc_kernel()
+{
+   if constexpr (N2 == 4096) return k_big_rows_tc<N1>;
+   else return nullptr;
+}
+
 template <int N2>
 constexpr size_t big_rows_smem()
 {
@@ -517,7 +687,7 @@ constexpr size_t big_rows_smem()
     {big_cols_smem_slots<N1_, C_, 1>(big_cols_slots<N1_, C_, 1>()),                               \
      big_cols_smem_slots<N1_, C_, 2>(big_cols_slots<N1_, C_, 2>()),                               \
      big_cols_smem_slots<N1_, C_, 8>(big_cols_slots<N1_, C_, 8>())},                              \
-    big_rows_smem<N2_>()}
+    big_rows_smem<N2_>(), big_rows_tc_kernel<N1_, N2_>(), big_rows_tc_smem(), kTcRowThreads}
 #define SWS_BIG(N1_, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3) SWS_BIG_C(N1_, 4, TA_, A1, A2, A3, N2_, TB_, B1, B2, B3)
 
 // Candidate splits per length; the first of each length is the default,

@@ -47,6 +47,8 @@ struct BigArgs {
    int N, S;
    float4 levels;
    int *status;                // set to 1 when a bounded wait gave up (null: not reported)
+   float tc_in_scale;          // tensor-core row pass: 2^-e applied to the scratch rows
+   float tc_out_comp;          // and 16^3 2^e restoring the scale of its outputs
 };
 
 typedef void (*BigColsKernel)(BigArgs);
@@ -58,6 +60,9 @@ struct BigPlan {
    BigColsKernel cols[3];       // nbit 1, 2, 8
    BigRowsKernel rows;
    size_t smem_cols[3], smem_rows;  // column pass per bit depth (1, 2, 8)
+   BigRowsKernel rows_tc;       // tensor-core split row pass (N2 = 4096), or null
+   size_t smem_rows_tc;
+   int TBtc;                    // its threads
 };
 
 bool find_big_plan(int N, BigPlan *out);

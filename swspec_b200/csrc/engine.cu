@@ -614,15 +614,27 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
    a.status = (int *)h->d_status.p;
-   if (h->rows_fn != (const void *)bp.rows || h->cols_fn != (const void *)bp.cols[nbi]) {
-      // persistent passes: as many CTAs as fit on the device at once
+   // tensor-core row pass: rows enter scaled by 2^-e, e chosen so that the
+   // bound sqrt(2) N1 max|level| of a column-pass output stays below 2^15
+   const bool tc = c.precision != SWSGPU_PREC_FP32;
+   const double lmax = nbit == 8 ? 128.0 : nbit == 2 ? 4.0 : 1.0;
+   const int e = std::max(0, (int)std::ceil(std::log2(1.4143 * bp.N1 * lmax / 32768.0)));
+   a.tc_in_scale = std::ldexp(1.0f, -e);
+   a.tc_out_comp = std::ldexp(4096.0f, e);
+   BigRowsKernel rows = tc ? bp.rows_tc : bp.rows;
+   const int TB = tc ? bp.TBtc : bp.TB;
+   const size_t smem_rows = tc ? bp.smem_rows_tc : bp.smem_rows;
+   if (!rows) return fail(h, SWSGPU_EINVAL, "split has no tensor-core row pass");
+   if (h->rows_fn != (const void *)rows || h->cols_fn != (const void *)bp.cols[nbi]) {
+      // persistent passes: as many CTAs as fit on the device at once (the
+      // tensor-core row pass holds 144 KB of shared memory: one per SM)
       int occ_r = 0, occ_c = 0, nsm = 0;
-      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, bp.rows, bp.TB, bp.smem_rows));
+      CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, rows, TB, smem_rows));
       CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, bp.cols[nbi], bp.TA, bp.smem_cols[nbi]));
       CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
       h->rows_grid = std::max(1, occ_r) * nsm;
       h->cols_grid = std::max(1, occ_c) * nsm;
-      h->rows_fn = (const void *)bp.rows;
+      h->rows_fn = (const void *)rows;
       h->cols_fn = (const void *)bp.cols[nbi];
    }
    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -638,7 +650,7 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
       bp.cols[nbi]<<<(unsigned)std::min((bp.N2 / bp.C) * b.y, h->cols_grid), bp.TA, bp.smem_cols[nbi], st>>>(a);
       a.nbitems = b.w;
       const int units = (bp.N1 / 2 + 1) * b.w;
-      bp.rows<<<(unsigned)std::min(units, h->rows_grid), bp.TB, bp.smem_rows, st>>>(a);
+      rows<<<(unsigned)std::min(units, h->rows_grid), TB, smem_rows, st>>>(a);
       CK(h, cudaGetLastError());
       launches += 2;
    }
@@ -992,8 +1004,9 @@ static int flush_chunk(swsgpu_handle *h, bool group_end, int *nspec)
 }
 
 static int autotune_big(swsgpu_handle *h, int iters);
+static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp);
 static std::mutex &tune_mutex();
-static int tuned_choice(int N, int nbit);
+static int tuned_choice(int N, int nbit, bool tc);
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -1099,9 +1112,19 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    }
    if (!cluster_plan && !four_step)
       return fail(nullptr, SWSGPU_EINVAL, "fft_points " + std::to_string(cfg->fft_points) + " has no GPU plan");
-   if (cfg->precision != SWSGPU_PREC_FP32 && !(cluster_plan && plan.kern_tc[1]))
-      return fail(nullptr, SWSGPU_EINVAL,
-                  "tensor-core split form not available for fft_points " + std::to_string(cfg->fft_points));
+   if (cfg->precision != SWSGPU_PREC_FP32) {
+      // cluster lengths: the plan's tensor-core kernels; four-step lengths:
+      // a split with 4096-point rows (the tensor-core row pass)
+      bool tc_ok = cluster_plan && plan.kern_tc[1];
+      if (!cluster_plan && four_step) {
+         BigPlan cand[16];
+         const int nc = big_plan_candidates(cfg->fft_points, cand, 16);
+         for (int k = 0; k < nc; k++) tc_ok = tc_ok || cand[k].rows_tc;
+      }
+      if (!tc_ok)
+         return fail(nullptr, SWSGPU_EINVAL,
+                     "tensor-core split form not available for fft_points " + std::to_string(cfg->fft_points));
+   }
    int ndev = 0;
    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
       return fail(nullptr, SWSGPU_ENODEV, "no CUDA device " + std::to_string(device));
@@ -1248,11 +1271,25 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       {
          BigPlan cand[16];
          h->big_cands = big_plan_candidates(cfg->fft_points, cand, 16);
-         // a split tuned earlier in this process for the same length and bits
-         const int t = tuned_choice(cfg->fft_points, nbit);
+         // a split tuned earlier in this process for the same length, bits and form
+         const bool tc = cfg->precision != SWSGPU_PREC_FP32;
+         const int t = tuned_choice(cfg->fft_points, nbit, tc);
+         if (tc) {
+            // the tensor-core form runs only splits with 4096-point rows
+            for (int k = 0; k < h->big_cands; k++)
+               if (cand[k].rows_tc) {
+                  h->bplan = cand[k];
+                  h->cand = k;
+                  break;
+               }
+         }
          if (cfg->plan_candidate > 0 && !cfg->autotune) {
             if (cfg->plan_candidate >= h->big_cands) {
                h->err = "plan_candidate beyond the candidates of this length";
+               return bail(SWSGPU_EINVAL);
+            }
+            if (tc && !cand[cfg->plan_candidate].rows_tc) {
+               h->err = "plan_candidate has no tensor-core row pass (rows of 4096 points)";
                return bail(SWSGPU_EINVAL);
             }
             h->bplan = cand[cfg->plan_candidate];
@@ -1263,10 +1300,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
             h->cand = t;
          }
       }
-      CKB(cudaFuncSetAttribute((const void *)h->bplan.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)h->bplan.smem_cols[nbi]));
-      CKB(cudaFuncSetAttribute((const void *)h->bplan.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)h->bplan.smem_rows));
+      CKB(set_big_attrs(h, h->bplan));
       for (int k = 0; k < 2; k++)
          for (int s = 0; s < cfg->num_streams; s++)
             CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
@@ -1676,7 +1710,7 @@ __global__ void k_fill_hash(uint32_t *p, size_t n, uint32_t seed)
 }
 
 static std::mutex g_tune_mu;
-static std::map<std::pair<int, int>, int> g_tuned;  // (N, nbit) -> chosen candidate
+static std::map<std::pair<int, int>, int> g_tuned;  // (N, nbit + 100 for the tensor-core form) -> candidate
 
 static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
 {
@@ -1685,6 +1719,10 @@ static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
    cudaError_t e = cudaFuncSetAttribute((const void *)bp.cols[nbi], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)bp.smem_cols[nbi]);
    if (e != cudaSuccess) return e;
+   if (h->cfg.precision != SWSGPU_PREC_FP32)
+      return bp.rows_tc ? cudaFuncSetAttribute((const void *)bp.rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)bp.smem_rows_tc)
+                        : cudaErrorInvalidValue;
    return cudaFuncSetAttribute((const void *)bp.rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)bp.smem_rows);
 }
@@ -1740,6 +1778,7 @@ static int autotune_big(swsgpu_handle *h, int iters)
    cudaEvent_t ev[17];
    for (int i = 0; i <= nit; i++) cudaEventCreate(&ev[i]);
    for (int k = 0; k < nc; k++) {
+      if (c.precision != SWSGPU_PREC_FP32 && !cand[k].rows_tc) continue;  // no tensor-core row pass
       if (set_big_attrs(h, cand[k]) != cudaSuccess) {
          cudaGetLastError();
          continue;
@@ -1777,7 +1816,7 @@ static int autotune_big(swsgpu_handle *h, int iters)
    h->cand = best;
    CK(h, set_big_attrs(h, h->bplan));
    std::lock_guard<std::mutex> lk(g_tune_mu);
-   g_tuned[std::make_pair(c.fft_points, nbit)] = best;
+   g_tuned[std::make_pair(c.fft_points, nbit + (c.precision != SWSGPU_PREC_FP32 ? 100 : 0))] = best;
    return SWSGPU_OK;
 }
 
@@ -2093,9 +2132,9 @@ void swsgpu_batch_destroy(swsgpu_batch *b)
 
 static std::mutex &tune_mutex() { return g_tune_mu; }
 
-static int tuned_choice(int N, int nbit)
+static int tuned_choice(int N, int nbit, bool tc)
 {
    std::lock_guard<std::mutex> lk(tune_mutex());
-   auto it = g_tuned.find(std::make_pair(N, nbit));
+   auto it = g_tuned.find(std::make_pair(N, nbit + (tc ? 100 : 0)));
    return it == g_tuned.end() ? -1 : it->second;
 }

@@ -122,10 +122,12 @@ def test_four_step_blanked_mark5b_pcal(gpu):
     assert np.max(np.abs(pc - rp)) / np.max(np.abs(rp)) < 1e-6
 
 
-def test_dynamic_range_vdif_8bit_2p22(gpu):
+@pytest.mark.parametrize("precision", ["fp32", "tcsplit"])
+def test_dynamic_range_vdif_8bit_2p22(gpu, precision):
     """Dynamic-range configuration: VDIF 8-bit, N = 2^22, Blackman-Harris,
     a carrier 50 dB above the per-bin noise floor drifting 1 Hz/s; noise
-    floor level and carrier leakage vs FP64."""
+    floor level and carrier leakage vs FP64, for the FP32 form and the
+    tensor-core split form (4096-point rows on tcgen05, FP16 hi/lo)."""
     N, cof, fs = 1 << 22, 3, 64e6
     nsamp = N * cof
     spf = 8000
@@ -138,8 +140,12 @@ def test_dynamic_range_vdif_8bit_2p22(gpu):
     codes = synth.quantize_vdif_8bit(x, 24.0)
     data = synth.vdif_frames(synth.pack_codes(codes[None, :], 8), 8000, 1, 8, 8000)
     lay = gpu.layout("vdif:8000", 1, 8)
-    cfg = gpu.make_config(lay, N, "blackmanharris", 1, cof, max_run_bytes=len(data), samplingfreq=fs)
+    prec = gpu.PREC_TCSPLIT if precision == "tcsplit" else gpu.PREC_FP32
+    cfg = gpu.make_config(lay, N, "blackmanharris", 1, cof, max_run_bytes=len(data), samplingfreq=fs,
+                          precision=prec)
     core = gpu.Core(cfg)
+    if precision == "tcsplit":
+        assert "4096" in core.plan_info(), core.plan_info()
     auto, _, _, ns = core.run([data])
     s = decode_channels(data, "VDIF_8000-512-1-8", 1, 8, [0], nfr * spf)
     ra, _, _, nref = oracle_run(s, N, "blackmanharris", 1, cof)
@@ -155,7 +161,9 @@ def test_dynamic_range_vdif_8bit_2p22(gpu):
     skirt = np.r_[kc - 200:kc - 4, kc + 5:kc + 200]
     assert np.max(np.abs(got[skirt] - ref[skirt]) / ref[skirt]) < 1e-4
     e_rob, e_rel, c_rob, c_rel = _check_auto(got, ref, r32[0, 0])
-    print(f"2^22: robust {e_rob:.2e} (FP32 CPU {c_rob:.2e}), max rel {e_rel:.2e} (FP32 CPU {c_rel:.2e})")
+    lk = np.max(np.abs(got[skirt] - ref[skirt]) / ref[skirt])
+    print(f"2^22 {precision}: floor ratio - 1 = {floor_g / floor_r - 1:.2e}, skirt max rel {lk:.2e}, "
+          f"robust {e_rob:.2e} (FP32 CPU {c_rob:.2e}), max rel {e_rel:.2e} (FP32 CPU {c_rel:.2e})")
 
 
 def test_spacecraft_tone_3p2M_cosine2_pcal(gpu):
@@ -218,9 +226,10 @@ def test_every_four_step_candidate(gpu, N, k):
     _check_auto(auto[0, 0], ra[0, 0], r32[0, 0], per_bin=False)
 
 
-@pytest.mark.parametrize("N,cof,window,nbit,fs", [(3_200_000, 100, "cosine2", 2, 32e6),
-                                                   (1 << 22, 76, "blackmanharris", 8, 64e6)])
-def test_integrated_spectrum_meets_the_bar(gpu, N, cof, window, nbit, fs):
+@pytest.mark.parametrize("N,cof,window,nbit,fs,precision", [(3_200_000, 100, "cosine2", 2, 32e6, "fp32"),
+                                                             (1 << 22, 76, "blackmanharris", 8, 64e6, "fp32"),
+                                                             (1 << 22, 76, "blackmanharris", 8, 64e6, "tcsplit")])
+def test_integrated_spectrum_meets_the_bar(gpu, N, cof, window, nbit, fs, precision):
     """The long lengths at their configurations' integrations -- N = 3.2M
     with 100 FFTs (10 s at 32 Msps) and N = 2^22 with 76 FFTs (5 s at
     64 Msps) -- on white noise: the integrated spectrum is within 2e-6 of
@@ -229,7 +238,8 @@ def test_integrated_spectrum_meets_the_bar(gpu, N, cof, window, nbit, fs):
     nsamp = N * cof
     pay = rng.integers(0, 256, nsamp * nbit // 8, dtype=np.uint8).tobytes()
     lay = gpu.layout("vdif:8000", 1, nbit, framed=False)
-    cfg = gpu.make_config(lay, N, window, 1, cof, max_run_bytes=len(pay), samplingfreq=fs)
+    cfg = gpu.make_config(lay, N, window, 1, cof, max_run_bytes=len(pay), samplingfreq=fs,
+                          precision=gpu.PREC_TCSPLIT if precision == "tcsplit" else gpu.PREC_FP32)
     core = gpu.Core(cfg)
     auto, _, _, ns = core.run([pay])
     x = O.decode(O.FMT_VDIF, 1, nbit, pay, nsamp, 0, payload_bytes=8000)
@@ -241,5 +251,5 @@ def test_integrated_spectrum_meets_the_bar(gpu, N, cof, window, nbit, fs):
     e = float(np.max(np.abs(got - ref) / ref))
     c = float(np.max(np.abs(r32[0, 0] - ref) / ref))
     rms = float(np.sqrt(np.mean(((got - ref) / ref) ** 2)))
-    print(f"N={N} x {cof} FFTs: GPU max rel {e:.2e} rms {rms:.2e}; FP32 CPU max rel {c:.2e}")
+    print(f"N={N} x {cof} FFTs ({precision}): GPU max rel {e:.2e} rms {rms:.2e}; FP32 CPU max rel {c:.2e}")
     assert e < REL_TOL, (e, c)
