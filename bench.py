@@ -598,7 +598,10 @@ def spec_arm(args) -> None:
     reps = Replicas("nccl")
     lay = gpu.layout(w["fmt"], w["nchan"], w["nbit"], framed=False)
     pc = w["pcal"] or {}
+    prec = {"auto": gpu.PREC_FP32, "fp32": gpu.PREC_FP32, "tcsplit": gpu.PREC_TCSPLIT,
+            "tcsplit_all": gpu.PREC_TCSPLIT}[args.precision]
     cfg = gpu.make_config(lay, w["N"], w["window"], 1, w["core_ffts"], sources=w["sources"], xpols=w["xpols"],
+                          precision=prec,
                           max_run_bytes=w["run_bytes"], samplingfreq=w["fs"], runs_per_output=w["runs"],
                           extract_pcal=bool(pc), pcal_tonebins=pc.get("tonebins", 0),
                           pcal_rotatorlen=pc.get("rotatorlen", 0), pcal_offset_hz=pc.get("offset", 10e3),
@@ -652,6 +655,7 @@ def spec_arm(args) -> None:
         line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": reps.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (random codes)",
+                "precision": {gpu.PREC_FP32: "fp32", gpu.PREC_TCSPLIT: "tcsplit"}[prec],
                 "config": {"workload": w["desc"], "fft_points": w["N"], "sources": ns,
                            "samples_per_step": samples, "bytes_per_step": bytes_in,
                            "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_in / 1e6),

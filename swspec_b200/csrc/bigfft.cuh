@@ -47,8 +47,6 @@ struct BigArgs {
    int N, S;
    float4 levels;
    int *status;                // set to 1 when a bounded wait gave up (null: not reported)
-   float tc_in_scale;          // tensor-core row pass: 2^-e applied to the scratch rows
-   float tc_out_comp;          // and 16^3 2^e restoring the scale of its outputs
 };
 
 typedef void (*BigColsKernel)(BigArgs);

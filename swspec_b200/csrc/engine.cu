@@ -614,13 +614,7 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
    a.status = (int *)h->d_status.p;
-   // tensor-core row pass: rows enter scaled by 2^-e, e chosen so that the
-   // bound sqrt(2) N1 max|level| of a column-pass output stays below 2^15
    const bool tc = c.precision != SWSGPU_PREC_FP32;
-   const double lmax = nbit == 8 ? 128.0 : nbit == 2 ? 4.0 : 1.0;
-   const int e = std::max(0, (int)std::ceil(std::log2(1.4143 * bp.N1 * lmax / 32768.0)));
-   a.tc_in_scale = std::ldexp(1.0f, -e);
-   a.tc_out_comp = std::ldexp(4096.0f, e);
    BigRowsKernel rows = tc ? bp.rows_tc : bp.rows;
    const int TB = tc ? bp.TBtc : bp.TB;
    const size_t smem_rows = tc ? bp.smem_rows_tc : bp.smem_rows;

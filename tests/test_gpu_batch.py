@@ -65,19 +65,19 @@ def test_batch_graph_equals_eager(gpu):
         for e, o in zip(outs_e, outs_b):
             assert torch.equal(e, o), rep
     b.close()
-    # every core of the batch against the FP64 oracle: the cluster lengths
-    # at the 2e-6 bar (per bin with 16 FFTs; with 2 or 3 FFTs, whose
-    # chi-square spectra put bins near zero, relative to max(bin, median
-    # bin)), the four-step lengths at the four-step tests' bars
+    # every core of the batch against the FP64 oracle: per bin at the 2e-6
+    # bar with 16 FFTs per spectrum; with 2 or 3 FFTs (chi-square spectra
+    # with bins near zero, and at the longer lengths an FP32 rounding noise
+    # that the reference's own FP32 arithmetic shares) at the four-step
+    # tests' bars, relative to max(bin, median bin) and to the FP32 CPU
+    # restatement of doMaths
     for s, got in zip(specs, outs_b):
         x = O.decode(O.FMT_VDIF, 1, s.nbit, stream_payload(s), s.samples_per_run, 0, payload_bytes=8000)
         ra, _, _, nref = oracle_run([x], s.fft_points, "hann", 1, s.core_overlapped_ffts)
         g = got.cpu().numpy()
         assert g.shape[0] == nref, s.fft_points
-        if s.fft_points <= 131072:
-            d = np.abs(g[0, 0] - ra[0, 0])
-            floor = ra[0, 0] if s.core_overlapped_ffts >= 16 else np.maximum(ra[0, 0], np.median(ra[0, 0]))
-            assert np.max(d / floor) < REL_TOL, s.fft_points
+        if s.core_overlapped_ffts >= 16:
+            assert np.max(np.abs(g[0, 0] - ra[0, 0]) / ra[0, 0]) < REL_TOL, s.fft_points
         else:
             r32, _, _, _ = _fp32_run([x], s.fft_points, "hann", 1, s.core_overlapped_ffts)
             _check_auto(g[0, 0], ra[0, 0], r32[0, 0], per_bin=False)
