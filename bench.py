@@ -575,16 +575,73 @@ def c4_arm(args) -> None:
 SPEC_WORKLOADS = {
     "c1": dict(desc="plain method: Mark5B-1024-16-2, channel 1 only, N=32768 Hann, 1 s (976 FFTs), "
                     "2 MiB runs x 61", fmt="mark5b", nchan=16, nbit=2, N=32768, window="hann", fs=32e6,
-               core_ffts=16, run_bytes=2 << 20, runs=61, sources=((0, 0),), xpols=(), pcal=None),
+               core_ffts=16, run_bytes=2 << 20, runs=61, sources=((0, 0),), xpols=(), pcal=None,
+               signal="Gaussian noise, CW tone at +3.1 MHz in channel 1 at 20 dB per FFT bin, +-0.98 sigma 2-bit"),
     "c2": dict(desc="spacecraft-tone tracking: Mark5B-1024-16-2, 16 channels, N=3,200,000 cosine2, 10 s "
                     "(100 FFTs), 51.2 MB runs x 25, phase-cal 32 bins / 3200 rotator, 16 tones",
                fmt="mark5b", nchan=16, nbit=2, N=3_200_000, window="cosine2", fs=32e6, core_ffts=4,
                run_bytes=51_200_000, runs=25, sources=tuple((0, c) for c in range(16)), xpols=(),
-               pcal=dict(tonebins=32, rotatorlen=3200, offset=10e3, ntones=16)),
+               pcal=dict(tonebins=32, rotatorlen=3200, offset=10e3, ntones=16),
+               signal="Gaussian noise plus a phase-cal comb (1 MHz spacing, +10 kHz, 5 % of sigma, seeded "
+                      "phases) in every channel, +-0.98 sigma 2-bit"),
     "c5": dict(desc="dynamic range: VDIF 8-bit 1 channel 64 Msps, N=2^22 Blackman-Harris, 5 s (76 FFTs), "
                     "16 MiB runs x 19", fmt="vdif:8000", nchan=1, nbit=8, N=1 << 22, window="blackmanharris",
-               fs=64e6, core_ffts=4, run_bytes=16 << 20, runs=19, sources=((0, 0),), xpols=(), pcal=None),
+               fs=64e6, core_ffts=4, run_bytes=16 << 20, runs=19, sources=((0, 0),), xpols=(), pcal=None,
+               signal="Gaussian noise plus a carrier at 12.3456 MHz 50 dB over the per-bin floor drifting "
+                      "1 Hz/s, 8-bit offset binary at 12 codes per sigma"),
 }
+
+
+def spec_payload(name: str, w: dict, seed: int):
+    """The workload's whole step of header-free payload on the device."""
+    import numpy as np
+
+    from swspec_b200 import synth_gpu
+    T = w["run_bytes"] * w["runs"] * 8 // (w["nbit"] * w["nchan"])
+    if name == "c1":
+        return synth_gpu.mark5b_payload(T, 16, w["fs"], seed, tone_hz=3.1e6,
+                                        tone_amp=float(np.sqrt(8 * 100.0 / w["N"])))
+    if name == "c2":
+        phases = np.random.default_rng(seed).uniform(0, 2 * np.pi, 16)
+        return synth_gpu.mark5b_payload(T, 16, w["fs"], seed, comb=(1e6, 10e3, 0.05, phases))
+    return synth_gpu.vdif8_carrier_payload(T, w["fs"], seed, 12.3456e6, 1.0, 50.0, w["N"])
+
+
+def spec_cpu_baseline(w: dict, payload, seconds_budget: float = 12.0) -> dict:
+    """The CPU restatement of the reference core (FP32 TaskCoreIPP::doMaths
+    after the mark5access decode of the packed bytes) on all host cores over
+    a bounded sample of the workload: each thread takes whole FFTs of one
+    source, as many as the budget allows."""
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    N, ns = w["N"], len(w["sources"])
+    nbit, nchan = w["nbit"], w["nchan"]
+    fmt = O.FMT_MARK5B if w["fmt"] == "mark5b" else O.FMT_VDIF
+    bpt = nbit * nchan // 8                          # payload bytes per sample-time
+    nfft_avail = len(payload) // (N * bpt)
+    cfg = O.make_cfg(N, core_overlapped_ffts=1, num_sources=1, window=O.WINDOW_NAMES[w["window"]], nthreads=1)
+    kw = {"payload_bytes": 8000} if fmt == O.FMT_VDIF else {}
+
+    def job(k):
+        f, src = k % nfft_avail, w["sources"][(k // nfft_avail) % ns][1]
+        seg = payload[f * N * bpt:(f + 1) * N * bpt].tobytes()
+        x = O.decode(fmt, nchan, nbit, seg, N, src, **kw)
+        O.domaths(cfg, [x], fp64=False)
+        return N
+
+    samples, k = 0, 0
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds_budget:
+            samples += sum(pool.map(job, range(k, k + cores)))
+            k += cores
+        dt = time.perf_counter() - t0
+    return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "port",
+            "sample": f"{k} FFTs of N = {N} from the workload's packed bytes (mark5access decode + FP32 "
+                      "restatement of TaskCoreIPP::doMaths), one FFT per thread at a time",
+            "seconds": dt}
 
 
 def spec_arm(args) -> None:
@@ -609,9 +666,9 @@ def spec_arm(args) -> None:
                           plan_family=gpu.PLAN_FOURSTEP if args.candidate >= 0 else gpu.PLAN_DEFAULT,
                           plan_candidate=max(args.candidate, 0))
     core = gpu.Core(cfg, device=local)
-    g = torch.Generator(device="cuda")
-    g.manual_seed(1000 + reps.rank)
-    raw = torch.randint(0, 256, (w["run_bytes"] * w["runs"],), dtype=torch.uint8, device="cuda", generator=g)
+    raw = spec_payload(args.workload, w, 1000 + reps.rank)
+    assert raw.numel() == w["run_bytes"] * w["runs"]
+    torch.cuda.synchronize()
     S = w["N"] // 2 + 1
     ns = len(w["sources"])
     d_auto = torch.zeros(ns, S, dtype=torch.float32, device="cuda")
@@ -646,6 +703,38 @@ def spec_arm(args) -> None:
     core.sync(st.cuda_stream)   # raises if a bounded device wait of any step gave up
     samples = w["runs"] * w["core_ffts"] * w["N"] * ns
     value = samples * reps.world / (ms * 1e-3) / 1e9
+
+    # ---- e2e: TaskCore path from pinned host memory, one submit per run ----
+    import numpy as np
+    host = torch.empty(raw.numel(), dtype=torch.uint8, pin_memory=True)
+    host.copy_(raw)
+    torch.cuda.synchronize()
+    ecore = gpu.Core(cfg, device=local)
+    ecore.set_sizes([w["run_bytes"]])
+    auto_h = np.zeros((1, ns, S), np.float32)
+    pcal_h = np.zeros((1, ns, max(pc.get("tonebins", 1), 1), 2), np.float32) if pc else None
+    tones_h = np.zeros((1, ns, max(pc.get("ntones", 1), 1), 2), np.float64) if pc else None
+    base = host.data_ptr()
+
+    def e2e_step():
+        for r in range(w["runs"]):
+            ecore.submit([base + r * w["run_bytes"]], payload_offsets=[r * w["run_bytes"]])
+            ecore.wait()
+        ecore.fetch_into(auto_h, None, pcal_h, tones_h)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    reps.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = reps.max(time.perf_counter() - t0)
+    ecore.close()
+    e2e_val = samples * args.steps * reps.world / e2e_s / 1e9
+    d2h = auto_h.nbytes + (pcal_h.nbytes + tones_h.nbytes if pc else 0)
+    cpu = None
+    if reps.rank == 0 and reps.world == 1 and not args.no_cpu:
+        cpu = spec_cpu_baseline(w, host.numpy())
     if reps.rank == 0:
         peaks = measured_peaks()
         kern_s = kms / max(nk, 1) * 1e-3
@@ -654,13 +743,17 @@ def spec_arm(args) -> None:
         p32 = fp32_peak(local)
         line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": reps.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (random codes)",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic: " + w["signal"],
                 "precision": {gpu.PREC_FP32: "fp32", gpu.PREC_TCSPLIT: "tcsplit"}[prec],
                 "config": {"workload": w["desc"], "fft_points": w["N"], "sources": ns,
                            "samples_per_step": samples, "bytes_per_step": bytes_in,
                            "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_in / 1e6),
                            "plan": core.plan_info()},
-                "clocks": cs.summary(), "gpu_launches": launches * args.steps, "e2e": None,
+                "clocks": cs.summary(), "gpu_launches": launches * args.steps,
+                "e2e": {"value": e2e_val, "unit": "Gsamples/s", "h2d_bytes_per_step": w["run_bytes"] * w["runs"],
+                        "d2h_bytes_per_step": d2h,
+                        "path": "swsgpu_submit/wait per run from pinned host memory (TaskCore path), device "
+                                "combine, one fetch per spectrum"},
                 "roofline": {"bound": "fp32", "achieved": flops / (ms * 1e-3) / 1e12, "peak": p32,
                              "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / p32 if p32 else None,
                              "traffic": None, "scope": "whole step (every kernel of the step)",
@@ -668,7 +761,7 @@ def spec_arm(args) -> None:
                              "hbm": {"achieved_gbs": bytes_in / (ms * 1e-3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
                                      "frac": bytes_in / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"]},
                              "fft_kernel_ms_per_launch": kern_s * 1e3, "fft_kernel_launches_per_step": nk / 3},
-                "cpu_baseline": None}
+                "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     core.close()
     reps.close()

@@ -77,3 +77,69 @@ def c3_framed(nsamp_time: int, N: int = 65536, npairs: int = 8, rho: float = 0.3
     frames[:, :4] = hdr
     frames[:, 4:] = payload
     return frames.reshape(-1).view(torch.uint8), nfr
+
+
+def _chunks(T: int, chunk: int = 1 << 24):
+    for t0 in range(0, T, chunk):
+        yield t0, min(chunk, T - t0)
+
+
+def mark5b_payload(T: int, nchan: int, fs: float, seed: int, tone_hz: float = 0.0, tone_amp: float = 0.0,
+                   comb: tuple | None = None, device: str = "cuda") -> torch.Tensor:
+    """Header-free Mark5B payload (nchan 2-bit channels, +-0.98 sigma
+    thresholds) of T sample-times on the device: seeded unit Gaussian noise
+    per channel, plus a CW tone in channel 0 (tone_hz, amplitude tone_amp in
+    sigma) and/or a phase-cal comb in every channel, comb = (spacing_hz,
+    offset_hz, amp_sigma, phases): tones at k spacing + offset below fs/2,
+    FP64 phase, periodic in fs / gcd(fs, offset) samples, so one period is
+    computed and tiled.  nchan * 2 = 32 bits per sample-time."""
+    assert nchan * 2 == 32
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = torch.empty(T, dtype=torch.int32, device=device)
+    period = None
+    if comb is not None:
+        spacing, offset, amp, phases = comb
+        per = int(round(fs / np.gcd(int(fs), int(offset))))
+        n = torch.arange(per, dtype=torch.float64, device=device)
+        period = torch.zeros(per, dtype=torch.float64, device=device)
+        for k, ph in enumerate(phases):
+            f = k * spacing + offset
+            if f >= fs / 2:
+                break
+            period += amp * torch.cos(2 * np.pi * torch.remainder(f * n, fs) / fs + ph)
+        period = period.to(torch.float32)
+    for t0, L in _chunks(T):
+        w = torch.zeros(L, dtype=torch.int64, device=device)
+        add = None
+        if period is not None:
+            idx = torch.remainder(torch.arange(t0, t0 + L, device=device), period.numel())
+            add = period[idx]
+        for c in range(nchan):
+            x = torch.randn(L, generator=g, device=device)
+            if add is not None:
+                x += add
+            if c == 0 and tone_amp:
+                n = torch.arange(t0, t0 + L, dtype=torch.float64, device=device)
+                x += (tone_amp * torch.cos(2 * np.pi * torch.remainder(tone_hz * n, fs) / fs)).to(torch.float32)
+            w |= quantize_mark5b_2bit(x).to(torch.int64) << (2 * c)
+        out[t0:t0 + L] = (w & 0xFFFFFFFF).to(torch.int32)
+    return out.view(torch.uint8)
+
+
+def vdif8_carrier_payload(T: int, fs: float, seed: int, f0: float, drift_hz_s: float, snr_bin_db: float,
+                          N: int, lsb_sigma: float = 24.0, device: str = "cuda") -> torch.Tensor:
+    """Header-free single-channel 8-bit VDIF payload (offset binary, code
+    b = floor(x lsb_sigma / 2 + 128) clipped to [0, 255]) of T samples:
+    unit Gaussian noise plus a carrier snr_bin_db above the per-bin noise
+    floor of an N-point FFT, at f0 drifting drift_hz_s, FP64 phase."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    A = float(np.sqrt(4 * 10 ** (snr_bin_db / 10) * 2.0 / N))
+    out = torch.empty(T, dtype=torch.uint8, device=device)
+    for t0, L in _chunks(T):
+        t = torch.arange(t0, t0 + L, dtype=torch.float64, device=device) / fs
+        cyc = torch.remainder(f0 * t + 0.5 * drift_hz_s * t * t, 1.0)
+        x = torch.randn(L, generator=g, device=device) + (A * torch.cos(2 * np.pi * cyc)).to(torch.float32)
+        out[t0:t0 + L] = torch.clamp(torch.floor(x * (lsb_sigma / 2.0) + 128.0), 0, 255).to(torch.uint8)
+    return out
