@@ -588,7 +588,7 @@ SPEC_WORKLOADS = {
                     "16 MiB runs x 19", fmt="vdif:8000", nchan=1, nbit=8, N=1 << 22, window="blackmanharris",
                fs=64e6, core_ffts=4, run_bytes=16 << 20, runs=19, sources=((0, 0),), xpols=(), pcal=None,
                signal="Gaussian noise plus a carrier at 12.3456 MHz 50 dB over the per-bin floor drifting "
-                      "1 Hz/s, 8-bit offset binary at 12 codes per sigma"),
+                      "1 Hz/s, 8-bit offset binary at 24 codes per sigma"),
 }
 
 
@@ -599,12 +599,15 @@ def spec_payload(name: str, w: dict, seed: int):
     from swspec_b200 import synth_gpu
     T = w["run_bytes"] * w["runs"] * 8 // (w["nbit"] * w["nchan"])
     if name == "c1":
-        return synth_gpu.mark5b_payload(T, 16, w["fs"], seed, tone_hz=3.1e6,
-                                        tone_amp=float(np.sqrt(8 * 100.0 / w["N"])))
+        # Hann: 20 dB per-bin SNR <=> A^2 N / (6 sigma^2) = 100
+        return synth_gpu.mark5b_payload(T, 16, w["fs"], 1001 + seed, tone_hz=3.1e6,
+                                        tone_amp=float(np.sqrt(6 * 100.0 / w["N"])))
     if name == "c2":
-        phases = np.random.default_rng(seed).uniform(0, 2 * np.pi, 16)
-        return synth_gpu.mark5b_payload(T, 16, w["fs"], seed, comb=(1e6, 10e3, 0.05, phases))
-    return synth_gpu.vdif8_carrier_payload(T, w["fs"], seed, 12.3456e6, 1.0, 50.0, w["N"])
+        phases = np.random.default_rng(1002 + seed).uniform(0, 2 * np.pi, 16)
+        return synth_gpu.mark5b_payload(T, 16, w["fs"], 1002 + seed, comb=(1e6, 10e3, 0.05, phases))
+    # 4-term Blackman-Harris (equivalent noise bandwidth about 2 bins): 50 dB
+    # over the per-bin floor <=> A = sigma sqrt(4e5 * 2 / N); sigma = 24 codes
+    return synth_gpu.vdif8_carrier_payload(T, w["fs"], 1005 + seed, 12.3456e6, 1.0, 50.0, w["N"], lsb_sigma=48.0)
 
 
 def spec_cpu_baseline(w: dict, payload, seconds_budget: float = 12.0) -> dict:
@@ -666,7 +669,7 @@ def spec_arm(args) -> None:
                           plan_family=gpu.PLAN_FOURSTEP if args.candidate >= 0 else gpu.PLAN_DEFAULT,
                           plan_candidate=max(args.candidate, 0))
     core = gpu.Core(cfg, device=local)
-    raw = spec_payload(args.workload, w, 1000 + reps.rank)
+    raw = spec_payload(args.workload, w, reps.rank)
     assert raw.numel() == w["run_bytes"] * w["runs"]
     torch.cuda.synchronize()
     S = w["N"] // 2 + 1

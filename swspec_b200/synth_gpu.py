@@ -130,12 +130,13 @@ def mark5b_payload(T: int, nchan: int, fs: float, seed: int, tone_hz: float = 0.
 def vdif8_carrier_payload(T: int, fs: float, seed: int, f0: float, drift_hz_s: float, snr_bin_db: float,
                           N: int, lsb_sigma: float = 24.0, device: str = "cuda") -> torch.Tensor:
     """Header-free single-channel 8-bit VDIF payload (offset binary, code
-    b = floor(x lsb_sigma / 2 + 128) clipped to [0, 255]) of T samples:
+    b = floor(x lsb_sigma / 2 + 128) clipped to [0, 255], so lsb_sigma / 2
+    codes per sigma) of T samples:
     unit Gaussian noise plus a carrier snr_bin_db above the per-bin noise
     floor of an N-point FFT, at f0 drifting drift_hz_s, FP64 phase."""
     g = torch.Generator(device=device)
     g.manual_seed(seed)
-    A = float(np.sqrt(4 * 10 ** (snr_bin_db / 10) * 2.0 / N))
+    A = float(np.sqrt(4 * 10 ** (snr_bin_db / 10) * 2.0 / N))  # equivalent noise bandwidth 2 bins
     out = torch.empty(T, dtype=torch.uint8, device=device)
     for t0, L in _chunks(T):
         t = torch.arange(t0, t0 + L, dtype=torch.float64, device=device) / fs
