@@ -456,7 +456,9 @@ def gpu_arm(args) -> None:
     # DRAM bytes of one k_spectra launch on this workload, from ncu captures
     # (dram__bytes_read.sum + dram__bytes_write.sum): the 2-bit codes read
     # plus the per-item partial spectra that k_reduce combines
-    traffic = {gpu.PREC_FP32: (256476672 + 208978176, "profiles/k_spectra_c3_fp32.md")}
+    traffic = {gpu.PREC_FP32: (256476672 + 208978176,
+                               "ncu --set full capture of one k_spectra launch of this workload "
+                               "(dram__bytes_read.sum + dram__bytes_write.sum)")}
     t = traffic.get(headline)
     roof["traffic"] = t[0] if t else None
     roof["traffic_source"] = t[1] if t else None

@@ -175,6 +175,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 // Bulk copy global -> shared by the TMA engine (addresses 16-byte aligned,
@@ -517,8 +522,10 @@ __global__ void __launch_bounds__(T, 65536 / (T * 128)) k_big_rows(BigArgs a)
 // inside the FP16 normal range where the hi/lo split keeps about 22 bits.
 // The outputs are multiplied back by 64 / 2^(8 - e), exact.  Both rows of
 // the pair land in shared memory for the pair separation, which with the
-// accumulation and the partial write is the FP32 row pass's.  One unit at
-// a time per CTA, one CTA per SM (144 KB of shared memory).
+// accumulation and the partial write is the FP32 row pass's.  The next
+// unit's rows stream into a staging slot by cp.async as soon as every
+// thread has taken this unit's last row into its registers.  One unit at a
+// time per CTA, one CTA per SM (208 KB of shared memory).
 constexpr int kTcRowThreads = 256;
 
 template <int N1>
@@ -532,6 +539,8 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
    float2 *w4096 = reinterpret_cast<float2 *>(smb + TC_OPND_BYTES + TC_BMAT_BYTES);
    float2 *fa = w4096 + N2;
    float2 *fb = fa + FS;
+   float2 *sa = fb + FS;        // staged rows of the unit in hand
+   float2 *sb = sa + N2;
    __shared__ uint32_t tmem_holder;
    __shared__ __align__(8) unsigned long long mma_bar;
    __shared__ float wmax[T / 32];
@@ -569,13 +578,27 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
       tc::fence_async_smem();
       __syncthreads();
    };
-   // the 4096-point DFT of one scratch row into out[bpad(k)]
-   auto transform = [&](const float2 *row, float2 *out) {
+   // stage the rows of unit uu, job jj (16-byte cp.async, 8 per thread and row)
+   auto stage = [&](int uu, int jj) {
+      const BigItem si = a.bitems[uu / NP];
+      const int rp = uu % NP;
+      const int k1b = (N1 - rp) % N1;
+      const float2 *ra = a.scratch + ((long long)(si.job0 + jj) * N1 + rp) * N2;
+      const float2 *rb = a.scratch + ((long long)(si.job0 + jj) * N1 + k1b) * N2;
+      for (int i = tid; i < N2 / 2; i += T) {
+         cp_async16(sa + 2 * i, ra + 2 * i);
+         if (k1b != rp) cp_async16(sb + 2 * i, rb + 2 * i);
+      }
+      cp_async_commit();
+   };
+   // the 4096-point DFT of one staged row into out[bpad(k)]; on_read runs
+   // once every thread holds the row in registers
+   auto transform = [&](const float2 *row, float2 *out, auto &&on_read) {
       float2 y[16];
       float m = 0.0f;
 #pragma unroll
       for (int q2 = 0; q2 < 16; q2++) {
-         y[q2] = __ldg(row + tid + 256 * q2);
+         y[q2] = row[tid + 256 * q2];
          m = fmaxf(m, fmaxf(fabsf(y[q2].x), fabsf(y[q2].y)));
       }
 #pragma unroll
@@ -590,6 +613,7 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
       for (int q2 = 0; q2 < 16; q2++) y[q2] = make_float2(y[q2].x * in_scale, y[q2].y * in_scale);
       store_k16(opnd, tid, y);
       handoff();
+      on_read();
       level(true);
       tc_load_row(tmem, y);
 #pragma unroll
@@ -617,12 +641,29 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
       for (int c = 0; c < 4; c++) acc[q][c] = 0.0f;
    int j = 0;
    BigItem bi = a.bitems[u / NP];
+   stage(u, 0);
    while (true) {
       const int rp = u % NP;
       const int k1b = (N1 - rp) % N1;
       const bool two = rp != k1b;
-      transform(a.scratch + ((long long)(bi.job0 + j) * N1 + rp) * N2, fa);
-      if (two) transform(a.scratch + ((long long)(bi.job0 + j) * N1 + k1b) * N2, fb);
+      int un = u, jn = j + 1;
+      if (jn >= bi.nfr) {
+         un = u + gridDim.x;
+         jn = 0;
+      }
+      const bool more = un < nunits;
+      cp_async_wait0();
+      __syncthreads();  // this unit's staged rows are visible
+      auto next = [&]() {
+         if (more) stage(un, jn);
+      };
+      auto none = []() {};
+      if (two) {
+         transform(sa, fa, none);
+         transform(sb, fb, next);
+      } else {
+         transform(sa, fa, next);
+      }
       tc::fence_before();
       __syncthreads();  // both rows' spectra visible
 #pragma unroll
@@ -655,12 +696,7 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
          }
       }
       __syncthreads();  // the row spectra are read before the next unit writes them
-      int un = u, jn = j + 1;
-      if (jn >= bi.nfr) {
-         un = u + gridDim.x;
-         jn = 0;
-      }
-      if (un >= nunits) break;
+      if (!more) break;
       if (un != u) bi = a.bitems[un / NP];
       u = un;
       j = jn;
@@ -675,7 +711,8 @@ __global__ void __launch_bounds__(kTcRowThreads, 1) k_big_rows_tc(BigArgs a)
 
 constexpr size_t big_rows_tc_smem()
 {
-   return (size_t)TC_OPND_BYTES + TC_BMAT_BYTES + sizeof(float2) * (4096 + 2 * (4096 + 4096 / 16));
+   // operand, DFT16 matrix, W_4096 table, two padded row spectra, two staged rows
+   return (size_t)TC_OPND_BYTES + TC_BMAT_BYTES + sizeof(float2) * (4096 + 2 * (4096 + 4096 / 16) + 2 * 4096);
 }
 
 // The tensor-core row pass of a split, or null where rows are not 4096 points.
