@@ -45,7 +45,8 @@ int load_ini(Settings &s, const std::string &inifile, std::string &err)
       return -1;
    }
    if (!ini.getKeyValue("BaseFilename2", s.basefilename2_pattern)) {
-      std::cerr << "Warning: No BaseFilename2 specified in INI, will use 'BaseFilename1_file2'" << std::endl;
+      std::cerr << "Note: the INI has no BaseFilename2; the second input's files are named after "
+                   "BaseFilename1 with '_file2' appended" << std::endl;
       s.basefilename2_pattern = s.basefilename1_pattern + "_file2";
    }
    // keys of the GPU core
@@ -137,8 +138,8 @@ int derive(Settings &s, int ninputs, std::string &err)
       return -1;
    }
    if (s.calc_Xpol && ninputs != 2) {
-      std::cerr << "Warning: only one of two input files provided, disabling cross-pol spectrum calculation."
-                << std::endl;
+      std::cerr << "Note: cross-polarisation needs two input files; one was given, so no cross spectrum "
+                   "is computed" << std::endl;
       s.calc_Xpol = false;
    }
    s.use_channel_file1--;
@@ -166,8 +167,8 @@ int derive(Settings &s, int ninputs, std::string &err)
       s.pcal_result_bytes = s.pcal_tonebins * 2 * sizeof(float);
       s.pcal_pulses_per_fft = (int)(s.fft_points / s.pcal_rotatorlen);
       if ((s.fft_points % s.pcal_rotatorlen) != 0) {
-         std::cerr << "Warning: disabling PCal extraction because " << s.pcal_rotatorlen
-                   << "-length vectors did not fit evenly into " << s.fft_points << " DFT points." << std::endl;
+         std::cerr << "Note: phase-cal extraction is off: the rotator period of " << s.pcal_rotatorlen
+                   << " samples does not divide the " << s.fft_points << "-point FFT" << std::endl;
          s.extract_PCal = false;
       }
    }
