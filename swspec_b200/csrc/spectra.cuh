@@ -282,6 +282,20 @@ __host__ __device__ constexpr int stage_slots()
    return (nb1 % SPW == 0) ? ST * ((((NW + ST - 1) / ST) + 3) / 4) * 4 : NW;
 }
 
+// Receive buffer of the cluster exchange, [p][hi][u]: one row of
+// rx_stride float2 per side.  The cluster stage's warp reads, for one p,
+// sides (u, hi) of 16 consecutive threads: u over 8 values, hi alternating;
+// rx_stride = 8 (mod 16) puts the hi row 16 banks away from the lo row, so
+// the 16 eight-byte reads of a wavefront hit distinct banks.  The
+// tensor-core forms keep the unpadded stride: their two CTAs per SM leave
+// no room for the 2 KB the padding costs at P = 16.
+template <int P, int Q, int PREC>
+__host__ __device__ constexpr int rx_stride()
+{
+   constexpr int UC = Q / (2 * P);
+   return PREC ? UC : UC + (24 - UC % 16) % 16;
+}
+
 // Shared memory layout of a plan: byte offsets of every region, used both
 // for the kernel's pointers and for the host-side launch size.
 template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
@@ -291,7 +305,7 @@ struct SmemLayout {
    static constexpr size_t bmat = buf + BUFB;                                   // DFT16 B operand
    static constexpr size_t w256 = bmat + (PREC ? TC_BMAT_BYTES : 0);            // W_256 table
    static constexpr size_t rbuf = w256 + (PREC ? 256 : 0) * 8;                  // receive [P][sides]
-   static constexpr size_t wsl = rbuf + (size_t)P * (Q / P) * 8;                // window slice (float)
+   static constexpr size_t wsl = rbuf + (size_t)P * 2 * rx_stride<P, Q, PREC>() * 8;  // window slice (float)
    static constexpr size_t tw2 = wsl + (size_t)Q * 4;                           // pass-2 twiddles
    static constexpr size_t tw3 = tw2 + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8;
    static constexpr size_t twc = tw3 + (size_t)nbases(R3) * R1 * R2 * 8;        // pass-3 bases
@@ -319,6 +333,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    constexpr uint32_t MASK = (NBIT >= 32) ? 0xffffffffu : ((1u << NBIT) - 1u);
    constexpr int UC = Q / (2 * P);          // k1-pairs per CTA
    constexpr int SIDES = 2 * UC;            // lo/hi sides per CTA
+   constexpr int RX = rx_stride<P, Q, PREC>();  // receive row stride (float2)
    constexpr int SPT = (SIDES + T - 1) / T; // sides per thread
    constexpr int HB = (P == 1) ? 1 : P / 2; // bins per side (regular)
    constexpr int NB = HB + 1;               // + the lo special's extra bin
@@ -604,7 +619,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       // every receiver's bounded wait for it runs out
       const bool send = !(a.drop_last_exchange && !job_valid(nxt));
       __syncthreads();  // this job's pass-1 output is visible
-      // push F_rank[k1] to the CTA that owns pair min(k1, Q-k1); receive layout [p][hi][u]
+      // push F_rank[k1] to the CTA that owns pair min(k1, Q-k1); receive layout
+      // [p][hi][u], rows of RX float2
       auto push = [&](int k1, float2 val) {
          int u, hi;
          if (k1 == 0) { u = 0; hi = 0; }
@@ -612,8 +628,8 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          else if (2 * k1 < Q) { u = k1; hi = 0; }
          else { u = Q - k1; hi = 1; }
          const int owner = u / UC;
-         const int slot = hi * UC + (u - owner * UC);
-         dsmem_st2_async(rbase[owner] + 8u * (uint32_t)(rank * SIDES + slot), val, rbar[owner]);
+         const int slot = hi * RX + (u - owner * UC);
+         dsmem_st2_async(rbase[owner] + 8u * (uint32_t)(rank * 2 * RX + slot), val, rbar[owner]);
       };
       if constexpr (PREC == 0) {
          // ---- pass 2 in shared memory, pass 3 into registers ----
@@ -630,12 +646,12 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
             const int j = tid + b * T;
             if ((nb3 % T == 0 || j < nb3) && send) {
                if constexpr (FASTPUSH) {
-                  const uint32_t self = 8u * (uint32_t)(rank * SIDES);
+                  const uint32_t self = 8u * (uint32_t)(rank * 2 * RX);
 #pragma unroll
                   for (int r = 0; r < R3; r++) {
                      const int k1 = j + r * NS3;
                      const int uu = (r < R3 / 2) ? k1 : ((Q - k1) & (Q / 2 - 1));
-                     const int slot = ((r < R3 / 2) ? 0 : UC) + (uu & (UC - 1));
+                     const int slot = ((r < R3 / 2) ? 0 : RX) + (uu & (UC - 1));
                      dsmem_st2_async(rbase[uu / UC] + self + 8u * (uint32_t)slot, v3[b][r], rbar[uu / UC]);
                   }
                } else {
@@ -734,7 +750,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          float2 z[P];
          if (active) {
 #pragma unroll
-            for (int p = 0; p < P; p++) z[p] = rbuf[p * SIDES + (hi ? UC : 0) + (s >> 1)];
+            for (int p = 0; p < P; p++) z[p] = rbuf[p * 2 * RX + (hi ? RX : 0) + (s >> 1)];
             if (u == 0) {
                // lo: k1 = 0 (no twiddle); hi: k1 = Q/2, W_N^{p Q/2} = W_{2P}^p
                if (hi) {
