@@ -286,14 +286,12 @@ __host__ __device__ constexpr int stage_slots()
 // rx_stride float2 per side.  The cluster stage's warp reads, for one p,
 // sides (u, hi) of 16 consecutive threads: u over 8 values, hi alternating;
 // rx_stride = 8 (mod 16) puts the hi row 16 banks away from the lo row, so
-// the 16 eight-byte reads of a wavefront hit distinct banks.  The
-// tensor-core forms keep the unpadded stride: their two CTAs per SM leave
-// no room for the 2 KB the padding costs at P = 16.
+// the 16 eight-byte reads of a wavefront hit distinct banks.
 template <int P, int Q, int PREC>
 __host__ __device__ constexpr int rx_stride()
 {
    constexpr int UC = Q / (2 * P);
-   return PREC ? UC : UC + (24 - UC % 16) % 16;
+   return UC + (24 - UC % 16) % 16;
 }
 
 // Shared memory layout of a plan: byte offsets of every region, used both
@@ -303,8 +301,7 @@ struct SmemLayout {
    static constexpr size_t BUFB = PREC ? (size_t)TC_OPND_BYTES : (size_t)(Q + Q / 16) * 8;
    static constexpr size_t buf = 0;                                             // FFT buffer / operand
    static constexpr size_t bmat = buf + BUFB;                                   // DFT16 B operand
-   static constexpr size_t w256 = bmat + (PREC ? TC_BMAT_BYTES : 0);            // W_256 table
-   static constexpr size_t rbuf = w256 + (PREC ? 256 : 0) * 8;                  // receive [P][sides]
+   static constexpr size_t rbuf = bmat + (PREC ? TC_BMAT_BYTES : 0);            // receive [P][hi][u]
    static constexpr size_t wsl = rbuf + (size_t)P * 2 * rx_stride<P, Q, PREC>() * 8;  // window slice (float)
    static constexpr size_t tw2 = wsl + (size_t)Q * 4;                           // pass-2 twiddles
    static constexpr size_t tw3 = tw2 + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8;
@@ -355,7 +352,6 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    using L = SmemLayout<P, Q, R1, R2, R3, NBIT, PREC>;
    char *smem = reinterpret_cast<char *>(smem_raw);
    float2 *buf = reinterpret_cast<float2 *>(smem + L::buf);
-   float2 *w256 = reinterpret_cast<float2 *>(smem + L::w256);
    float2 *rbuf = reinterpret_cast<float2 *>(smem + L::rbuf);
    float *wsl = reinterpret_cast<float *>(smem + L::wsl);
    float2 *tw2 = reinterpret_cast<float2 *>(smem + L::tw2);
@@ -380,7 +376,6 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
    __shared__ __align__(8) unsigned long long mma_bar;
    const uint32_t mma_bar_addr = (uint32_t)__cvta_generic_to_shared(&mma_bar);
    if constexpr (PREC >= 1) {
-      for (int i = tid; i < 256; i += T) w256[i] = __ldg(a.twQ + 16 * i);  // W_256^i = W_4096^{16 i}
       fill_dft16_bmat(bmat_addr, T);
       tc::fence_async_smem();
       if (tid < 32) tc::tmem_alloc((uint32_t)__cvta_generic_to_shared(&tmem_holder), TC_TMEM_COLS);
@@ -706,7 +701,14 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
          {
             const int q0 = (tid >> 3) & 15;
 #pragma unroll
-            for (int k1 = 1; k1 < 16; k1++) y[k1] = cmul(y[k1], w256[(q0 * k1) & 255]);
+            for (int k1 = 1; k1 < 16; k1++) {
+               // W_256^m = W_4096^(16 m): the last pass's base table holds
+               // W_4096^(8 k), k < 256, so W_256^m = +-tw3[768 + 2 (m mod 128)]
+               const int m = (q0 * k1) & 255;
+               float2 w = tw3[3 * NS3 + 2 * (m & 127)];
+               if (m & 128) w = make_float2(-w.x, -w.y);
+               y[k1] = cmul(y[k1], w);
+            }
             store_mn16(opnd_addr, k0, 16 + k0, q0, y);
             handoff();
          }
