@@ -161,6 +161,24 @@ struct SchedEntry {
    }
 };
 
+// Device buffers of one pipeline launch: frame validity, decoded codes,
+// blank bitmap and per-item partial spectra.  The submit path keeps two
+// sets, so that consecutive chunks run on two streams and one chunk's
+// unpack and FFT fill the SMs that the previous chunk's last wave leaves.
+struct Scratch {
+   DevBuf d_valid[SWSGPU_MAX_STREAMS];
+   DevBuf d_codes, d_codes1, d_blank, d_blank_any, d_partial;
+   void release()
+   {
+      for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) d_valid[s].release();
+      d_codes.release();
+      d_codes1.release();
+      d_blank.release();
+      d_blank_any.release();
+      d_partial.release();
+   }
+};
+
 struct swsgpu_handle {
    swsgpu_config cfg;
    int device = 0;
@@ -179,6 +197,9 @@ struct swsgpu_handle {
    std::string err;
    cudaStream_t stream = nullptr;     // kernels and result copies
    cudaStream_t cstream = nullptr;    // input copies of submit()
+   cudaStream_t stream2 = nullptr;    // chunks of input region 1 (cluster path)
+   cudaEvent_t acc_done = nullptr;    // the last chunk's sums and phase-cal folds added
+   bool acc_pending = false;          // acc_done recorded since `stream` last waited on it
    cudaEvent_t done = nullptr;        // results of the last submitted run copied back
    // two device input slots per stream: run r+1's copy overlaps run r's kernels
    DevBuf d_slot[2][SWSGPU_MAX_STREAMS];
@@ -192,7 +213,10 @@ struct swsgpu_handle {
    // cluster kernel's CTAs idle at the end of each launch
    DevBuf d_region[2][SWSGPU_MAX_STREAMS];
    cudaEvent_t region_free[2] = {nullptr, nullptr};
-   int chunk_max = 1, chunk_n = 0, chunk_region = 0;
+   // chunk_target: size of the open chunk, chosen when its first run
+   // arrives; the last chunks of a group shrink so that little compute is
+   // left once the group's last copy lands
+   int chunk_max = 1, chunk_n = 0, chunk_region = 0, chunk_target = 1;
    bool chunk_group_first = false;
    size_t chunk_run_bytes = 0;
    long long chunk_off0[SWSGPU_MAX_STREAMS] = {0, 0};
@@ -211,9 +235,11 @@ struct swsgpu_handle {
    DevBuf d_scratch, d_bjobs, d_bitems;             // four-step intermediate and job lists
    DevBuf d_status;                                 // kernel status word (1: a bounded wait gave up)
    // per-call buffers
-   DevBuf d_raw[SWSGPU_MAX_STREAMS], d_valid[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
-   DevBuf d_codes, d_blank, d_blank_any, d_items, d_entries, d_outs, d_partial;
-   DevBuf d_codes1;   // undecimated copy for phase-cal when the four-step path uses the column layout
+   DevBuf d_raw[SWSGPU_MAX_STREAMS], d_chans[SWSGPU_MAX_STREAMS];
+   DevBuf d_items, d_entries, d_outs;
+   // launch buffers: set 0 on `stream`, set 1 on `stream2` (d_codes1 is the
+   // undecimated copy for phase-cal when the four-step path uses the column layout)
+   Scratch scr[2];
    DevBuf d_pcal_jobs, d_pcal_part, d_pcal_entries, d_pcal_outs;
    DevBuf d_out_auto, d_out_xpol, d_out_pcal, d_out_tones;
    HostBuf h_out;   // pinned staging of one run's outputs
@@ -583,7 +609,7 @@ static void big_batches(const swsgpu_handle *h, const Schedule &sc, std::vector<
 }
 
 static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_words, long long wpp, bool col,
-                      long long blank_words,
+                      long long blank_words, Scratch &x,
                       cudaStream_t st, int &launches)
 {
    const swsgpu_config &c = h->cfg;
@@ -595,13 +621,13 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    for (const int4 &b : se.batches) max_jobs = std::max(max_jobs, b.y);
    CK(h, h->d_scratch.ensure(job_bytes * (size_t)max_jobs));
    BigArgs a;
-   a.codes = (const uint32_t *)h->d_codes.p;
+   a.codes = (const uint32_t *)x.d_codes.p;
    a.code_words = code_words;
    a.wpp = wpp;
    a.col_layout = col ? 1 : 0;
-   a.blank = (const uint32_t *)h->d_blank.p;
+   a.blank = (const uint32_t *)x.d_blank.p;
    a.blank_words = blank_words;
-   a.blank_any = (const int *)h->d_blank_any.p;
+   a.blank_any = (const int *)x.d_blank_any.p;
    a.code_stream = (const int *)h->d_code_stream.p;
    a.window = (const float *)h->d_window.p;
    a.tw1 = (const float2 *)h->d_tw1.p + h->tw_off[h->cand].x;
@@ -609,7 +635,7 @@ static int launch_big(swsgpu_handle *h, const SchedEntry &se, long long code_wor
    a.twA = (const double2 *)h->d_twA.p;
    a.twB = (const double2 *)h->d_twB.p;
    a.scratch = (float2 *)h->d_scratch.p;
-   a.partial = (float *)h->d_partial.p;
+   a.partial = (float *)x.d_partial.p;
    a.N = c.fft_points;
    a.S = h->S;
    a.levels = level_table(c.layout[0].format, nbit);
@@ -772,9 +798,16 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
                         const long long *grid_off, size_t run_bytes, int nruns,
                         int runs_per_output, float *d_auto, float *d_xpol, float *d_pcal,
                         cudaStream_t st, int *nspec_out, int acc_mode = 0, int pcal_zero = 1,
-                        int pcal_write = 1, double *d_tones = nullptr)
+                        int pcal_write = 1, double *d_tones = nullptr, int set = 0,
+                        cudaEvent_t after_k1 = nullptr, cudaEvent_t acc_wait = nullptr,
+                        cudaEvent_t acc_rec = nullptr)
 {
+   // set: the scratch set (and so the stream) of this launch; after_k1:
+   // recorded once K1 has read the raw bytes; acc_wait / acc_rec: ordering
+   // of the reduction and phase-cal folds, which add into sums shared with
+   // the chunks of the other stream
    const swsgpu_config &c = h->cfg;
+   Scratch &x = h->scr[set];
    SchedEntry *se = nullptr;
    {
       int rc = get_schedule(h, run_bytes, nruns, runs_per_output, d_auto, d_xpol, d_pcal, acc_mode, &se);
@@ -801,13 +834,13 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
    const bool pcal_copy = col && c.extract_pcal && d_pcal && !sc.pcal_jobs.empty();
    const long long wpp1 = (nsamp + spw - 1) / spw + 2;
 
-   CK(h, h->d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 64));
-   if (pcal_copy) CK(h, h->d_codes1.ensure(sizeof(uint32_t) * (size_t)wpp1 * ncode + 64));
-   CK(h, h->d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
-   CK(h, h->d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
+   CK(h, x.d_codes.ensure(sizeof(uint32_t) * (size_t)code_words * ncode + 64));
+   if (pcal_copy) CK(h, x.d_codes1.ensure(sizeof(uint32_t) * (size_t)wpp1 * ncode + 64));
+   CK(h, x.d_blank.ensure(sizeof(uint32_t) * (size_t)blank_words * c.num_streams + 16));
+   CK(h, x.d_blank_any.ensure(sizeof(int) * SWSGPU_MAX_STREAMS));
    // the blank bitmap is written by K1 and read by K2/PCal only for streams
    // with a blanked frame (blank_any), so it needs no clearing
-   CK(h, cudaMemsetAsync(h->d_blank_any.p, 0, sizeof(int) * SWSGPU_MAX_STREAMS, st));
+   CK(h, cudaMemsetAsync(x.d_blank_any.p, 0, sizeof(int) * SWSGPU_MAX_STREAMS, st));
 
    // K1 per stream
    for (int s = 0; s < c.num_streams; s++) {
@@ -825,40 +858,41 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       si.msb2 = is_msb2(L);
       const long long last_v = si.grid_offset + ((nsamp * (long long)L.nchan * L.nbit - 1) >> 3);
       si.nframes = last_v / si.payload_bytes + 1;
-      CK(h, h->d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes));
+      CK(h, x.d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes));
       k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(
-          si, (int2 *)h->d_valid[s].p, (int *)h->d_blank_any.p + s);
+          si, (int2 *)x.d_valid[s].p, (int *)x.d_blank_any.p + s);
       launches++;
       const std::vector<int> &chans = h->chans_of[s];
       if (chans.empty()) continue;
-      uint32_t *codes = (uint32_t *)h->d_codes.p + (size_t)h->first_code[s] * code_words;
-      uint32_t *blank = (uint32_t *)h->d_blank.p + (size_t)s * blank_words;
+      uint32_t *codes = (uint32_t *)x.d_codes.p + (size_t)h->first_code[s] * code_words;
+      uint32_t *blank = (uint32_t *)x.d_blank.p + (size_t)s * blank_words;
       CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(), codes, D, wpp,
-                                (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank, launches));
+                                (const int2 *)x.d_valid[s].p, (const int *)x.d_blank_any.p + s, blank, launches));
       if (pcal_copy)
          CK(h, launch_unpack_codes(st, si, nsamp, (const int *)h->d_chans[s].p, (int)chans.size(),
-                                   (uint32_t *)h->d_codes1.p + (size_t)h->first_code[s] * wpp1, 1, wpp1,
-                                   (const int2 *)h->d_valid[s].p, (const int *)h->d_blank_any.p + s, blank,
+                                   (uint32_t *)x.d_codes1.p + (size_t)h->first_code[s] * wpp1, 1, wpp1,
+                                   (const int2 *)x.d_valid[s].p, (const int *)x.d_blank_any.p + s, blank,
                                    launches));
    }
    CK(h, cudaGetLastError());
+   if (after_k1) CK(h, cudaEventRecord(after_k1, st));
 
    // K2
    const int nitems = (int)sc.items.size();
    if (nitems > 0) {
-      CK(h, h->d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
+      CK(h, x.d_partial.ensure(sizeof(float) * 4 * (size_t)S * nitems));
       if (h->big) {
-         int rc = launch_big(h, *se, code_words, wpp, col, blank_words, st, launches);
+         int rc = launch_big(h, *se, code_words, wpp, col, blank_words, x, st, launches);
          if (rc != SWSGPU_OK) return rc;
       } else {
          SpecArgs a;
-         a.codes = (const uint32_t *)h->d_codes.p;
+         a.codes = (const uint32_t *)x.d_codes.p;
          a.code_words = code_words;
          a.wpp = wpp;
          a.D = D;
-         a.blank = (const uint32_t *)h->d_blank.p;
+         a.blank = (const uint32_t *)x.d_blank.p;
          a.blank_words = blank_words;
-         a.blank_any = (const int *)h->d_blank_any.p;
+         a.blank_any = (const int *)x.d_blank_any.p;
          a.code_stream = (const int *)h->d_code_stream.p;
          a.items = (const Item *)se->d_items.p;
          a.nitems = nitems;
@@ -866,7 +900,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          a.window = (const float *)h->d_window.p;
          a.twQ = (const float2 *)h->d_twQ.p;
          a.twN = (const float2 *)h->d_twN.p;
-         a.partial = (float *)h->d_partial.p;
+         a.partial = (float *)x.d_partial.p;
          a.N = c.fft_points;
          a.S = S;
          a.levels = level_table(c.layout[0].format, nbit);
@@ -898,12 +932,14 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          }
          launches++;
       }
-
+   }
+   if (acc_wait) CK(h, cudaStreamWaitEvent(st, acc_wait, 0));
+   if (nitems > 0) {
       // K3
       const int nouts = (int)sc.outs.size();
       if (nouts > 0) {
          dim3 grid((S + 255) / 256, nouts);
-         k_reduce<<<grid, 256, 0, st>>>((const float *)h->d_partial.p, S,
+         k_reduce<<<grid, 256, 0, st>>>((const float *)x.d_partial.p, S,
                                          (const RedEntry *)se->d_entries.p, (const OutVec *)se->d_outs.p);
          launches++;
       }
@@ -922,13 +958,13 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          CK(h, h->d_pcal_part.ensure(sizeof(double) * (2 * c.pcal_tonebins + 1) * (size_t)nout));
          int njobs = (int)sc.pcal_jobs.size();
          PcalArgs pa;
-         pa.codes = (const uint32_t *)(pcal_copy ? h->d_codes1.p : h->d_codes.p);
+         pa.codes = (const uint32_t *)(pcal_copy ? x.d_codes1.p : x.d_codes.p);
          pa.code_words = pcal_copy ? wpp1 : code_words;
          pa.wpp = pcal_copy ? wpp1 : wpp;
          pa.D = pcal_copy ? 1 : D;
-         pa.blank = (const uint32_t *)h->d_blank.p;
+         pa.blank = (const uint32_t *)x.d_blank.p;
          pa.blank_words = blank_words;
-         pa.blank_any = (const int *)h->d_blank_any.p;
+         pa.blank_any = (const int *)x.d_blank_any.p;
          pa.code_stream = (const int *)h->d_code_stream.p;
          pa.jobs = (const PcalJob *)se->d_pcal_jobs.p;
          pa.njobs = njobs;
@@ -951,6 +987,7 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          launches += 2;
       }
    }
+   if (acc_rec) CK(h, cudaEventRecord(acc_rec, st));
    CK(h, cudaGetLastError());
    h->last_launches = launches;
    return SWSGPU_OK;
@@ -963,6 +1000,17 @@ static void drop_prof_events(swsgpu_handle *h)
       cudaEventDestroy(pr.second);
    }
    h->prof_events.clear();
+}
+
+// Makes `stream` wait for every chunk launched so far (the last chunk's
+// sums were added after all earlier chunks' sums).
+static int join_chunks(swsgpu_handle *h)
+{
+   if (h->acc_pending) {
+      CK(h, cudaStreamWaitEvent(h->stream, h->acc_done, 0));
+      h->acc_pending = false;
+   }
+   return SWSGPU_OK;
 }
 
 // Launches the open chunk of collected runs as one multi-run chunk whose
@@ -983,14 +1031,21 @@ static int flush_chunk(swsgpu_handle *h, bool group_end, int *nspec)
    }
    const bool first = h->chunk_group_first;
    const int acc_mode = group_end ? (first ? 0 : 3) : (first ? 1 : 2);
-   CK(h, cudaStreamWaitEvent(h->stream, h->last_h2d, 0));
+   // cluster path: region 1's chunks run on the second stream with the
+   // second scratch set; the four-step path shares its intermediate buffer
+   // between launches and keeps one stream
+   const int set = (!h->big && h->stream2 && region == 1) ? 1 : 0;
+   cudaStream_t st = set ? h->stream2 : h->stream;
+   CK(h, cudaStreamWaitEvent(st, h->last_h2d, 0));
+   // the region is free for the next copies once K1 has decoded it
    const int rc = launch_chunk(h, d_raw, raw_bytes, grid_off, h->chunk_run_bytes, h->chunk_n, h->chunk_n,
                                (float *)h->d_out_auto.p, c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
-                               c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, nspec, acc_mode,
+                               c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, st, nspec, acc_mode,
                                first ? 1 : 0, group_end ? 1 : 0,
-                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
+                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr, set,
+                               h->region_free[region], h->acc_done, h->acc_done);
    if (rc) return rc;
-   CK(h, cudaEventRecord(h->region_free[region], h->stream));
+   h->acc_pending = true;
    h->chunk_region ^= 1;
    h->chunk_n = 0;
    h->chunk_group_first = false;
@@ -1185,6 +1240,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    h->chunk_max = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(1, cfg->runs_per_output),
                                                             ((size_t)32 << 20) / std::max<size_t>(1, cfg->max_run_bytes)));
    if (!ev_ok || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->acc_done, cudaEventDisableTiming) != cudaSuccess ||
        cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming) != cudaSuccess) {
       h->err = "stream/event creation failed";
       return bail(SWSGPU_ECUDA);
@@ -1352,13 +1409,14 @@ void swsgpu_destroy(swsgpu_handle *h)
    if (!h) return;
    cudaSetDevice(h->device);
    if (h->stream) cudaStreamSynchronize(h->stream);
-   DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_codes, &h->d_codes1,
-                     &h->d_blank, &h->d_blank_any, &h->d_items, &h->d_entries, &h->d_outs,
-                     &h->d_partial, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
+   if (h->stream2) cudaStreamSynchronize(h->stream2);
+   DevBuf *bufs[] = {&h->d_window, &h->d_twQ, &h->d_twN, &h->d_code_stream, &h->d_items, &h->d_entries,
+                     &h->d_outs, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
                      &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal, &h->d_out_tones,
                      &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs, &h->d_status,
                      &h->d_bitems};
    for (DevBuf *b : bufs) b->release();
+   for (Scratch &x : h->scr) x.release();
    drop_schedules(h);
    if (h->cstream) cudaStreamSynchronize(h->cstream);
    for (int k = 0; k < 2; k++) {
@@ -1370,14 +1428,15 @@ void swsgpu_destroy(swsgpu_handle *h)
    }
    for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) {
       h->d_raw[s].release();
-      h->d_valid[s].release();
       h->d_chans[s].release();
    }
    h->h_out.release();
    h->d_acc64.release();
    drop_prof_events(h);
    if (h->done) cudaEventDestroy(h->done);
+   if (h->acc_done) cudaEventDestroy(h->acc_done);
    if (h->stream) cudaStreamDestroy(h->stream);
+   if (h->stream2) cudaStreamDestroy(h->stream2);
    if (h->cstream) cudaStreamDestroy(h->cstream);
    delete h;
 }
@@ -1476,6 +1535,11 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
          for (int s = 0; s < c.num_streams; s++) h->chunk_off0[s] = offs[s];
          h->chunk_run_bytes = nbytes[0];
          h->chunk_group_first = h->group_pos == 0;
+         // R runs left in the group: full chunks while R > 2 chunk_max,
+         // then about half of what is left (8, 8, ..., 6, 3, 2, 1, 1)
+         const int left = rpo - h->group_pos;
+         h->chunk_target = left > 2 * h->chunk_max ? h->chunk_max
+                                                   : std::max(1, std::min(h->chunk_max, left / 2));
       }
       for (int s = 0; s < c.num_streams; s++)
          CK(h, cudaMemcpyAsync((char *)h->d_region[region][s].p + (size_t)h->chunk_n * h->chunk_run_bytes, raw[s],
@@ -1486,7 +1550,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       h->next_slot ^= 1;
       h->chunk_n++;
       h->group_pos = group_end ? 0 : h->group_pos + 1;
-      if (h->chunk_n == h->chunk_max || group_end) {
+      if (h->chunk_n >= h->chunk_target || group_end) {
          const int rc = flush_chunk(h, group_end, &nspec);
          if (rc) return rc;
       } else {
@@ -1494,6 +1558,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       }
    } else {
       // one run per launch through the two input slots
+      if (int rc = join_chunks(h)) return rc;
       const int slot = h->next_slot;
       CK(h, cudaStreamWaitEvent(h->cstream, h->slot_free[slot], 0));
       const void *d_raw[SWSGPU_MAX_STREAMS];
@@ -1512,7 +1577,8 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
                                c.num_xpols ? (float *)h->d_out_xpol.p : nullptr,
                                c.extract_pcal ? (float *)h->d_out_pcal.p : nullptr, h->stream, &nspec,
                                acc_mode, pcal_zero, pcal_write,
-                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr);
+                               h->h_tones_bytes ? (double *)h->d_out_tones.p : nullptr, 0, nullptr,
+                               nullptr, h->acc_done);
          if (rc) return rc;
          if (rpo > 1) h->group_pos = group_end ? 0 : h->group_pos + 1;
       } else {
@@ -1522,6 +1588,7 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
    }
    h->fetch_ready = group_end;
    if (nsp > 0 && group_end) {
+      if (int rc = join_chunks(h)) return rc;
       char *hp = (char *)h->h_out.p;
       CK(h, cudaMemcpyAsync(hp, h->d_out_auto.p, h->h_auto_bytes, cudaMemcpyDeviceToHost, h->stream));
       if (h->h_xpol_bytes)
@@ -1585,6 +1652,7 @@ int swsgpu_sync(swsgpu_handle *h, void *cuda_stream)
    if (!h) return SWSGPU_EINVAL;
    CK(h, cudaSetDevice(h->device));
    CK(h, cudaStreamSynchronize(cuda_stream ? (cudaStream_t)cuda_stream : h->stream));
+   if (!cuda_stream && h->stream2) CK(h, cudaStreamSynchronize(h->stream2));
    if (h->d_status.p) {
       int st = 0;
       CK(h, cudaMemcpy(&st, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));

@@ -365,6 +365,55 @@ def test_group_runs_chunked_and_per_run(gpu):
     assert np.max(np.abs(a1 - a2) / a1) < 1e-6 and np.max(np.abs(a1 - a3) / a1) < 1e-6
 
 
+def test_group_chunks_alternate_streams(gpu):
+    """Two 10-run output groups of 8 MiB runs: the submit path collects 4
+    runs per device chunk (32 MiB), so each group is 3 chunks and
+    consecutive chunks run on alternating streams with their own scratch
+    buffers, their sums added in submission order.  Both groups' combined
+    spectra match the FP64 oracle, and a chunk's input region is refilled
+    only after its decode."""
+    N, cof, nrun = 4096, 512, 10
+    run = N * cof * 4                         # 16 channels x 2 bit: 4 bytes per sample-time
+    rng = np.random.default_rng(77)
+    pay = rng.integers(0, 256, size=2 * nrun * run, dtype=np.uint8)
+    w = pay.view(np.uint32)
+    w[w == 0x11223344] ^= 1                   # no mark5access fill words
+    S = N // 2 + 1
+    lay = gpu.layout("mark5b", 16, 2, framed=False)
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 3), (0, 12)), xpols=((0, 1),),
+                          max_run_bytes=run, samplingfreq=64e6, runs_per_output=nrun)
+    core = gpu.Core(cfg)
+    core.set_sizes([run])
+    outs = []
+    for g in range(2):
+        auto = np.zeros((1, 2, S), np.float32)
+        xp = np.zeros((1, 1, S, 2), np.float32)
+        for r in range(nrun):
+            off = (g * nrun + r) * run
+            core.submit([pay[off:off + run]], payload_offsets=[off])
+            assert core.wait() == (1 if r == nrun - 1 else 0)
+        core.fetch_into(auto, xp)
+        outs.append((auto[0], xp[0, 0, :, 0] + 1j * xp[0, 0, :, 1]))
+    core.close()
+    for g, (a, x) in enumerate(outs):
+        ra = np.zeros((2, S))
+        rx = np.zeros(S, complex)
+        for r in range(nrun):
+            off = (g * nrun + r) * run
+            s = [O_decode(pay[off:off + run].tobytes(), run // 4, c) for c in (3, 12)]
+            aa, xx, _, n = oracle_run(s, N, "hann", 1, cof, nxpols=1)
+            assert n == 1
+            ra += aa[0]
+            rx += xx[0, 0]
+        assert np.max(np.abs(a - ra) / ra) < REL_TOL, g
+        assert np.max(np.abs(x - rx) / np.sqrt(ra[0] * ra[1])) < REL_TOL, g
+
+
+def O_decode(buf: bytes, nsamp: int, chan: int):
+    import oracle as O
+    return O.decode(O.FMT_MARK5B, 16, 2, buf, nsamp, chan, payload_bytes=10000)
+
+
 @pytest.mark.parametrize("N,nbit,fmt,nchan", [(65536, 2, "mark5b", 16), (1 << 20, 8, "vdif:8000", 1)])
 def test_workspace_size_covers_allocations(gpu, N, nbit, fmt, nchan):
     """swsgpu_workspace_size predicts the device memory a first
