@@ -134,13 +134,15 @@ typedef struct swsgpu_config {
                                        tones (k * spacing + offset, k < ntones <= tonebins/2),
                                        the PCal library's tone output (src/IA-32/PhaseCal/
                                        PCal.cpp:654-678), computed in FP64 */
-   int autotune;                    /* 1: swsgpu_create times the candidate splits of a
-                                       four-step length and keeps the fastest (once per
-                                       length and bit depth per process; see swsgpu_autotune) */
+   int autotune;                    /* 1: swsgpu_create times the candidate plans of the
+                                       length -- four-step splits, or cluster plans (cluster
+                                       size, threads per CTA, radix order) -- and keeps the
+                                       fastest (once per length, bit depth and form per
+                                       process; see swsgpu_autotune) */
    int plan_family;                 /* SWSGPU_PLAN_*: which FFT path a length with both uses */
-   int plan_candidate;              /* four-step path: 0 = default split, k > 0 = the k-th
-                                       candidate (as the autotuner numbers them); ignored
-                                       when autotune is set */
+   int plan_candidate;              /* 0 = the default plan, k > 0 = the k-th candidate
+                                       split or cluster plan (as the autotuner numbers them);
+                                       ignored when autotune is set */
 } swsgpu_config;
 
 typedef struct swsgpu_handle swsgpu_handle;
@@ -222,10 +224,13 @@ int swsgpu_host_unregister(void *p);
  * plan per length): for a length on the four-step path, times every
  * candidate split N = N1 x N2 and columns-per-CTA width on a hash-filled run
  * with this core's sources, pairs and window (enough frames for about 16
- * pair FFTs), and keeps the one with the shortest of `iterations` (at most
- * 16) timed iterations; later cores of the same length and bit depth in this
- * process start with that choice.  Cluster lengths have one plan and return
- * at once.  Synchronous; call it with no run pending. */
+ * pair FFTs); for a cluster length, every cluster plan of the handle's form
+ * (cluster size, threads per CTA, radix order: 4096, 20000 and 131072 have
+ * several) on one hash-filled run of max_run_bytes (at most 64 MiB of
+ * payload).  Keeps the candidate with the shortest of `iterations` (at most
+ * 16) timed iterations; later cores of the same length, bit depth and form
+ * in this process start with that choice.  Synchronous; call it with no run
+ * pending. */
 int swsgpu_autotune(swsgpu_handle *h, int iterations);
 
 /* Text description of the plan a core uses (split, tile, candidate). */

@@ -1053,9 +1053,58 @@ static int flush_chunk(swsgpu_handle *h, bool group_end, int *nspec)
 }
 
 static int autotune_big(swsgpu_handle *h, int iters);
+static int autotune_cluster(swsgpu_handle *h, int iters);
+
+// Makes `pl` the handle's cluster plan: its per-CTA twiddle table W_Q, the
+// launch attributes of its kernel and the number of co-resident clusters
+// (the grid of every launch).  Kept schedules depend on the plan's cluster
+// size and grid, so they are dropped.
+static int set_cluster_plan(swsgpu_handle *h, const Plan &pl)
+{
+   const swsgpu_config &c = h->cfg;
+   const int nbit = c.layout[0].nbit;
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   const SpecKernel kern = plan_kernel(pl, c.precision, nbi);
+   if (!kern) return fail(h, SWSGPU_EINVAL, "the plan has no kernel of this form");
+   const size_t smem = plan_smem(pl, c.precision, nbi);
+   std::vector<float2> twQ;
+   make_twiddles(pl.Q, pl.Q, twQ);
+   CK(h, cudaStreamSynchronize(h->stream));
+   CK(h, h->d_twQ.ensure(sizeof(float2) * twQ.size()));
+   CK(h, cudaMemcpy(h->d_twQ.p, twQ.data(), sizeof(float2) * twQ.size(), cudaMemcpyHostToDevice));
+   CK(h, cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+   if (pl.P > 8) CK(h, cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+   cudaLaunchConfig_t cfgl = {};
+   cfgl.gridDim = dim3(pl.P);
+   cfgl.blockDim = dim3(pl.T);
+   cfgl.dynamicSmemBytes = smem;
+   cudaLaunchAttribute attr[2];
+   cfgl.numAttrs = cluster_attrs(attr, pl.P, c.precision);
+   cfgl.attrs = attr;
+   // The occupancy query reports one resident CTA per SM for any kernel
+   // that allocates tensor memory, whatever its footprint; two 113 KB
+   // tensor-core CTAs (128 TMEM columns each, 512 per SM) do co-reside,
+   // and a grid sized for one CTA per SM runs at 0.69x the speed of one
+   // sized for two.  So the grid of a tensor-core form is sized by the
+   // FP32 form's kernel of the same plan (same threads and register cap)
+   // at the tensor-core form's shared-memory footprint.
+   const void *occ_kern = (const void *)kern;
+   if (c.precision != SWSGPU_PREC_FP32) {
+      occ_kern = (const void *)pl.kern[nbi];
+      CK(h, cudaFuncSetAttribute(occ_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      if (pl.P > 8) CK(h, cudaFuncSetAttribute(occ_kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+   }
+   int ncl = 0;
+   CK(h, cudaOccupancyMaxActiveClusters(&ncl, occ_kern, &cfgl));
+   if (ncl < 1) return fail(h, SWSGPU_ECUDA, "cluster configuration does not fit on this device");
+   h->max_clusters = ncl;
+   h->plan = pl;
+   drop_schedules(h);
+   return SWSGPU_OK;
+}
 static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp);
 static std::mutex &tune_mutex();
-static int tuned_choice(int N, int nbit, bool tc);
+static int tuned_choice(int N, int nbit, bool tc, bool big);
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -1248,11 +1297,8 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    }
    std::vector<float> win;
    make_window(cfg->window, cfg->fft_points, win);
-   std::vector<float2> twQ, twN;
-   if (!h->big) {
-      make_twiddles(plan.Q, plan.Q, twQ);
-      make_twiddles(cfg->fft_points, cfg->fft_points / 2 + 1, twN);
-   }
+   std::vector<float2> twN;
+   if (!h->big) make_twiddles(cfg->fft_points, cfg->fft_points / 2 + 1, twN);
 #define CKB(call)                                                                                  \
    do {                                                                                           \
       cudaError_t e_ = (call);                                                                    \
@@ -1264,8 +1310,6 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    CKB(h->d_window.ensure(sizeof(float) * win.size()));
    CKB(cudaMemcpy(h->d_window.p, win.data(), sizeof(float) * win.size(), cudaMemcpyHostToDevice));
    if (!h->big) {
-      CKB(h->d_twQ.ensure(sizeof(float2) * twQ.size()));
-      CKB(cudaMemcpy(h->d_twQ.p, twQ.data(), sizeof(float2) * twQ.size(), cudaMemcpyHostToDevice));
       CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
       CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
    } else {
@@ -1324,7 +1368,7 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
          h->big_cands = big_plan_candidates(cfg->fft_points, cand, 16);
          // a split tuned earlier in this process for the same length, bits and form
          const bool tc = cfg->precision != SWSGPU_PREC_FP32;
-         const int t = tuned_choice(cfg->fft_points, nbit, tc);
+         const int t = tuned_choice(cfg->fft_points, nbit, tc, true);
          if (tc) {
             // the tensor-core form runs only splits with 4096-point rows
             for (int k = 0; k < h->big_cands; k++)
@@ -1362,44 +1406,42 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
       *out = h;
       return SWSGPU_OK;
    }
-   SpecKernel kern = plan_kernel(plan, cfg->precision, nbi);
-   const size_t smem = plan_smem(plan, cfg->precision, nbi);
-   CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-   if (plan.P > 8)
-      CKB(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
    {
-      cudaLaunchConfig_t cfgl = {};
-      cfgl.gridDim = dim3(plan.P);
-      cfgl.blockDim = dim3(plan.T);
-      cfgl.dynamicSmemBytes = smem;
-      cudaLaunchAttribute attr[2];
-      cfgl.numAttrs = cluster_attrs(attr, plan.P, cfg->precision);
-      cfgl.attrs = attr;
-      // The occupancy query reports one resident CTA per SM for any kernel
-      // that allocates tensor memory, whatever its footprint; two 113 KB
-      // tensor-core CTAs (128 TMEM columns each, 512 per SM) do co-reside,
-      // and a grid sized for one CTA per SM runs at 0.69x the speed of one
-      // sized for two.  So the grid of a tensor-core form is sized by the
-      // FP32 form's kernel of the same plan (same threads and register cap)
-      // at the tensor-core form's shared-memory footprint.
-      const void *occ_kern = (const void *)kern;
-      if (cfg->precision != SWSGPU_PREC_FP32) {
-         occ_kern = (const void *)plan.kern[nbi];
-         CKB(cudaFuncSetAttribute(occ_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-         if (plan.P > 8) CKB(cudaFuncSetAttribute(occ_kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      // the default plan, a candidate asked for, or the one the autotuner
+      // chose earlier in this process for this length, bit depth and form
+      Plan cand[8];
+      const int nc = plan_candidates(cfg->fft_points, cand, 8);
+      const bool tc = cfg->precision != SWSGPU_PREC_FP32;
+      int pick = 0;
+      if (cfg->plan_candidate > 0 && !cfg->autotune) {
+         if (cfg->plan_candidate >= nc) {
+            h->err = "plan_candidate beyond the candidates of this length";
+            return bail(SWSGPU_EINVAL);
+         }
+         if (!plan_kernel(cand[cfg->plan_candidate], cfg->precision, nbi)) {
+            h->err = "plan_candidate has no kernel of this form";
+            return bail(SWSGPU_EINVAL);
+         }
+         pick = cfg->plan_candidate;
+      } else {
+         const int t = tuned_choice(cfg->fft_points, nbit, tc, false);
+         if (t >= 0 && t < nc && plan_kernel(cand[t], cfg->precision, nbi)) {
+            pick = t;
+            h->tuned = t;
+         }
       }
-      int ncl = 0;
-      CKB(cudaOccupancyMaxActiveClusters(&ncl, occ_kern, &cfgl));
-      if (ncl < 1) {
-         h->err = "cluster configuration does not fit on this device";
-         return bail(SWSGPU_ECUDA);
-      }
-      h->max_clusters = ncl;
+      h->cand = pick;
+      const int rc = set_cluster_plan(h, cand[pick]);
+      if (rc != SWSGPU_OK) return bail(rc);
    }
    // device buffers for submit()
    for (int k = 0; k < 2; k++)
       for (int s = 0; s < cfg->num_streams; s++) CKB(h->d_slot[k][s].ensure(cfg->max_run_bytes + (cfg->max_run_bytes / 8) + 1024 + 128));
 #undef CKB
+   if (cfg->autotune && h->tuned < 0) {
+      const int rc = autotune_cluster(h, 3);
+      if (rc != SWSGPU_OK) return bail(rc);
+   }
    *out = h;
    return SWSGPU_OK;
 }
@@ -1772,7 +1814,9 @@ __global__ void k_fill_hash(uint32_t *p, size_t n, uint32_t seed)
 }
 
 static std::mutex g_tune_mu;
-static std::map<std::pair<int, int>, int> g_tuned;  // (N, nbit + 100 for the tensor-core form) -> candidate
+static std::map<std::pair<int, int>, int> g_tuned;  // (N, tune_key) -> candidate
+// bit depth, + 100 for a tensor-core form, + 1000 for the four-step family
+static int tune_key(int nbit, bool tc, bool big) { return nbit + (tc ? 100 : 0) + (big ? 1000 : 0); }
 
 static cudaError_t set_big_attrs(const swsgpu_handle *h, const BigPlan &bp)
 {
@@ -1878,7 +1922,115 @@ static int autotune_big(swsgpu_handle *h, int iters)
    h->cand = best;
    CK(h, set_big_attrs(h, h->bplan));
    std::lock_guard<std::mutex> lk(g_tune_mu);
-   g_tuned[std::make_pair(c.fft_points, nbit + (c.precision != SWSGPU_PREC_FP32 ? 100 : 0))] = best;
+   g_tuned[std::make_pair(c.fft_points, tune_key(nbit, c.precision != SWSGPU_PREC_FP32, true))] = best;
+   return SWSGPU_OK;
+}
+
+// Times every cluster plan of the length that has a kernel of the handle's
+// form (cluster size, threads per CTA, radix order) on one run of
+// max_run_bytes of synthetic codes -- the job count the core's runs give --
+// and keeps the fastest single iteration.  The choice is remembered per
+// length, bit depth and form for the rest of the process.
+static int autotune_cluster(swsgpu_handle *h, int iters)
+{
+   const swsgpu_config &c = h->cfg;
+   Plan cand[8];
+   const int nc = plan_candidates(c.fft_points, cand, 8);
+   const int nbit = c.layout[0].nbit;
+   const int nbi = nbit == 1 ? 0 : nbit == 2 ? 1 : 2;
+   int nrun_ok = 0;
+   for (int k = 0; k < nc; k++) nrun_ok += plan_kernel(cand[k], c.precision, nbi) ? 1 : 0;
+   if (nrun_ok <= 1) return SWSGPU_OK;
+   const Plan keep = h->plan;
+   const int keep_cand = h->cand;
+   const int pb = payload_bytes(c.layout[0]);
+   // one run's samples (at least two FFTs per source), capped at 64 MiB of payload
+   size_t pay = std::min<size_t>(c.max_run_bytes, (size_t)64 << 20);
+   if (c.layout[0].header_bytes) pay = pay / c.layout[0].frame_bytes * (size_t)pb;
+   long long nsamp = samples_of(c.layout[0], pay);
+   nsamp = std::max<long long>(nsamp, 2LL * c.fft_points);
+   pay = (size_t)((nsamp * c.layout[0].nchan * nbit + 7) / 8);
+   pay = ((pay + pb - 1) / pb) * pb;
+   const RunShape rs = run_shape(c, samples_of(c.layout[0], pay));
+   const int nspec = std::max(rs.nspec, 1) + 1;
+   DevBuf raw[SWSGPU_MAX_STREAMS], oa, ox;
+   const void *d_raw[SWSGPU_MAX_STREAMS];
+   size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   long long grid_off[SWSGPU_MAX_STREAMS];
+   auto cleanup = [&]() {
+      cudaStreamSynchronize(h->stream);
+      for (auto &r : raw) r.release();
+      oa.release();
+      ox.release();
+      drop_schedules(h);
+   };
+   for (int s = 0; s < c.num_streams; s++) {
+      const swsgpu_layout &L = c.layout[s];
+      raw_bytes[s] = L.header_bytes ? (pay / pb) * (size_t)L.frame_bytes : pay;
+      grid_off[s] = 0;
+      if (raw[s].ensure(raw_bytes[s] + 64) != cudaSuccess) {
+         cleanup();
+         return fail(h, SWSGPU_ECUDA, "autotune: allocation failed");
+      }
+      const size_t nw = raw_bytes[s] / 4;
+      k_fill_hash<<<(unsigned)((nw + 255) / 256), 256, 0, h->stream>>>((uint32_t *)raw[s].p, nw, 1234u + s);
+      d_raw[s] = raw[s].p;
+   }
+   if (oa.ensure(sizeof(float) * (size_t)h->S * c.num_sources * nspec + 64) != cudaSuccess ||
+       ox.ensure(sizeof(float) * 2 * (size_t)h->S * std::max(c.num_xpols, 1) * nspec + 64) != cudaSuccess) {
+      cleanup();
+      return fail(h, SWSGPU_ECUDA, "autotune: allocation failed");
+   }
+   int best = -1;
+   float best_ms = 0.0f;
+   const int nit = std::max(1, std::min(iters, 16));
+   cudaEvent_t ev[17];
+   for (int i = 0; i <= nit; i++) cudaEventCreate(&ev[i]);
+   for (int k = 0; k < nc; k++) {
+      if (!plan_kernel(cand[k], c.precision, nbi)) continue;
+      if (set_cluster_plan(h, cand[k]) != SWSGPU_OK) {
+         cudaGetLastError();
+         continue;
+      }
+      h->cand = k;
+      int ns = 0, rc = SWSGPU_OK;
+      // one untimed iteration, then nit timed ones
+      for (int it = 0; it <= nit && rc == SWSGPU_OK; it++) {
+         if (it >= 1) cudaEventRecord(ev[it - 1], h->stream);
+         rc = launch_chunk(h, d_raw, raw_bytes, grid_off, pay, 1, 1, (float *)oa.p,
+                           c.num_xpols ? (float *)ox.p : nullptr, nullptr, h->stream, &ns);
+      }
+      cudaEventRecord(ev[nit], h->stream);
+      if (rc != SWSGPU_OK || cudaEventSynchronize(ev[nit]) != cudaSuccess) {
+         cudaGetLastError();
+         continue;
+      }
+      float ms = 0.0f;
+      for (int i = 0; i < nit; i++) {
+         float t = 0.0f;
+         cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+         if (i == 0 || t < ms) ms = t;
+      }
+      if (best < 0 || ms < best_ms) {
+         best = k;
+         best_ms = ms;
+      }
+   }
+   for (int i = 0; i <= nit; i++) cudaEventDestroy(ev[i]);
+   cleanup();
+   if (best < 0) {
+      set_cluster_plan(h, keep);
+      h->cand = keep_cand;
+      return fail(h, SWSGPU_ECUDA, "autotune: no candidate ran");
+   }
+   {
+      const int rc = set_cluster_plan(h, cand[best]);
+      if (rc != SWSGPU_OK) return rc;
+   }
+   h->tuned = best;
+   h->cand = best;
+   std::lock_guard<std::mutex> lk(g_tune_mu);
+   g_tuned[std::make_pair(c.fft_points, tune_key(nbit, c.precision != SWSGPU_PREC_FP32, false))] = best;
    return SWSGPU_OK;
 }
 
@@ -2046,8 +2198,7 @@ int swsgpu_autotune(swsgpu_handle *h, int iterations)
    if (!h || iterations < 1) return SWSGPU_EINVAL;
    CK(h, cudaSetDevice(h->device));
    if (h->pending) return fail(h, SWSGPU_ESTATE, "autotune while a run is pending");
-   if (!h->big) return SWSGPU_OK;  // one plan per cluster length
-   return autotune_big(h, iterations);
+   return h->big ? autotune_big(h, iterations) : autotune_cluster(h, iterations);
 }
 
 int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len)
@@ -2058,8 +2209,11 @@ int swsgpu_plan_info(const swsgpu_handle *h, char *buf, size_t len)
                h->bplan.C, h->cand, h->big_cands,
                h->tuned >= 0 ? " (tuned)" : (h->cand > 0 ? " (pinned)" : " (default)"));
    } else {
-      snprintf(buf, len, "cluster %d x %d (CTAs x points), radices %d/%d/%d, %s form", h->plan.P, h->plan.Q,
-               h->plan.R1, h->plan.R2, h->plan.R3,
+      Plan cand[8];
+      const int nc = plan_candidates(h->cfg.fft_points, cand, 8);
+      snprintf(buf, len, "cluster %d x %d (CTAs x points), %d threads, radices %d/%d/%d, candidate %d of %d%s, %s form",
+               h->plan.P, h->plan.Q, h->plan.T, h->plan.R1, h->plan.R2, h->plan.R3, h->cand, nc,
+               h->tuned >= 0 ? " (tuned)" : (h->cand > 0 ? " (pinned)" : " (default)"),
                h->cfg.precision == SWSGPU_PREC_TCSPLIT       ? "tensor-core split (tcgen05 levels 2-3)"
                : h->cfg.precision == SWSGPU_PREC_TCSPLIT_ALL ? "tensor-core split (tcgen05 levels 1-3)"
                                                              : "FP32");
@@ -2194,9 +2348,9 @@ void swsgpu_batch_destroy(swsgpu_batch *b)
 
 static std::mutex &tune_mutex() { return g_tune_mu; }
 
-static int tuned_choice(int N, int nbit, bool tc)
+static int tuned_choice(int N, int nbit, bool tc, bool big)
 {
    std::lock_guard<std::mutex> lk(tune_mutex());
-   auto it = g_tuned.find(std::make_pair(N, nbit + (tc ? 100 : 0)));
+   auto it = g_tuned.find(std::make_pair(N, tune_key(nbit, tc, big)));
    return it == g_tuned.end() ? -1 : it->second;
 }

@@ -18,7 +18,10 @@ struct Plan {
    size_t smem_tc2[3];
 };
 
-// Returns false when N has no single-launch plan.
+// Returns false when N has no single-launch plan; *out = the default plan.
 bool find_plan(int N, Plan *out);
+
+// Every plan of length N, the default first; returns how many (<= max).
+int plan_candidates(int N, Plan *out, int max);
 
 }  // namespace sws

@@ -113,6 +113,53 @@ def test_autotune_four_step(gpu):
     _check_auto(auto[0, 0], ra[0, 0], r32[0, 0])
     c2 = _core(gpu, s)
     assert c2.plan_info() == info
-    # a cluster length has one plan
+    # a cluster length with one plan keeps it
     c3 = _core(gpu, _spec(1, 65536, 2, 2))
-    assert "cluster" in c3.autotune()
+    assert "candidate 0 of 1" in c3.autotune()
+
+
+# cluster plans per length, as the autotuner numbers them
+CLUSTER_CANDIDATES = {4096: 3, 20000: 2, 131072: 2}
+
+
+@pytest.mark.parametrize("N,k", [(N, k) for N, n in CLUSTER_CANDIDATES.items() for k in range(n)])
+def test_every_cluster_candidate(gpu, N, k):
+    """Each cluster plan the autotuner may choose (cluster size, threads per
+    CTA, radix order), pinned through plan_candidate: 16 FFTs of a 2-bit
+    stream against the FP64 oracle at the 2e-6 bar in every bin."""
+    s = _spec(k, N, 2, 16)
+    lay = gpu.layout("vdif:8000", 1, 2, framed=False)
+    cfg = gpu.make_config(lay, N, "hann", 1, 16, max_run_bytes=s.run_bytes, samplingfreq=s.samplingfreq,
+                          plan_candidate=k)
+    c = gpu.Core(cfg)
+    info = c.plan_info()
+    assert f"candidate {k} of {CLUSTER_CANDIDATES[N]}" in info and "cluster" in info, info
+    pay = stream_payload(s)
+    auto, _, _, ns = c.run([pay])
+    x = O.decode(O.FMT_VDIF, 1, 2, pay, s.samples_per_run, 0, payload_bytes=8000)
+    ra, _, _, nref = oracle_run([x], N, "hann", 1, 16)
+    assert ns == nref == 1
+    assert np.max(np.abs(auto[0, 0] - ra[0, 0]) / ra[0, 0]) < REL_TOL, info
+    c.close()
+
+
+def test_autotune_cluster_plans(gpu):
+    """N = 4096, 2-bit: the three cluster plans are timed on one run of
+    max_run_bytes, the fastest is kept and meets the bar; a later core of
+    the same length, bits and form starts from it; a pinned candidate
+    beyond the list is refused."""
+    N, cof = 4096, 64
+    s = _spec(0, N, 2, cof)
+    c = _core(gpu, s, autotune=True)
+    info = c.plan_info()
+    assert "tuned" in info and "of 3" in info, info
+    pay = stream_payload(s)
+    auto, _, _, ns = c.run([pay])
+    x = O.decode(O.FMT_VDIF, 1, 2, pay, s.samples_per_run, 0, payload_bytes=8000)
+    ra, _, _, nref = oracle_run([x], N, "hann", 1, cof)
+    assert ns == nref == 1
+    assert np.max(np.abs(auto[0, 0] - ra[0, 0]) / ra[0, 0]) < REL_TOL
+    assert _core(gpu, s).plan_info() == info
+    lay = gpu.layout("vdif:8000", 1, 2, framed=False)
+    with pytest.raises(gpu.SwsError, match="beyond"):
+        gpu.Core(gpu.make_config(lay, N, "hann", 1, cof, max_run_bytes=s.run_bytes, plan_candidate=3))
