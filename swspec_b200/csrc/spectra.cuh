@@ -306,7 +306,8 @@ struct SmemLayout {
    static constexpr size_t tw2 = wsl + (size_t)Q * 4;                           // pass-2 twiddles
    static constexpr size_t tw3 = tw2 + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8;
    static constexpr size_t twc = tw3 + (size_t)nbases(R3) * R1 * R2 * 8;        // pass-3 bases
-   static constexpr size_t stage = ((twc + (size_t)nbases(P) * (Q / (2 * P)) * 8) + 15) / 16 * 16;
+   // cluster-stage bases: lo sides, and (FP32 form) hi sides
+   static constexpr size_t stage = ((twc + (size_t)(PREC ? 1 : 2) * nbases(P) * (Q / (2 * P)) * 8) + 15) / 16 * 16;
    static constexpr size_t total = stage + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4;
 };
 
@@ -381,10 +382,15 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       if (tid < 32) tc::tmem_alloc((uint32_t)__cvta_generic_to_shared(&tmem_holder), TC_TMEM_COLS);
       if (tid == 0) tc::mbar_init_cta(mma_bar_addr, 1);
    }
-   // twc[i*UC + u_local] = W_N^{2^i u}, read by both sides of pair u
+   // twc[i*UC + u_local] = W_N^{2^i u} (lo side of pair u); the FP32 form
+   // adds twc[(NBASE + i)*UC + u_local] = W_N^{2^i (Q - u)} for the hi side
+   // (index <= N/2, inside the W_N table), so that neither side needs a
+   // conjugation or a further rotation; the tensor-core forms, short of
+   // shared memory, derive the hi side's from the lo side's
    for (int idx = tid; idx < nbases(P) * UC; idx += T) {
-      const int i = idx / UC, uu = idx % UC;
-      twc[idx] = __ldg(a.twN + ((long long)(rank * UC + uu) << i));
+      const int i = idx / UC, uu = idx % UC, u = rank * UC + uu;
+      twc[idx] = __ldg(a.twN + ((long long)u << i));
+      if constexpr (PREC == 0) twc[nbases(P) * UC + idx] = __ldg(a.twN + ((long long)(u ? Q - u : 0) << i));
    }
 
    const uint32_t rbuf_addr = (uint32_t)__cvta_generic_to_shared(rbuf);
@@ -762,20 +768,27 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                   });
                }
             } else {
-               // z[p] *= W_N^{p u} (lo) or conj of it (hi), from the power bases
+               // z[p] *= W_N^{p u} (lo) or W_N^{p (Q - u)} (hi), from the power bases
                float2 base[nbases(P)];
+               if constexpr (PREC == 0) {
+                  const float2 *tb = twc + (hi ? nbases(P) * UC : 0) + (s >> 1);
 #pragma unroll
-               for (int i = 0; i < nbases(P); i++) {
-                  const float2 w = twc[i * UC + (s >> 1)];
-                  base[i] = hi ? make_float2(w.x, -w.y) : w;
-               }
-               twiddle_by_powers<P>(z, base);
-               if (hi) {
-                  // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
-                  static_for<1, P>([&](auto I) {
-                     constexpr int p = decltype(I)::value;
-                     z[p] = twmul<p, P>(z[p]);
-                  });
+                  for (int i = 0; i < nbases(P); i++) base[i] = tb[i * UC];
+                  twiddle_by_powers<P>(z, base);
+               } else {
+#pragma unroll
+                  for (int i = 0; i < nbases(P); i++) {
+                     const float2 w = twc[i * UC + (s >> 1)];
+                     base[i] = hi ? make_float2(w.x, -w.y) : w;
+                  }
+                  twiddle_by_powers<P>(z, base);
+                  if (hi) {
+                     // W_N^{p(Q-u)} = W_P^p conj(W_N^{p u})
+                     static_for<1, P>([&](auto I) {
+                        constexpr int p = decltype(I)::value;
+                        z[p] = twmul<p, P>(z[p]);
+                     });
+                  }
                }
             }
             DFT<P>::run(z);
