@@ -294,6 +294,11 @@ __host__ __device__ constexpr int rx_stride()
    return UC + (24 - UC % 16) % 16;
 }
 
+// The FP32 form's hi-side cluster bases start TWC_HI_PAD float2 after the
+// lo-side ones: the lanes of a half-warp read the lo and hi bases of the same
+// 8 pairs, and the 64-byte offset puts the two halves in different banks.
+constexpr int TWC_HI_PAD = 8;
+
 // Shared memory layout of a plan: byte offsets of every region, used both
 // for the kernel's pointers and for the host-side launch size.
 template <int P, int Q, int R1, int R2, int R3, int NBIT, int PREC>
@@ -307,7 +312,8 @@ struct SmemLayout {
    static constexpr size_t tw3 = tw2 + (size_t)(PREC ? 0 : pass_tw_entries<Q, R2, R1>()) * 8;
    static constexpr size_t twc = tw3 + (size_t)nbases(R3) * R1 * R2 * 8;        // pass-3 bases
    // cluster-stage bases: lo sides, and (FP32 form) hi sides
-   static constexpr size_t stage = ((twc + (size_t)(PREC ? 1 : 2) * nbases(P) * (Q / (2 * P)) * 8) + 15) / 16 * 16;
+   static constexpr size_t stage =
+       ((twc + ((size_t)(PREC ? 1 : 2) * nbases(P) * (Q / (2 * P)) + (PREC ? 0 : TWC_HI_PAD)) * 8) + 15) / 16 * 16;
    static constexpr size_t total = stage + (size_t)2 * 2 * stage_slots<Q, R1, NBIT>() * 4;
 };
 
@@ -383,14 +389,15 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
       if (tid == 0) tc::mbar_init_cta(mma_bar_addr, 1);
    }
    // twc[i*UC + u_local] = W_N^{2^i u} (lo side of pair u); the FP32 form
-   // adds twc[(NBASE + i)*UC + u_local] = W_N^{2^i (Q - u)} for the hi side
+   // adds twc[(NBASE + i)*UC + TWC_HI_PAD + u_local] = W_N^{2^i (Q - u)} for the hi side
    // (index <= N/2, inside the W_N table), so that neither side needs a
    // conjugation or a further rotation; the tensor-core forms, short of
    // shared memory, derive the hi side's from the lo side's
    for (int idx = tid; idx < nbases(P) * UC; idx += T) {
       const int i = idx / UC, uu = idx % UC, u = rank * UC + uu;
       twc[idx] = __ldg(a.twN + ((long long)u << i));
-      if constexpr (PREC == 0) twc[nbases(P) * UC + idx] = __ldg(a.twN + ((long long)(u ? Q - u : 0) << i));
+      if constexpr (PREC == 0)
+         twc[nbases(P) * UC + TWC_HI_PAD + idx] = __ldg(a.twN + ((long long)(u ? Q - u : 0) << i));
    }
 
    const uint32_t rbuf_addr = (uint32_t)__cvta_generic_to_shared(rbuf);
@@ -771,7 +778,7 @@ __global__ void __launch_bounds__(T, MINB) k_spectra(SpecArgs a)
                // z[p] *= W_N^{p u} (lo) or W_N^{p (Q - u)} (hi), from the power bases
                float2 base[nbases(P)];
                if constexpr (PREC == 0) {
-                  const float2 *tb = twc + (hi ? nbases(P) * UC : 0) + (s >> 1);
+                  const float2 *tb = twc + (hi ? nbases(P) * UC + TWC_HI_PAD : 0) + (s >> 1);
 #pragma unroll
                   for (int i = 0; i < nbases(P); i++) base[i] = tb[i * UC];
                   twiddle_by_powers<P>(z, base);

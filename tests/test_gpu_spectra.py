@@ -366,11 +366,12 @@ def test_group_runs_chunked_and_per_run(gpu):
 
 
 def test_group_chunks_alternate_streams(gpu):
-    """Two 10-run output groups of 8 MiB runs: the submit path collects 4
-    runs per device chunk (32 MiB), so each group is 3 chunks and
-    consecutive chunks run on alternating streams with their own scratch
-    buffers, their sums added in submission order.  Both groups' combined
-    spectra match the FP64 oracle, and a chunk's input region is refilled
+    """Two 10-run output groups of 8 MiB runs: the submit path collects up
+    to 4 runs per device chunk (32 MiB; the group's last chunks shrink:
+    4, 3, 1, 1, 1), and consecutive chunks run on alternating streams with
+    their own scratch buffers, their spectrum sums and phase-cal folds added
+    in submission order.  Both groups' combined spectra and phase-cal
+    vectors match the FP64 oracle, and a chunk's input region is refilled
     only after its decode."""
     N, cof, nrun = 4096, 512, 10
     run = N * cof * 4                         # 16 channels x 2 bit: 4 bytes per sample-time
@@ -380,33 +381,40 @@ def test_group_chunks_alternate_streams(gpu):
     w[w == 0x11223344] ^= 1                   # no mark5access fill words
     S = N // 2 + 1
     lay = gpu.layout("mark5b", 16, 2, framed=False)
+    # phase-cal: 64 tone bins, rotator period 4096 at 64 Msps (15625 Hz offset)
+    pc_args = dict(tonebins=64, rotatorlen=4096, fs=64e6, offset=15625.0)
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 3), (0, 12)), xpols=((0, 1),),
-                          max_run_bytes=run, samplingfreq=64e6, runs_per_output=nrun)
+                          max_run_bytes=run, samplingfreq=64e6, runs_per_output=nrun,
+                          extract_pcal=True, pcal_tonebins=64, pcal_rotatorlen=4096, pcal_offset_hz=15625.0)
     core = gpu.Core(cfg)
     core.set_sizes([run])
     outs = []
     for g in range(2):
         auto = np.zeros((1, 2, S), np.float32)
         xp = np.zeros((1, 1, S, 2), np.float32)
+        pc = np.zeros((1, 2, 64, 2), np.float32)
         for r in range(nrun):
             off = (g * nrun + r) * run
             core.submit([pay[off:off + run]], payload_offsets=[off])
             assert core.wait() == (1 if r == nrun - 1 else 0)
-        core.fetch_into(auto, xp)
-        outs.append((auto[0], xp[0, 0, :, 0] + 1j * xp[0, 0, :, 1]))
+        core.fetch_into(auto, xp, pc)
+        outs.append((auto[0], xp[0, 0, :, 0] + 1j * xp[0, 0, :, 1], pc[0, :, :, 0] + 1j * pc[0, :, :, 1]))
     core.close()
-    for g, (a, x) in enumerate(outs):
+    for g, (a, x, p) in enumerate(outs):
         ra = np.zeros((2, S))
         rx = np.zeros(S, complex)
+        rp = np.zeros((2, 64), complex)
         for r in range(nrun):
             off = (g * nrun + r) * run
             s = [O_decode(pay[off:off + run].tobytes(), run // 4, c) for c in (3, 12)]
-            aa, xx, _, n = oracle_run(s, N, "hann", 1, cof, nxpols=1)
+            aa, xx, pp, n = oracle_run(s, N, "hann", 1, cof, nxpols=1, pcal=pc_args)
             assert n == 1
             ra += aa[0]
             rx += xx[0, 0]
+            rp += pp[0]
         assert np.max(np.abs(a - ra) / ra) < REL_TOL, g
         assert np.max(np.abs(x - rx) / np.sqrt(ra[0] * ra[1])) < REL_TOL, g
+        assert np.max(np.abs(p - rp)) / np.max(np.abs(rp)) < 1e-6, g
 
 
 def O_decode(buf: bytes, nsamp: int, chan: int):
