@@ -456,8 +456,8 @@ def gpu_arm(args) -> None:
     # DRAM bytes of one k_spectra launch on this workload, from ncu captures
     # (dram__bytes_read.sum + dram__bytes_write.sum): the 2-bit codes read
     # plus the per-item partial spectra that k_reduce combines
-    traffic = {gpu.PREC_FP32: (256476672 + 208978176,
-                               "ncu --set full capture of one k_spectra launch of this workload "
+    traffic = {gpu.PREC_FP32: (257874176 + 215790080,
+                               "ncu section capture of one k_spectra launch of this workload "
                                "(dram__bytes_read.sum + dram__bytes_write.sum)")}
     t = traffic.get(headline)
     roof["traffic"] = t[0] if t else None
