@@ -55,6 +55,13 @@ CONFIG = {"workload": "dual-pol cross-spectra: Mark5B-2048-16-2, 8 subband pairs
 METRIC = "input Gsamples/s unpack->FFT->integrate"
 
 
+def pinned_np(shape, dtype):
+    """A zeroed page-locked host array (the GPU core's device-to-host copies
+    land in it directly)."""
+    import torch
+    return torch.zeros(shape, dtype=dtype, pin_memory=True).numpy()
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -383,15 +390,15 @@ def gpu_arm(args) -> None:
     torch.cuda.synchronize()
     core = make_core(headline, framed=False, rpo=RUNS_PER_SPECTRUM)
     core.set_sizes([RUN_BYTES])
-    auto_h = np.zeros((1, NCHAN, S), np.float32)
-    xpol_h = np.zeros((1, NPAIRS, S, 2), np.float32)
+    # output buffers handed to the run, as TaskCore::run takes them, page-locked
+    auto_h = pinned_np((1, NCHAN, S), torch.float32)
+    xpol_h = pinned_np((1, NPAIRS, S, 2), torch.float32)
     base = host.data_ptr()
 
     def e2e_step():
         for r in range(RUNS_PER_SPECTRUM):
-            core.submit([base + r * RUN_BYTES], payload_offsets=[r * RUN_BYTES])
+            core.submit([base + r * RUN_BYTES], payload_offsets=[r * RUN_BYTES], dest=(auto_h, xpol_h))
             core.wait()
-        core.fetch_into(auto_h, xpol_h)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
@@ -478,8 +485,8 @@ def gpu_arm(args) -> None:
             "e2e": {"value": e2e_val, "unit": "Gsamples/s",
                     "h2d_bytes_per_step": RUNS_PER_SPECTRUM * RUN_BYTES,
                     "d2h_bytes_per_step": d2h,
-                    "path": "swsgpu_submit/wait per 4 MiB run (TaskCore path), device combine, "
-                            "one fetch per spectrum"},
+                    "path": "swsgpu_submit_out/wait per 4 MiB run (TaskCore path, the run given its "
+                            "output buffers), device combine, spectra copied into pinned host arrays"},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "parity": parity}
     print(json.dumps(line), flush=True)
@@ -548,6 +555,40 @@ def c4_arm(args) -> None:
     bytes_in = sum(s.run_bytes for s in specs)
     value = samples * reps.world / (ms * 1e-3) / 1e9
     b.close()
+
+    # ---- e2e: every stream's run from pinned host memory through its own
+    # core's submit / wait / fetch (the TaskCore path), all cores in flight
+    # as the reference's dispatcher runs its cores, then joins each ----
+    import numpy as np
+    hosts, houts = [], []
+    for s, c, r in zip(specs, cores, raws):
+        h = torch.empty(s.run_bytes, dtype=torch.uint8, pin_memory=True)
+        h.copy_(r)
+        hosts.append(h)
+        ns, _, _ = c.run_shape(s.run_bytes)
+        houts.append(pinned_np((max(ns, 1), 1, c.S), torch.float32))
+        c.set_sizes([s.run_bytes])
+    torch.cuda.synchronize()
+
+    def e2e_step():
+        for c, h, o in zip(cores, hosts, houts):
+            c.submit([h.data_ptr()], dest=(o,))
+        for c in cores:
+            c.wait()
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    reps.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = reps.max(time.perf_counter() - t0)
+    reps.barrier()
+    e2e_val = samples * args.steps * reps.world / e2e_s / 1e9
+    d2h = sum(o.nbytes for o in houts)
+    log(f"[c4 e2e] {e2e_val:.3f} Gsamples/s")
     if reps.rank == 0:
         from collections import Counter
         peaks = measured_peaks()
@@ -563,7 +604,10 @@ def c4_arm(args) -> None:
                            "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_in / 1e6),
                            "autotune_s": t_tune},
                 "clocks": cs.summary(), "gpu_launches": kernels * args.steps, "graph_launches_per_step": 1,
-                "e2e": None,
+                "e2e": {"value": e2e_val, "unit": "Gsamples/s", "h2d_bytes_per_step": bytes_in,
+                        "d2h_bytes_per_step": d2h,
+                        "path": "swsgpu_submit_out/wait per stream from pinned host buffers into pinned output "
+                                "arrays, all 64 cores submitted before the waits (one outstanding run per core)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                              "note": "packed input bytes per step over the step time"},
@@ -716,16 +760,17 @@ def spec_arm(args) -> None:
     torch.cuda.synchronize()
     ecore = gpu.Core(cfg, device=local)
     ecore.set_sizes([w["run_bytes"]])
-    auto_h = np.zeros((1, ns, S), np.float32)
-    pcal_h = np.zeros((1, ns, max(pc.get("tonebins", 1), 1), 2), np.float32) if pc else None
-    tones_h = np.zeros((1, ns, max(pc.get("ntones", 1), 1), 2), np.float64) if pc else None
+    # output buffers handed to the run (TaskCore::run's out / pcal), page-locked
+    auto_h = pinned_np((1, ns, S), torch.float32)
+    pcal_h = pinned_np((1, ns, max(pc.get("tonebins", 1), 1), 2), torch.float32) if pc else None
+    tones_h = pinned_np((1, ns, max(pc.get("ntones", 1), 1), 2), torch.float64) if pc else None
     base = host.data_ptr()
 
     def e2e_step():
         for r in range(w["runs"]):
-            ecore.submit([base + r * w["run_bytes"]], payload_offsets=[r * w["run_bytes"]])
+            ecore.submit([base + r * w["run_bytes"]], payload_offsets=[r * w["run_bytes"]],
+                         dest=(auto_h, None, pcal_h, tones_h))
             ecore.wait()
-        ecore.fetch_into(auto_h, None, pcal_h, tones_h)
 
     for _ in range(max(1, min(args.warmup, 2))):
         e2e_step()
@@ -757,8 +802,8 @@ def spec_arm(args) -> None:
                 "clocks": cs.summary(), "gpu_launches": launches * args.steps,
                 "e2e": {"value": e2e_val, "unit": "Gsamples/s", "h2d_bytes_per_step": w["run_bytes"] * w["runs"],
                         "d2h_bytes_per_step": d2h,
-                        "path": "swsgpu_submit/wait per run from pinned host memory (TaskCore path), device "
-                                "combine, one fetch per spectrum"},
+                        "path": "swsgpu_submit_out/wait per run from pinned host memory (TaskCore path, the "
+                                "run given its output buffers), device combine, spectra into pinned host arrays"},
                 "roofline": {"bound": "fp32", "achieved": flops / (ms * 1e-3) / 1e12, "peak": p32,
                              "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / p32 if p32 else None,
                              "traffic": None, "scope": "whole step (every kernel of the step)",

@@ -211,6 +211,17 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra);
 /* Copy the spectra of the completed run into caller memory. */
 int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out);
 
+/* TaskCore::run(in, out, xpol, pcal) (TaskCore.h:58) with its output
+ * buffers: swsgpu_submit, plus where the spectra of this run go if it
+ * completes any (layouts as swsgpu_fetch; NULL members are not written).
+ * Destinations in page-locked memory (cudaHostAlloc, swsgpu_host_register)
+ * are written by the run's own device-to-host copies, with no host copy;
+ * others through the library's staging buffer during swsgpu_wait.  Either
+ * way they hold the spectra once swsgpu_wait returns, and must stay valid
+ * until then; swsgpu_fetch is not used for such a run (SWSGPU_ESTATE). */
+int swsgpu_submit_out(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                      const int64_t *stream_payload_offset, const swsgpu_outputs *dest);
+
 /* Page-lock caller memory that will be passed to swsgpu_submit, so its
  * input copies are DMA transfers that overlap kernels (the reference's raw
  * buffers are allocated once by main, src/swspectrometer.cpp:373-413, and

@@ -248,6 +248,10 @@ struct swsgpu_handle {
    DevBuf d_acc64;
    int group_pos = 0;
    bool fetch_ready = false;
+   // spectra delivered by the submit that completed them (swsgpu_submit_out):
+   // straight into pinned caller memory, or through h_out and a copy at wait
+   bool delivered = false;
+   swsgpu_outputs deliver_copy = {nullptr, nullptr, nullptr, nullptr};  // pageable destinations
    // device-resident schedules (a few distinct run shapes per handle)
    std::vector<SchedEntry *> sched;
    // per-stream channel lists of the code arrays (K1), uploaded at create
@@ -1493,8 +1497,20 @@ int swsgpu_run_shape(const swsgpu_handle *h, size_t nbytes, int *nspectra, int *
    return SWSGPU_OK;
 }
 
-int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
-                  const int64_t *stream_payload_offset)
+// True when host pointer p is page-locked memory the GPU can copy into
+// asynchronously.
+static bool host_pinned(const void *p)
+{
+   cudaPointerAttributes at;
+   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+   }
+   return at.type == cudaMemoryTypeHost;
+}
+
+static int submit_impl(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                       const int64_t *stream_payload_offset, const swsgpu_outputs *dest)
 {
    if (!h || !raw || !nbytes) return SWSGPU_EINVAL;
    if (h->pending && h->pending_out)
@@ -1628,26 +1644,49 @@ int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes
       }
       CK(h, cudaEventRecord(h->slot_free[slot], h->stream));
    }
-   h->fetch_ready = group_end;
+   h->fetch_ready = group_end && !dest;
+   h->delivered = false;
+   h->deliver_copy = swsgpu_outputs{nullptr, nullptr, nullptr, nullptr};
    if (nsp > 0 && group_end) {
       if (int rc = join_chunks(h)) return rc;
       char *hp = (char *)h->h_out.p;
-      CK(h, cudaMemcpyAsync(hp, h->d_out_auto.p, h->h_auto_bytes, cudaMemcpyDeviceToHost, h->stream));
-      if (h->h_xpol_bytes)
-         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes, h->d_out_xpol.p, h->h_xpol_bytes,
-                               cudaMemcpyDeviceToHost, h->stream));
-      if (h->h_pcal_bytes)
-         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes, h->d_out_pcal.p,
-                               h->h_pcal_bytes, cudaMemcpyDeviceToHost, h->stream));
-      if (h->h_tones_bytes)
-         CK(h, cudaMemcpyAsync(hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->d_out_tones.p,
-                               h->h_tones_bytes, cudaMemcpyDeviceToHost, h->stream));
+      // each output goes to pinned caller memory directly, else to the
+      // staging buffer (copied to a pageable destination at wait, or kept
+      // for swsgpu_fetch)
+      void *const stage[4] = {hp, hp + h->h_auto_bytes, hp + h->h_auto_bytes + h->h_xpol_bytes,
+                              hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes};
+      const void *const src[4] = {h->d_out_auto.p, h->d_out_xpol.p, h->d_out_pcal.p, h->d_out_tones.p};
+      const size_t bytes[4] = {h->h_auto_bytes, h->h_xpol_bytes, h->h_pcal_bytes, h->h_tones_bytes};
+      void *const want[4] = {dest ? (void *)dest->auto_out : nullptr, dest ? (void *)dest->xpol_out : nullptr,
+                             dest ? (void *)dest->pcal_out : nullptr, dest ? (void *)dest->tones_out : nullptr};
+      void **later[4] = {(void **)&h->deliver_copy.auto_out, (void **)&h->deliver_copy.xpol_out,
+                         (void **)&h->deliver_copy.pcal_out, (void **)&h->deliver_copy.tones_out};
+      for (int k = 0; k < 4; k++) {
+         if (bytes[k] == 0 || (dest && !want[k])) continue;
+         const bool direct = want[k] && host_pinned(want[k]);
+         CK(h, cudaMemcpyAsync(direct ? want[k] : stage[k], src[k], bytes[k], cudaMemcpyDeviceToHost, h->stream));
+         if (want[k] && !direct) *later[k] = want[k];
+      }
+      h->delivered = dest != nullptr;
    }
    CK(h, cudaEventRecord(h->done, h->stream));
    h->pending = true;
    h->pending_out = nsp > 0 && group_end;
    h->pending_nspec = group_end ? nspec : 0;
    return SWSGPU_OK;
+}
+
+int swsgpu_submit(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                  const int64_t *stream_payload_offset)
+{
+   return submit_impl(h, raw, nbytes, stream_payload_offset, nullptr);
+}
+
+int swsgpu_submit_out(swsgpu_handle *h, const void *const *raw, const size_t *nbytes,
+                      const int64_t *stream_payload_offset, const swsgpu_outputs *dest)
+{
+   if (!dest) return SWSGPU_EINVAL;
+   return submit_impl(h, raw, nbytes, stream_payload_offset, dest);
 }
 
 int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
@@ -1684,6 +1723,17 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
          cudaMemset(h->d_status.p, 0, sizeof(int));
          return fail(h, SWSGPU_ECUDA, "a device-side wait for cluster data gave up; the spectra are invalid");
       }
+   }
+   if (had_out) {
+      // pageable destinations of swsgpu_submit_out: from the staging buffer
+      const char *hp = (const char *)h->h_out.p;
+      const swsgpu_outputs &d = h->deliver_copy;
+      if (d.auto_out) memcpy(d.auto_out, hp, h->h_auto_bytes);
+      if (d.xpol_out) memcpy(d.xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);
+      if (d.pcal_out) memcpy(d.pcal_out, hp + h->h_auto_bytes + h->h_xpol_bytes, h->h_pcal_bytes);
+      if (d.tones_out)
+         memcpy(d.tones_out, hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->h_tones_bytes);
+      h->deliver_copy = swsgpu_outputs{nullptr, nullptr, nullptr, nullptr};
    }
    if (nspectra) *nspectra = h->pending_nspec;
    return SWSGPU_OK;
@@ -1752,6 +1802,8 @@ int swsgpu_fetch(swsgpu_handle *h, const swsgpu_outputs *out)
    if (!h || !out) return SWSGPU_EINVAL;
    if (h->pending) return fail(h, SWSGPU_ESTATE, "fetch before wait");
    const char *hp = (const char *)h->h_out.p;
+   if (h->delivered)
+      return fail(h, SWSGPU_ESTATE, "the spectra went to the destination given to swsgpu_submit_out");
    if (!hp || !h->fetch_ready) return fail(h, SWSGPU_ESTATE, "no completed spectra to fetch");
    if (out->auto_out) memcpy(out->auto_out, hp, h->h_auto_bytes);
    if (out->xpol_out && h->h_xpol_bytes) memcpy(out->xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);

@@ -72,6 +72,8 @@ def lib():
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.swsgpu_submit.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                                     C.POINTER(C.c_int64)]
+        L.swsgpu_submit_out.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                                        C.POINTER(C.c_int64), C.POINTER(Outputs)]
         L.swsgpu_wait.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.swsgpu_fetch.argtypes = [C.c_void_p, C.POINTER(Outputs)]
         L.swsgpu_process_device.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_size_t, C.c_int,
@@ -207,7 +209,10 @@ class Core:
         _check(lib().swsgpu_profile_read(self.h, C.byref(n), C.byref(ms)), self.h)
         return n.value, ms.value
 
-    def submit(self, raws: list, payload_offsets=None) -> None:
+    def submit(self, raws: list, payload_offsets=None, dest=None) -> None:
+        """swsgpu_submit; with dest = (auto, xpol, pcal, tones) arrays (None
+        for any not wanted) swsgpu_submit_out, which writes a completed run's
+        spectra there (page-locked arrays get the device copies directly)."""
         n = len(raws)
         # argument arrays kept across calls: a run's submit is on the
         # per-run critical path of the host loop
@@ -219,7 +224,15 @@ class Core:
         for i, r in enumerate(raws):
             self._sub_ptrs[i] = int(r) if isinstance(r, int) else r.ctypes.data
             self._sub_offs[i] = payload_offsets[i] if payload_offsets else 0
-        _check(lib().swsgpu_submit(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs), self.h)
+        if dest is None:
+            _check(lib().swsgpu_submit(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs), self.h)
+            return
+        key = tuple(None if a is None else a.ctypes.data for a in (tuple(dest) + (None,) * 4)[:4])
+        if getattr(self, "_dest_key", None) != key:
+            self._dest_key = key
+            self._dest = Outputs(*key)
+        _check(lib().swsgpu_submit_out(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs,
+                                       C.byref(self._dest)), self.h)
 
     def set_sizes(self, sizes: list[int]) -> None:
         self._sizes = list(sizes)

@@ -417,6 +417,53 @@ def test_group_chunks_alternate_streams(gpu):
         assert np.max(np.abs(p - rp)) / np.max(np.abs(rp)) < 1e-6, g
 
 
+def test_submit_out_matches_fetch(gpu):
+    """swsgpu_submit_out (the run's output buffers given with the run, as
+    TaskCore::run takes them) delivers the same spectra, bit for bit, as
+    submit + fetch: into page-locked arrays by the run's own device copies,
+    into pageable arrays through the staging buffer at wait; fetch after it
+    is refused.  Two 6-run groups of 1 MiB runs (chunks of 3, 1, 1, 1)."""
+    import torch
+    N, cof, nrun = 4096, 64, 6
+    run = N * cof * 4
+    rng = np.random.default_rng(91)
+    pay = rng.integers(0, 256, size=2 * nrun * run, dtype=np.uint8)
+    w = pay.view(np.uint32)
+    w[w == 0x11223344] ^= 1
+    S = N // 2 + 1
+    lay = gpu.layout("mark5b", 16, 2, framed=False)
+    got = {}
+    for mode in ("fetch", "pinned", "pageable"):
+        cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, 3), (0, 12)), xpols=((0, 1),),
+                              max_run_bytes=run, samplingfreq=64e6, runs_per_output=nrun)
+        core = gpu.Core(cfg)
+        core.set_sizes([run])
+        for g in range(2):
+            if mode == "pinned":
+                a = torch.zeros((1, 2, S), dtype=torch.float32, pin_memory=True).numpy()
+                x = torch.zeros((1, 1, S, 2), dtype=torch.float32, pin_memory=True).numpy()
+            else:
+                a = np.zeros((1, 2, S), np.float32)
+                x = np.zeros((1, 1, S, 2), np.float32)
+            for r in range(nrun):
+                off = (g * nrun + r) * run
+                core.submit([pay[off:off + run]], payload_offsets=[off],
+                            dest=None if mode == "fetch" else (a, x))
+                assert core.wait() == (1 if r == nrun - 1 else 0)
+            if mode == "fetch":
+                core.fetch_into(a, x)
+            else:
+                with pytest.raises(gpu.SwsError, match="submit_out"):
+                    core.fetch_into(np.zeros_like(a), np.zeros_like(x))
+            got.setdefault(mode, []).append((a.copy(), x.copy()))
+        core.close()
+    for mode in ("pinned", "pageable"):
+        for g in range(2):
+            assert np.array_equal(got[mode][g][0], got["fetch"][g][0]), (mode, g)
+            assert np.array_equal(got[mode][g][1], got["fetch"][g][1]), (mode, g)
+    assert np.all(got["fetch"][0][0] > 0)
+
+
 def O_decode(buf: bytes, nsamp: int, chan: int):
     import oracle as O
     return O.decode(O.FMT_MARK5B, 16, 2, buf, nsamp, chan, payload_bytes=10000)
