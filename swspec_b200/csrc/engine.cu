@@ -251,7 +251,7 @@ struct swsgpu_handle {
    // spectra delivered by the submit that completed them (swsgpu_submit_out):
    // straight into pinned caller memory, or through h_out and a copy at wait
    bool delivered = false;
-   swsgpu_outputs deliver_copy = {nullptr, nullptr, nullptr, nullptr};  // pageable destinations
+   void *deliver_copy[4] = {nullptr, nullptr, nullptr, nullptr};  // pageable destinations (auto, xpol, pcal, tones)
    // device-resident schedules (a few distinct run shapes per handle)
    std::vector<SchedEntry *> sched;
    // per-stream channel lists of the code arrays (K1), uploaded at create
@@ -1646,7 +1646,7 @@ static int submit_impl(swsgpu_handle *h, const void *const *raw, const size_t *n
    }
    h->fetch_ready = group_end && !dest;
    h->delivered = false;
-   h->deliver_copy = swsgpu_outputs{nullptr, nullptr, nullptr, nullptr};
+   for (void *&p : h->deliver_copy) p = nullptr;
    if (nsp > 0 && group_end) {
       if (int rc = join_chunks(h)) return rc;
       char *hp = (char *)h->h_out.p;
@@ -1659,13 +1659,11 @@ static int submit_impl(swsgpu_handle *h, const void *const *raw, const size_t *n
       const size_t bytes[4] = {h->h_auto_bytes, h->h_xpol_bytes, h->h_pcal_bytes, h->h_tones_bytes};
       void *const want[4] = {dest ? (void *)dest->auto_out : nullptr, dest ? (void *)dest->xpol_out : nullptr,
                              dest ? (void *)dest->pcal_out : nullptr, dest ? (void *)dest->tones_out : nullptr};
-      void **later[4] = {(void **)&h->deliver_copy.auto_out, (void **)&h->deliver_copy.xpol_out,
-                         (void **)&h->deliver_copy.pcal_out, (void **)&h->deliver_copy.tones_out};
       for (int k = 0; k < 4; k++) {
          if (bytes[k] == 0 || (dest && !want[k])) continue;
          const bool direct = want[k] && host_pinned(want[k]);
          CK(h, cudaMemcpyAsync(direct ? want[k] : stage[k], src[k], bytes[k], cudaMemcpyDeviceToHost, h->stream));
-         if (want[k] && !direct) *later[k] = want[k];
+         if (want[k] && !direct) h->deliver_copy[k] = want[k];
       }
       h->delivered = dest != nullptr;
    }
@@ -1725,15 +1723,16 @@ int swsgpu_wait(swsgpu_handle *h, int timeout_ms, int *nspectra)
       }
    }
    if (had_out) {
-      // pageable destinations of swsgpu_submit_out: from the staging buffer
+      // pageable destinations of swsgpu_submit_out: from the staging buffer,
+      // whose four regions follow one another
       const char *hp = (const char *)h->h_out.p;
-      const swsgpu_outputs &d = h->deliver_copy;
-      if (d.auto_out) memcpy(d.auto_out, hp, h->h_auto_bytes);
-      if (d.xpol_out) memcpy(d.xpol_out, hp + h->h_auto_bytes, h->h_xpol_bytes);
-      if (d.pcal_out) memcpy(d.pcal_out, hp + h->h_auto_bytes + h->h_xpol_bytes, h->h_pcal_bytes);
-      if (d.tones_out)
-         memcpy(d.tones_out, hp + h->h_auto_bytes + h->h_xpol_bytes + h->h_pcal_bytes, h->h_tones_bytes);
-      h->deliver_copy = swsgpu_outputs{nullptr, nullptr, nullptr, nullptr};
+      const size_t bytes[4] = {h->h_auto_bytes, h->h_xpol_bytes, h->h_pcal_bytes, h->h_tones_bytes};
+      size_t at = 0;
+      for (int k = 0; k < 4; k++) {
+         if (h->deliver_copy[k]) memcpy(h->deliver_copy[k], hp + at, bytes[k]);
+         h->deliver_copy[k] = nullptr;
+         at += bytes[k];
+      }
    }
    if (nspectra) *nspectra = h->pending_nspec;
    return SWSGPU_OK;
