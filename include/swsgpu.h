@@ -61,6 +61,22 @@ extern "C" {
  * {+1, -1, +H, -H}.  No fill-pattern blanking. */
 #define SWSGPU_FMT_RAW_SIGNED 2
 #define SWSGPU_FMT_RAW_UNSIGNED 3
+/* Track formats, decoded as mark5access decodes them (VLBA1_f / MKIV1_f
+ * modes, mark5_format_vlba.c, mark5_format_mark4.c; the reference's
+ * VLBAUnpacker / MarkIVUnpacker, src/IA-32/DataUnpackers.cpp:459-658, go
+ * through mark5access): a track-word of ntrack bits (tracks 8, 16, 32 or 64,
+ * the low track in bit 0 of the first byte) carries `fanout` consecutive
+ * samples of every channel, ntrack = nchan * nbit * fanout, fanout 1, 2 or 4,
+ * nbit 1 or 2, nchan * nbit <= 32; levels as Mark5B's.  A frame is 20000
+ * track-words: frame_bytes = 2500 * ntrack, header_bytes = 0.  VLBA: the
+ * payload stream with the frame headers removed (the 96 track-words before
+ * and the 64 after each frame's 20000); every sample of track-word i of a
+ * frame is negated where the VLBA modulation sequence has bit i set.  Mark4
+ * (data replacement): whole frames, whose first 160 track-words (auxiliary
+ * data, sync word, time code) decode as blanked samples.  No fill-pattern
+ * blanking. */
+#define SWSGPU_FMT_VLBA 4
+#define SWSGPU_FMT_MARK4 5
 
 /* Window functions: the reference's WindowFunctionType (src/Settings.h:45)
  * plus BlackmanHarris (4-term Harris 1978), which the reference lacks. */
@@ -329,8 +345,10 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
  * synchronises its stream (it reads the sample count back), so it cannot
  * be issued on a stream that is being captured.  All calls share the one
  * scratch array: calls that overlap on the GPU (for example on two streams
- * at once) race and must be serialised by the caller.  Returns like
- * swsgpu_unpack_device; on a CUDA error swsgpu_last_error(NULL) describes it. */
+ * at once) race and must be serialised by the caller.  Track formats (VLBA,
+ * Mark4) need a conversion buffer of the data's size and return
+ * SWSGPU_EINVAL here.  Returns like swsgpu_unpack_device; on a CUDA error
+ * swsgpu_last_error(NULL) describes it. */
 #define SWSGPU_NOALLOC_MAX_FRAMES 16384
 #define SWSGPU_NOALLOC_SCRATCH_BYTES (SWSGPU_NOALLOC_MAX_FRAMES * 8 + 256)
 int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,

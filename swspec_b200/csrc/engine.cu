@@ -30,6 +30,8 @@ cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, co
                                 uint32_t *codes, int D, long long wpp, const int2 *valid,
                                 const int *blank_any, uint32_t *blank, int &launches);
 bool unpack_decimation_ok(int D, int nchan, int nbit);
+cudaError_t launch_track_turn(cudaStream_t st, const uint8_t *in, long long nbytes, long long grid_offset,
+                              int ntrack, int nbit, int nchan, int format, uint32_t *out);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
 __global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
@@ -168,9 +170,11 @@ struct SchedEntry {
 struct Scratch {
    DevBuf d_valid[SWSGPU_MAX_STREAMS];
    DevBuf d_codes, d_codes1, d_blank, d_blank_any, d_partial;
+   DevBuf d_trk[SWSGPU_MAX_STREAMS];  // track formats: the chunk in Mark5B's sample layout
    void release()
    {
       for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) d_valid[s].release();
+      for (int s = 0; s < SWSGPU_MAX_STREAMS; s++) d_trk[s].release();
       d_codes.release();
       d_codes1.release();
       d_blank.release();
@@ -324,7 +328,27 @@ static int payload_bytes(const swsgpu_layout &l) { return l.frame_bytes - l.head
 // Raw single-channel 2-bit data stores the oldest sample in the byte's MSBs.
 static int is_msb2(const swsgpu_layout &l)
 {
-   return (l.format >= SWSGPU_FMT_RAW_SIGNED && l.nbit == 2 && l.nchan == 1) ? 1 : 0;
+   return ((l.format == SWSGPU_FMT_RAW_SIGNED || l.format == SWSGPU_FMT_RAW_UNSIGNED) && l.nbit == 2 &&
+           l.nchan == 1) ? 1 : 0;
+}
+
+// Checks a track-format layout (VLBA / Mark4): frame_bytes = 2500 ntrack
+// (20000 track-words), tracks 8..64, fanout 1, 2 or 4, at most 32 bits per
+// sample-time, payload only.  Returns the number of tracks, or 0.
+static int track_layout_ok(const swsgpu_layout &l, std::string &why)
+{
+   const int ntrack = l.frame_bytes / 2500;
+   if (l.header_bytes != 0 || l.frame_bytes % 2500 || (ntrack != 8 && ntrack != 16 && ntrack != 32 && ntrack != 64)) {
+      why = "track formats: frame_bytes must be 2500 x tracks (8, 16, 32 or 64) with header_bytes 0";
+      return 0;
+   }
+   if ((l.nbit != 1 && l.nbit != 2) || l.nchan * l.nbit > 32 || ntrack % (l.nchan * l.nbit)) {
+      why = "track formats: nbit 1 or 2, nchan * nbit <= 32 and dividing the tracks";
+      return 0;
+   }
+   const int fanout = ntrack / (l.nchan * l.nbit);
+   if (fanout != 1 && fanout != 2 && fanout != 4) { why = "track formats: fanout must be 1, 2 or 4"; return 0; }
+   return ntrack;
 }
 
 // ---------------------------------------------------------------------------
@@ -851,6 +875,14 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       const swsgpu_layout &L = c.layout[s];
       StreamIn si;
       si.data = (const uint8_t *)d_raw[s];
+      if (track_format(L.format)) {
+         // VLBA / Mark4 track-words into Mark5B's sample layout (same size and grid)
+         CK(h, x.d_trk[s].ensure((raw_bytes[s] + 3) / 4 * 4 + 16));
+         CK(h, launch_track_turn(st, (const uint8_t *)d_raw[s], (long long)raw_bytes[s], grid_off[s],
+                                 payload_bytes(L) / 2500, L.nbit, L.nchan, L.format, (uint32_t *)x.d_trk[s].p));
+         si.data = (const uint8_t *)x.d_trk[s].p;
+         launches++;
+      }
       si.nbytes = (long long)raw_bytes[s];
       si.grid_offset = grid_off[s];
       si.frame_bytes = L.frame_bytes;
@@ -1136,8 +1168,9 @@ static int validate_config(const swsgpu_config *c, std::string &why)
       const swsgpu_layout &l = c->layout[s];
       if (l.nbit != 1 && l.nbit != 2 && l.nbit != 8) { why = "nbit must be 1, 2 or 8"; return 0; }
       if (l.nchan < 1 || l.nchan * l.nbit > 64) { why = "nchan*nbit must be 1..64"; return 0; }
-      if (l.format < SWSGPU_FMT_MARK5B || l.format > SWSGPU_FMT_RAW_UNSIGNED) { why = "unknown format"; return 0; }
-      if (l.format >= SWSGPU_FMT_RAW_SIGNED) {
+      if (l.format < SWSGPU_FMT_MARK5B || l.format > SWSGPU_FMT_MARK4) { why = "unknown format"; return 0; }
+      if (track_format(l.format) && !track_layout_ok(l, why)) return 0;
+      if (l.format == SWSGPU_FMT_RAW_SIGNED || l.format == SWSGPU_FMT_RAW_UNSIGNED) {
          // the reference's raw unpackers (DataUnpackerFactory.h:44-67)
          if (l.nbit == 1) { why = "raw formats have no 1-bit unpacker"; return 0; }
          if (l.nbit == 2 && !(l.nchan == 1 || l.nchan % 4 == 0)) {
@@ -2165,6 +2198,9 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    const int pb = lay->frame_bytes - lay->header_bytes;
    if (pb <= 0 || (pb % 8) || (lay->header_bytes % 4) || (payload_offset % 4)) return SWSGPU_EINVAL;
    if (lay->header_bytes > 0 && payload_offset != 0) return SWSGPU_EINVAL;
+   std::string why;
+   const int ntrack = track_format(lay->format) ? track_layout_ok(*lay, why) : 0;
+   if (track_format(lay->format) && (!ntrack || payload_offset % (ntrack / 8))) return SWSGPU_EINVAL;
    cudaStream_t st = (cudaStream_t)cuda_stream;
    StreamIn si;
    si.data = (const uint8_t *)d_raw;
@@ -2190,7 +2226,21 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    int2 *d_valid = nullptr;
    int *d_any = nullptr;
    unsigned long long *d_cnt = nullptr;
-   if (cudaMalloc(&d_valid, sizeof(int2) * si.nframes) != cudaSuccess) return SWSGPU_ECUDA;
+   uint32_t *d_trk = nullptr;
+   if (ntrack) {
+      // VLBA / Mark4 track-words into Mark5B's sample layout first
+      if (cudaMalloc(&d_trk, (nbytes + 3) / 4 * 4 + 16) != cudaSuccess) return SWSGPU_ECUDA;
+      if (launch_track_turn(st, (const uint8_t *)d_raw, (long long)nbytes, si.grid_offset, ntrack, lay->nbit,
+                            lay->nchan, lay->format, d_trk) != cudaSuccess) {
+         cudaFree(d_trk);
+         return SWSGPU_ECUDA;
+      }
+      si.data = (const uint8_t *)d_trk;
+   }
+   if (cudaMalloc(&d_valid, sizeof(int2) * si.nframes) != cudaSuccess) {
+      if (d_trk) cudaFree(d_trk);
+      return SWSGPU_ECUDA;
+   }
    cudaMalloc(&d_any, sizeof(int));
    cudaMalloc(&d_cnt, sizeof(unsigned long long));
    cudaMemsetAsync(d_any, 0, sizeof(int), st);
@@ -2205,6 +2255,7 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    cudaFree(d_valid);
    cudaFree(d_any);
    cudaFree(d_cnt);
+   if (d_trk) cudaFree(d_trk);
    if (e != cudaSuccess) {
       g_create_error = cudaGetErrorString(e);
       return SWSGPU_ECUDA;

@@ -37,7 +37,8 @@ struct StreamIn {
 __host__ __device__ inline float4 level_table(int format, int nbit)
 {
    const float H = 3.3359f;  // OPTIMAL_2BIT_HIGH (mark5access) = the reference's 2-bit high level
-   if (format == SWSGPU_FMT_MARK5B) {
+   if (format == SWSGPU_FMT_MARK5B || format == SWSGPU_FMT_VLBA || format == SWSGPU_FMT_MARK4) {
+      // the track formats are turned into Mark5B's sample layout first
       if (nbit == 2) return make_float4(-H, 1.0f, -1.0f, H);
       return make_float4(1.0f, -1.0f, 0.0f, 0.0f);
    }
@@ -51,6 +52,52 @@ __host__ __device__ inline float4 level_table(int format, int nbit)
    if (nbit == 2) return make_float4(-H, -1.0f, 1.0f, H);
    if (nbit == 8) return make_float4(1.0f / 128.0f, -255.0f / 256.0f, 0.0f, 0.0f);
    return make_float4(-1.0f, 1.0f, 0.0f, 0.0f);
+}
+
+__host__ __device__ inline bool track_format(int format)
+{
+   return format == SWSGPU_FMT_VLBA || format == SWSGPU_FMT_MARK4;
+}
+
+// Tracks of sample j (< fanout) of channel c in a track-word of a VLBA /
+// Mark4 mode: the sign bit's track, and for 2-bit samples the magnitude
+// bit's (-1 for 1-bit).  Up to 16 tracks a channel's tracks are contiguous
+// (sign tracks then magnitude tracks, f of each); with 32 and 64 tracks the
+// channels interleave within groups of 32 tracks (4 bytes): a group holds
+// 32 / (nbit f) channels, and the rules below give, per group, the
+// assignment mark5access's decoders read (mark5_format_vlba.c and
+// mark5_format_mark4.c: the 32/64-track decoders, their byte reordering of
+// fanout-4 2-bit modes included).
+__host__ __device__ inline int2 track_of(int ntrack, int fanout, int nbit, int c, int j)
+{
+   const int f = fanout;
+   if (ntrack <= 16) {
+      if (nbit == 1) return make_int2(f * c + j, -1);
+      const int s = 2 * f * c + j;
+      return make_int2(s, s + f);
+   }
+   if (nbit == 1) {
+      if (f == 1) {
+         const int g = c / 32, q = c % 32;
+         return make_int2(32 * g + 2 * (q % 16) + q / 16, -1);
+      }
+      if (f == 2) {
+         const int g = c / 16, q = c % 16;
+         return make_int2(32 * g + 4 * (q % 8) + q / 8 + 2 * j, -1);
+      }
+      const int g = c / 8, q = c % 8;
+      return make_int2(32 * g + 8 * (q % 4) + q / 4 + 2 * j, -1);
+   }
+   if (f == 1) {
+      const int g = c / 16, q = c % 16, s = 32 * g + 4 * (q % 8) + q / 8;
+      return make_int2(s, s + 2);
+   }
+   if (f == 2) {
+      const int g = c / 8, q = c % 8, s = 32 * g + 8 * (q % 4) + q / 4 + 2 * j;
+      return make_int2(s, s + 4);
+   }
+   const int g = c / 4, q = c % 4, s = 32 * g + 16 * (q % 2) + q / 2 + 2 * j;
+   return make_int2(s, s + 8);
 }
 
 // Reverses the order of the four 2-bit fields of every byte of w.

@@ -71,6 +71,9 @@ extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void
    const int pb = lay->frame_bytes - lay->header_bytes;
    if (pb <= 0 || (pb % 8) || (lay->header_bytes % 4) || (payload_offset % 4)) return SWSGPU_EINVAL;
    if (lay->header_bytes > 0 && payload_offset != 0) return SWSGPU_EINVAL;
+   // track formats (VLBA, Mark4) are decoded through a conversion buffer of
+   // the data's size, which this entry has no room for
+   if (lay->format == SWSGPU_FMT_VLBA || lay->format == SWSGPU_FMT_MARK4) return SWSGPU_EINVAL;
    if (nsamp == 0) {
       if (nvalid) *nvalid = 0;
       return SWSGPU_OK;

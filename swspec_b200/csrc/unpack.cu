@@ -83,8 +83,14 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
    const int big = 1 << 30;
    int vs = 0, ve = big;
    const int nword = s.payload_bytes / 8;
-   if (s.format >= SWSGPU_FMT_RAW_SIGNED) {
+   if (s.format == SWSGPU_FMT_RAW_SIGNED || s.format == SWSGPU_FMT_RAW_UNSIGNED) {
       // raw sampler data: the reference's raw unpackers blank nothing
+   } else if (s.format == SWSGPU_FMT_VLBA) {
+      // the frame headers are not part of the payload stream
+   } else if (s.format == SWSGPU_FMT_MARK4) {
+      // data replacement: the frame's first 160 track-words (of ntrack / 8
+      // bytes) are its header and decode as blanked samples
+      vs = 160 * (s.payload_bytes / 20000);
    } else if (s.format == SWSGPU_FMT_VDIF) {
       // VDIF: invalid bit in header word 0 (framed layouts only), then fill check
       bool bad = false;
@@ -105,6 +111,86 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
    }
    valid[f] = make_int2(vs, ve);
    if (!(vs <= 0 && ve >= s.payload_bytes)) atomicOr(blank_any, 1);
+}
+
+// The VLBA modulation sequence: the 16-stage feedback shift register of the
+// VLBA recording format (feedback from stages 10, 12, 13 and 15, all ones at
+// the start of a frame, one extra step after every eighth output, which
+// skips the parity bit), one bit per track-word of a frame; every sample of
+// track-word i is negated where bit i is set.  Generated at compile time.
+struct VlbaModulation {
+   uint32_t w[625];
+};
+constexpr VlbaModulation make_vlba_modulation()
+{
+   VlbaModulation m{};
+   uint32_t reg = 0xFFFFu;  // bit n = stage n
+   for (int i = 0; i < 20000; i++) {
+      uint32_t k = ((reg >> 10) ^ (reg >> 12) ^ (reg >> 13) ^ (reg >> 15)) & 1u;
+      reg = ((reg << 1) | k) & 0xFFFFu;
+      if (k) m.w[i >> 5] |= 1u << (i & 31);
+      if (i % 8 == 7) {
+         k = ((reg >> 10) ^ (reg >> 12) ^ (reg >> 13) ^ (reg >> 15)) & 1u;
+         reg = ((reg << 1) | k) & 0xFFFFu;
+      }
+   }
+   return m;
+}
+__constant__ VlbaModulation c_vlba_mod = make_vlba_modulation();
+
+// Track-word stream (VLBA payload or Mark4 frames) -> Mark5B's sample layout:
+// sample-time t of the chunk takes bits [t B, t B + B) of the output, B =
+// nchan * nbit, channel c at bit offset c * nbit, 2-bit codes sign + 2 mag.
+// The output has the input's size and frame grid (a track-word of ntrack
+// bits is `fanout` sample-times of B bits), so frame validity, blanking and
+// the corner turn treat it as Mark5B payload.  One thread per output word;
+// the chunk starts on a track-word (grid_offset a multiple of ntrack / 8).
+__global__ void k_track_turn(const uint8_t *__restrict__ in, long long nbytes, long long grid_offset, int ntrack,
+                             int fanout, int nbit, int nchan, int vlba, uint32_t *__restrict__ out)
+{
+   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (k >= (nbytes + 3) / 4) return;
+   const int B = nchan * nbit;  // bits per sample-time, <= 32
+   const int S = 32 / B;        // sample-times per output word
+   const int tb = ntrack / 8;   // bytes per track-word
+   const long long W0 = 8 * grid_offset / ntrack;         // grid track-word of the chunk's first byte
+   const long long T0 = W0 * fanout + 32 * k / B;        // grid sample-time of the word's first sample
+   const uint32_t all = (1u << nbit) - 1u;
+   uint32_t word = 0;
+   long long cur = -1;
+   unsigned long long tw = 0;
+   for (int t = 0; t < S; t++) {
+      const long long T = T0 + t;
+      const long long W = T / fanout;
+      const int j = (int)(T - W * fanout);
+      if (W != cur) {
+         cur = W;
+         tw = 0;
+         const long long a = (W - W0) * tb;
+         if (a + tb <= nbytes)
+            for (int b = 0; b < tb; b++) tw |= (unsigned long long)in[a + b] << (8 * b);
+      }
+      const int i = (int)(W % 20000);
+      const uint32_t flip = (vlba && ((c_vlba_mod.w[i >> 5] >> (i & 31)) & 1u)) ? all : 0u;
+      for (int c = 0; c < nchan; c++) {
+         const int2 tr = track_of(ntrack, fanout, nbit, c, j);
+         uint32_t code = (uint32_t)(tw >> tr.x) & 1u;
+         if (nbit == 2) code |= ((uint32_t)(tw >> tr.y) & 1u) << 1;
+         word |= (code ^ flip) << (t * B + c * nbit);
+      }
+   }
+   out[k] = word;
+}
+
+cudaError_t launch_track_turn(cudaStream_t st, const uint8_t *in, long long nbytes, long long grid_offset,
+                              int ntrack, int nbit, int nchan, int format, uint32_t *out)
+{
+   const long long nw = (nbytes + 3) / 4;
+   if (nw == 0) return cudaSuccess;
+   const int fanout = ntrack / (nchan * nbit);
+   k_track_turn<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(in, nbytes, grid_offset, ntrack, fanout, nbit, nchan,
+                                                              format == SWSGPU_FMT_VLBA ? 1 : 0, out);
+   return cudaGetLastError();
 }
 
 // Corner turn into a phase-decimated code layout.  For decimation D (the

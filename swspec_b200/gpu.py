@@ -13,7 +13,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libswsgpu.so")
 
-FMT_MARK5B, FMT_VDIF, FMT_RAW_SIGNED, FMT_RAW_UNSIGNED = 0, 1, 2, 3
+FMT_MARK5B, FMT_VDIF, FMT_RAW_SIGNED, FMT_RAW_UNSIGNED, FMT_VLBA, FMT_MARK4 = 0, 1, 2, 3, 4, 5
 WIN = {"none": 0, "cosine": 1, "cosine2": 2, "hamming": 3, "hann": 4, "blackman": 5,
        "blackmanharris": 6}
 PREC_FP32, PREC_TCSPLIT, PREC_TCSPLIT_ALL = 0, 1, 2
@@ -124,8 +124,13 @@ def _check(rc: int, h=None) -> None:
 
 
 def layout(fmt: str, nchan: int, nbit: int, framed: bool = True) -> Layout:
-    """Layout of a Mark5B or VDIF stream ("mark5b" / "vdif:<payload>"), or of
-    header-free raw sampler data ("raw_signed" / "raw_unsigned")."""
+    """Layout of a Mark5B or VDIF stream ("mark5b" / "vdif:<payload>"), of
+    header-free raw sampler data ("raw_signed" / "raw_unsigned"), or of a
+    track format ("vlba:<tracks>": header-free payload; "mark4:<tracks>":
+    whole frames) of 20000 track-words per frame."""
+    if fmt.lower().startswith(("vlba", "mark4")):
+        ntrack = int(fmt.split(":")[1])
+        return Layout(FMT_VLBA if fmt.lower().startswith("vlba") else FMT_MARK4, nchan, nbit, 2500 * ntrack, 0)
     if fmt.lower().startswith("raw"):
         code = FMT_RAW_SIGNED if fmt.lower() == "raw_signed" else FMT_RAW_UNSIGNED
         return Layout(code, nchan, nbit, 8192, 0)

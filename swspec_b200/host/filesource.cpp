@@ -20,8 +20,14 @@ int FileSource::open(const std::string &uri)
    const Settings &s = *cfg_;
    const bool mark5b = (s.sourceformat == Mark5B || s.sourceformat == Mk5B);
    const bool raw = (s.sourceformat == RawSigned || s.sourceformat == RawUnsigned);
+   const bool tracks = (s.sourceformat == VLBA || s.sourceformat == MKIV);
+   const int tb = s.layout.frame_bytes / 20000;  // track formats: bytes per track-word
    if (raw) header_bytes_ = 0;
    else if (s.sourceformat == iBOB) header_bytes_ = 4;  // packet sequence header (src/FileSource.cpp:53-57)
+   // VLBA frames are 20160 track-words with the payload at 96 .. 20095
+   // (mark5access's framebytes and payloadoffset): 160 track-words lie
+   // between two payloads; Mark4 frames (data replacement) are read whole
+   else if (tracks) header_bytes_ = s.sourceformat == VLBA ? 160 * tb : 0;
    else header_bytes_ = mark5b ? 16 : (s.sourceformat_str.size() > 4 && s.sourceformat_str[4] == '_' ? 32 : 16);
    frame_bytes_ = header_bytes_ + s.layout.frame_bytes;
    ifile_.open(uri.c_str(), std::ios::binary | std::ios::in);
@@ -77,6 +83,33 @@ int FileSource::open(const std::string &uri)
          }
       }
    }
+   if (tracks) {
+      // the frame sync word: 32 track-words of all ones, two frames apart
+      // (as mark5access's findfirstframe); VLBA frames start with it, Mark4
+      // frames carry it after 64 track-words of auxiliary data
+      const int64_t sync_len = 32 * tb, sync_at = s.sourceformat == VLBA ? 0 : 64 * tb;
+      std::vector<unsigned char> win((size_t)(3 * frame_bytes_ + sync_len));
+      ifile_.read(reinterpret_cast<char *>(win.data()), win.size());
+      const int64_t got = ifile_.gcount();
+      auto ones = [&](int64_t at) {
+         for (int64_t k = 0; k < sync_len; k++)
+            if (win[at + k] != 0xFF) return false;
+         return true;
+      };
+      int64_t found = -1;
+      for (int64_t i = 0; i + frame_bytes_ + sync_len <= got && found < 0; i++)
+         if (ones(i) && ones(i + frame_bytes_)) found = i;
+      if (found < 0) {
+         *cfg_->tlog << "FileSource: no " << (s.sourceformat == VLBA ? "VLBA" : "Mark4") << " frame found in " << uri
+                     << std::endl;
+         return -1;
+      }
+      // the first whole frame
+      first_frame_ = found >= sync_at ? found - sync_at : found - sync_at + frame_bytes_;
+      if (first_frame_ > 0)
+         *cfg_->tlog << "FileSource: first frame at byte " << first_frame_ << " (" << first_frame_
+                     << " leading bytes skipped)" << std::endl;
+   }
    // skip whole seconds (FileSource.cpp:132-153)
    int64_t seek = first_frame_;
    if (s.seconds_to_skip > 0) {
@@ -98,6 +131,11 @@ int FileSource::open(const std::string &uri)
    got_eof_ = false;
    pending_header_ = true;
    in_frame_ = 0;
+   if (s.sourceformat == VLBA) {
+      // the first payload follows the frame's 96-track-word header
+      ifile_.seekg(seek + 96 * tb, std::ios::beg);
+      pending_header_ = false;
+   }
    return 0;
 }
 

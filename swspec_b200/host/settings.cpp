@@ -96,6 +96,21 @@ int parse_format(Settings &s, std::string &err)
       s.layout = {SWSGPU_FMT_VDIF, nch, nbit, payload, 0};
       s.source_channels = nch;
       s.bits_per_sample = nbit;
+   } else if ((strncasecmp(f.c_str(), "VLBA1_", 6) == 0 || strncasecmp(f.c_str(), "MKIV1_", 6) == 0) &&
+              sscanf(f.c_str() + 6, "%d-%d-%d-%d", &payload, &mbps, &nch, &nbit) == 4) {
+      // mark5access's VLBA1_<fanout>-<Mbps>-<nchan>-<nbit> and MKIV1_ modes:
+      // frames of 20000 track-words of nchan * nbit * fanout tracks; the GPU
+      // core takes VLBA payloads with the headers removed, Mark4 frames whole
+      const bool vlba = strncasecmp(f.c_str(), "VLBA1_", 6) == 0;
+      const int fanout = payload, ntrack = nch * nbit * fanout;
+      if ((fanout != 1 && fanout != 2 && fanout != 4) || (ntrack != 8 && ntrack != 16 && ntrack != 32 && ntrack != 64)) {
+         err = "source format '" + f + "': fanout 1, 2 or 4 and 8, 16, 32 or 64 tracks";
+         return -1;
+      }
+      s.sourceformat = vlba ? VLBA : MKIV;
+      s.layout = {vlba ? SWSGPU_FMT_VLBA : SWSGPU_FMT_MARK4, nch, nbit, 2500 * ntrack, 0};
+      s.source_channels = nch;
+      s.bits_per_sample = nbit;
    } else if (strcasecmp(f.c_str(), "Mk5B") == 0) {
       // the reference's framed Mark5B: 16-byte headers, 10000-byte payloads
       s.sourceformat = Mk5B;
@@ -116,8 +131,8 @@ int parse_format(Settings &s, std::string &err)
       s.sourceformat = iBOB;
       s.layout = {SWSGPU_FMT_RAW_SIGNED, s.source_channels, s.bits_per_sample, 4096, 0};
    } else {
-      err = "source format '" + f + "' is not decoded by the GPU core (Mark5B-*, VDIF_*, Mk5B, VDIF, RawSigned, "
-            "RawUnsigned, iBob)";
+      err = "source format '" + f + "' is not decoded by the GPU core (Mark5B-*, VDIF_*, VLBA1_*, MKIV1_*, Mk5B, "
+            "VDIF, RawSigned, RawUnsigned, iBob)";
       return -1;
    }
    if (nbit != 0 && nbit != 1 && nbit != 2 && nbit != 8) {

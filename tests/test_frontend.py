@@ -155,3 +155,47 @@ def test_vdif_thread_selection(tmp_path):
     r, info, got = _read(tmp_path, inter, fmt="VDIF_8000-64-1-2", extra="VdifThread = 1\n")
     assert r.returncode == 0, r.stderr
     assert got == pays[1]
+
+
+def _track_file(kind: str, ntrack: int, nfr: int, lead: int, seed: int):
+    """A VLBA (20160 track-words per frame: sync, time code, payload of
+    20000, 64 trailing) or Mark4 (20000 per frame: 64 auxiliary, sync, time
+    code, data) recording after `lead` bytes of other data; returns the file
+    and the payload stream the GPU core takes."""
+    tb = ntrack // 8
+    rng = np.random.default_rng(seed)
+    frames, payload = [], []
+    for _ in range(nfr):
+        if kind == "VLBA":
+            data = rng.integers(0, 256, 20000 * tb, dtype=np.uint8)
+            fr = np.concatenate([np.full(32 * tb, 0xFF, np.uint8), np.zeros(64 * tb, np.uint8), data,
+                                 np.zeros(64 * tb, np.uint8)])
+            payload.append(data)
+        else:
+            data = rng.integers(0, 256, 19840 * tb, dtype=np.uint8)
+            fr = np.concatenate([np.zeros(64 * tb, np.uint8), np.full(32 * tb, 0xFF, np.uint8),
+                                 np.zeros(64 * tb, np.uint8), data])
+            payload.append(fr)
+        frames.append(fr)
+    head = rng.integers(0, 200, lead, dtype=np.uint8)
+    return np.concatenate([head] + frames).tobytes(), np.concatenate(payload).tobytes()
+
+
+def test_vlba_frames_headers_removed(tmp_path):
+    data, pay = _track_file("VLBA", 32, 6, 1000, 8)
+    r, info, got = _read(tmp_path, data, fmt="VLBA1_2-256-8-2")
+    assert r.returncode == 0, r.stderr
+    assert got == pay
+    assert "leading bytes skipped" in r.stderr
+
+
+def test_mark4_frames_read_whole(tmp_path):
+    data, pay = _track_file("MKIV", 16, 5, 0, 9)
+    r, info, got = _read(tmp_path, data, fmt="MKIV1_1-256-8-2")
+    assert r.returncode == 0, r.stderr
+    assert got == pay
+
+
+def test_track_format_settings(tmp_path):
+    s = _settings(tmp_path, fmt="MKIV1_2-512-8-2")
+    assert s["source_channels"] == 8 and s["bits_per_sample"] == 2

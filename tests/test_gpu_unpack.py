@@ -141,3 +141,37 @@ def test_raw_formats_bit_exact(gpu, fmt, nchan, nbit):
         ref = O.decode(ofmt, nchan, nbit, raw, nsamp, c)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (fmt, nchan, nbit, c)
         assert nv == nsamp
+
+
+# VLBA / Mark4 modes: (mark5access format, tracks); fanouts 1, 2 and 4, 1- and
+# 2-bit, 8 to 64 tracks; MKIV1_2-512-8-2 is the reference's own example mode
+# (src/democonfig.ini)
+TRACK_MODES = [("VLBA1_1-128-8-2", 16), ("VLBA1_2-256-8-2", 32), ("VLBA1_4-512-8-2", 64),
+               ("VLBA1_2-512-32-1", 64), ("VLBA1_4-64-2-1", 8), ("MKIV1_2-512-8-2", 32),
+               ("MKIV1_4-256-4-2", 32), ("MKIV1_1-256-32-1", 32), ("MKIV1_2-1024-16-2", 64),
+               ("MKIV1_1-64-4-2", 8)]
+
+
+@pytest.mark.parametrize("fmt,ntrack", TRACK_MODES)
+def test_track_formats_bit_exact(gpu, fmt, ntrack):
+    """Every channel of three frames of random track-words, against
+    mark5access's header-free unpack of the same bytes (its VLBA modulation
+    and Mark4 header blanking included), float bit for float bit; then the
+    same from the second frame on through a payload offset of one frame."""
+    info = O.m5_format_info(fmt)
+    nchan, nbit = info["nchan"], info["nbit"]
+    fanout = ntrack // (nchan * nbit)
+    rng = np.random.default_rng(ntrack * 10 + nchan)
+    frame = 2500 * ntrack
+    pay = rng.integers(0, 256, size=3 * frame, dtype=np.uint8).tobytes()
+    nsamp = 3 * 20000 * fanout
+    ref, nref = O.m5_unpack(fmt, pay, nsamp)
+    lay = gpu.layout(("vlba:" if fmt.startswith("VLBA") else "mark4:") + str(ntrack), nchan, nbit)
+    for c in range(nchan):
+        got, nv = _gpu_decode(gpu, lay, pay, c, nsamp)
+        assert np.array_equal(got.view(np.uint32), ref[c].view(np.uint32)), (fmt, c)
+        assert nv == nref, (fmt, nv, nref)
+    # from frame 1: the payload offset keeps the frame grid (modulation, header)
+    ref1, _ = O.m5_unpack(fmt, pay[frame:], 2 * 20000 * fanout)
+    got1, _ = _gpu_decode(gpu, lay, pay[frame:], nchan - 1, 2 * 20000 * fanout, payload_offset=frame)
+    assert np.array_equal(got1.view(np.uint32), ref1[nchan - 1].view(np.uint32)), fmt

@@ -348,3 +348,45 @@ BaseFilename1 = b_%channel%
     assert np.max(np.abs(a1 - ra[:, 1]) / ra[:, 1]) < 2e-6
     xc = xp[..., 0] + 1j * xp[..., 1]
     assert np.max(np.abs(xc - rx) / np.sqrt(ra[:, 0] * ra[:, 1])) < 2e-6
+
+
+@pytest.mark.gpu
+def test_cli_mark4_spectra_per_buffer(tmp_path, gpu):
+    """A Mark4 recording in the reference's own example mode
+    (MKIV1_2-512-8-2: 32 tracks, 8 channels, 2-bit, fanout 2) through the
+    front end (frames read whole after 1000 leading bytes) and the GPU core:
+    channel 3's spectra, four per buffer, against the FP64 oracle on
+    mark5access's decode of the same frames (header track-words blanked)."""
+    from test_frontend import _track_file
+    N = 8192
+    data, pay = _track_file("MKIV", 32, 60, 1000, 12)
+    (tmp_path / "in.m4").write_bytes(data)
+    ini = _ini(tmp_path, f"""[Spectrometer]
+FFTpoints = {N}
+FFTIntegrationTimeSec = 0.004096
+FFToverlapFactor = 1
+BandwidthHz = 16e6
+WindowType = Hann
+SourceFormat = MKIV1_2-512-8-2
+UseFile1Channel = 3
+MaxSourceBufferMB = 1
+BaseFilename1 = m4_%channel%
+""")
+    s = _settings(ini, 1)
+    rawbuf, cof, nsp = s["rawbuf_size"], s["core_overlapped_ffts"], s["max_spectra_per_buffer"]
+    assert nsp >= 1 and s["max_buffers_per_spectrum"] == 0, s
+    _run_cli(tmp_path, ini, ["in.m4"])
+    S = N // 2 + 1
+    nbuf = len(pay) // rawbuf
+    assert nbuf >= 3
+    per_buf = rawbuf * 8 // 16                       # samples per channel in a buffer
+    dec, _ = O.m5_unpack("MKIV1_2-512-8-2", pay, nbuf * per_buf)
+    ra = []
+    for b in range(nbuf):
+        cfg = O.make_cfg(N, core_overlapped_ffts=cof, num_sources=1, window=O.W_HANN, nthreads=os.cpu_count() or 1)
+        a, _, _, n = O.domaths(cfg, [dec[2, b * per_buf:(b + 1) * per_buf]])
+        ra.append(a[:nsp, 0])
+    ra = np.concatenate(ra)
+    got = np.fromfile(tmp_path / "m4_3_swspec.bin", dtype=np.float32).reshape(-1, S)
+    assert got.shape[0] == ra.shape[0] == nbuf * nsp
+    assert np.max(np.abs(got - ra) / ra) < 2e-6
