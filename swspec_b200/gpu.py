@@ -232,21 +232,27 @@ class Core:
         if dest is None:
             _check(lib().swsgpu_submit(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs), self.h)
             return
-        key = tuple(None if a is None else a.ctypes.data for a in (tuple(dest) + (None,) * 4)[:4])
-        if getattr(self, "_dest_key", None) != key:
-            self._dest_key = key
+        # the destination descriptor is rebuilt only when other arrays come
+        # (the arrays are kept referenced, so identity means same memory)
+        prev = getattr(self, "_dest_arrays", None)
+        if prev is None or len(prev) != len(dest) or any(a is not b for a, b in zip(dest, prev)):
+            self._dest_arrays = tuple(dest)
+            key = tuple(None if a is None else a.ctypes.data for a in (tuple(dest) + (None,) * 4)[:4])
             self._dest = Outputs(*key)
+            self._dest_ref = C.byref(self._dest)
         _check(lib().swsgpu_submit_out(self.h, self._sub_ptrs, self._sub_sizes, self._sub_offs,
-                                       C.byref(self._dest)), self.h)
+                                       self._dest_ref), self.h)
 
     def set_sizes(self, sizes: list[int]) -> None:
         self._sizes = list(sizes)
         self._sub_n = 0
 
     def wait(self, timeout_ms: int = 60000) -> int:
-        ns = C.c_int()
-        _check(lib().swsgpu_wait(self.h, timeout_ms, C.byref(ns)), self.h)
-        return ns.value
+        if getattr(self, "_wait_ns", None) is None:
+            self._wait_ns = C.c_int()
+            self._wait_ref = C.byref(self._wait_ns)
+        _check(lib().swsgpu_wait(self.h, timeout_ms, self._wait_ref), self.h)
+        return self._wait_ns.value
 
     def fetch_into(self, auto: np.ndarray, xpol: np.ndarray | None = None,
                    pcal: np.ndarray | None = None, tones: np.ndarray | None = None) -> None:
