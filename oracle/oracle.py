@@ -214,7 +214,11 @@ def m5_unpack(fmt: str, payload: bytes, nsamp: int) -> tuple[np.ndarray, int]:
     r = ref()
     info = m5_format_info(fmt)
     out = np.zeros((info["nchan"], nsamp), dtype=np.float32)
-    buf = np.frombuffer(payload, dtype=np.uint8).copy()
+    # mark5_unpack moves on to the frame after the last sample it decodes
+    # and runs the blanker there: zero bytes of one frame (at most 64 tracks
+    # x 2520 bytes) past the payload keep those reads inside the buffer
+    buf = np.zeros(len(payload) + 64 * 2520, dtype=np.uint8)
+    buf[:len(payload)] = np.frombuffer(payload, dtype=np.uint8)
     rc = r.m5ref_unpack(fmt.encode(), buf.ctypes.data, nsamp, info["nchan"], out.ctypes.data)
     return out, rc
 

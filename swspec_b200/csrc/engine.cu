@@ -875,14 +875,6 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       const swsgpu_layout &L = c.layout[s];
       StreamIn si;
       si.data = (const uint8_t *)d_raw[s];
-      if (track_format(L.format)) {
-         // VLBA / Mark4 track-words into Mark5B's sample layout (same size and grid)
-         CK(h, x.d_trk[s].ensure((raw_bytes[s] + 3) / 4 * 4 + 16));
-         CK(h, launch_track_turn(st, (const uint8_t *)d_raw[s], (long long)raw_bytes[s], grid_off[s],
-                                 payload_bytes(L) / 2500, L.nbit, L.nchan, L.format, (uint32_t *)x.d_trk[s].p));
-         si.data = (const uint8_t *)x.d_trk[s].p;
-         launches++;
-      }
       si.nbytes = (long long)raw_bytes[s];
       si.grid_offset = grid_off[s];
       si.frame_bytes = L.frame_bytes;
@@ -892,12 +884,22 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
       si.nbit = L.nbit;
       si.format = L.format;
       si.msb2 = is_msb2(L);
+      set_zones(si);
       const long long last_v = si.grid_offset + ((nsamp * (long long)L.nchan * L.nbit - 1) >> 3);
       si.nframes = last_v / si.payload_bytes + 1;
-      CK(h, x.d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes));
+      CK(h, x.d_valid[s].ensure(sizeof(int2) * (size_t)si.nframes * si.zpf));
       k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(
           si, (int2 *)x.d_valid[s].p, (int *)x.d_blank_any.p + s);
       launches++;
+      if (track_format(L.format)) {
+         // VLBA / Mark4 track-words into Mark5B's sample layout (same size
+         // and grid; validity above was read from the track-words)
+         CK(h, x.d_trk[s].ensure((raw_bytes[s] + 3) / 4 * 4 + 16));
+         CK(h, launch_track_turn(st, (const uint8_t *)d_raw[s], (long long)raw_bytes[s], grid_off[s],
+                                 payload_bytes(L) / 2500, L.nbit, L.nchan, L.format, (uint32_t *)x.d_trk[s].p));
+         si.data = (const uint8_t *)x.d_trk[s].p;
+         launches++;
+      }
       const std::vector<int> &chans = h->chans_of[s];
       if (chans.empty()) continue;
       uint32_t *codes = (uint32_t *)x.d_codes.p + (size_t)h->first_code[s] * code_words;
@@ -2213,6 +2215,7 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    si.nbit = lay->nbit;
    si.format = lay->format;
    si.msb2 = is_msb2(*lay);
+   set_zones(si);
    if (nsamp == 0) {
       if (nvalid) *nvalid = 0;
       return SWSGPU_OK;
@@ -2227,25 +2230,32 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    int *d_any = nullptr;
    unsigned long long *d_cnt = nullptr;
    uint32_t *d_trk = nullptr;
+   if (cudaMalloc(&d_valid, sizeof(int2) * si.nframes * si.zpf) != cudaSuccess) return SWSGPU_ECUDA;
+   if (cudaMalloc(&d_any, sizeof(int)) != cudaSuccess || cudaMalloc(&d_cnt, sizeof(unsigned long long)) != cudaSuccess) {
+      cudaFree(d_valid);
+      if (d_any) cudaFree(d_any);
+      return SWSGPU_ECUDA;
+   }
+   cudaMemsetAsync(d_any, 0, sizeof(int), st);
+   cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
+   // validity from the stream's own bytes (the track-words, for VLBA / Mark4)
+   k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(si, d_valid, d_any);
    if (ntrack) {
-      // VLBA / Mark4 track-words into Mark5B's sample layout first
-      if (cudaMalloc(&d_trk, (nbytes + 3) / 4 * 4 + 16) != cudaSuccess) return SWSGPU_ECUDA;
-      if (launch_track_turn(st, (const uint8_t *)d_raw, (long long)nbytes, si.grid_offset, ntrack, lay->nbit,
-                            lay->nchan, lay->format, d_trk) != cudaSuccess) {
-         cudaFree(d_trk);
+      // VLBA / Mark4 track-words into Mark5B's sample layout
+      cudaError_t e = cudaMalloc(&d_trk, (nbytes + 3) / 4 * 4 + 16);
+      if (e == cudaSuccess)
+         e = launch_track_turn(st, (const uint8_t *)d_raw, (long long)nbytes, si.grid_offset, ntrack, lay->nbit,
+                               lay->nchan, lay->format, d_trk);
+      if (e != cudaSuccess) {
+         cudaStreamSynchronize(st);
+         cudaFree(d_valid);
+         cudaFree(d_any);
+         cudaFree(d_cnt);
+         if (d_trk) cudaFree(d_trk);
          return SWSGPU_ECUDA;
       }
       si.data = (const uint8_t *)d_trk;
    }
-   if (cudaMalloc(&d_valid, sizeof(int2) * si.nframes) != cudaSuccess) {
-      if (d_trk) cudaFree(d_trk);
-      return SWSGPU_ECUDA;
-   }
-   cudaMalloc(&d_any, sizeof(int));
-   cudaMalloc(&d_cnt, sizeof(unsigned long long));
-   cudaMemsetAsync(d_any, 0, sizeof(int), st);
-   cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
-   k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(si, d_valid, d_any);
    k_unpack_float<<<(unsigned)((nsamp + 255) / 256), 256, 0, st>>>(si, nsamp, chan,
                                                                     level_table(lay->format, lay->nbit),
                                                                     d_out, d_valid, d_cnt);

@@ -29,6 +29,10 @@ struct StreamIn {
    int format;   // SWSGPU_FMT_*
    long long nframes;  // frames touched by the chunk
    int msb2;     // 2-bit samples stored oldest-first from the byte's MSB (raw single channel)
+   // blanking zones: a frame's valid byte ranges are valid[f * zpf + (o >> zshift)]
+   // for payload byte o of frame f (set by set_zones)
+   int zpf;
+   int zshift;
 };
 
 // Level table of a format, as decode_level reads it: 1-bit {x, y}; 2-bit
@@ -57,6 +61,24 @@ __host__ __device__ inline float4 level_table(int format, int nbit)
 __host__ __device__ inline bool track_format(int format)
 {
    return format == SWSGPU_FMT_VLBA || format == SWSGPU_FMT_MARK4;
+}
+
+// mark5access blanks VLBA and Mark4 payloads by 32 KiB zones, each with its
+// own valid byte range (blanker_mark5.c:126-280, log2blankzonesize = 15);
+// the other formats have one range per frame.
+inline void set_zones(StreamIn &s)
+{
+   if (track_format(s.format)) {
+      s.zshift = 15;
+      s.zpf = (s.payload_bytes + 32767) >> 15;
+   } else {
+      s.zshift = 31;
+      s.zpf = 1;
+   }
+}
+__device__ __forceinline__ int2 valid_range(const StreamIn &s, const int2 *valid, long long f, int o)
+{
+   return valid[f * s.zpf + (o >> s.zshift)];
 }
 
 // Tracks of sample j (< fanout) of channel c in a track-word of a VLBA /

@@ -89,6 +89,7 @@ extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void
    si.nbit = lay->nbit;
    si.format = lay->format;
    si.msb2 = (lay->format >= SWSGPU_FMT_RAW_SIGNED && lay->nbit == 2 && lay->nchan == 1) ? 1 : 0;
+   set_zones(si);  // one range per frame for every format taken here
    const long long last_v = si.grid_offset + ((nsamp * (long long)lay->nchan * lay->nbit - 1) >> 3);
    si.nframes = last_v / pb + 1;
    // the fixed scratch holds one valid range per frame

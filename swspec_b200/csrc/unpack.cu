@@ -51,31 +51,50 @@ __device__ __forceinline__ uint32_t frame_word32(const StreamIn &s, long long f,
    return *reinterpret_cast<const uint32_t *>(s.data + a);
 }
 
-// blanker_mark5's findfirstinvalid / findfirstvalid over words [0, n)
-__device__ int m5_first_invalid(const StreamIn &s, long long f, int n)
+// blanker_mark5's findfirstinvalid / findfirstvalid: binary search of words
+// [b, e) of a frame for the start / end of its fill pattern, in bytes, with
+// the 32-bit straggler check just before the found word.
+__device__ int m5_first_invalid(const StreamIn &s, long long f, int b, int e)
 {
+   const int n = e - b;
    int i = n / 2, r = n - 1;
    for (int st = n / 4; st > 0; st >>= 1) {
-      if (frame_word64(s, f, i) == FILL64) { r = i; i -= st; }
+      if (frame_word64(s, f, b + i) == FILL64) { r = i; i -= st; }
       else i += st;
    }
-   r = 8 * r;
+   r = 8 * (b + r);
    if (frame_word32(s, f, r / 4 - 1) == FILL32) r -= 4;
    return r;
 }
-__device__ int m5_first_valid(const StreamIn &s, long long f, int n)
+__device__ int m5_first_valid(const StreamIn &s, long long f, int b, int e)
 {
+   const int n = e - b;
    int i = n / 2, r = n - 1;
    for (int st = n / 4; st > 0; st >>= 1) {
-      if (frame_word64(s, f, i) != FILL64) { r = i; i -= st; }
+      if (frame_word64(s, f, b + i) != FILL64) { r = i; i -= st; }
       else i += st;
    }
-   r = 8 * r;
+   r = 8 * (b + r);
    if (frame_word32(s, f, r / 4 - 2) == FILL32) r += 4;
    return r;
 }
 
-// Valid payload byte range of every frame the chunk touches.
+// Valid byte range of words [b, e) of frame f from the fill pattern at their
+// two ends (blanker_mark5.c:159-196).
+__device__ int2 fill_zone(const StreamIn &s, long long f, int b, int e)
+{
+   const int big = 1 << 30;
+   const bool startOK = frame_word64(s, f, b) != FILL64;
+   const bool endOK = frame_word64(s, f, e - 1) != FILL64;
+   if (startOK && endOK) return make_int2(0, big);
+   if (!startOK && !endOK) return make_int2(big, 0);
+   if (startOK) return make_int2(0, m5_first_invalid(s, f, b, e));
+   return make_int2(m5_first_valid(s, f, b, e), big);
+}
+
+// Valid payload byte ranges of every frame the chunk touches (zpf per frame).
+// Reads the stream's own bytes: for the track formats, the track-words
+// before they are turned.
 __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
 {
    long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,12 +104,31 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
    const int nword = s.payload_bytes / 8;
    if (s.format == SWSGPU_FMT_RAW_SIGNED || s.format == SWSGPU_FMT_RAW_UNSIGNED) {
       // raw sampler data: the reference's raw unpackers blank nothing
-   } else if (s.format == SWSGPU_FMT_VLBA) {
-      // the frame headers are not part of the payload stream
-   } else if (s.format == SWSGPU_FMT_MARK4) {
-      // data replacement: the frame's first 160 track-words (of ntrack / 8
-      // bytes) are its header and decode as blanked samples
-      vs = 160 * (s.payload_bytes / 20000);
+   } else if (track_format(s.format)) {
+      // VLBA (blanker_mark5 on the header-free payload) and Mark4
+      // (blanker_mark5.c:199-280, blanker_mark4, on the whole frame): 4096-word zones.
+      // Mark4 starts its first zone after the frame's 160 header
+      // track-words (20 n words, n = ntrack / 8 bytes per track-word) by
+      // moving the loop's start, so each later zone is examined 20 n words
+      // past its place on the 32 KiB grid the decoders look it up by; its
+      // first zone starts no earlier than byte 160 n.  The decoders test a
+      // track-word's first byte, so ranges are rounded up to whole
+      // track-words.
+      const int n = s.payload_bytes / 20000;
+      const bool mk4 = s.format == SWSGPU_FMT_MARK4;
+      int z = 0;
+      for (int b = 0; b < nword && z < s.zpf; b += 4096, z++) {
+         const int e = min(b + 4096, nword);
+         if (mk4 && b == 0) b = 20 * n;
+         int2 r = fill_zone(s, f, b, e);
+         if (mk4 && z == 0) r.x = max(r.x, 160 * n);
+         r.x = (r.x + n - 1) / n * n;
+         r.y = (r.y + n - 1) / n * n;
+         valid[f * s.zpf + z] = r;
+         if (!(r.x <= 32768 * z && r.y >= min(32768 * (z + 1), s.payload_bytes))) atomicOr(blank_any, 1);
+      }
+      for (; z < s.zpf; z++) valid[f * s.zpf + z] = make_int2(0, big);
+      return;
    } else if (s.format == SWSGPU_FMT_VDIF) {
       // VDIF: invalid bit in header word 0 (framed layouts only), then fill check
       bool bad = false;
@@ -102,12 +140,9 @@ __global__ void k_frame_valid(StreamIn s, int2 *valid, int *blank_any)
       else if (frame_word64(s, f, 0) == FILL64 || frame_word64(s, f, nword - 1) == FILL64) { vs = 0; ve = 0; }
    } else {
       // Mark5B: one 32 KiB zone per 10000-byte payload
-      bool startOK = frame_word64(s, f, 0) != FILL64;
-      bool endOK = frame_word64(s, f, nword - 1) != FILL64;
-      if (startOK && endOK) { vs = 0; ve = big; }
-      else if (!startOK && !endOK) { vs = big; ve = 0; }
-      else if (startOK) { vs = 0; ve = m5_first_invalid(s, f, nword); }
-      else { vs = m5_first_valid(s, f, nword); ve = big; }
+      const int2 r = fill_zone(s, f, 0, nword);
+      vs = r.x;
+      ve = r.y;
    }
    valid[f] = make_int2(vs, ve);
    if (!(vs <= 0 && ve >= s.payload_bytes)) atomicOr(blank_any, 1);
@@ -337,8 +372,8 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
                if (s.msb2) x = swap2_in_bytes(x);
                if (gw + i >= g.words_total) x = 0u;
                else if (any) {
-                  const int2 vr = valid[fu[u]];
                   const int oi = ou[u] + 4 * i;
+                  const int2 vr = valid_range(s, valid, fu[u], oi);
                   if (!(oi >= vr.x && oi < vr.y)) x = 0u;
                }
                sm[jl + i + piece / SPW] = x;  // one pad word per code word's block
@@ -395,8 +430,8 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             for (int i = 0; i < 4; i++) {
                if (w + i >= g.words_total) val[i] = 0u;
                else if (any) {
-                  const int2 vr = valid[fu[u]];
                   const int oi = ou[u] + 4 * i;
+                  const int2 vr = valid_range(s, valid, fu[u], oi);
                   if (!(oi >= vr.x && oi < vr.y)) {
                      val[i] = 0u;
                      atomicOr(&vbits[(j + i) >> 5], 1u << ((j + i) & 31));
@@ -419,7 +454,7 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
             if (a + 4 <= s.nbytes) val = __ldg(reinterpret_cast<const uint32_t *>(s.data + a));
             if (s.msb2) val = swap2_in_bytes(val);
             if (any) {
-               const int2 vr = valid[f];
+               const int2 vr = valid_range(s, valid, f, o);
                if (!(o >= vr.x && o < vr.y)) {
                   val = 0u;
                   atomicOr(&vbits[j >> 5], 1u << (j & 31));
@@ -558,7 +593,7 @@ __global__ void k_blank_bits(StreamIn s, long long nsamp, long long words_total,
       const long long v = s.grid_offset + 4 * w;
       const long long f = v / s.payload_bytes;
       const int o = (int)(v - f * s.payload_bytes);
-      const int2 vr = valid[f];
+      const int2 vr = valid_range(s, valid, f, o);
       if (!(o >= vr.x && o < vr.y)) m |= 1u << i;
    }
    blank[j] = m;
@@ -575,7 +610,7 @@ __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 lev
    long long v0 = s.grid_offset + ((t * (long long)s.nchan * nbit) >> 3);
    long long f = v0 / s.payload_bytes;
    int o = (int)(v0 - f * s.payload_bytes);
-   int2 vr = valid[f];
+   const int2 vr = valid_range(s, valid, f, o);
    float val = 0.0f;
    if (o >= vr.x && o < vr.y) {
       long long widx = bit >> 5;

@@ -56,3 +56,40 @@ def fill_zone(raw: bytes, frame: int, start: int, end: int, frame_bytes: int, hd
     base = frame * frame_bytes + hdr
     a[base + start: base + end] = bytes.fromhex("44332211") * ((end - start) // 4)
     return bytes(a)
+
+
+def track_fill_plants(ntrack: int):
+    """Fill-pattern regions (frame, start, end) of a header-free VLBA payload
+    or whole Mark4 frames (2500 * ntrack bytes) that exercise mark5access's
+    32 KiB blanking zones (blanker_mark5.c:126-280): zone 0 filled to its end
+    from a byte 4 past a 64-bit word (the 32-bit straggler check; at 64
+    tracks the range boundary falls inside a track-word), the second frame's
+    start (through the Mark4 header), its zone 1 whole, the first frame's
+    zone 1 from a mid point to its end on the 32 KiB grid (Mark4 examines
+    that zone 20 * ntrack / 8 words late and so blanks nothing there), a fill
+    that touches neither end of its zone (not blanked) and the third frame's
+    end."""
+    frame = 2500 * ntrack
+    z0e = min(32768, frame)
+    plants = [(0, 4 + 8 * (z0e // 24), z0e), (1, 0, 8 * (z0e // 40) + 4), (2, 4000, 8000),
+              (2, frame - 8004, frame)]
+    if frame > 65536:
+        plants.append((0, 32768 + 7820, 65536))
+    if frame > 32768:
+        plants.append((1, 32768, min(65536, frame)))
+    return plants
+
+
+def plant_track_fill(pay: bytes, ntrack: int, limit: int | None = None) -> bytes:
+    """`pay` with track_fill_plants(ntrack) written in; with `limit`, only the
+    plants whose zone (and the Mark4 blanker's shifted view of it) lies
+    inside the first `limit` bytes."""
+    frame = 2500 * ntrack
+    for f, a, b in track_fill_plants(ntrack):
+        if (f + 1) * frame > len(pay):
+            continue
+        z = a >> 15
+        if limit is not None and f * frame + min((z + 1) * 32768 + 20 * ntrack, frame) > limit:
+            continue
+        pay = fill_zone(pay, f, a, b, frame, 0)
+    return pay

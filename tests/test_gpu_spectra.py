@@ -417,15 +417,20 @@ def test_group_chunks_alternate_streams(gpu):
         assert np.max(np.abs(p - rp)) / np.max(np.abs(rp)) < 1e-6, g
 
 
-@pytest.mark.parametrize("fmt,ntrack,N,prec", [("MKIV1_2-512-8-2", 32, 4096, "fp32"),
-                                                ("VLBA1_4-512-8-2", 64, 4096, "fp32"),
-                                                ("MKIV1_2-512-8-2", 32, 8192, "tcsplit_all")])
-def test_track_format_spectra(gpu, fmt, ntrack, N, prec):
+@pytest.mark.parametrize("fmt,ntrack,N,prec,fill", [("MKIV1_2-512-8-2", 32, 4096, "fp32", False),
+                                                     ("VLBA1_4-512-8-2", 64, 4096, "fp32", False),
+                                                     ("MKIV1_2-512-8-2", 32, 8192, "tcsplit_all", False),
+                                                     ("MKIV1_2-512-8-2", 32, 4096, "fp32", True),
+                                                     ("VLBA1_4-512-8-2", 64, 4096, "fp32", True)])
+def test_track_format_spectra(gpu, fmt, ntrack, N, prec, fill):
     """VLBA / Mark4 track-words through the track turn, the corner turn and
     the FFT: auto spectra of two channels and their cross spectrum (16 FFTs)
     against the FP64 oracle on mark5access's decode of the same bytes
-    (Mark4 header track-words blanked, VLBA modulation removed)."""
+    (Mark4 header track-words blanked, VLBA modulation removed); with `fill`,
+    fill-pattern regions planted at zone ends blank whole track-words through
+    the blank bitmap as mark5access blanks them."""
     import oracle as O
+    from helpers import plant_track_fill
     info = O.m5_format_info(fmt)
     nchan, nbit = info["nchan"], info["nbit"]
     fanout = ntrack // (nchan * nbit)
@@ -433,6 +438,8 @@ def test_track_format_spectra(gpu, fmt, ntrack, N, prec):
     nfr = -(-N * cof // (20000 * fanout))
     rng = np.random.default_rng(N + ntrack)
     pay = rng.integers(0, 256, size=nfr * 2500 * ntrack, dtype=np.uint8).tobytes()
+    if fill:
+        pay = plant_track_fill(pay, ntrack, limit=N * cof * nchan * nbit // 8)
     lay = gpu.layout(("vlba:" if fmt.startswith("VLBA") else "mark4:") + str(ntrack), nchan, nbit)
     chans = [1, nchan - 2]
     cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=tuple((0, c) for c in chans), xpols=((0, 1),),
@@ -441,6 +448,8 @@ def test_track_format_spectra(gpu, fmt, ntrack, N, prec):
     run = pay[:N * cof * nchan * nbit // 8]            # exactly one spectrum's samples
     auto, xp, _, ns = core.run([run])
     dec, _ = O.m5_unpack(fmt, pay, nfr * 20000 * fanout)
+    if fill:
+        assert (dec[chans[0], :N * cof] == 0.0).any()
     ra, rx, _, nref = oracle_run([dec[c, :N * cof] for c in chans], N, "hann", 1, cof, nxpols=1)
     assert ns == nref == 1
     assert rel_err_auto(auto, ra) < REL_TOL

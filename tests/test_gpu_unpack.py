@@ -175,3 +175,33 @@ def test_track_formats_bit_exact(gpu, fmt, ntrack):
     ref1, _ = O.m5_unpack(fmt, pay[frame:], 2 * 20000 * fanout)
     got1, _ = _gpu_decode(gpu, lay, pay[frame:], nchan - 1, 2 * 20000 * fanout, payload_offset=frame)
     assert np.array_equal(got1.view(np.uint32), ref1[nchan - 1].view(np.uint32)), fmt
+
+
+@pytest.mark.parametrize("fmt,ntrack", TRACK_MODES)
+def test_track_formats_fill_blanking(gpu, fmt, ntrack):
+    """Fill-pattern blanking of VLBA / Mark4 data as mark5access does it:
+    32 KiB zones per frame, each blanked from the fill pattern at its ends
+    (binary search for the boundary, 32-bit straggler), Mark4's first zone
+    starting after the header and its later zones examined 20 n words late,
+    whole track-words blanked; every channel of three planted frames float
+    bit for float bit and the count of unblanked samples, then from the
+    second frame on through a payload offset."""
+    from helpers import plant_track_fill
+    info = O.m5_format_info(fmt)
+    nchan, nbit = info["nchan"], info["nbit"]
+    fanout = ntrack // (nchan * nbit)
+    rng = np.random.default_rng(ntrack * 7 + nchan)
+    frame = 2500 * ntrack
+    pay = plant_track_fill(rng.integers(0, 256, size=3 * frame, dtype=np.uint8).tobytes(), ntrack)
+    nsamp = 3 * 20000 * fanout
+    ref, nref = O.m5_unpack(fmt, pay, nsamp)
+    assert nref < nsamp                      # the plants blank something
+    lay = gpu.layout(("vlba:" if fmt.startswith("VLBA") else "mark4:") + str(ntrack), nchan, nbit)
+    for c in range(nchan):
+        got, nv = _gpu_decode(gpu, lay, pay, c, nsamp)
+        assert np.array_equal(got.view(np.uint32), ref[c].view(np.uint32)), (fmt, c)
+        assert nv == nref, (fmt, nv, nref)
+    ref1, nref1 = O.m5_unpack(fmt, pay[frame:], 2 * 20000 * fanout)
+    got1, nv1 = _gpu_decode(gpu, lay, pay[frame:], 0, 2 * 20000 * fanout, payload_offset=frame)
+    assert np.array_equal(got1.view(np.uint32), ref1[0].view(np.uint32)), fmt
+    assert nv1 == nref1
