@@ -342,8 +342,8 @@ static int track_layout_ok(const swsgpu_layout &l, std::string &why)
       why = "track formats: frame_bytes must be 2500 x tracks (8, 16, 32 or 64) with header_bytes 0";
       return 0;
    }
-   if ((l.nbit != 1 && l.nbit != 2) || l.nchan * l.nbit > 32 || ntrack % (l.nchan * l.nbit)) {
-      why = "track formats: nbit 1 or 2, nchan * nbit <= 32 and dividing the tracks";
+   if ((l.nbit != 1 && l.nbit != 2) || l.nchan * l.nbit > 64 || ntrack % (l.nchan * l.nbit)) {
+      why = "track formats: nbit 1 or 2, nchan * nbit <= 64 and dividing the tracks";
       return 0;
    }
    const int fanout = ntrack / (l.nchan * l.nbit);

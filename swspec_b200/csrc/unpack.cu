@@ -178,18 +178,23 @@ __constant__ VlbaModulation c_vlba_mod = make_vlba_modulation();
 // nchan * nbit, channel c at bit offset c * nbit, 2-bit codes sign + 2 mag.
 // The output has the input's size and frame grid (a track-word of ntrack
 // bits is `fanout` sample-times of B bits), so frame validity, blanking and
-// the corner turn treat it as Mark5B payload.  One thread per output word;
-// the chunk starts on a track-word (grid_offset a multiple of ntrack / 8).
+// the corner turn treat it as Mark5B payload.  One thread per output word,
+// which holds 32 / B sample-times, or for B = 64 (64 tracks, fanout 1) half
+// of one: the channels of that half.  The chunk starts on a track-word
+// (grid_offset a multiple of ntrack / 8).
 __global__ void k_track_turn(const uint8_t *__restrict__ in, long long nbytes, long long grid_offset, int ntrack,
                              int fanout, int nbit, int nchan, int vlba, uint32_t *__restrict__ out)
 {
    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (k >= (nbytes + 3) / 4) return;
-   const int B = nchan * nbit;  // bits per sample-time, <= 32
-   const int S = 32 / B;        // sample-times per output word
-   const int tb = ntrack / 8;   // bytes per track-word
-   const long long W0 = 8 * grid_offset / ntrack;         // grid track-word of the chunk's first byte
-   const long long T0 = W0 * fanout + 32 * k / B;        // grid sample-time of the word's first sample
+   const int B = nchan * nbit;          // bits per sample-time, <= 64
+   const bool half = B > 32;            // one output word is half a sample-time
+   const int S = half ? 1 : 32 / B;     // sample-times per output word
+   const int cn = half ? 32 / nbit : nchan;  // channels per output word
+   const int c0 = half ? (int)(k & 1) * cn : 0;
+   const int tb = ntrack / 8;           // bytes per track-word
+   const long long W0 = 8 * grid_offset / ntrack;  // grid track-word of the chunk's first byte
+   const long long T0 = W0 * fanout + (half ? k / 2 : 32 * k / B);  // grid sample-time of the word's first sample
    const uint32_t all = (1u << nbit) - 1u;
    uint32_t word = 0;
    long long cur = -1;
@@ -207,8 +212,8 @@ __global__ void k_track_turn(const uint8_t *__restrict__ in, long long nbytes, l
       }
       const int i = (int)(W % 20000);
       const uint32_t flip = (vlba && ((c_vlba_mod.w[i >> 5] >> (i & 31)) & 1u)) ? all : 0u;
-      for (int c = 0; c < nchan; c++) {
-         const int2 tr = track_of(ntrack, fanout, nbit, c, j);
+      for (int c = 0; c < cn; c++) {
+         const int2 tr = track_of(ntrack, fanout, nbit, c0 + c, j);
          uint32_t code = (uint32_t)(tw >> tr.x) & 1u;
          if (nbit == 2) code |= ((uint32_t)(tw >> tr.y) & 1u) << 1;
          word |= (code ^ flip) << (t * B + c * nbit);

@@ -10,6 +10,7 @@ import os
 import subprocess
 
 import numpy as np
+import pytest
 
 from swspec_b200 import synth
 
@@ -196,6 +197,8 @@ def test_mark4_frames_read_whole(tmp_path):
     assert got == pay
 
 
-def test_track_format_settings(tmp_path):
-    s = _settings(tmp_path, fmt="MKIV1_2-512-8-2")
-    assert s["source_channels"] == 8 and s["bits_per_sample"] == 2
+@pytest.mark.parametrize("fmt,nchan,nbit", [("MKIV1_2-512-8-2", 8, 2), ("VLBA1_1-512-32-2", 32, 2),
+                                             ("MKIV1_1-512-64-1", 64, 1)])
+def test_track_format_settings(tmp_path, fmt, nchan, nbit):
+    s = _settings(tmp_path, fmt=fmt)
+    assert s["source_channels"] == nchan and s["bits_per_sample"] == nbit

@@ -421,7 +421,8 @@ def test_group_chunks_alternate_streams(gpu):
                                                      ("VLBA1_4-512-8-2", 64, 4096, "fp32", False),
                                                      ("MKIV1_2-512-8-2", 32, 8192, "tcsplit_all", False),
                                                      ("MKIV1_2-512-8-2", 32, 4096, "fp32", True),
-                                                     ("VLBA1_4-512-8-2", 64, 4096, "fp32", True)])
+                                                     ("VLBA1_4-512-8-2", 64, 4096, "fp32", True),
+                                                     ("VLBA1_1-512-32-2", 64, 4096, "fp32", True)])
 def test_track_format_spectra(gpu, fmt, ntrack, N, prec, fill):
     """VLBA / Mark4 track-words through the track turn, the corner turn and
     the FFT: auto spectra of two channels and their cross spectrum (16 FFTs)

@@ -144,12 +144,12 @@ def test_raw_formats_bit_exact(gpu, fmt, nchan, nbit):
 
 
 # VLBA / Mark4 modes: (mark5access format, tracks); fanouts 1, 2 and 4, 1- and
-# 2-bit, 8 to 64 tracks; MKIV1_2-512-8-2 is the reference's own example mode
-# (src/democonfig.ini)
+# 2-bit, 8 to 64 tracks, 64 bits per sample-time (64 tracks, fanout 1);
+# MKIV1_2-512-8-2 is the reference's own example mode (src/democonfig.ini)
 TRACK_MODES = [("VLBA1_1-128-8-2", 16), ("VLBA1_2-256-8-2", 32), ("VLBA1_4-512-8-2", 64),
                ("VLBA1_2-512-32-1", 64), ("VLBA1_4-64-2-1", 8), ("MKIV1_2-512-8-2", 32),
                ("MKIV1_4-256-4-2", 32), ("MKIV1_1-256-32-1", 32), ("MKIV1_2-1024-16-2", 64),
-               ("MKIV1_1-64-4-2", 8)]
+               ("MKIV1_1-64-4-2", 8), ("VLBA1_1-512-32-2", 64), ("MKIV1_1-512-64-1", 64)]
 
 
 @pytest.mark.parametrize("fmt,ntrack", TRACK_MODES)
