@@ -425,27 +425,28 @@ def gpu_arm(args) -> None:
             core.submit([base + r * RUN_BYTES], payload_offsets=[r * RUN_BYTES], dest=(auto_h, xpol_h))
             core.wait()
 
-    # two cores, one integration each, their runs interleaved: each core's
+    # K cores, one integration each, their runs interleaved: each core's
     # next run is submitted as soon as its previous run's input has landed,
-    # so one core's copy is always queued behind the other's
-    core2 = make_core(headline, framed=False, rpo=RUNS_PER_SPECTRUM)
-    core2.set_sizes([RUN_BYTES])
-    auto_h2 = pinned_np((1, NCHAN, S), torch.float32)
-    xpol_h2 = pinned_np((1, NPAIRS, S, 2), torch.float32)
+    # so the other cores' copies are already queued behind it
+    K = max(2, args.e2e_cores)
+    extra = [make_core(headline, framed=False, rpo=RUNS_PER_SPECTRUM) for _ in range(K - 1)]
+    for c in extra:
+        c.set_sizes([RUN_BYTES])
+    group = [(core, (auto_h, xpol_h))] + [(c, (pinned_np((1, NCHAN, S), torch.float32),
+                                              pinned_np((1, NPAIRS, S, 2), torch.float32))) for c in extra]
 
-    def e2e_pair():
-        pair = ((core, (auto_h, xpol_h)), (core2, (auto_h2, xpol_h2)))
-        for c, d in pair:
+    def e2e_group():
+        for c, d in group:
             c.submit([base], payload_offsets=[0], dest=d)
         for r in range(1, RUNS_PER_SPECTRUM + 1):
-            for c, d in pair:
+            for c, d in group:
                 c.wait()
                 if r < RUNS_PER_SPECTRUM:
                     c.submit([base + r * RUN_BYTES], payload_offsets=[r * RUN_BYTES], dest=d)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
-        e2e_pair()
+        e2e_group()
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -454,21 +455,22 @@ def gpu_arm(args) -> None:
     torch.cuda.synchronize()
     e2e1_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
-    npair = (args.steps + 1) // 2
+    ngroup = (args.steps + K - 1) // K
     t0 = time.perf_counter()
-    for _ in range(npair):
-        e2e_pair()
+    for _ in range(ngroup):
+        e2e_group()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
     core.close()
-    core2.close()
+    for c in extra:
+        c.close()
     e2e1_val = SAMPLES_PER_STEP * args.steps * world / e2e1_s / 1e9
-    e2e_val = SAMPLES_PER_STEP * 2 * npair * world / e2e_s / 1e9
-    # the two cores' spectra of the same input (expected: bit for bit)
-    cores_agree = bool(np.array_equal(auto_h, auto_h2) and np.array_equal(xpol_h, xpol_h2))
+    e2e_val = SAMPLES_PER_STEP * K * ngroup * world / e2e_s / 1e9
+    # the cores' spectra of the same input (expected: bit for bit)
+    cores_agree = all(np.array_equal(auto_h, d[0]) and np.array_equal(xpol_h, d[1]) for _, d in group[1:])
     d2h = auto_h.nbytes + xpol_h.nbytes
-    log(f"[e2e] {e2e_val:.3f} Gsamples/s two cores ({e2e1_val:.3f} one core)")
+    log(f"[e2e] {e2e_val:.3f} Gsamples/s {K} cores ({e2e1_val:.3f} one core)")
 
     # ---- parity of the headline form on this workload ----
     parity = None
@@ -544,8 +546,8 @@ def gpu_arm(args) -> None:
                     "d2h_bytes_per_step": d2h,
                     "path": "swsgpu_submit_out/wait per 4 MiB run (TaskCore path, the run given its "
                             "output buffers), device combine, spectra copied into pinned host arrays; "
-                            "two cores with one integration each, runs interleaved",
-                    "one_core": e2e1_val, "cores_agree": cores_agree},
+                            f"{K} cores with one integration each, runs interleaved",
+                    "cores": K, "one_core": e2e1_val, "cores_agree": cores_agree},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "parity": parity}
     print(json.dumps(line), flush=True)
@@ -883,6 +885,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "tcsplit", "tcsplit_all"])
+    ap.add_argument("--e2e-cores", type=int, default=2,
+                    help="cores of the end-to-end leg, one integration each, runs interleaved (>= 2)")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plan", default="auto", choices=["auto", "cluster", "fourstep"],
