@@ -67,3 +67,17 @@ int m5ref_unpack(const char *fmt, void *payload, int nsamp, int nchan_max, float
    delete_mark5_stream(ms);
    return r;
 }
+
+/* Time of the first frame of an in-memory framed stream, as mark5access
+ * decodes its header (mark5_stream_get_frame_time); returns 0 on success. */
+int m5ref_frame_time(const char *fmt, void *data, unsigned nbytes, int *mjd, int *sec, double *ns,
+                     int *frameoffset)
+{
+   struct mark5_stream *ms = new_mark5_stream(new_mark5_stream_memory(data, nbytes),
+                                              new_mark5_format_generic_from_string(fmt));
+   if (!ms) return -100;
+   *frameoffset = ms->frameoffset;
+   int r = mark5_stream_get_frame_time(ms, mjd, sec, ns);
+   delete_mark5_stream(ms);
+   return r;
+}

@@ -76,6 +76,8 @@ def ref():
                                       C.c_void_p, C.POINTER(C.c_int)]
         _ref.m5ref_unpack.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         _ref.m5ref_format_info.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 6
+        _ref.m5ref_frame_time.argtypes = [C.c_char_p, C.c_void_p, C.c_uint, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     return _ref
 
 
@@ -208,6 +210,18 @@ def m5_decode(fmt: str, framed: bytes, nsamp: int) -> tuple[np.ndarray, int]:
     rc = r.m5ref_decode(fmt.encode(), buf.ctypes.data, len(buf), nsamp, info["nchan"],
                         out.ctypes.data, C.byref(off))
     return out, rc
+
+
+def m5_frame_time(fmt: str, framed: bytes) -> tuple[int, int, float, int]:
+    """(mjd, second, ns, frame offset) of the first frame mark5access finds."""
+    r = ref()
+    mjd, sec, ns, off = C.c_int(), C.c_int(), C.c_double(), C.c_int()
+    buf = np.frombuffer(framed, dtype=np.uint8).copy()
+    rc = r.m5ref_frame_time(fmt.encode(), buf.ctypes.data, len(buf), C.byref(mjd), C.byref(sec), C.byref(ns),
+                            C.byref(off))
+    if rc != 0:
+        raise RuntimeError(f"mark5access found no frame time ({rc})")
+    return mjd.value, sec.value, ns.value, off.value
 
 
 def m5_unpack(fmt: str, payload: bytes, nsamp: int) -> tuple[np.ndarray, int]:

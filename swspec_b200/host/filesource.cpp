@@ -109,6 +109,46 @@ int FileSource::open(const std::string &uri)
       if (first_frame_ > 0)
          *cfg_->tlog << "FileSource: first frame at byte " << first_frame_ << " (" << first_frame_
                      << " leading bytes skipped)" << std::endl;
+      if (cfg_->startlog) {
+         // the time code follows the sync word: BCD nibbles of four
+         // track-words each, most significant bit first, every bit the
+         // majority of the track-word's tracks as mark5access reads it (set
+         // when more than ntrack / 16 tracks are set;
+         // mark5_format_vlba.c:314-334).  VLBA: JJJ SSSSS ssss (MJD mod
+         // 1000, second of day, 0.1 ms); Mark4: Y DDD HH MM SS ss s (last
+         // digit of the year, day of year, time of day)
+         const int nnib = s.sourceformat == VLBA ? 12 : 13;
+         const int64_t t0 = found + sync_len;
+         int nib[13] = {0};
+         bool bcd_ok = t0 + (int64_t)4 * nnib * tb <= got;
+         for (int i = 0; bcd_ok && i < nnib; i++) {
+            for (int b = 0; b < 4; b++) {
+               int c = 0;
+               for (int j = 0; j < tb; j++) c += __builtin_popcount(win[t0 + (int64_t)tb * (4 * i + 3 - b) + j]);
+               if (c > tb / 2) nib[i] |= 1 << b;
+            }
+            bcd_ok = bcd_ok && nib[i] <= 9;
+         }
+         *cfg_->startlog << "First frame at byte " << first_frame_ << ": ";
+         if (s.sourceformat == VLBA) {
+            const int mjd3 = nib[0] * 100 + nib[1] * 10 + nib[2];
+            const int sec = nib[3] * 10000 + nib[4] * 1000 + nib[5] * 100 + nib[6] * 10 + nib[7];
+            const int frac = nib[8] * 1000 + nib[9] * 100 + nib[10] * 10 + nib[11];
+            *cfg_->startlog << "MJD(mod 1000) " << mjd3 << " second " << sec << " + " << frac << " x 0.1 ms"
+                            << std::endl;
+            bcd_ok = bcd_ok && sec < 86400;
+         } else {
+            const int doy = nib[1] * 100 + nib[2] * 10 + nib[3];
+            const int sec = (nib[4] * 10 + nib[5]) * 3600 + (nib[6] * 10 + nib[7]) * 60 + nib[8] * 10 + nib[9];
+            *cfg_->startlog << "year digit " << nib[0] << " day " << doy << " second " << sec << std::endl;
+            bcd_ok = bcd_ok && doy >= 1 && doy <= 366 && sec < 86400;
+         }
+         if (!bcd_ok) {
+            *cfg_->tlog << "FileSource: time code of the first frame is not a valid BCD time (digits";
+            for (int i = 0; i < nnib; i++) *cfg_->tlog << " " << nib[i];
+            *cfg_->tlog << ")" << std::endl;
+         }
+      }
    }
    // skip whole seconds (FileSource.cpp:132-153)
    int64_t seek = first_frame_;

@@ -158,24 +158,42 @@ def test_vdif_thread_selection(tmp_path):
     assert got == pays[1]
 
 
-def _track_file(kind: str, ntrack: int, nfr: int, lead: int, seed: int):
+def _time_words(digits, tb: int) -> np.ndarray:
+    """BCD nibbles as header track-words: four per nibble, most significant
+    bit first, all tracks of a track-word carrying the bit."""
+    out = np.zeros(4 * len(digits) * tb, np.uint8)
+    for i, d in enumerate(digits):
+        for b in range(4):
+            if (d >> b) & 1:
+                out[(4 * i + 3 - b) * tb:(4 * i + 4 - b) * tb] = 0xFF
+    return out
+
+
+def _track_file(kind: str, ntrack: int, nfr: int, lead: int, seed: int, digits=None):
     """A VLBA (20160 track-words per frame: sync, time code, payload of
     20000, 64 trailing) or Mark4 (20000 per frame: 64 auxiliary, sync, time
     code, data) recording after `lead` bytes of other data; returns the file
-    and the payload stream the GPU core takes."""
+    and the payload stream the GPU core takes.  `digits`: the time code's
+    BCD digits (12 for VLBA, 13 for Mark4) in every frame's header."""
     tb = ntrack // 8
     rng = np.random.default_rng(seed)
     frames, payload = [], []
     for _ in range(nfr):
         if kind == "VLBA":
+            hdr = np.zeros(64 * tb, np.uint8)
+            if digits is not None:
+                hdr[:48 * tb] = _time_words(digits, tb)
             data = rng.integers(0, 256, 20000 * tb, dtype=np.uint8)
-            fr = np.concatenate([np.full(32 * tb, 0xFF, np.uint8), np.zeros(64 * tb, np.uint8), data,
+            fr = np.concatenate([np.full(32 * tb, 0xFF, np.uint8), hdr, data,
                                  np.zeros(64 * tb, np.uint8)])
             payload.append(data)
         else:
+            hdr = np.zeros(64 * tb, np.uint8)
+            if digits is not None:
+                hdr[:52 * tb] = _time_words(digits, tb)
             data = rng.integers(0, 256, 19840 * tb, dtype=np.uint8)
             fr = np.concatenate([np.zeros(64 * tb, np.uint8), np.full(32 * tb, 0xFF, np.uint8),
-                                 np.zeros(64 * tb, np.uint8), data])
+                                 hdr, data])
             payload.append(fr)
         frames.append(fr)
     head = rng.integers(0, 200, lead, dtype=np.uint8)
@@ -195,6 +213,46 @@ def test_mark4_frames_read_whole(tmp_path):
     r, info, got = _read(tmp_path, data, fmt="MKIV1_1-256-8-2")
     assert r.returncode == 0, r.stderr
     assert got == pay
+
+
+def _pin_time(fmt, data, offset, check):
+    """The same header through mark5access (oracle/_ref), where it was built."""
+    import oracle as O
+    if O.ref() is None:
+        return
+    mjd, sec, ns, off = O.m5_frame_time(fmt, data)
+    assert off == offset and check(mjd, sec, ns), (mjd, sec, ns, off)
+
+
+def test_vlba_start_time_code(tmp_path):
+    """The first VLBA frame's time code (MJD mod 1000, second of day, 0.1 ms)
+    in the start-timing file, each bit the majority of its track-word."""
+    data, pay = _track_file("VLBA", 32, 4, 3000, 9, digits=[1, 2, 3, 4, 5, 6, 7, 8, 1, 2, 3, 4])
+    r, info, got = _read(tmp_path, data, fmt="VLBA1_2-256-8-2")
+    assert r.returncode == 0, r.stderr
+    assert got == pay
+    timing = (tmp_path / "out.bin.starttiming.txt").read_text()
+    assert "First frame at byte 3000: MJD(mod 1000) 123 second 45678 + 1234 x 0.1 ms" in timing
+    assert "BCD" not in r.stderr
+    _pin_time("VLBA1_2-256-8-2", data, 3000, lambda mjd, sec, ns: (mjd % 1000, sec, ns) == (123, 45678, 1.234e8))
+
+
+def test_mark4_start_time_code(tmp_path):
+    """Mark4: year digit, day of year and time of day (12:34:56 = second
+    45296); a day above 366 is reported."""
+    data, pay = _track_file("MKIV", 32, 4, 0, 10, digits=[6, 1, 2, 3, 1, 2, 3, 4, 5, 6, 0, 0, 0])
+    r, info, got = _read(tmp_path, data, fmt="MKIV1_2-512-8-2")
+    assert r.returncode == 0, r.stderr
+    timing = (tmp_path / "out.bin.starttiming.txt").read_text()
+    assert "First frame at byte 0: year digit 6 day 123 second 45296" in timing
+    assert "BCD" not in r.stderr
+    # mark5access: MJD 51543 + 365 y + day + (y + 3) // 4 (decade 0), its frame pointer at the sync word
+    _pin_time("MKIV1_2-512-8-2", data, 64 * 4,
+              lambda mjd, sec, ns: (mjd, sec, ns) == (51543 + 365 * 6 + 123 + 9 // 4, 45296, 0.0))
+    data, _ = _track_file("MKIV", 32, 4, 0, 10, digits=[6, 3, 9, 9, 1, 2, 3, 4, 5, 6, 0, 0, 0])
+    r, _, _ = _read(tmp_path, data, fmt="MKIV1_2-512-8-2")
+    assert r.returncode == 0, r.stderr
+    assert "not a valid BCD time (digits 6 3 9 9 1 2 3 4 5 6 0 0 0)" in r.stderr
 
 
 @pytest.mark.parametrize("fmt,nchan,nbit", [("MKIV1_2-512-8-2", 8, 2), ("VLBA1_1-512-32-2", 32, 2),
