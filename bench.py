@@ -565,6 +565,49 @@ def tc_available(gpu) -> bool:
         return False
 
 
+def c4_cpu_baseline(specs, seconds_per_length: float = 3.0) -> dict:
+    """The CPU restatement of the reference core (mark5access VDIF decode +
+    FP32 TaskCoreIPP::doMaths) on all host cores, per FFT length and bit
+    depth of the mix over a bounded sample of whole FFTs, combined as the
+    time the step's samples of each length would take at its rate."""
+    from collections import Counter
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    share = Counter()
+    for s in specs:
+        share[(s.fft_points, s.nbit)] += s.samples_per_run
+    rng = np.random.default_rng(7)
+    rates, nfft = {}, 0
+    t_all = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        for N, nbit in sorted(share):
+            seg = rng.integers(0, 256, N * nbit // 8, dtype=np.uint8).tobytes()
+            cfg = O.make_cfg(N, core_overlapped_ffts=1, num_sources=1, window=O.W_HANN, nthreads=1)
+
+            def job(_):
+                x = O.decode(O.FMT_VDIF, 1, nbit, seg, N, 0, payload_bytes=8000)
+                O.domaths(cfg, [x], fp64=False)
+                return N
+
+            samples = 0
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < seconds_per_length:
+                samples += sum(pool.map(job, range(cores)))
+                nfft += cores
+            rates[(N, nbit)] = samples / (time.perf_counter() - t0)
+    t_step = sum(share[k] / rates[k] for k in share)
+    return {"value": sum(share.values()) / t_step / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "port",
+            "sample": f"{nfft} whole FFTs over the mix's {len(share)} (length, bits) classes, about "
+                      f"{seconds_per_length:.0f} s each on all threads (mark5access VDIF decode + FP32 "
+                      "restatement of TaskCoreIPP::doMaths); the step's samples of each class at that "
+                      "class's rate",
+            "seconds": time.perf_counter() - t_all}
+
+
 def c4_arm(args) -> None:
     """Batched uneven streams: 64 single-channel streams of mixed FFT length
     (4096 .. 3.2M), bit depth, bandwidth and integration, one core run each
@@ -672,7 +715,7 @@ def c4_arm(args) -> None:
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                              "note": "packed input bytes per step over the step time"},
-                "cpu_baseline": None}
+                "cpu_baseline": c4_cpu_baseline(specs) if (reps.world == 1 and not args.no_cpu) else None}
         print(json.dumps(line), flush=True)
     reps.close()
 
