@@ -739,6 +739,11 @@ SPEC_WORKLOADS = {
                fs=64e6, core_ffts=4, run_bytes=16 << 20, runs=19, sources=((0, 0),), xpols=(), pcal=None,
                signal="Gaussian noise plus a carrier at 12.3456 MHz 50 dB over the per-bin floor drifting "
                       "1 Hz/s, 8-bit offset binary at 24 codes per sigma"),
+    "vlba": dict(desc="VLBA track format: VLBA1_2-512-8-2 (32 tracks, fanout 2, 8 channels 2-bit, 32 Msps), "
+                      "header-free payload, N=65536 Hann, 1.016 s (992 FFTs), 4 MiB runs x 31",
+                 fmt="vlba:32", m5fmt="VLBA1_2-512-8-2", nchan=8, nbit=2, N=65536, window="hann", fs=32e6,
+                 core_ffts=32, run_bytes=4 << 20, runs=31, sources=tuple((0, c) for c in range(8)), xpols=(),
+                 pcal=None, signal="uniform random track-words (every sample code equally likely)"),
 }
 
 
@@ -748,6 +753,11 @@ def spec_payload(name: str, w: dict, seed: int):
 
     from swspec_b200 import synth_gpu
     T = w["run_bytes"] * w["runs"] * 8 // (w["nbit"] * w["nchan"])
+    if name == "vlba":
+        import torch
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1006 + seed)
+        return torch.randint(0, 256, (w["run_bytes"] * w["runs"],), dtype=torch.uint8, device="cuda", generator=g)
     if name == "c1":
         # Hann: 20 dB per-bin SNR <=> A^2 N / (6 sigma^2) = 100
         return synth_gpu.mark5b_payload(T, 16, w["fs"], 1001 + seed, tone_hz=3.1e6,
@@ -771,6 +781,8 @@ def spec_cpu_baseline(w: dict, payload, seconds_budget: float = 12.0) -> dict:
     cores = os.cpu_count() or 1
     N, ns = w["N"], len(w["sources"])
     nbit, nchan = w["nbit"], w["nchan"]
+    if "m5fmt" in w:
+        return track_cpu_baseline(w, payload, seconds_budget)
     fmt = O.FMT_MARK5B if w["fmt"] == "mark5b" else O.FMT_VDIF
     bpt = nbit * nchan // 8                          # payload bytes per sample-time
     nfft_avail = len(payload) // (N * bpt)
@@ -794,6 +806,43 @@ def spec_cpu_baseline(w: dict, payload, seconds_budget: float = 12.0) -> dict:
     return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "port",
             "sample": f"{k} FFTs of N = {N} from the workload's packed bytes (mark5access decode + FP32 "
                       "restatement of TaskCoreIPP::doMaths), one FFT per thread at a time",
+            "seconds": dt}
+
+
+def track_cpu_baseline(w: dict, payload, seconds_budget: float = 12.0) -> dict:
+    """VLBA / Mark4 on the CPU: mark5access's own unpack (built from the
+    reference sources) of N sample-times of every channel from a frame
+    boundary, then the FP32 restatement of TaskCoreIPP::doMaths on each
+    channel, on all host cores over a bounded sample."""
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    N, nchan, nbit = w["N"], w["nchan"], w["nbit"]
+    ntrack = int(w["fmt"].split(":")[1])
+    frame = 2500 * ntrack
+    need = N * nchan * nbit // 8
+    nseg = (len(payload) - need) // frame
+    cfg = O.make_cfg(N, core_overlapped_ffts=1, num_sources=1, window=O.WINDOW_NAMES[w["window"]], nthreads=1)
+
+    def job(k):
+        seg = payload[(k % nseg) * frame:(k % nseg) * frame + need].tobytes()
+        dec, _ = O.m5_unpack(w["m5fmt"], seg, N)
+        for c in range(nchan):
+            O.domaths(cfg, [dec[c]], fp64=False)
+        return N * nchan
+
+    samples, k = 0, 0
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds_budget:
+            samples += sum(pool.map(job, range(k, k + cores)))
+            k += cores
+        dt = time.perf_counter() - t0
+    return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "reference",
+            "sample": f"{k} blocks of N = {N} sample-times x {nchan} channels: mark5access's header-free "
+                      "unpack (the reference's own decoder library) + the FP32 restatement of "
+                      "TaskCoreIPP::doMaths per channel",
             "seconds": dt}
 
 
@@ -936,7 +985,7 @@ def main():
                     help="FFT path for the cross-spectra workload (auto: cluster kernel)")
     ap.add_argument("--candidate", type=int, default=-1,
                     help="c2/c5: pin four-step split k of the length's candidates instead of autotuning")
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "vlba"],
                     help="c3: dual-pol cross-spectra (the default line); c1: plain single channel; "
                          "c2: 3.2M-point spectra with phase-cal tones; c4: batched uneven streams; "
                          "c5: 2^22-point 8-bit dynamic range")

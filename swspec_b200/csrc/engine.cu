@@ -30,8 +30,9 @@ cudaError_t launch_unpack_codes(cudaStream_t st, StreamIn s, long long nsamp, co
                                 uint32_t *codes, int D, long long wpp, const int2 *valid,
                                 const int *blank_any, uint32_t *blank, int &launches);
 bool unpack_decimation_ok(int D, int nchan, int nbit);
+void track_turn_table(int ntrack, int nbit, int nchan, uint32_t *table);
 cudaError_t launch_track_turn(cudaStream_t st, const uint8_t *in, long long nbytes, long long grid_offset,
-                              int ntrack, int nbit, int nchan, int format, uint32_t *out);
+                              int ntrack, int format, const uint32_t *table, uint32_t *out);
 __global__ void k_unpack_float(StreamIn s, long long nsamp, int chan, float4 levels, float *out,
                                const int2 *valid, unsigned long long *nvalid);
 __global__ void k_reduce(const float *partial, int S, const RedEntry *ent, const OutVec *ov);
@@ -235,6 +236,7 @@ struct swsgpu_handle {
    std::vector<int> auto_owner;   // source -> xpol index that owns its auto (-1: none)
    // constant tables
    DevBuf d_window, d_twQ, d_twN, d_code_stream;
+   DevBuf d_trk_table;  // track formats: the track turn's unit-byte tables
    DevBuf d_tw1, d_tw2, d_twA, d_twB;               // four-step tables
    DevBuf d_scratch, d_bjobs, d_bitems;             // four-step intermediate and job lists
    DevBuf d_status;                                 // kernel status word (1: a bounded wait gave up)
@@ -896,7 +898,8 @@ static int launch_chunk(swsgpu_handle *h, const void *const *d_raw, const size_t
          // and grid; validity above was read from the track-words)
          CK(h, x.d_trk[s].ensure((raw_bytes[s] + 3) / 4 * 4 + 16));
          CK(h, launch_track_turn(st, (const uint8_t *)d_raw[s], (long long)raw_bytes[s], grid_off[s],
-                                 payload_bytes(L) / 2500, L.nbit, L.nchan, L.format, (uint32_t *)x.d_trk[s].p));
+                                 payload_bytes(L) / 2500, L.format, (const uint32_t *)h->d_trk_table.p,
+                                 (uint32_t *)x.d_trk[s].p));
          si.data = (const uint8_t *)x.d_trk[s].p;
          launches++;
       }
@@ -1348,6 +1351,14 @@ int swsgpu_create(const swsgpu_config *cfg, int device, swsgpu_handle **out)
    } while (0)
    CKB(h->d_window.ensure(sizeof(float) * win.size()));
    CKB(cudaMemcpy(h->d_window.p, win.data(), sizeof(float) * win.size(), cudaMemcpyHostToDevice));
+   if (track_format(cfg->layout[0].format)) {
+      // the track turn's unit-byte tables (every stream shares the mode)
+      const swsgpu_layout &L = cfg->layout[0];
+      std::vector<uint32_t> tab(TRACK_TABLE_WORDS);
+      track_turn_table(L.frame_bytes / 2500, L.nbit, L.nchan, tab.data());
+      CKB(h->d_trk_table.ensure(sizeof(uint32_t) * tab.size()));
+      CKB(cudaMemcpy(h->d_trk_table.p, tab.data(), sizeof(uint32_t) * tab.size(), cudaMemcpyHostToDevice));
+   }
    if (!h->big) {
       CKB(h->d_twN.ensure(sizeof(float2) * twN.size()));
       CKB(cudaMemcpy(h->d_twN.p, twN.data(), sizeof(float2) * twN.size(), cudaMemcpyHostToDevice));
@@ -1495,7 +1506,7 @@ void swsgpu_destroy(swsgpu_handle *h)
                      &h->d_outs, &h->d_pcal_jobs, &h->d_pcal_part, &h->d_pcal_entries,
                      &h->d_pcal_outs, &h->d_out_auto, &h->d_out_xpol, &h->d_out_pcal, &h->d_out_tones,
                      &h->d_tw1, &h->d_tw2, &h->d_twA, &h->d_twB, &h->d_scratch, &h->d_bjobs, &h->d_status,
-                     &h->d_bitems};
+                     &h->d_bitems, &h->d_trk_table};
    for (DevBuf *b : bufs) b->release();
    for (Scratch &x : h->scr) x.release();
    drop_schedules(h);
@@ -2240,18 +2251,25 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
    // validity from the stream's own bytes (the track-words, for VLBA / Mark4)
    k_frame_valid<<<(unsigned)((si.nframes + 127) / 128), 128, 0, st>>>(si, d_valid, d_any);
+   uint32_t *d_tab = nullptr;
    if (ntrack) {
       // VLBA / Mark4 track-words into Mark5B's sample layout
+      std::vector<uint32_t> tab(TRACK_TABLE_WORDS);
+      track_turn_table(ntrack, lay->nbit, lay->nchan, tab.data());
       cudaError_t e = cudaMalloc(&d_trk, (nbytes + 3) / 4 * 4 + 16);
+      if (e == cudaSuccess) e = cudaMalloc(&d_tab, sizeof(uint32_t) * tab.size());
       if (e == cudaSuccess)
-         e = launch_track_turn(st, (const uint8_t *)d_raw, (long long)nbytes, si.grid_offset, ntrack, lay->nbit,
-                               lay->nchan, lay->format, d_trk);
+         e = cudaMemcpyAsync(d_tab, tab.data(), sizeof(uint32_t) * tab.size(), cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+         e = launch_track_turn(st, (const uint8_t *)d_raw, (long long)nbytes, si.grid_offset, ntrack, lay->format,
+                               d_tab, d_trk);
       if (e != cudaSuccess) {
          cudaStreamSynchronize(st);
          cudaFree(d_valid);
          cudaFree(d_any);
          cudaFree(d_cnt);
          if (d_trk) cudaFree(d_trk);
+         if (d_tab) cudaFree(d_tab);
          return SWSGPU_ECUDA;
       }
       si.data = (const uint8_t *)d_trk;
@@ -2266,6 +2284,7 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
    cudaFree(d_any);
    cudaFree(d_cnt);
    if (d_trk) cudaFree(d_trk);
+   if (d_tab) cudaFree(d_tab);
    if (e != cudaSuccess) {
       g_create_error = cudaGetErrorString(e);
       return SWSGPU_ECUDA;

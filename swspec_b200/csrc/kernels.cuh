@@ -63,6 +63,10 @@ __host__ __device__ inline bool track_format(int format)
    return format == SWSGPU_FMT_VLBA || format == SWSGPU_FMT_MARK4;
 }
 
+// Unit-byte tables of a VLBA / Mark4 mode's track turn: [8 bytes][256 values]
+// x two 32-bit output words (unpack.cu, track_turn_table).
+constexpr int TRACK_TABLE_WORDS = 8 * 256 * 2;
+
 // mark5access blanks VLBA and Mark4 payloads by 32 KiB zones, each with its
 // own valid byte range (blanker_mark5.c:126-280, log2blankzonesize = 15);
 // the other formats have one range per frame.

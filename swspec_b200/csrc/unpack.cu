@@ -176,60 +176,115 @@ __constant__ VlbaModulation c_vlba_mod = make_vlba_modulation();
 // Track-word stream (VLBA payload or Mark4 frames) -> Mark5B's sample layout:
 // sample-time t of the chunk takes bits [t B, t B + B) of the output, B =
 // nchan * nbit, channel c at bit offset c * nbit, 2-bit codes sign + 2 mag.
-// The output has the input's size and frame grid (a track-word of ntrack
-// bits is `fanout` sample-times of B bits), so frame validity, blanking and
-// the corner turn treat it as Mark5B payload.  One thread per output word,
-// which holds 32 / B sample-times, or for B = 64 (64 tracks, fanout 1) half
-// of one: the channels of that half.  The chunk starts on a track-word
-// (grid_offset a multiple of ntrack / 8).
-__global__ void k_track_turn(const uint8_t *__restrict__ in, long long nbytes, long long grid_offset, int ntrack,
-                             int fanout, int nbit, int nchan, int vlba, uint32_t *__restrict__ out)
+// A track-word of ntrack bits is `fanout` sample-times of B bits, so the
+// output has the input's size and frame grid (frame validity, blanking and
+// the corner turn treat it as Mark5B payload), and the turn is a fixed
+// permutation of the bits of every unit of max(32, ntrack) bits: output bit
+// o of a unit comes from one input bit of the same unit.  The permutation
+// is tabulated per mode as unit-byte tables (track_turn_table): the output
+// unit is the OR of one table entry per input byte.  VLBA modulation
+// negates every sample of a modulated track-word, i.e. flips all of its
+// bits before the permutation.
+void track_turn_table(int ntrack, int nbit, int nchan, uint32_t *table)
 {
-   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (k >= (nbytes + 3) / 4) return;
-   const int B = nchan * nbit;          // bits per sample-time, <= 64
-   const bool half = B > 32;            // one output word is half a sample-time
-   const int S = half ? 1 : 32 / B;     // sample-times per output word
-   const int cn = half ? 32 / nbit : nchan;  // channels per output word
-   const int c0 = half ? (int)(k & 1) * cn : 0;
+   std::fill(table, table + TRACK_TABLE_WORDS, 0u);
+   const int B = nchan * nbit, fanout = ntrack / B;
+   const int U = ntrack > 32 ? 64 : 32;  // unit bits
+   for (int o = 0; o < U; o++) {
+      const int wi = o / ntrack, r = o % ntrack;  // track-word of the unit, bit of its sample-times
+      const int j = r / B, c = (r % B) / nbit, b = r % nbit;
+      const int2 tr = track_of(ntrack, fanout, nbit, c, j);
+      const int src = wi * ntrack + (b == 0 ? tr.x : tr.y);
+      for (int v = 0; v < 256; v++)
+         if ((v >> (src & 7)) & 1) table[((src >> 3) * 256 + v) * 2 + (o >> 5)] |= 1u << (o & 31);
+   }
+}
+
+// One thread per unit (4 bytes, or 8 at 64 tracks), the tables in shared
+// memory.  The chunk starts on a track-word (grid_offset a multiple of
+// ntrack / 8); the bytes of a track-word cut off by the chunk's end read as
+// zero (modulation still applied).
+__global__ void __launch_bounds__(256) k_track_turn(const uint8_t *__restrict__ in, long long nbytes,
+                                                    long long grid_offset, int ntrack, int vlba, int aligned,
+                                                    const uint2 *__restrict__ table, uint32_t *__restrict__ out)
+{
+   __shared__ uint2 s_tab[8 * 256];
+   const int UB = ntrack > 32 ? 8 : 4;  // bytes per unit
+   for (int i = threadIdx.x; i < UB * 256; i += blockDim.x) s_tab[i] = table[i];
+   __syncthreads();
    const int tb = ntrack / 8;           // bytes per track-word
+   const int tpu = UB / tb;             // track-words per unit
    const long long W0 = 8 * grid_offset / ntrack;  // grid track-word of the chunk's first byte
-   const long long T0 = W0 * fanout + (half ? k / 2 : 32 * k / B);  // grid sample-time of the word's first sample
-   const uint32_t all = (1u << nbit) - 1u;
-   uint32_t word = 0;
-   long long cur = -1;
-   unsigned long long tw = 0;
-   for (int t = 0; t < S; t++) {
-      const long long T = T0 + t;
-      const long long W = T / fanout;
-      const int j = (int)(T - W * fanout);
-      if (W != cur) {
-         cur = W;
-         tw = 0;
-         const long long a = (W - W0) * tb;
-         if (a + tb <= nbytes)
-            for (int b = 0; b < tb; b++) tw |= (unsigned long long)in[a + b] << (8 * b);
+   const long long nunit = (nbytes + UB - 1) / UB;
+   const long long nw = (nbytes + 3) / 4;
+   for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < nunit;
+        u += (long long)gridDim.x * blockDim.x) {
+      const long long a = u * UB;
+      uint32_t lo = 0u, hi = 0u;
+      if (aligned && a + UB <= nbytes) {
+         if (UB == 8) {
+            const uint2 v = __ldg(reinterpret_cast<const uint2 *>(in + a));
+            lo = v.x;
+            hi = v.y;
+         } else {
+            lo = __ldg(reinterpret_cast<const uint32_t *>(in + a));
+         }
+      } else {
+         // bytes of whole track-words (an unaligned source reads bytewise)
+         const int whole = (int)std::min<long long>((nbytes - a) / tb * tb, UB);
+         for (int k = 0; k < whole; k++) {
+            if (k < 4) lo |= (uint32_t)in[a + k] << (8 * k);
+            else hi |= (uint32_t)in[a + k] << (8 * (k - 4));
+         }
       }
-      const int i = (int)(W % 20000);
-      const uint32_t flip = (vlba && ((c_vlba_mod.w[i >> 5] >> (i & 31)) & 1u)) ? all : 0u;
-      for (int c = 0; c < cn; c++) {
-         const int2 tr = track_of(ntrack, fanout, nbit, c0 + c, j);
-         uint32_t code = (uint32_t)(tw >> tr.x) & 1u;
-         if (nbit == 2) code |= ((uint32_t)(tw >> tr.y) & 1u) << 1;
-         word |= (code ^ flip) << (t * B + c * nbit);
+      if (vlba) {
+         for (int t = 0; t < tpu; t++) {
+            const int i = (int)((W0 + u * tpu + t) % 20000);
+            if ((c_vlba_mod.w[i >> 5] >> (i & 31)) & 1u) {
+               if (tb >= 4) {
+                  lo = ~lo;
+                  if (tb == 8) hi = ~hi;
+               } else {
+                  lo ^= ((1u << (8 * tb)) - 1u) << (8 * tb * t);
+               }
+            }
+         }
+      }
+      uint32_t r0 = 0u, r1 = 0u;
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+         const uint2 e = s_tab[p * 256 + ((lo >> (8 * p)) & 0xFFu)];
+         r0 |= e.x;
+         r1 |= e.y;
+      }
+      if (UB == 8) {
+#pragma unroll
+         for (int p = 0; p < 4; p++) {
+            const uint2 e = s_tab[(4 + p) * 256 + ((hi >> (8 * p)) & 0xFFu)];
+            r0 |= e.x;
+            r1 |= e.y;
+         }
+         out[2 * u] = r0;
+         if (2 * u + 1 < nw) out[2 * u + 1] = r1;
+      } else {
+         out[u] = r0;
       }
    }
-   out[k] = word;
 }
 
 cudaError_t launch_track_turn(cudaStream_t st, const uint8_t *in, long long nbytes, long long grid_offset,
-                              int ntrack, int nbit, int nchan, int format, uint32_t *out)
+                              int ntrack, int format, const uint32_t *table, uint32_t *out)
 {
-   const long long nw = (nbytes + 3) / 4;
-   if (nw == 0) return cudaSuccess;
-   const int fanout = ntrack / (nchan * nbit);
-   k_track_turn<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(in, nbytes, grid_offset, ntrack, fanout, nbit, nchan,
-                                                              format == SWSGPU_FMT_VLBA ? 1 : 0, out);
+   const int UB = ntrack > 32 ? 8 : 4;
+   const long long nunit = (nbytes + UB - 1) / UB;
+   if (nunit == 0) return cudaSuccess;
+   // a resident grid (8 CTAs of 256 threads per SM) striding over the
+   // units, so each CTA loads the tables once for many units
+   const long long nblk = std::min<long long>((nunit + 255) / 256, 148LL * 8);
+   const int aligned = ((uintptr_t)in % UB) == 0 ? 1 : 0;
+   k_track_turn<<<(unsigned)nblk, 256, 0, st>>>(in, nbytes, grid_offset, ntrack,
+                                                 format == SWSGPU_FMT_VLBA ? 1 : 0, aligned,
+                                                 reinterpret_cast<const uint2 *>(table), out);
    return cudaGetLastError();
 }
 
