@@ -370,8 +370,11 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
    const bool any = *blank_any != 0;
    const long long w0 = (long long)blockIdx.x * nw;
    const bool tpath = (s.nchan * NBIT == 32);
+   // half-word sample-times (8 x 2 bit, 16 x 1, 2 x 8) at an even number of
+   // phases: a payload word holds the same row's two consecutive phases
+   const bool tpath2 = (2 * s.nchan * NBIT == 32) && (Dt % 2 == 0);
    for (int j = threadIdx.x; j < nch; j += blockDim.x) sch[j] = chans[j];
-   if (tpath)
+   if (tpath || tpath2)
       for (int c = threadIdx.x; c < SPW; c += blockDim.x) {
          int p = -1;
          for (int k = 0; k < nch; k++)
@@ -560,6 +563,31 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
       for (int iw = threadIdx.x; iw < g.G; iw += blockDim.x) {
          const long long iwg = (long long)blockIdx.x * g.G + iw;
          if (iwg < g.wpp) codes[iwg] = sm[(size_t)iw * SWp];
+      }
+   } else if (tpath2) {
+      // Row k of a code word's block holds phases ph and ph + 1 (ph even)
+      // in one payload word, so the SPW x SPW transpose gives both phases'
+      // code words of every channel: code word c' is channel c' % nchan of
+      // phase ph + c' / nchan.
+      const int nc = SPW / 2;
+      const int ntask = (Dt / 2) * (g.G / 32);
+      for (int t = warp; t < ntask; t += nwarp) {
+         const int pp = t % (Dt / 2);
+         const int iw = (t / (Dt / 2)) * 32 + lane;
+         const long long iwg = (long long)blockIdx.x * g.G + iw;
+         const uint32_t *blk = sm + (size_t)iw * SWp;
+         uint32_t x[SPW];
+#pragma unroll
+         for (int k = 0; k < SPW; k++) x[k] = blk[k * (Dt / 2) + pp];
+         transpose_codes<NBIT>(x);
+         if (iwg < g.wpp) {
+#pragma unroll
+            for (int c = 0; c < SPW; c++) {
+               const int p = pos[c % nc];
+               if (p >= 0)
+                  codes[(long long)p * code_words + (long long)(ph0 + 2 * pp + c / nc) * g.wpp + iwg] = x[c];
+            }
+         }
       }
    } else {
    const int ntask = Dt * (g.G / 32);
