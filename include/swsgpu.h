@@ -288,7 +288,9 @@ void swsgpu_batch_destroy(swsgpu_batch *b);
  * writes the sum of every `runs_per_output` consecutive runs' spectra --
  * the dispatcher's combineResults path (src/TaskDispatcher.cpp:143-171) --
  * into the device outputs, using runs * nspectra_per_run / runs_per_output
- * spectrum slots.  `cuda_stream` is a cudaStream_t (NULL: the handle's). */
+ * spectrum slots.  `cuda_stream` is a cudaStream_t (NULL: the handle's).
+ * Every d_raw[s] must be 4-byte aligned (SWSGPU_EINVAL otherwise; the
+ * decoders read 32-bit words), as for swsgpu_batch_set. */
 int swsgpu_process_device(swsgpu_handle *h, const void *const *d_raw, size_t run_bytes, int nruns,
                           int runs_per_output, const swsgpu_outputs *d_out, void *cuda_stream);
 
@@ -322,7 +324,8 @@ int swsgpu_workspace_size(const swsgpu_handle *h, size_t run_bytes, int nruns, s
 /* Unpack test entry: decode channel `chan` of `nsamp` samples from the
  * device stream d_raw (layout `lay`, payload offset `payload_offset`) to
  * float32 d_out on the device, with mark5access blanking.  Returns the
- * number of non-blanked samples through *nvalid (may be NULL). */
+ * number of non-blanked samples through *nvalid (may be NULL).  d_raw and
+ * d_out must be 4-byte aligned (SWSGPU_EINVAL otherwise). */
 int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nbytes,
                          int64_t payload_offset, int chan, int64_t nsamp, float *d_out,
                          int64_t *nvalid, void *cuda_stream);

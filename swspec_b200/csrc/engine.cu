@@ -1879,6 +1879,9 @@ static int process_device_on(swsgpu_handle *h, const void *const *d_raw, size_t 
    const swsgpu_config &c = h->cfg;
    long long grid_off[SWSGPU_MAX_STREAMS];
    size_t raw_bytes[SWSGPU_MAX_STREAMS];
+   for (int s = 0; s < c.num_streams; s++)
+      if (!d_raw[s] || ((uintptr_t)d_raw[s] % 4))
+         return fail(h, SWSGPU_EINVAL, "device input must be 4-byte aligned (the decoders read 32-bit words)");
    for (int s = 0; s < c.num_streams; s++) {
       const swsgpu_layout &L = c.layout[s];
       const int pb = payload_bytes(L);
@@ -2208,6 +2211,7 @@ int swsgpu_unpack_device(const swsgpu_layout *lay, const void *d_raw, size_t nby
 {
    if (!lay || !d_raw || !d_out || chan < 0 || chan >= lay->nchan || nsamp < 0) return SWSGPU_EINVAL;
    if (lay->nbit != 1 && lay->nbit != 2 && lay->nbit != 8) return SWSGPU_EINVAL;
+   if ((uintptr_t)d_raw % 4 || (uintptr_t)d_out % 4) return SWSGPU_EINVAL;  // 32-bit loads and stores
    const int pb = lay->frame_bytes - lay->header_bytes;
    if (pb <= 0 || (pb % 8) || (lay->header_bytes % 4) || (payload_offset % 4)) return SWSGPU_EINVAL;
    if (lay->header_bytes > 0 && payload_offset != 0) return SWSGPU_EINVAL;
@@ -2384,6 +2388,9 @@ int swsgpu_batch_set(swsgpu_batch *b, int i, const void *const *d_raw, size_t ru
 {
    if (!b || i < 0 || i >= (int)b->cores.size() || !d_raw || !d_out || nruns < 1 || runs_per_output < 1)
       return fail(nullptr, SWSGPU_EINVAL, "batch_set: bad argument");
+   for (int s = 0; s < b->cores[i]->cfg.num_streams; s++)
+      if (!d_raw[s] || ((uintptr_t)d_raw[s] % 4))
+         return fail(nullptr, SWSGPU_EINVAL, "batch_set: device input must be 4-byte aligned");
    swsgpu_batch::Work &w = b->work[i];
    for (int s = 0; s < b->cores[i]->cfg.num_streams; s++) w.d_raw[s] = d_raw[s];
    w.run_bytes = run_bytes;

@@ -68,6 +68,7 @@ extern "C" int swsgpu_unpack_device_noalloc(const swsgpu_layout *lay, const void
 {
    if (!lay || !d_raw || !d_out || chan < 0 || chan >= lay->nchan || nsamp < 0) return SWSGPU_EINVAL;
    if (lay->nbit != 1 && lay->nbit != 2 && lay->nbit != 8) return SWSGPU_EINVAL;
+   if ((uintptr_t)d_raw % 4 || (uintptr_t)d_out % 4) return SWSGPU_EINVAL;  // 32-bit loads and stores
    const int pb = lay->frame_bytes - lay->header_bytes;
    if (pb <= 0 || (pb % 8) || (lay->header_bytes % 4) || (payload_offset % 4)) return SWSGPU_EINVAL;
    if (lay->header_bytes > 0 && payload_offset != 0) return SWSGPU_EINVAL;

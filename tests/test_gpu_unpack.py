@@ -175,6 +175,16 @@ def test_track_formats_bit_exact(gpu, fmt, ntrack):
     ref1, _ = O.m5_unpack(fmt, pay[frame:], 2 * 20000 * fanout)
     got1, _ = _gpu_decode(gpu, lay, pay[frame:], nchan - 1, 2 * 20000 * fanout, payload_offset=frame)
     assert np.array_equal(got1.view(np.uint32), ref1[nchan - 1].view(np.uint32)), fmt
+    # a source 4 bytes past an 8-byte boundary (64 tracks: the turn reads
+    # its 8-byte units bytewise); a source off 4-byte alignment is refused
+    import torch
+    d = torch.zeros(len(pay) + 4, dtype=torch.uint8, device="cuda")
+    d[4:] = _dev(pay)
+    out = torch.empty(nsamp, dtype=torch.float32, device="cuda")
+    nv = gpu.unpack_device(lay, d.data_ptr() + 4, len(pay), 0, 0, nsamp, out.data_ptr())
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref[0].view(np.uint32)) and nv == nref, fmt
+    with pytest.raises(gpu.SwsError):
+        gpu.unpack_device(lay, d.data_ptr() + 1, len(pay) - 1, 0, 0, nsamp, out.data_ptr())
 
 
 @pytest.mark.parametrize("fmt,ntrack", TRACK_MODES)
