@@ -370,9 +370,13 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
    const bool any = *blank_any != 0;
    const long long w0 = (long long)blockIdx.x * nw;
    const bool tpath = (s.nchan * NBIT == 32);
-   // half-word sample-times (8 x 2 bit, 16 x 1, 2 x 8) at an even number of
-   // phases: a payload word holds the same row's two consecutive phases
-   const bool tpath2 = (2 * s.nchan * NBIT == 32) && (Dt % 2 == 0);
+   // sample-times of a 1/R payload word (R = 2: 8 x 2 bit, 16 x 1, 2 x 8;
+   // R = 4: 4 x 2 bit, 8 x 1; R = 8, 16: 2 x 2 bit, 4 x 1, 2 x 1) at a phase
+   // count that R divides: a payload word holds R consecutive phases of
+   // the same row
+   const int BW = s.nchan * NBIT;
+   const int RPW = (s.nchan > 1 && BW < 32 && 32 % BW == 0) ? 32 / BW : 0;
+   const bool tpath2 = RPW > 0 && Dt % RPW == 0;
    for (int j = threadIdx.x; j < nch; j += blockDim.x) sch[j] = chans[j];
    if (tpath || tpath2)
       for (int c = threadIdx.x; c < SPW; c += blockDim.x) {
@@ -565,27 +569,27 @@ __global__ void __launch_bounds__(256) k_unpack_codes(StreamIn s, long long nsam
          if (iwg < g.wpp) codes[iwg] = sm[(size_t)iw * SWp];
       }
    } else if (tpath2) {
-      // Row k of a code word's block holds phases ph and ph + 1 (ph even)
-      // in one payload word, so the SPW x SPW transpose gives both phases'
+      // Row k of a code word's block holds phases R pp ... R pp + R - 1 in
+      // one payload word, so the SPW x SPW transpose gives those phases'
       // code words of every channel: code word c' is channel c' % nchan of
-      // phase ph + c' / nchan.
-      const int nc = SPW / 2;
-      const int ntask = (Dt / 2) * (g.G / 32);
+      // phase R pp + c' / nchan.
+      const int nc = s.nchan, WR = Dt / RPW;  // payload words per row
+      const int ntask = WR * (g.G / 32);
       for (int t = warp; t < ntask; t += nwarp) {
-         const int pp = t % (Dt / 2);
-         const int iw = (t / (Dt / 2)) * 32 + lane;
+         const int pp = t % WR;
+         const int iw = (t / WR) * 32 + lane;
          const long long iwg = (long long)blockIdx.x * g.G + iw;
          const uint32_t *blk = sm + (size_t)iw * SWp;
          uint32_t x[SPW];
 #pragma unroll
-         for (int k = 0; k < SPW; k++) x[k] = blk[k * (Dt / 2) + pp];
+         for (int k = 0; k < SPW; k++) x[k] = blk[k * WR + pp];
          transpose_codes<NBIT>(x);
          if (iwg < g.wpp) {
 #pragma unroll
             for (int c = 0; c < SPW; c++) {
                const int p = pos[c % nc];
                if (p >= 0)
-                  codes[(long long)p * code_words + (long long)(ph0 + 2 * pp + c / nc) * g.wpp + iwg] = x[c];
+                  codes[(long long)p * code_words + (long long)(ph0 + RPW * pp + c / nc) * g.wpp + iwg] = x[c];
             }
          }
       }

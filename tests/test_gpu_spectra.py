@@ -273,6 +273,39 @@ def test_blanked_vdif_frames(gpu):
     assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
 
 
+@pytest.mark.parametrize("nchan,nbit,N", [(4, 2, 16384), (2, 2, 65536), (8, 1, 16384), (4, 1, 65536),
+                                          (2, 1, 65536), (8, 2, 16384)])
+def test_vdif_fractional_word_sample_times(gpu, nchan, nbit, N):
+    """Multi-channel VDIF whose sample-times fill 1/R of a 32-bit word (R
+    consecutive FFT phases per word: R = 2 .. 16) at cluster sizes R
+    divides, so the corner turn transposes R phases at once; a frame with
+    fill at its end is blanked whole.  Two channels and their cross
+    spectrum, two whole spectra of 4 FFTs, against the FP64 oracle."""
+    cof = 4
+    spf = 8000 * 8 // (nchan * nbit)
+    T = N * cof * 2
+    nfr = -(-T // spf)
+    rng = np.random.default_rng(nchan * 100 + nbit * 10 + N % 97)
+    x = rng.standard_normal((nchan, nfr * spf))
+    codes = synth.quantize_vdif_2bit(x, 0.98) if nbit == 2 else synth.quantize_vdif_1bit(x)
+    data = synth.vdif_frames(synth.pack_codes(codes, nbit), 8000, nchan, nbit, 4000)
+    data = fill_zone(data, 2, 7992, 8000, 8032, 32)
+    pay = T * nchan * nbit // 8                      # exactly two spectra's samples
+    run = data[:(pay // 8000) * 8032 + (32 + pay % 8000 if pay % 8000 else 0)]
+    lay = gpu.layout("vdif:8000", nchan, nbit)
+    chans = [1, nchan - 1]
+    cfg = gpu.make_config(lay, N, "hann", 1, cof, sources=((0, chans[0]), (0, chans[1])), xpols=((0, 1),),
+                          max_run_bytes=len(run))
+    core = gpu.Core(cfg)
+    auto, xp, _, ns = core.run([run])
+    s = decode_channels(data, f"VDIF_8000-64-{nchan}-{nbit}", nchan, nbit, chans, T)
+    assert np.count_nonzero(s[0][2 * spf:3 * spf]) == 0
+    ra, rx, _, nref = oracle_run(s, N, "hann", 1, cof, nxpols=1)
+    assert ns == nref == 2
+    assert rel_err_auto(auto[:, 0], ra[:, 0]) < REL_TOL and rel_err_auto(auto[:, 1], ra[:, 1]) < REL_TOL
+    assert rel_err_xpol(xp[:, 0], rx[:, 0], ra[:, 0], ra[:, 1]) < REL_TOL
+
+
 def test_pcal_tones_known_answer(gpu):
     """Tone phasors on the GPU (PCal.cpp:654-678 final step, FP64) equal the
     FP64 oracle's from the same folded samples, and reproduce the PCal
