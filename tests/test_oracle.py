@@ -328,3 +328,71 @@ def test_pcallib_shifting_matches_direct_restatement():
     want = dft[:p.ntones]
     assert used == len(x1) + len(x2)
     assert np.max(np.abs(tones - want)) < 1e-9 * np.max(np.abs(want))
+
+
+def _track_zones(frame: bytes, ntrack: int, mark4: bool) -> np.ndarray:
+    """Blanked track-words of one VLBA payload / Mark4 frame by the rules the
+    GPU's frame-validity kernel restates (blanker_mark5.c:126-280): 32 KiB
+    zones judged by the fill pattern at their two ends, a binary search for
+    the boundary with the 32-bit straggler check, Mark4's first zone after
+    the header and its later zones examined 20 * ntrack / 8 words late, and
+    a track-word blanked by its first byte."""
+    tb, nword = ntrack // 8, len(frame) // 8
+    w64 = np.frombuffer(frame, "<u8")
+    w32 = np.frombuffer(frame, "<u4")
+    F64, F32, big = 0x1122334411223344, 0x11223344, 1 << 30
+
+    def first(b, e, invalid):
+        n = e - b
+        i, r, st = n // 2, n - 1, n // 4
+        while st > 0:
+            if (int(w64[b + i]) == F64) == invalid:
+                r, i = i, i - st
+            else:
+                i += st
+            st >>= 1
+        r = 8 * (b + r)
+        if invalid and int(w32[r // 4 - 1]) == F32:
+            r -= 4
+        if not invalid and int(w32[r // 4 - 2]) == F32:
+            r += 4
+        return r
+
+    zones, b = [], 0
+    while b < nword:
+        e = min(b + 4096, nword)
+        if mark4 and b == 0:
+            b = 20 * tb
+        s_ok, e_ok = int(w64[b]) != F64, int(w64[e - 1]) != F64
+        r = [0, big] if s_ok and e_ok else [big, 0] if not (s_ok or e_ok) else \
+            [0, first(b, e, True)] if s_ok else [first(b, e, False), big]
+        if mark4 and not zones:
+            r[0] = max(r[0], 160 * tb)
+        zones.append(r)
+        b += 4096
+    m = np.arange(20000) * tb
+    lo = np.array([zones[k][0] for k in m >> 15])
+    hi = np.array([zones[k][1] for k in m >> 15])
+    return (m < lo) | (m >= hi)
+
+
+@pytest.mark.parametrize("fmt,ntrack", [("VLBA1_1-128-8-2", 16), ("VLBA1_4-512-8-2", 64), ("VLBA1_4-64-2-1", 8),
+                                        ("MKIV1_2-512-8-2", 32), ("MKIV1_2-1024-16-2", 64)])
+def test_track_zone_blanking_matches_live_mark5access(fmt, ntrack):
+    """VLBA / Mark4 fill-pattern zones: the rules above against mark5access's
+    own header-free unpack of planted frames (the blanked track-words decode
+    to 0.0 in every channel)."""
+    from helpers import plant_track_fill
+    if O.ref() is None:
+        pytest.skip("mark5access (oracle/_ref) not built")
+    info = O.m5_format_info(fmt)
+    fanout = ntrack // (info["nchan"] * info["nbit"])
+    frame = 2500 * ntrack
+    rng = np.random.default_rng(ntrack + 3)
+    pay = plant_track_fill(rng.integers(0, 256, 3 * frame, dtype=np.uint8).tobytes(), ntrack)
+    ref, nref = O.m5_unpack(fmt, pay, 3 * 20000 * fanout)
+    seen = (ref[0] == 0.0).reshape(3, 20000, fanout).all(axis=2)
+    want = np.stack([_track_zones(pay[f * frame:(f + 1) * frame], ntrack, fmt.startswith("MKIV"))
+                     for f in range(3)])
+    assert np.array_equal(seen, want)
+    assert nref == int((~want).sum()) * fanout
